@@ -1,0 +1,388 @@
+"""Benchmark: batched RPN program evaluation with fused per-program MSE on one or more B200s.
+
+Workload (one step = one pass of the hot path over one batch): the evaluation-only scale test
+-- 1,048,576 random valid RPN programs (lengths U{3..64}, L = 64, ops + - * / sin cos exp log
+sqrt neg), 5 variables, 8 constants U[-5,5] per program, X ~ U[-3,3]^{5 x 100,000} fp32,
+y from a seeded depth-5 random tree; output the per-program MSE (classic-path semantics, which
+is what the reference uses at this shape).  Synthetic, seeded data; no dataset is downloaded.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun, one process per GPU): every rank evaluates its own full batch (programs
+are independent; no collective on the data path), so per-GPU work is fixed ("weak" scaling);
+`value` is the node-evals of all ranks / max over ranks of the timed region.
+`--impl reference` times the CPU restatement of the reference evaluator (the reference has no
+CPU evaluator of its own) on all host cores, on a bounded program sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+import __graft_entry__ as entry  # noqa: E402
+
+METRIC = "program-node evals/s"
+UNIT = "node-evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--programs", type=int, default=1_048_576)
+    ap.add_argument("--rows", type=int, default=100_000)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="target CPU time of the bounded CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def load_oracle():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("ws_oracle_py", os.path.join(REPO, "oracle", "oracle.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload(args, rank):
+    pkg = entry.load_package()
+    from warpsymbolic_b200 import synthetic
+    return synthetic.eval_scale_workload(seed=args.seed + rank, n_programs=args.programs,
+                                         n_rows=args.rows)
+
+
+def config_dict(args, n_gpus, wl=None):
+    return {"workload": "evaluation-only scale test: %d programs (len U{3..64}, L=64), 5 vars, "
+                        "K=8, D=%d rows, MSE" % (args.programs, args.rows),
+            "programs_per_gpu": args.programs, "rows": args.rows, "num_vars": 5, "max_len": 64,
+            "constants": 8, "ops": "+ - * / sin cos exp log sqrt neg",
+            "semantics": "classic evaluate_batch path (protected ops, fp32)",
+            "parallelism": "program-sharded dp%d (no collective)" % n_gpus,
+            "l2": "L2 flushed (256 MB write) between timed steps; per-step CUDA events"}
+
+
+# ---------------------------------------------------------------------------------------
+def cpu_baseline(args, wl, n_tok, oracle, tmap):
+    """Times the oracle (C++ restatement, all host threads) on a bounded program sample."""
+    threads = len(os.sched_getaffinity(0))
+    D = wl.X.shape[1]
+    n = 8
+    t = 0.0
+    while True:
+        t0 = time.perf_counter()
+        oracle.fitness(tmap, wl.population[:n], wl.X, wl.constants[:n], wl.y, policy="classic",
+                       loss="mse", nthreads=threads)
+        t = time.perf_counter() - t0
+        if t > args.cpu_seconds / 4 or n >= wl.population.shape[0]:
+            break
+        n = min(wl.population.shape[0], n * 4)
+    evals = float(n_tok[:n].sum()) * D
+    return {"value": evals / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "first %d programs x %d rows of the same workload (%.1f s)" % (n, D, t)}
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per fitness-kernel launch from the committed ncu summary (if present)."""
+    p = os.path.join(REPO, "profiles", "fitness_kernel_c2.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("dram_bytes_per_launch_full"), d
+    return None, None
+
+
+# ---------------------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    entry.load_package()
+    from warpsymbolic_b200.cuda_vm import CudaRPNVM
+    from warpsymbolic_b200 import _native as N
+
+    wl = workload(args, rank)
+    n_tok = wl.n_tokens()
+    D = wl.X.shape[1]
+    evals_per_step = float(n_tok.sum()) * D
+    vm = CudaRPNVM(wl.grammar, dev)
+    pop = torch.from_numpy(wl.population).to(dev)
+    consts = torch.from_numpy(wl.constants).to(dev)
+    X = torch.from_numpy(wl.X).to(dev)
+    y = torch.from_numpy(wl.y).to(dev)
+    B, L = wl.population.shape
+    out = torch.empty(B, dtype=torch.float32, device=dev)
+    nbytes = N.lib().ws_fitness_workspace_bytes(B, L, N.WS_F32)
+    wsp = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(phase=0):
+        vm.eval_fitness(pop, X, consts, y, policy="classic", loss="mse", out=out,
+                        workspace_tensor=wsp, phase=phase)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    ev_k = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        barrier()
+        wall0 = time.perf_counter()
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        barrier()
+        wall = time.perf_counter() - wall0
+        # the dominant kernel alone: compile once, then time evaluate-only launches
+        step(phase=N.WS_PHASE_COMPILE)
+        for i in range(args.steps):
+            flush.zero_()
+            ev_k[i][0].record(stream)
+            step(phase=N.WS_PHASE_EVALUATE)
+            ev_k[i][1].record(stream)
+        barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    kern_ms = [a.elapsed_time(b) for a, b in ev_k]
+    t_total = sum(step_ms) / 1e3
+    if world > 1:
+        tt = torch.tensor([t_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_total = float(tt.item())
+    total_evals = evals_per_step * args.steps * world
+    value = total_evals / t_total
+
+    # ---- end to end through the public API with host buffers -------------------------------
+    e2e = None
+    if not args.no_e2e:
+        h_pop = torch.from_numpy(wl.population).pin_memory()
+        h_c = torch.from_numpy(wl.constants).pin_memory()
+        h_X = torch.from_numpy(wl.X).pin_memory()
+        h_y = torch.from_numpy(wl.y).pin_memory()
+        h_out = torch.empty(B, dtype=torch.float32).pin_memory()
+        d_pop, d_c, d_X, d_y = (torch.empty_like(t, device=dev) for t in (h_pop, h_c, h_X, h_y))
+        e_ms = []
+        for i in range(args.steps + 1):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for d_, h_ in ((d_pop, h_pop), (d_c, h_c), (d_X, h_X), (d_y, h_y)):
+                d_.copy_(h_, non_blocking=True)
+            r = vm.eval_fitness(d_pop, d_X, d_c, d_y, policy="classic", loss="mse")
+            h_out.copy_(r, non_blocking=True)
+            b.record(stream)
+            b.synchronize()
+            if i > 0:
+                e_ms.append(a.elapsed_time(b))
+        h2d = sum(t.numel() * t.element_size() for t in (h_pop, h_c, h_X, h_y))
+        t_e2e = sum(e_ms) / 1e3
+        if world > 1:
+            tt = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t_e2e = float(tt.item())
+        e2e = {"value": evals_per_step * args.steps * world / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(B * 4),
+               "ms_per_step": 1e3 * t_e2e / args.steps}
+
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    # ---- roofline ---------------------------------------------------------------------------
+    peaks, peak_src = measured_peaks()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    clocks = clk.summary()
+    f_max = float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = sms * 128 * f_max * 1e6  # FP32 lane-ops/s at the max SM clock
+    k_s = statistics.mean(kern_ms) / 1e3
+    achieved = evals_per_step / k_s
+    traffic_full, prof = profile_traffic()
+    alg_bytes = B * (L + 4 * wl.constants.shape[1] + 4) + 4 * (X.shape[0] + 1) * D + 4 * B
+    roof = {"bound": "fp32", "achieved": achieved / 1e12, "peak": fp32_peak / 1e12,
+            "unit": "T node-evals/s (1 FP32 lane-op per node-eval)", "frac": achieved / fp32_peak,
+            "traffic": traffic_full, "kernel": "fitness_kernel<float,8,false>",
+            "kernel_ms": statistics.mean(kern_ms),
+            "peak_source": "%d SMs x 128 FP32 lanes x sm_max_mhz %.0f (%s MEASURED_PEAKS.json)"
+                           % (sms, f_max, peak_src),
+            "hbm": {"algorithmic_bytes_per_launch": int(alg_bytes),
+                    "achieved_gbs": alg_bytes / k_s / 1e9,
+                    "peak_gbs": float(peaks.get("hbm_gbs", 6650.0)),
+                    "frac": alg_bytes / k_s / 1e9 / float(peaks.get("hbm_gbs", 6650.0))}}
+    if clocks.get("sm_mhz"):
+        roof["frac_at_sampled_clock"] = achieved / (sms * 128 * clocks["sm_mhz"] * 1e6)
+
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        oracle = load_oracle()
+        cpu = cpu_baseline(args, wl, n_tok, oracle, vm.token_map())
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t_total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded; shapes/distributions of the evaluation-only scale test)",
+            "config": config_dict(args, world),
+            "node_evals_per_step_per_gpu": evals_per_step,
+            "hbm_gbs": alg_bytes / (t_total / args.steps) / 1e9,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": 2 * args.steps * world,
+            "wall_s_timed_region": wall}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """Reference arm: the CPU restatement of the reference evaluator (all host threads)."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    oracle = load_oracle()
+    wl = workload(args, 0)
+    n_tok = wl.n_tokens()
+    entry.load_package()
+    from warpsymbolic_b200 import _native as N
+    from warpsymbolic_b200.grammar import PI_VAL, E_VAL
+    tmap = N.TokenMap.from_args(*wl.grammar.scalar_ids(), pi_val=PI_VAL, e_val=E_VAL)
+    threads = len(os.sched_getaffinity(0))
+    D = wl.X.shape[1]
+    # sample size: ~ cpu-seconds / (steps + warmup) per step
+    per_step = max(1.0, args.cpu_seconds * 2 / max(1, args.steps + args.warmup))
+    n = 4
+    while True:
+        t0 = time.perf_counter()
+        oracle.fitness(tmap, wl.population[:n], wl.X, wl.constants[:n], wl.y, policy="classic",
+                       loss="mse", nthreads=threads)
+        dt = time.perf_counter() - t0
+        if dt > per_step / 3 or n >= wl.population.shape[0]:
+            break
+        n *= 2
+    for _ in range(args.warmup):
+        oracle.fitness(tmap, wl.population[:n], wl.X, wl.constants[:n], wl.y, policy="classic",
+                       loss="mse", nthreads=threads)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.fitness(tmap, wl.population[:n], wl.X, wl.constants[:n], wl.y, policy="classic",
+                       loss="mse", nthreads=threads)
+        ts.append(time.perf_counter() - t0)
+    evals = float(n_tok[:n].sum()) * D
+    value = evals * len(ts) / sum(ts)
+    sample = "first %d of %d programs x %d rows per step" % (n, wl.population.shape[0], D)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(ts) / len(ts), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": config_dict(args, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference has no CPU evaluator (rpn_kernels.cu:10,382 rejects CPU "
+                    "tensors); this arm times the C++ restatement of its evaluator"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

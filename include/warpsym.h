@@ -1,0 +1,171 @@
+/*
+ * warpsym.h -- C ABI of the B200-native evaluation and constant-fitting core.
+ *
+ * This library replaces the native extension `rpn_cuda_native` of WarpSymbolic
+ * (src/warpsymbolic/gpu/cuda/, pybind11 exports in bindings.cpp:434-581).  Every entry point
+ * below names the reference interface it stands in for.  The contract is plain C: raw device
+ * pointers, element counts and a CUDA stream (passed as `void*`, a `cudaStream_t`), no torch
+ * types.  The Python drop-in module `rpn_cuda_native.py` binds these symbols with ctypes.
+ *
+ * Conventions shared by every entry point
+ *   - All array arguments are DEVICE pointers to contiguous row-major storage, unless a
+ *     parameter says "host".  Layouts are the reference's: population uint8 [B, L]
+ *     (PAD-terminated, left-packed), x [num_vars, D] (variables-major), constants [B, K],
+ *     y [D].
+ *   - Outputs are caller-allocated and written in place (bindings.cpp contract).
+ *   - Work is enqueued on `stream` (NULL = legacy default stream); nothing synchronises the
+ *     host.  Entry points never allocate device memory: scratch comes from a caller-provided
+ *     workspace whose size is given by the matching *_workspace_bytes() query.
+ *   - Return value: WS_OK or an error code; ws_last_error() returns the message (the text the
+ *     reference's TORCH_CHECK would raise where the same check exists).
+ *   - dtype: WS_F32 or WS_F64 for x / constants / y / floating outputs (the reference
+ *     dispatches both via AT_DISPATCH_FLOATING_TYPES).
+ */
+#ifndef WARPSYM_H
+#define WARPSYM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t ws_status;
+
+enum {
+  WS_OK = 0,
+  WS_ERR_INVALID_ARGUMENT = 1, /* shape / dtype / envelope check failed            */
+  WS_ERR_CUDA = 2,             /* a CUDA runtime call or launch failed              */
+  WS_ERR_WORKSPACE = 3,        /* workspace pointer missing or too small            */
+  WS_ERR_UNSUPPORTED = 4       /* request outside what this build implements       */
+};
+
+enum { WS_F32 = 0, WS_F64 = 1 };
+
+/* Fitness semantics: which reference code path's validity / overflow rules to reproduce. */
+enum {
+  WS_POLICY_FUSED = 0,   /* rpn_eval_fused_kernel epilogue, rpn_kernels.cu:2405-2501          */
+  WS_POLICY_CLASSIC = 1  /* GPUEvaluator.evaluate_batch classic path, evaluation.py:153-189   */
+};
+
+/* Per-program loss written by ws_eval_fitness. */
+enum {
+  WS_LOSS_RMSE = 0,  /* sqrt(mean squared error) -- the reference's fitness                 */
+  WS_LOSS_MSE = 1,   /* mean squared error                                                   */
+  WS_LOSS_R2 = 2,    /* 1 - MSE / Var(y), Var over the same rows in FP64                     */
+  WS_LOSS_SSE = 3    /* raw sum of squared errors, always written as double                  */
+};
+
+/*
+ * Token-ID map.  The reference passes these ~40 scalars to every evaluator entry point
+ * (bindings.cpp:7-27, cuda_vm.py:34-82): absent tokens carry -100 / -1 / -999 and never match a
+ * uint8 token.  Field order follows the reference's argument order.
+ */
+typedef struct ws_token_map {
+  int32_t pad_id, id_x_start;
+  int32_t id_C, id_pi, id_e;
+  int32_t id_0, id_1, id_2, id_3, id_4, id_5, id_6, id_10;
+  int32_t op_add, op_sub, op_mul, op_div, op_pow, op_mod;
+  int32_t op_sin, op_cos, op_tan, op_log, op_exp;
+  int32_t op_sqrt, op_abs, op_neg;
+  int32_t op_fact, op_floor, op_ceil, op_sign;
+  int32_t op_gamma, op_lgamma;
+  int32_t op_asin, op_acos, op_atan;
+  double pi_val, e_val;
+} ws_token_map;
+
+/* Phases of ws_eval_fitness: both (the normal call), or one of them.  An evaluate-only call
+ * reuses the tape that a compile-only call with the same population, constants, L, dtype and
+ * strict_mode left in the same workspace (used to time the evaluation kernel alone). */
+enum { WS_PHASE_ALL = 0, WS_PHASE_COMPILE = 1, WS_PHASE_EVALUATE = 2 };
+
+/* Options of the general fitness evaluator. */
+typedef struct ws_fitness_opts {
+  int32_t strict_mode;   /* 0 = protected operators (search), 1 = strict domain errors      */
+  int32_t policy;        /* WS_POLICY_FUSED or WS_POLICY_CLASSIC                              */
+  int32_t loss;          /* WS_LOSS_*                                                         */
+  int32_t schedule;      /* 0 = autotuned; otherwise an index into ws_schedule_count()        */
+  double invalid_value;  /* loss written for invalid programs (reference: 1e15 f32, 1e100 f64) */
+  int32_t phase;         /* WS_PHASE_*                                                        */
+  int32_t reserved;
+} ws_fitness_opts;
+
+/* Library identification (host). */
+const char* ws_version(void);
+
+/* Message of the most recent failed call on this host thread ("" when none). */
+const char* ws_last_error(void);
+
+/*
+ * Classic per-(program,row) interpreter.  Replaces `eval_rpn` (bindings.cpp:434 ->
+ * launch_rpn_kernel, rpn_kernels.cu:361-429; kernel rpn_kernels.cu:202-358).
+ * Writes out_preds[B*D] (dtype), out_sp[B*D] (int32), out_error[B*D] (uint8) exactly as the
+ * reference does (stack top or 1e30, final stack depth, error byte).  K == 0 allowed
+ * (constants may be NULL; `C` then pushes 1.0).  Indices are 64-bit (no B*D < 2^31 limit).
+ */
+ws_status ws_eval_rpn(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
+                      const void* x, int64_t num_vars, int64_t D, const void* constants,
+                      int64_t K, void* out_preds, int32_t* out_sp, uint8_t* out_error,
+                      const ws_token_map* ids, int32_t strict_mode, void* stream);
+
+/*
+ * Fused evaluation + RMSE.  Replaces `eval_rpn_fused` (bindings.cpp:436 ->
+ * launch_rpn_eval_fused, rpn_kernels.cu:2505-2594) with the same argument checks and envelope
+ * (1..4 variables, L <= 256, 1 <= D <= 1024, B > 0) and the same error texts; launch_mode
+ * (0 = block, 1 = warp in the reference) is validated and otherwise ignored because the
+ * schedule here is chosen by the autotuner.  out_rmse[B] uses the reference's sentinels
+ * (1e15 / sqrt(1e15) in f32, 1e100 / 1e50 in f64).  Needs ws_fitness_workspace_bytes(B, L).
+ */
+ws_status ws_eval_rpn_fused(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
+                            const void* x, int64_t num_vars, int64_t D, const void* constants,
+                            int64_t K, const void* y, void* out_rmse, const ws_token_map* ids,
+                            int32_t strict_mode, int32_t launch_mode, void* workspace,
+                            size_t workspace_bytes, void* stream);
+
+/*
+ * General batched fitness (no envelope): any number of variables (<= 64), any D >= 1,
+ * L <= 256.  This is the hot path behind GPUEvaluator.evaluate_batch (evaluation.py:45-198):
+ * both the fused-kernel semantics and the classic chunked-path semantics are available
+ * through opts->policy, so one launch replaces the reference's [B, D] materialisation.
+ * out_loss[B] has `dtype` (double for WS_LOSS_SSE); out_ninvalid[B] (optional, may be NULL)
+ * receives the number of rows whose evaluation is invalid (the reference's per-row
+ * `err != 0 | sp != 1 | non-finite` count, evaluation.py:379-382).
+ */
+ws_status ws_eval_fitness(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
+                          const void* x, int64_t num_vars, int64_t D, const void* constants,
+                          int64_t K, const void* y, void* out_loss, int32_t* out_ninvalid,
+                          const ws_token_map* ids, const ws_fitness_opts* opts,
+                          void* workspace, size_t workspace_bytes, void* stream);
+
+/* Bytes of device workspace ws_eval_fitness / ws_eval_rpn_fused need for B programs of
+ * length L (256-byte aligned base required). */
+size_t ws_fitness_workspace_bytes(int64_t B, int64_t L, int32_t dtype);
+
+/* Number of compiled (rows-per-thread x warps x rows-per-chunk) schedules. */
+int32_t ws_schedule_count(void);
+
+/*
+ * Host-only introspection (no GPU needed; not an evaluation path).  They expose the pieces
+ * the evaluator is built from so that they can be verified exactly on a CPU:
+ *   ws_debug_token_lut  -- token byte -> internal class / argument table built from the IDs
+ *                          with the reference's precedence (rpn_kernels.cu:249-346);
+ *   ws_debug_compile    -- compiles ONE host program into the evaluator's tape (ctrl words and
+ *                          immediates, capacity max(L,1)); hdr_out = {n_instr, status
+ *                          (0 ok / 1 statically invalid), spill slots, tokens};
+ *   ws_debug_run_tape   -- scalar host interpretation of such a tape over D rows of a host x.
+ */
+ws_status ws_debug_token_lut(const ws_token_map* ids, int64_t num_vars, int32_t fused_order,
+                             uint8_t* cls_out, uint8_t* arg_out);
+ws_status ws_debug_compile(int32_t dtype, const uint8_t* prog, int64_t L, const void* consts,
+                           int64_t K, const ws_token_map* ids, int64_t num_vars,
+                           int32_t strict_mode, int32_t fused_order, uint32_t* ctrl_out,
+                           double* imm_out, int32_t* hdr_out);
+ws_status ws_debug_run_tape(int32_t dtype, const uint32_t* ctrl, const double* imm, int32_t n,
+                            const void* x, int64_t D, int32_t strict_mode, void* out_pred,
+                            uint8_t* out_err);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WARPSYM_H */

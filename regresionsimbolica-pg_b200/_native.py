@@ -1,0 +1,113 @@
+"""ctypes binding of libwarpsym.so (the C ABI declared in include/warpsym.h).
+
+The library is loaded from this package directory.  There is no fallback: if the shared
+library is missing or fails to load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG_DIR, "libwarpsym.so")
+
+WS_OK = 0
+WS_F32, WS_F64 = 0, 1
+WS_POLICY_FUSED, WS_POLICY_CLASSIC = 0, 1
+WS_LOSS_RMSE, WS_LOSS_MSE, WS_LOSS_R2, WS_LOSS_SSE = 0, 1, 2, 3
+
+
+class TokenMap(C.Structure):
+    """Mirror of ws_token_map: the reference's scalar token-ID arguments (bindings.cpp:7-27)."""
+
+    _fields_ = [(n, C.c_int32) for n in (
+        "pad_id", "id_x_start", "id_C", "id_pi", "id_e",
+        "id_0", "id_1", "id_2", "id_3", "id_4", "id_5", "id_6", "id_10",
+        "op_add", "op_sub", "op_mul", "op_div", "op_pow", "op_mod",
+        "op_sin", "op_cos", "op_tan", "op_log", "op_exp",
+        "op_sqrt", "op_abs", "op_neg",
+        "op_fact", "op_floor", "op_ceil", "op_sign",
+        "op_gamma", "op_lgamma",
+        "op_asin", "op_acos", "op_atan")] + [("pi_val", C.c_double), ("e_val", C.c_double)]
+
+    INT_FIELDS = tuple(n for n, _ in _fields_[:-2])
+
+    @classmethod
+    def from_args(cls, *ids, pi_val: float, e_val: float) -> "TokenMap":
+        """Builds the map from the reference's positional ID arguments (same order)."""
+        if len(ids) != len(cls.INT_FIELDS):
+            raise TypeError("expected %d token ids, got %d" % (len(cls.INT_FIELDS), len(ids)))
+        m = cls()
+        for name, v in zip(cls.INT_FIELDS, ids):
+            setattr(m, name, int(v))
+        m.pi_val = float(pi_val)
+        m.e_val = float(e_val)
+        return m
+
+    def key(self) -> tuple:
+        return tuple(getattr(self, n) for n in self.INT_FIELDS) + (self.pi_val, self.e_val)
+
+
+WS_PHASE_ALL, WS_PHASE_COMPILE, WS_PHASE_EVALUATE = 0, 1, 2
+
+
+class FitnessOpts(C.Structure):
+    _fields_ = [("strict_mode", C.c_int32), ("policy", C.c_int32), ("loss", C.c_int32),
+                ("schedule", C.c_int32), ("invalid_value", C.c_double), ("phase", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+_P = C.c_void_p
+_I64 = C.c_int64
+_I32 = C.c_int32
+_SIGS = {
+    "ws_version": (C.c_char_p, []),
+    "ws_last_error": (C.c_char_p, []),
+    "ws_fitness_workspace_bytes": (C.c_size_t, [_I64, _I64, _I32]),
+    "ws_schedule_count": (_I32, []),
+    "ws_eval_rpn": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P, _P,
+                           C.POINTER(TokenMap), _I32, _P]),
+    "ws_eval_rpn_fused": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
+                                 C.POINTER(TokenMap), _I32, _I32, _P, C.c_size_t, _P]),
+    "ws_eval_fitness": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P, _P,
+                               C.POINTER(TokenMap), C.POINTER(FitnessOpts), _P, C.c_size_t, _P]),
+    "ws_debug_token_lut": (_I32, [C.POINTER(TokenMap), _I64, _I32, _P, _P]),
+    "ws_debug_compile": (_I32, [_I32, _P, _I64, _P, _I64, C.POINTER(TokenMap), _I64, _I32, _I32,
+                                _P, _P, _P]),
+    "ws_debug_run_tape": (_I32, [_I32, _P, _P, _I32, _P, _I64, _I32, _P, _P]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib():
+    """Loads libwarpsym.so once (raises OSError/RuntimeError when it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    "libwarpsym.so not found at %s: build it with __graft_entry__.build() "
+                    "(there is no CPU fallback)" % LIB_PATH)
+            handle = C.CDLL(LIB_PATH)
+            for name, (res, args) in _SIGS.items():
+                fn = getattr(handle, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = handle
+    return _lib
+
+
+def check(status: int) -> None:
+    """Raises RuntimeError carrying the library's message when status != WS_OK."""
+    if status != WS_OK:
+        msg = lib().ws_last_error().decode("utf-8", "replace")
+        raise RuntimeError(msg or "warpsym error %d" % status)
+
+
+def exported_symbols() -> list:
+    return sorted(_SIGS)

@@ -1,0 +1,89 @@
+"""Build recipes for the native pieces: libwarpsym.so (product) and the CPU oracle (tests).
+
+libwarpsym.so is compiled for sm_100a only, with the reference's floating-point flags
+(-O3 --use_fast_math, src/warpsymbolic/gpu/cuda/setup.py:35) so that per-operation results are
+bit-identical to the reference evaluator.  Objects are rebuilt when a source or header is newer.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import glob
+import os
+import shutil
+import subprocess
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+REPO_DIR = os.path.dirname(PKG_DIR)
+CSRC = os.path.join(PKG_DIR, "csrc")
+BUILD_DIR = os.path.join(PKG_DIR, "_build")
+LIB_PATH = os.path.join(PKG_DIR, "libwarpsym.so")
+ORACLE_DIR = os.path.join(REPO_DIR, "oracle")
+ORACLE_LIB = os.path.join(ORACLE_DIR, "libws_oracle.so")
+
+NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "--use_fast_math", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-Xptxas", "-warn-spills", "-I", os.path.join(REPO_DIR, "include")]
+
+
+def _newest(paths):
+    return max((os.path.getmtime(p) for p in paths), default=0.0)
+
+
+def _run(cmd):
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("command failed: %s\n%s%s" % (" ".join(cmd), res.stdout, res.stderr))
+    return res.stdout + res.stderr
+
+
+def build_native(verbose: bool = False, jobs: int = 8) -> str:
+    """Compiles csrc/*.cu into libwarpsym.so (sm_100a).  Returns the library path."""
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
+        glob.glob(os.path.join(REPO_DIR, "include", "*.h")) + [os.path.abspath(__file__)]
+    hdr_time = _newest(headers)
+    objs, todo = [], []
+    for src in sources:
+        obj = os.path.join(BUILD_DIR, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        if not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src), hdr_time):
+            todo.append((src, obj))
+
+    def compile_one(pair):
+        src, obj = pair
+        return _run([NVCC, "-c", src, "-o", obj] + ARCH + NVCC_FLAGS)
+
+    if todo:
+        with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+            for out in ex.map(compile_one, todo):
+                if verbose and out.strip():
+                    print(out)
+    if todo or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < _newest(objs):
+        _run([NVCC, "-shared", "-o", LIB_PATH] + objs + ARCH + ["-lcudart"])
+    return LIB_PATH
+
+
+def build_oracle() -> str:
+    """Compiles the CPU oracle (test infrastructure) into oracle/libws_oracle.so."""
+    src = os.path.join(ORACLE_DIR, "ws_oracle.cpp")
+    deps = [src, os.path.join(REPO_DIR, "include", "warpsym.h")]
+    if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < _newest(deps):
+        _run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off",
+              "-fno-fast-math", src, "-o", ORACLE_LIB])
+    return ORACLE_LIB
+
+
+def build_reference_checker() -> None:
+    """Builds the reference extension from its sources into oracle/_ref when the reference
+    checkout is present (it is absent on GPU boxes, which use the prebuilt copy)."""
+    script = os.path.join(ORACLE_DIR, "build_ref.sh")
+    ref_root = os.environ.get("WS_REFERENCE_ROOT", "/root/reference")
+    if os.path.isdir(os.path.join(ref_root, "src")):
+        _run(["bash", script, ref_root])
+
+
+if __name__ == "__main__":
+    print(build_native(verbose=True))
+    print(build_oracle())

@@ -1,0 +1,373 @@
+// ws_compile.cuh -- per-program compiler: uint8 RPN tokens -> accumulator-machine tape.
+//
+// The reference interprets every token for every row with a 32-slot stack per thread
+// (rpn_kernels.cu:245-350).  Here each program is compiled ONCE (one thread per program) into
+// a short tape for an accumulator machine, and the evaluator runs that tape over tiles of rows:
+//
+//   * terminals (x_v, C, literals) emit no instruction: they become operands of the operator
+//     that consumes them (vector operand = a variable row of the staged X tile; scalar operand =
+//     an immediate or a constant-slot parameter);
+//   * the value of the last operator lives in the accumulator ACC (registers, R rows/thread);
+//   * subtrees whose leaves are all immediates are folded here with the same device operator
+//     code the evaluator runs, so the folded value is bit-identical to per-row evaluation
+//     (an operator error while folding makes every row invalid, as it would per row);
+//   * binary nodes with two non-terminal children evaluate the subtree with the larger
+//     Sethi-Ullman need first and keep the other operand in a shared-memory spill slot; with
+//     this order a program of L tokens needs at most floor(log2((L+1)/3)) slots (4 for L=64).
+//
+// Evaluation order of independent subtrees does not change any value (operators are pure and
+// constant slots are resolved in token order here), and any row that errors in the reference
+// also errors here, so per-row results and validity match the reference exactly.  The
+// reference's push-drop at depth 32 (rpn_kernels.cu:289-293) and constant-slot clamp
+// (rpn_kernels.cu:263-271) are applied while parsing.  Programs with a stack underflow, an
+// unknown token (rpn_kernels.cu:346) or a final depth != 1 are statically invalid: every row
+// of them is invalid, so they are never evaluated.
+#pragma once
+
+#include "ws_ops.cuh"
+
+namespace ws {
+
+// ---- tape format -----------------------------------------------------------------------
+// ctrl word:
+//   [0:7)   case: 0 = NOP, unary class id (16..32), or binary 64 + 4*(cls-T_ADD) + form
+//   [7]     SPILL: store ACC into spill slot [8:13) before anything else
+//   [13:15) LOADA kind (0 none, 1 X variable, 2 immediate, 3 parameter), index [15:21)
+//   [21:23) operand kind (0 none, 1 X variable, 2 spill slot, 3 scalar), [23] scalar is a
+//           parameter (else the immediate), index [24:30)
+enum : uint32_t {
+  CASE_MASK = 0x7Fu,
+  F_SPILL = 1u << 7,
+  SH_SLOT = 8,
+  SH_LA = 13,
+  SH_LA_IDX = 15,
+  SH_OPK = 21,
+  F_OP_PARAM = 1u << 23,
+  SH_OP_IDX = 24,
+};
+enum { LA_NONE = 0, LA_X = 1, LA_IMM = 2, LA_PARAM = 3 };
+enum { OK_NONE = 0, OK_X = 1, OK_SLOT = 2, OK_SCALAR = 3 };
+// binary forms: AV: ACC = ACC o V, VA: ACC = V o ACC, AS: ACC = ACC o s, SA: ACC = s o ACC
+enum { FORM_AV = 0, FORM_VA = 1, FORM_AS = 2, FORM_SA = 3 };
+enum { CASE_NOP = 0, CASE_BIN = 64 };
+WS_HD uint32_t bin_case(int cls, int form) { return CASE_BIN + 4u * (uint32_t)(cls - T_ADD) + form; }
+
+template <typename T> struct Instr;
+template <> struct alignas(8) Instr<float> {
+  uint32_t ctrl;
+  float imm;
+};
+template <> struct alignas(16) Instr<double> {
+  uint32_t ctrl;
+  uint32_t pad;
+  double imm;
+};
+
+enum { PROG_OK = 0, PROG_INVALID = 1 };
+struct alignas(16) ProgHdr {
+  int32_t n_instr;  // tape length
+  int32_t status;   // PROG_OK / PROG_INVALID
+  int32_t n_slots;  // spill slots used
+  int32_t n_tok;    // tokens before the first PAD (algorithmic node count)
+};
+
+// Spill slots sufficient for any program of L tokens under Sethi-Ullman ordering.
+WS_HD int spill_slots_bound(int L) {
+  int n = (L + 1) / 3;  // most "need-1" units (unary(leaf) or binary(leaf,leaf)) in L tokens
+  int s = 0;
+  while ((2 << s) <= n) ++s;  // floor(log2(n)) for n >= 1
+  return n >= 1 ? s : 0;
+}
+
+// ---- compiler --------------------------------------------------------------------------
+enum { N_VAR = 0, N_IMM = 1, N_PARAM = 2, N_OP = 3 };
+
+template <typename T> struct Node {
+  T imm;
+  int16_t l, r;
+  uint8_t kind, cls, idx, need;
+};
+
+struct Frame {
+  int16_t node;
+  uint8_t phase;
+  uint8_t spill;  // 1 = first emitted instruction must spill ACC into `slot`
+  uint8_t slot;
+  uint8_t first_left;
+};
+
+template <typename T>
+struct Emitter {
+  Instr<T>* out;
+  int n;
+  WS_HD void put(uint32_t ctrl, T imm) {
+    Instr<T> ins;
+    ins.ctrl = ctrl;
+    ins.imm = imm;
+    if constexpr (sizeof(Instr<T>) == 16) reinterpret_cast<Instr<double>&>(ins).pad = 0;
+    out[n++] = ins;
+  }
+};
+
+// Loads leaf `nd` into ACC: returns the ctrl bits and sets `imm` for an immediate.
+template <typename T>
+WS_HD uint32_t loada_bits(const Node<T>& nd, T& imm) {
+  if (nd.kind == N_VAR) return ((uint32_t)LA_X << SH_LA) | ((uint32_t)nd.idx << SH_LA_IDX);
+  if (nd.kind == N_PARAM) return ((uint32_t)LA_PARAM << SH_LA) | ((uint32_t)nd.idx << SH_LA_IDX);
+  imm = nd.imm;
+  return (uint32_t)LA_IMM << SH_LA;
+}
+// Uses leaf `nd` as the second operand.
+template <typename T>
+WS_HD uint32_t opnd_bits(const Node<T>& nd, T& imm, bool& is_vec) {
+  if (nd.kind == N_VAR) {
+    is_vec = true;
+    return ((uint32_t)OK_X << SH_OPK) | ((uint32_t)nd.idx << SH_OP_IDX);
+  }
+  is_vec = false;
+  if (nd.kind == N_PARAM)
+    return ((uint32_t)OK_SCALAR << SH_OPK) | F_OP_PARAM | ((uint32_t)nd.idx << SH_OP_IDX);
+  imm = nd.imm;
+  return (uint32_t)OK_SCALAR << SH_OPK;
+}
+WS_HD uint32_t spill_bits(bool spill, int slot) {
+  return spill ? (F_SPILL | ((uint32_t)slot << SH_SLOT)) : 0u;
+}
+// a o b == b o a bit-for-bit for + and *, so the reversed forms are canonicalised away.
+WS_HD int canon_form(int cls, int form) {
+  if (cls == T_ADD || cls == T_MUL) {
+    if (form == FORM_VA) return FORM_AV;
+    if (form == FORM_SA) return FORM_AS;
+  }
+  return form;
+}
+
+// Compiles program `prog` (L tokens) into `tape`.  `consts` (K values, may be null when K == 0)
+// are baked into immediates when BAKE, otherwise `C` leaves become parameters (slot index).
+// `nodes`/`stk`/`frames` are per-thread scratch of LMAX entries.
+template <typename T, bool STRICT, bool BAKE, int LMAX>
+__host__ __device__ ProgHdr compile_program(const uint8_t* __restrict__ prog, int L,
+                                   const T* __restrict__ consts, int K, const TokenLut& lut,
+                                   Instr<T>* __restrict__ tape) {
+  Node<T> nodes[LMAX];
+  int16_t stk[33];
+  ProgHdr h;
+  h.n_instr = 0;
+  h.status = PROG_OK;
+  h.n_slots = 0;
+  h.n_tok = 0;
+  int sp = 0, nn = 0, c_idx = 0;
+  const int Lr = L < LMAX ? L : LMAX;
+
+  for (int pc = 0; pc < Lr; ++pc) {
+    const int tok = prog[pc];
+    const int cls = lut.cls[tok];
+    if (cls == T_PAD) break;
+    h.n_tok++;
+    if (is_leaf(cls)) {
+      Node<T> nd;
+      nd.l = nd.r = -1;
+      nd.need = 0;
+      nd.cls = 0;
+      nd.idx = 0;
+      nd.imm = (T)0;
+      if (cls == T_VAR) {
+        nd.kind = N_VAR;
+        nd.idx = lut.arg[tok];
+      } else if (cls == T_CONST) {
+        if (K > 0) {
+          int slot = c_idx < K ? c_idx : K - 1;
+          c_idx++;
+          if (BAKE) {
+            nd.kind = N_IMM;
+            nd.imm = consts[slot];
+          } else {
+            nd.kind = N_PARAM;
+            nd.idx = (uint8_t)slot;
+          }
+        } else {
+          nd.kind = N_IMM;
+          nd.imm = (T)1.0;
+        }
+      } else {
+        nd.kind = N_IMM;
+        nd.imm = (T)lut.lit[lut.arg[tok]];
+      }
+      if (sp < 32) {  // a push at depth 32 is dropped (the C slot was still consumed)
+        nodes[nn] = nd;
+        stk[sp++] = (int16_t)nn++;
+      }
+      continue;
+    }
+    if (is_binary(cls)) {
+      if (sp < 2) { h.status = PROG_INVALID; break; }
+      const int r = stk[--sp], l = stk[--sp];
+      Node<T> nd;
+      nd.cls = (uint8_t)cls;
+      nd.idx = 0;
+      if (nodes[l].kind == N_IMM && nodes[r].kind == N_IMM) {
+        bool e = false;
+        nd.imm = apply_binary<T, STRICT>(cls, nodes[l].imm, nodes[r].imm, e);
+        if (e) { h.status = PROG_INVALID; break; }
+        nd.kind = N_IMM;
+        nd.l = nd.r = -1;
+        nd.need = 0;
+      } else {
+        nd.kind = N_OP;
+        nd.l = (int16_t)l;
+        nd.r = (int16_t)r;
+        nd.imm = (T)0;
+        const int a = nodes[l].need, b = nodes[r].need;
+        int need;
+        if (a == 0 && b == 0) need = 1;
+        else if (a == 0) need = b;
+        else if (b == 0) need = a;
+        else need = (a == b) ? a + 1 : (a > b ? a : b);
+        nd.need = (uint8_t)need;
+      }
+      nodes[nn] = nd;
+      stk[sp++] = (int16_t)nn++;
+      continue;
+    }
+    // unary or unknown token
+    if (sp < 1) { h.status = PROG_INVALID; break; }
+    const int c = stk[--sp];
+    if (!is_unary(cls)) { h.status = PROG_INVALID; break; }
+    Node<T> nd;
+    nd.cls = (uint8_t)cls;
+    nd.idx = 0;
+    nd.r = -1;
+    if (nodes[c].kind == N_IMM) {
+      bool e = false;
+      nd.imm = apply_unary<T, STRICT>(cls, nodes[c].imm, e);
+      if (e) { h.status = PROG_INVALID; break; }
+      nd.kind = N_IMM;
+      nd.l = -1;
+      nd.need = 0;
+    } else {
+      nd.kind = N_OP;
+      nd.l = (int16_t)c;
+      nd.imm = (T)0;
+      nd.need = (uint8_t)(nodes[c].need > 1 ? nodes[c].need : 1);
+    }
+    nodes[nn] = nd;
+    stk[sp++] = (int16_t)nn++;
+  }
+  if (h.status == PROG_OK && sp != 1) h.status = PROG_INVALID;
+  if (h.status != PROG_OK) return h;
+
+  // ---- emission: post-order walk with Sethi-Ullman child order ---------------------------
+  Emitter<T> em{tape, 0};
+  const int root = stk[0];
+  if (nodes[root].kind != N_OP) {  // the whole program is one terminal (or folded constant)
+    T imm = (T)0;
+    uint32_t bits = loada_bits(nodes[root], imm);
+    em.put(CASE_NOP | bits, imm);
+    h.n_instr = em.n;
+    return h;
+  }
+  Frame fr[LMAX];
+  int top = 0, depth = 0, max_depth = 0;
+  fr[0] = Frame{(int16_t)root, 0, 0, 0, 0};
+  while (top >= 0) {
+    Frame& f = fr[top];
+    const Node<T>& nd = nodes[f.node];
+    if (is_unary(nd.cls)) {
+      const Node<T>& ch = nodes[nd.l];
+      if (f.phase == 0 && ch.kind != N_OP) {
+        T imm = (T)0;
+        uint32_t bits = spill_bits(f.spill, f.slot) | loada_bits(ch, imm) | nd.cls;
+        em.put(bits, imm);
+        --top;
+      } else if (f.phase == 0) {
+        f.phase = 1;
+        fr[top + 1] = Frame{nd.l, 0, f.spill, f.slot, 0};
+        ++top;
+      } else {
+        em.put((uint32_t)nd.cls, (T)0);
+        --top;
+      }
+      continue;
+    }
+    // binary
+    const Node<T>& L_ = nodes[nd.l];
+    const Node<T>& R_ = nodes[nd.r];
+    const bool lop = L_.kind == N_OP, rop = R_.kind == N_OP;
+    if (!lop && !rop) {
+      T imm = (T)0;
+      uint32_t bits = spill_bits(f.spill, f.slot);
+      bool is_vec;
+      if (L_.kind == N_VAR) {
+        bits |= loada_bits(L_, imm);
+        bits |= opnd_bits(R_, imm, is_vec);
+        bits |= bin_case(nd.cls, canon_form(nd.cls, is_vec ? FORM_AV : FORM_AS));
+      } else if (R_.kind == N_VAR) {
+        bits |= loada_bits(R_, imm);
+        bits |= opnd_bits(L_, imm, is_vec);  // scalar left operand
+        bits |= bin_case(nd.cls, canon_form(nd.cls, FORM_SA));
+      } else {  // two scalars that could not be folded (at least one parameter)
+        bits |= loada_bits(L_, imm);
+        bits |= opnd_bits(R_, imm, is_vec);
+        bits |= bin_case(nd.cls, canon_form(nd.cls, FORM_AS));
+      }
+      em.put(bits, imm);
+      --top;
+      continue;
+    }
+    if (lop && !rop) {
+      if (f.phase == 0) {
+        f.phase = 1;
+        fr[top + 1] = Frame{nd.l, 0, f.spill, f.slot, 0};
+        ++top;
+      } else {
+        T imm = (T)0;
+        bool is_vec;
+        uint32_t bits = opnd_bits(R_, imm, is_vec);
+        bits |= bin_case(nd.cls, canon_form(nd.cls, is_vec ? FORM_AV : FORM_AS));
+        em.put(bits, imm);
+        --top;
+      }
+      continue;
+    }
+    if (!lop && rop) {
+      if (f.phase == 0) {
+        f.phase = 1;
+        fr[top + 1] = Frame{nd.r, 0, f.spill, f.slot, 0};
+        ++top;
+      } else {
+        T imm = (T)0;
+        bool is_vec;
+        uint32_t bits = opnd_bits(L_, imm, is_vec);
+        bits |= bin_case(nd.cls, canon_form(nd.cls, is_vec ? FORM_VA : FORM_SA));
+        em.put(bits, imm);
+        --top;
+      }
+      continue;
+    }
+    // both children are operators
+    if (f.phase == 0) {
+      f.first_left = (L_.need >= R_.need) ? 1 : 0;
+      f.phase = 1;
+      fr[top + 1] = Frame{f.first_left ? nd.l : nd.r, 0, f.spill, f.slot, 0};
+      ++top;
+    } else if (f.phase == 1) {
+      f.phase = 2;
+      const int slot = depth++;
+      if (depth > max_depth) max_depth = depth;
+      fr[top + 1] = Frame{f.first_left ? nd.r : nd.l, 0, 1, (uint8_t)slot, 0};
+      ++top;
+    } else {
+      const int slot = --depth;
+      uint32_t bits = ((uint32_t)OK_SLOT << SH_OPK) | ((uint32_t)slot << SH_OP_IDX);
+      // first_left: the left value sits in the slot and ACC holds the right value
+      bits |= bin_case(nd.cls, canon_form(nd.cls, f.first_left ? FORM_VA : FORM_AV));
+      em.put(bits, (T)0);
+      --top;
+    }
+  }
+  h.n_instr = em.n;
+  h.n_slots = max_depth;
+  return h;
+}
+
+}  // namespace ws

@@ -1,0 +1,122 @@
+// ws_debug.cu -- host-only introspection entry points (ws_debug_*).
+//
+// These run the program compiler (ws_compile.cuh) and a scalar interpreter of its tape on the
+// HOST, with the C library's math, so the compiler can be verified exactly on a machine
+// without a GPU: per-row results of compile+run must equal a direct stack interpretation with
+// the same math.  They are not an evaluation path: no fitness entry point calls them.
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "ws_internal.h"
+#include "ws_compile.cuh"
+
+namespace ws {
+namespace {
+
+template <typename T, bool STRICT>
+int32_t compile_host(const uint8_t* prog, int64_t L, const T* consts, int64_t K,
+                     const TokenLut& lut, uint32_t* ctrl_out, double* imm_out, int32_t* hdr_out) {
+  const int Lcap = L > 1 ? (int)L : 1;
+  std::vector<Instr<T>> tape((size_t)Lcap);
+  const ProgHdr h = compile_program<T, STRICT, true, 256>(prog, (int)L, consts, (int)K, lut,
+                                                          tape.data());
+  hdr_out[0] = h.n_instr;
+  hdr_out[1] = h.status;
+  hdr_out[2] = h.n_slots;
+  hdr_out[3] = h.n_tok;
+  for (int i = 0; i < h.n_instr; ++i) {
+    ctrl_out[i] = tape[i].ctrl;
+    imm_out[i] = (double)tape[i].imm;
+  }
+  return h.n_instr;
+}
+
+template <typename T, bool STRICT>
+void run_host(const uint32_t* ctrl, const double* imm, int n, const T* x, int64_t D,
+              T* out_pred, uint8_t* out_err) {
+  for (int64_t d = 0; d < D; ++d) {
+    T acc = (T)0, slots[32];
+    bool err = false;
+    for (int i = 0; i < n; ++i) {
+      const uint32_t c = ctrl[i];
+      const T im = (T)imm[i];
+      if (c & F_SPILL) slots[(c >> SH_SLOT) & 31u] = acc;
+      const uint32_t la = (c >> SH_LA) & 3u;
+      if (la == LA_X) acc = x[((c >> SH_LA_IDX) & 63u) * D + d];
+      else if (la == LA_IMM) acc = im;
+      const uint32_t ok = (c >> SH_OPK) & 3u, oi = (c >> SH_OP_IDX) & 63u;
+      T v = (T)0;
+      if (ok == OK_X) v = x[oi * D + d];
+      else if (ok == OK_SLOT) v = slots[oi];
+      else if (ok == OK_SCALAR) v = im;
+      const uint32_t cs = c & CASE_MASK;
+      bool e = false;
+      if (cs == CASE_NOP) {
+      } else if (cs >= CASE_BIN) {
+        const int cls = T_ADD + (int)((cs - CASE_BIN) >> 2), form = (int)((cs - CASE_BIN) & 3u);
+        const bool acc_left = form == FORM_AV || form == FORM_AS;
+        acc = acc_left ? apply_binary<T, STRICT>(cls, acc, v, e)
+                       : apply_binary<T, STRICT>(cls, v, acc, e);
+      } else {
+        acc = apply_unary<T, STRICT>((int)cs, acc, e);
+      }
+      err = err || e;
+    }
+    out_pred[d] = acc;
+    out_err[d] = err ? 1 : 0;
+  }
+}
+
+}  // namespace
+}  // namespace ws
+
+using namespace ws;
+
+extern "C" {
+
+ws_status ws_debug_token_lut(const ws_token_map* ids, int64_t num_vars, int32_t fused_order,
+                             uint8_t* cls_out, uint8_t* arg_out) {
+  clear_error();
+  if (!ids || !cls_out || !arg_out) return fail("null pointer");
+  const TokenLut lut = build_lut(*ids, num_vars, fused_order != 0);
+  std::memcpy(cls_out, lut.cls, 256);
+  std::memcpy(arg_out, lut.arg, 256);
+  return WS_OK;
+}
+
+ws_status ws_debug_compile(int32_t dtype, const uint8_t* prog, int64_t L, const void* consts,
+                           int64_t K, const ws_token_map* ids, int64_t num_vars,
+                           int32_t strict_mode, int32_t fused_order, uint32_t* ctrl_out,
+                           double* imm_out, int32_t* hdr_out) {
+  clear_error();
+  if (!ids || !ctrl_out || !imm_out || !hdr_out) return fail("null pointer");
+  if (L < 0 || L > 256) return fail("program length must be in [0, 256]");
+  if (K < 0 || (K > 0 && !consts)) return fail("bad constants");
+  const TokenLut lut = build_lut(*ids, num_vars, fused_order != 0);
+  if (dtype == WS_F32) {
+    if (strict_mode) compile_host<float, true>(prog, L, (const float*)consts, K, lut, ctrl_out, imm_out, hdr_out);
+    else compile_host<float, false>(prog, L, (const float*)consts, K, lut, ctrl_out, imm_out, hdr_out);
+  } else {
+    if (strict_mode) compile_host<double, true>(prog, L, (const double*)consts, K, lut, ctrl_out, imm_out, hdr_out);
+    else compile_host<double, false>(prog, L, (const double*)consts, K, lut, ctrl_out, imm_out, hdr_out);
+  }
+  return WS_OK;
+}
+
+ws_status ws_debug_run_tape(int32_t dtype, const uint32_t* ctrl, const double* imm, int32_t n,
+                            const void* x, int64_t D, int32_t strict_mode, void* out_pred,
+                            uint8_t* out_err) {
+  clear_error();
+  if (!ctrl || !imm || !out_pred || !out_err || n < 0 || D < 0) return fail("bad arguments");
+  if (dtype == WS_F32) {
+    if (strict_mode) run_host<float, true>(ctrl, imm, n, (const float*)x, D, (float*)out_pred, out_err);
+    else run_host<float, false>(ctrl, imm, n, (const float*)x, D, (float*)out_pred, out_err);
+  } else {
+    if (strict_mode) run_host<double, true>(ctrl, imm, n, (const double*)x, D, (double*)out_pred, out_err);
+    else run_host<double, false>(ctrl, imm, n, (const double*)x, D, (double*)out_pred, out_err);
+  }
+  return WS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,64 @@
+// ws_internal.h -- host-side helpers shared by the translation units of libwarpsym.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <string>
+
+#include "../../include/warpsym.h"
+#include "ws_ops.cuh"
+
+namespace ws {
+
+// Thread-local message of the last failed API call (read back by ws_last_error()).
+void set_error(const std::string& msg);
+void clear_error();
+
+// Returns WS_ERR_INVALID_ARGUMENT with `msg` recorded.
+ws_status fail(const std::string& msg);
+ws_status fail_cuda(cudaError_t e, const char* where);
+
+// Builds the token lookup table from the reference's scalar IDs.  `fused_order` selects the
+// unary comparison order of rpn_eval_fused_kernel (rpn_kernels.cu:2381-2398) instead of
+// rpn_eval_kernel's (rpn_kernels.cu:329-346); they differ only when two operators share an ID.
+TokenLut build_lut(const ws_token_map& m, int64_t num_vars, bool fused_order);
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Device properties cached per device.
+struct DeviceInfo {
+  int sm_count;
+  size_t smem_optin;
+};
+const DeviceInfo& device_info();
+
+// Workspace layout of the fitness evaluator for B programs of L tokens.
+struct FitnessWorkspace {
+  size_t hdr_off, tape_off, part_off, cnt_off, misc_off, total;
+  int64_t max_partials;  // partial records available (B * n_splits must not exceed it)
+};
+FitnessWorkspace fitness_workspace_layout(int64_t B, int64_t L, int dtype);
+
+// Launch of the compile + evaluate pipeline (ws_fitness.cu).
+struct FitnessRequest {
+  int dtype;
+  const uint8_t* pop;
+  int64_t B, L;
+  const void* x;
+  int64_t V, D;
+  const void* consts;
+  int64_t K;
+  const void* y;
+  void* out_loss;
+  int32_t* out_ninv;
+  int strict, policy, loss, schedule, phase;
+  double invalid_value;
+  TokenLut lut;
+  void* workspace;
+  size_t workspace_bytes;
+  cudaStream_t stream;
+};
+ws_status launch_fitness(const FitnessRequest& rq);
+
+}  // namespace ws
