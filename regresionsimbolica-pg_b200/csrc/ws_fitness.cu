@@ -426,20 +426,49 @@ constexpr int kW = 8;       // warps per CTA
 constexpr int kPBMax = 64;  // programs per block (upper bound)
 constexpr size_t kSmemBudget = 72 * 1024;
 
+// Largest dynamic shared memory the kernel may request (opt-in limit minus its static shared
+// memory); the attribute is raised to it once per device.
+template <typename T, int R, bool STRICT>
+size_t max_dynamic_smem() {
+  static std::mutex mu;
+  static size_t cache[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  std::lock_guard<std::mutex> g(mu);
+  if (cache[dev] == 0) {
+    cudaFuncAttributes fa;
+    size_t stat = 0;
+    if (cudaFuncGetAttributes(&fa, fitness_kernel<T, R, STRICT>) == cudaSuccess)
+      stat = fa.sharedSizeBytes;
+    size_t lim = device_info().smem_optin > stat ? device_info().smem_optin - stat : 0;
+    if (cudaFuncSetAttribute(fitness_kernel<T, R, STRICT>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) != cudaSuccess) {
+      (void)cudaGetLastError();  // clear our own failed attribute call; fall back to 48 KB
+      lim = 48 * 1024 - stat;
+    }
+    cache[dev] = lim;
+  }
+  return cache[dev];
+}
+
 template <typename T, int R, bool STRICT>
 int occupancy_for(size_t smem, int threads) {
   static std::mutex mu;
   static std::map<std::pair<int, size_t>, int> cache;
   int dev = 0;
   cudaGetDevice(&dev);
+  if (smem > max_dynamic_smem<T, R, STRICT>()) return 0;
   std::lock_guard<std::mutex> g(mu);
   auto key = std::make_pair(dev, smem);
   auto it = cache.find(key);
   if (it != cache.end()) return it->second;
-  cudaFuncSetAttribute(fitness_kernel<T, R, STRICT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)device_info().smem_optin);
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fitness_kernel<T, R, STRICT>, threads, smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fitness_kernel<T, R, STRICT>, threads,
+                                                    smem) != cudaSuccess) {
+    (void)cudaGetLastError();
+    occ = 0;
+  }
   cache[key] = occ;
   return occ;
 }
@@ -497,7 +526,7 @@ ws_status launch_typed(const FitnessRequest& rq) {
   int64_t rc_cap = kSmemBudget > fixed + per_row * PASS
                        ? (int64_t)((kSmemBudget - fixed) / per_row) / PASS * PASS
                        : PASS;
-  const size_t optin = device_info().smem_optin;
+  const size_t optin = max_dynamic_smem<T, R, STRICT>();
   if (fixed + per_row * PASS > optin) return fail("too many variables for the shared-memory tile");
   int RC = (int)(d_pad < rc_cap ? d_pad : rc_cap);
   if (RC < PASS) RC = PASS;

