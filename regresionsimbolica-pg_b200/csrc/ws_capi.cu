@@ -118,7 +118,7 @@ size_t ws_fitness_workspace_bytes(int64_t B, int64_t L, int32_t dtype) {
   return fitness_workspace_layout(B, L, dtype).total;
 }
 
-int32_t ws_schedule_count(void) { return 1; }
+int32_t ws_schedule_count(void) { return schedule_count(); }
 
 ws_status ws_eval_rpn(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
                       const void* x, int64_t num_vars, int64_t D, const void* constants,

@@ -63,7 +63,9 @@ template <> struct alignas(16) Instr<double> {
   double imm;
 };
 
-enum { PROG_OK = 0, PROG_INVALID = 1 };
+// PROG_UNREPRESENTABLE: an operand offset does not fit the tape word (the host sizes chunks so
+// that this cannot happen; the evaluator treats it as an internal error).
+enum { PROG_OK = 0, PROG_INVALID = 1, PROG_UNREPRESENTABLE = 2 };
 struct alignas(16) ProgHdr {
   int32_t n_instr;  // tape length
   int32_t status;   // PROG_OK / PROG_INVALID
@@ -96,18 +98,80 @@ struct Frame {
   uint8_t first_left;
 };
 
+// ---- evaluator tape word (the lowering of the logical fields above) ---------------------
+//   [0:6)   dense case: 0 = NOP, 1..17 unary (cls - T_SIN + 1), 18..41 binary
+//           (18 + 4*(cls-T_ADD) + form)
+//   [6]     SPILL: store ACC into spill slot [7:10) first
+//   [10]    LOADA_X: ACC <- X row at offset [12:21); [11] LOADA_S: ACC <- immediate
+//   [21]    FETCH: V <- shared row at offset [23:32), from a spill slot when [22] is set
+// Offsets are in units of one pass (32*R rows): variable v of a chunk of RC rows sits at
+// v * (RC / pass), spill slot s at s.  Scalar operands are the immediate.  `xmul` = RC / pass
+// is fixed by the schedule before compiling.  Spill slots below kSharedSlots live in shared
+// memory, deeper ones (0.2% of random 64-token programs) in a per-warp global scratch area.
+enum : uint32_t {
+  P_CASE_MASK = 0x3Fu,
+  P_SPILL = 1u << 6,
+  P_SH_SLOT = 7,
+  P_LOADA_X = 1u << 10,
+  P_LOADA_S = 1u << 11,
+  P_SH_LA = 12,
+  P_FETCH = 1u << 21,
+  P_FETCH_SLOT = 1u << 22,
+  P_SH_V = 23,
+  P_OFF_MASK = 0x1FFu,
+};
+enum { PCASE_NOP = 0, PCASE_UNARY0 = 1, PCASE_BIN = 18, PCASE_COUNT = 42 };
+constexpr int kSharedSlots = 2;
+
+WS_HD uint32_t lower_case(uint32_t logical) {
+  const uint32_t c = logical & CASE_MASK;
+  if (c == CASE_NOP) return PCASE_NOP;
+  if (c < CASE_BIN) return PCASE_UNARY0 + (c - T_SIN);
+  return PCASE_BIN + (c - CASE_BIN);
+}
+
 template <typename T>
 struct Emitter {
   Instr<T>* out;
   int n;
-  WS_HD void put(uint32_t ctrl, T imm) {
+  int xmul;        // RC / pass
+  int cap;         // capacity of `out`
+  bool ok = true;  // false if an operand is not representable in the tape word
+  WS_HD void put(uint32_t c, T imm) {
+    uint32_t w = lower_case(c);
+    if (c & F_SPILL) w |= P_SPILL | (((c >> SH_SLOT) & 7u) << P_SH_SLOT);
+    const uint32_t la = (c >> SH_LA) & 3u, lai = (c >> SH_LA_IDX) & 63u;
+    if (la == LA_X) {
+      const uint32_t off = lai * (uint32_t)xmul;
+      ok = ok && off <= P_OFF_MASK;
+      w |= P_LOADA_X | ((off & P_OFF_MASK) << P_SH_LA);
+    } else if (la == LA_IMM) {
+      w |= P_LOADA_S;
+    } else if (la == LA_PARAM) {
+      ok = false;  // parameters are baked into immediates for this tape
+    }
+    const uint32_t opk = (c >> SH_OPK) & 3u, oi = (c >> SH_OP_IDX) & 63u;
+    if (opk == OK_X) {
+      const uint32_t off = oi * (uint32_t)xmul;
+      ok = ok && off <= P_OFF_MASK;
+      w |= P_FETCH | ((off & P_OFF_MASK) << P_SH_V);
+    } else if (opk == OK_SLOT) {
+      w |= P_FETCH | P_FETCH_SLOT | (oi << P_SH_V);
+    } else if (opk == OK_SCALAR && (c & F_OP_PARAM)) {
+      ok = false;
+    }
+    if (n >= cap) { ok = false; return; }
     Instr<T> ins;
-    ins.ctrl = ctrl;
+    ins.ctrl = w;
     ins.imm = imm;
     if constexpr (sizeof(Instr<T>) == 16) reinterpret_cast<Instr<double>&>(ins).pad = 0;
     out[n++] = ins;
   }
 };
+
+// Tape capacity for programs of L tokens: one word per operator (a single-terminal program
+// still needs one).
+WS_HD int tape_capacity(int L) { return L > 1 ? L : 1; }
 
 // Loads leaf `nd` into ACC: returns the ctrl bits and sets `imm` for an immediate.
 template <typename T>
@@ -144,11 +208,12 @@ WS_HD int canon_form(int cls, int form) {
 
 // Compiles program `prog` (L tokens) into `tape`.  `consts` (K values, may be null when K == 0)
 // are baked into immediates when BAKE, otherwise `C` leaves become parameters (slot index).
-// `nodes`/`stk`/`frames` are per-thread scratch of LMAX entries.
+// `xmul` = rows per chunk / rows per pass of the evaluator schedule (tape offsets are scaled by
+// it).  `nodes`/`stk`/`frames` are per-thread scratch of LMAX entries.
 template <typename T, bool STRICT, bool BAKE, int LMAX>
 __host__ __device__ ProgHdr compile_program(const uint8_t* __restrict__ prog, int L,
                                    const T* __restrict__ consts, int K, const TokenLut& lut,
-                                   Instr<T>* __restrict__ tape) {
+                                   Instr<T>* __restrict__ tape, int xmul) {
   Node<T> nodes[LMAX];
   int16_t stk[33];
   ProgHdr h;
@@ -257,13 +322,14 @@ __host__ __device__ ProgHdr compile_program(const uint8_t* __restrict__ prog, in
   if (h.status != PROG_OK) return h;
 
   // ---- emission: post-order walk with Sethi-Ullman child order ---------------------------
-  Emitter<T> em{tape, 0};
+  Emitter<T> em{tape, 0, xmul, tape_capacity(Lr)};
   const int root = stk[0];
   if (nodes[root].kind != N_OP) {  // the whole program is one terminal (or folded constant)
     T imm = (T)0;
     uint32_t bits = loada_bits(nodes[root], imm);
     em.put(CASE_NOP | bits, imm);
     h.n_instr = em.n;
+    if (!em.ok) h.status = PROG_UNREPRESENTABLE;
     return h;
   }
   Frame fr[LMAX];
@@ -367,6 +433,7 @@ __host__ __device__ ProgHdr compile_program(const uint8_t* __restrict__ prog, in
   }
   h.n_instr = em.n;
   h.n_slots = max_depth;
+  if (!em.ok) h.status = PROG_UNREPRESENTABLE;
   return h;
 }
 

@@ -17,10 +17,11 @@ namespace {
 template <typename T, bool STRICT>
 int32_t compile_host(const uint8_t* prog, int64_t L, const T* consts, int64_t K,
                      const TokenLut& lut, uint32_t* ctrl_out, double* imm_out, int32_t* hdr_out) {
-  const int Lcap = L > 1 ? (int)L : 1;
+  const int Lcap = tape_capacity((int)L);
   std::vector<Instr<T>> tape((size_t)Lcap);
+  // xmul = 1: tape offsets are plain variable / slot indices
   const ProgHdr h = compile_program<T, STRICT, true, 256>(prog, (int)L, consts, (int)K, lut,
-                                                          tape.data());
+                                                          tape.data(), 1);
   hdr_out[0] = h.n_instr;
   hdr_out[1] = h.status;
   hdr_out[2] = h.n_slots;
@@ -35,31 +36,31 @@ int32_t compile_host(const uint8_t* prog, int64_t L, const T* consts, int64_t K,
 template <typename T, bool STRICT>
 void run_host(const uint32_t* ctrl, const double* imm, int n, const T* x, int64_t D,
               T* out_pred, uint8_t* out_err) {
+  // xmul = 1: tape offsets of X operands are variable indices
   for (int64_t d = 0; d < D; ++d) {
     T acc = (T)0, slots[32];
     bool err = false;
     for (int i = 0; i < n; ++i) {
       const uint32_t c = ctrl[i];
       const T im = (T)imm[i];
-      if (c & F_SPILL) slots[(c >> SH_SLOT) & 31u] = acc;
-      const uint32_t la = (c >> SH_LA) & 3u;
-      if (la == LA_X) acc = x[((c >> SH_LA_IDX) & 63u) * D + d];
-      else if (la == LA_IMM) acc = im;
-      const uint32_t ok = (c >> SH_OPK) & 3u, oi = (c >> SH_OP_IDX) & 63u;
-      T v = (T)0;
-      if (ok == OK_X) v = x[oi * D + d];
-      else if (ok == OK_SLOT) v = slots[oi];
-      else if (ok == OK_SCALAR) v = im;
-      const uint32_t cs = c & CASE_MASK;
+      if (c & P_SPILL) slots[(c >> P_SH_SLOT) & 7u] = acc;
+      if (c & P_LOADA_X) acc = x[((c >> P_SH_LA) & P_OFF_MASK) * D + d];
+      else if (c & P_LOADA_S) acc = im;
+      T v = im;
+      if (c & P_FETCH) {
+        const uint32_t off = c >> P_SH_V;
+        v = (c & P_FETCH_SLOT) ? slots[off & 31u] : x[off * D + d];
+      }
+      const uint32_t cs = c & P_CASE_MASK;
       bool e = false;
-      if (cs == CASE_NOP) {
-      } else if (cs >= CASE_BIN) {
-        const int cls = T_ADD + (int)((cs - CASE_BIN) >> 2), form = (int)((cs - CASE_BIN) & 3u);
+      if (cs == PCASE_NOP) {
+      } else if (cs >= PCASE_BIN) {
+        const int cls = T_ADD + (int)((cs - PCASE_BIN) >> 2), form = (int)((cs - PCASE_BIN) & 3u);
         const bool acc_left = form == FORM_AV || form == FORM_AS;
         acc = acc_left ? apply_binary<T, STRICT>(cls, acc, v, e)
                        : apply_binary<T, STRICT>(cls, v, acc, e);
       } else {
-        acc = apply_unary<T, STRICT>((int)cs, acc, e);
+        acc = apply_unary<T, STRICT>(T_SIN + (int)cs - PCASE_UNARY0, acc, e);
       }
       err = err || e;
     }

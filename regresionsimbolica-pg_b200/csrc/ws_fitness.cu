@@ -18,8 +18,9 @@
 //
 // Per-row values are bit-identical to the reference kernels when this file is compiled with
 // the reference's flags (--use_fast_math): same operator code (ws_ops.cuh), same FP32 rounding
-// of pred - y and of its square.  Only the order of the sum differs (FP64 here, FP32 warp
-// butterflies in the reference).
+// of pred - y and of its square.  Only the order of the sum differs: each lane sums the R
+// squared errors of a pass in T, passes and lanes are combined in FP64 (the reference sums in
+// FP32 warp butterflies).
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
@@ -47,14 +48,16 @@ __global__ void __launch_bounds__(128) compile_kernel(const uint8_t* __restrict_
                                                       TokenLut lut, Instr<T>* __restrict__ tape,
                                                       int Lcap, ProgHdr* __restrict__ hdr,
                                                       unsigned* __restrict__ prog_cnt,
-                                                      unsigned* __restrict__ misc, int S) {
+                                                      unsigned* __restrict__ misc, int S,
+                                                      int xmul) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p == 0) misc[0] = 0u;  // work-queue head of the evaluator launch that follows
   if (p >= B) return;
   ProgHdr h = compile_program<T, STRICT, true, LMAX>(pop + p * (int64_t)L, L,
                                                       K > 0 ? consts + p * (int64_t)K : nullptr,
-                                                      K, lut, tape + p * (int64_t)Lcap);
-  if (h.status == PROG_OK && h.n_slots > S) {  // cannot happen (Sethi-Ullman bound); guard
+                                                      K, lut, tape + p * (int64_t)Lcap, xmul);
+  // Neither can happen (Sethi-Ullman bound; chunk size chosen for the offsets): guard anyway.
+  if ((h.status == PROG_OK && h.n_slots > S) || h.status == PROG_UNREPRESENTABLE) {
     h.status = PROG_INVALID;
     atomicAdd(&misc[1], 1u);
   }
@@ -118,6 +121,10 @@ struct FitParams {
   unsigned* prog_cnt;
   unsigned* work;
   const double* yvar;
+  const int64_t* perm;  // programs in evaluation order (sorted by tape length)
+  T* gspill;            // per-warp scratch for spill slots beyond the shared ones
+  int count;            // 1: exact per-row invalid counts (out_ninv requested)
+  int async_stage;      // 1: chunk rows are 16-byte aligned -> cp.async staging
 };
 
 template <typename T> struct Vec16;
@@ -158,74 +165,99 @@ __device__ __forceinline__ void lane_store(T* s, const T (&d)[R]) {
 
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float m_max(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double m_max(double a, double b) { return fmax(a, b); }
 
 // Runs one program tape over one pass of 32*R rows.  xp: X tile at this pass and lane
 // (variable v at xp + v*RC); sp: this warp's spill slots at this lane.
+// Runs one program tape over one pass of 32*R rows.  xb: the X tile at this pass and lane;
+// sb: this warp's spill slots at this lane.  Tape offsets are in units of one pass.
+template <int R, typename F>
+__device__ __forceinline__ void for_rows(F&& f) {
+#pragma unroll
+  for (int k = 0; k < R; ++k) f(k);
+}
+
+// Runs one program tape over one pass of 32*R rows.  xb: the X tile at this pass and lane;
+// sb / gb: this warp's shared / global spill slots at this lane.  Tape offsets are in units
+// of one pass.
 template <typename T, int R, bool STRICT>
 __device__ __forceinline__ void run_tape(const Instr<T>* __restrict__ tp, int n,
-                                         const T* __restrict__ xp, int RC, T* __restrict__ sp,
-                                         T (&acc)[R], uint32_t& err) {
-  constexpr int SLOT = 32 * R;
+                                         const T* __restrict__ xb, T* __restrict__ sb,
+                                         T* __restrict__ gb, T (&acc)[R], uint32_t& err) {
+  constexpr int PASS = 32 * R;
   err = 0u;
+  // The next tape word is loaded while the current one executes.
+  Instr<T> nxt = tp[0];
 #pragma unroll 1
   for (int i = 0; i < n; ++i) {
-    const Instr<T> ins = tp[i];
+    const Instr<T> ins = nxt;
+    nxt = tp[i + 1 < n ? i + 1 : i];
     const uint32_t c = ins.ctrl;
-    if (c & F_SPILL) lane_store<T, R>(sp + ((c >> SH_SLOT) & 31u) * SLOT, acc);
-    const uint32_t la = (c >> SH_LA) & 3u;
-    if (la == LA_X) {
-      lane_load<T, R>(acc, xp + ((c >> SH_LA_IDX) & 63u) * RC);
-    } else if (la != LA_NONE) {  // immediate (parameters are not used by the baked tape)
+    if (c & P_SPILL) {
+      const uint32_t sl = (c >> P_SH_SLOT) & 7u;
+      if (sl < (uint32_t)kSharedSlots) lane_store<T, R>(sb + sl * PASS, acc);
+      else lane_store<T, R>(gb + (sl - kSharedSlots) * PASS, acc);
+    }
+    if (c & P_LOADA_X) {
+      lane_load<T, R>(acc, xb + ((c >> P_SH_LA) & P_OFF_MASK) * PASS);
+    } else if (c & P_LOADA_S) {
 #pragma unroll
       for (int k = 0; k < R; ++k) acc[k] = ins.imm;
     }
-    const uint32_t ok = (c >> SH_OPK) & 3u;
-    const uint32_t oi = (c >> SH_OP_IDX) & 63u;
     T v[R];
-    T s = ins.imm;
-    if (ok == OK_X) lane_load<T, R>(v, xp + oi * RC);
-    else if (ok == OK_SLOT) lane_load<T, R>(v, sp + oi * SLOT);
+    if (c & P_FETCH) {
+      const uint32_t off = c >> P_SH_V;
+      if (!(c & P_FETCH_SLOT)) lane_load<T, R>(v, xb + off * PASS);
+      else if (off < (uint32_t)kSharedSlots) lane_load<T, R>(v, sb + off * PASS);
+      else lane_load<T, R>(v, gb + (off - kSharedSlots) * PASS);
+    }
+    const T s = ins.imm;
 
 #define WS_ROWS(BODY) _Pragma("unroll") for (int k = 0; k < R; ++k) { BODY; } break
 #define WS_ERR(EXPR) { bool e_ = false; acc[k] = (EXPR); err |= (uint32_t)e_ << k; }
-#define WS_BIN4(CLS, F)                                                                  \
-  case CASE_BIN + 4 * (CLS - T_ADD) + FORM_AV: WS_ROWS(F(acc[k], v[k]));                \
-  case CASE_BIN + 4 * (CLS - T_ADD) + FORM_VA: WS_ROWS(F(v[k], acc[k]));                \
-  case CASE_BIN + 4 * (CLS - T_ADD) + FORM_AS: WS_ROWS(F(acc[k], s));                   \
-  case CASE_BIN + 4 * (CLS - T_ADD) + FORM_SA: WS_ROWS(F(s, acc[k]));
+#define WS_BIN4(CLS, F)                                                          \
+  case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_AV: WS_ROWS(F(acc[k], v[k]));        \
+  case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_VA: WS_ROWS(F(v[k], acc[k]));        \
+  case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_AS: WS_ROWS(F(acc[k], s));           \
+  case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_SA: WS_ROWS(F(s, acc[k]));
 #define F_ADD(a, b) acc[k] = (a) + (b)
 #define F_SUB(a, b) acc[k] = (a) - (b)
 #define F_MUL(a, b) acc[k] = (a) * (b)
 #define F_DIV(a, b) WS_ERR((op_div<T, STRICT>((a), (b), e_)))
 #define F_POW(a, b) WS_ERR((op_pow<T, STRICT>((a), (b), e_)))
 #define F_MOD(a, b) WS_ERR((op_mod<T, STRICT>((a), (b), e_)))
-    switch (c & CASE_MASK) {
-      case CASE_NOP: break;
+#define U_(CLS) (PCASE_UNARY0 + (CLS - T_SIN))
+    switch (c & P_CASE_MASK) {
+      case PCASE_NOP: break;
       WS_BIN4(T_ADD, F_ADD)
       WS_BIN4(T_SUB, F_SUB)
       WS_BIN4(T_MUL, F_MUL)
       WS_BIN4(T_DIV, F_DIV)
       WS_BIN4(T_POW, F_POW)
       WS_BIN4(T_MOD, F_MOD)
-      case T_SIN: WS_ROWS(acc[k] = m_sin(acc[k]));
-      case T_COS: WS_ROWS(acc[k] = m_cos(acc[k]));
-      case T_TAN: WS_ROWS(acc[k] = m_tan(acc[k]));
-      case T_LOG: WS_ROWS(WS_ERR((op_log<T, STRICT>(acc[k], e_))));
-      case T_EXP: WS_ROWS(WS_ERR((op_exp<T, STRICT>(acc[k], e_))));
-      case T_SQRT: WS_ROWS(WS_ERR((op_sqrt<T, STRICT>(acc[k], e_))));
-      case T_ABS: WS_ROWS(acc[k] = m_abs(acc[k]));
-      case T_NEG: WS_ROWS(acc[k] = -acc[k]);
-      case T_FACT: WS_ROWS(WS_ERR((op_tgamma<T, STRICT>(acc[k] + (T)1.0, e_))));
-      case T_FLOOR: WS_ROWS(acc[k] = m_floor(acc[k]));
-      case T_CEIL: WS_ROWS(acc[k] = m_ceil(acc[k]));
-      case T_SIGN: WS_ROWS(acc[k] = op_sign<T>(acc[k]));
-      case T_GAMMA: WS_ROWS(WS_ERR((op_tgamma<T, STRICT>(acc[k], e_))));
-      case T_LGAMMA: WS_ROWS(WS_ERR((op_lgamma<T, STRICT>(acc[k], e_))));
-      case T_ASIN: WS_ROWS(WS_ERR((op_asin<T, STRICT>(acc[k], e_))));
-      case T_ACOS: WS_ROWS(WS_ERR((op_acos<T, STRICT>(acc[k], e_))));
-      case T_ATAN: WS_ROWS(acc[k] = m_atan(acc[k]));
+      case U_(T_SIN): WS_ROWS(acc[k] = m_sin(acc[k]));
+      case U_(T_COS): WS_ROWS(acc[k] = m_cos(acc[k]));
+      case U_(T_TAN): WS_ROWS(acc[k] = m_tan(acc[k]));
+      case U_(T_LOG): WS_ROWS(WS_ERR((op_log<T, STRICT>(acc[k], e_))));
+      case U_(T_EXP): WS_ROWS(WS_ERR((op_exp<T, STRICT>(acc[k], e_))));
+      case U_(T_SQRT): WS_ROWS(WS_ERR((op_sqrt<T, STRICT>(acc[k], e_))));
+      case U_(T_ABS): WS_ROWS(acc[k] = m_abs(acc[k]));
+      case U_(T_NEG): WS_ROWS(acc[k] = -acc[k]);
+      case U_(T_FACT): WS_ROWS(WS_ERR((op_tgamma<T, STRICT>(acc[k] + (T)1.0, e_))));
+      case U_(T_FLOOR): WS_ROWS(acc[k] = m_floor(acc[k]));
+      case U_(T_CEIL): WS_ROWS(acc[k] = m_ceil(acc[k]));
+      case U_(T_SIGN): WS_ROWS(acc[k] = op_sign<T>(acc[k]));
+      case U_(T_GAMMA): WS_ROWS(WS_ERR((op_tgamma<T, STRICT>(acc[k], e_))));
+      case U_(T_LGAMMA): WS_ROWS(WS_ERR((op_lgamma<T, STRICT>(acc[k], e_))));
+      case U_(T_ASIN): WS_ROWS(WS_ERR((op_asin<T, STRICT>(acc[k], e_))));
+      case U_(T_ACOS): WS_ROWS(WS_ERR((op_acos<T, STRICT>(acc[k], e_))));
+      case U_(T_ATAN): WS_ROWS(acc[k] = m_atan(acc[k]));
       default: err = 0xFFFFFFFFu; break;  // malformed tape: every row invalid
     }
+#undef U_
 #undef F_ADD
 #undef F_SUB
 #undef F_MUL
@@ -236,6 +268,66 @@ __device__ __forceinline__ void run_tape(const Instr<T>* __restrict__ tp, int n,
 #undef WS_ERR
 #undef WS_ROWS
   }
+}
+
+// Per-pass epilogue: squared errors of this lane's rows, summed in T (then widened by the
+// caller), invalid-row count and per-row metric-overflow flag (WS_POLICY_FUSED only).
+template <typename T, int R, bool FUSED>
+__device__ __forceinline__ T pass_epilogue(const T (&a)[R], uint32_t err, const T* __restrict__ yb,
+                                           int lane, int first_row, int rows, int& ninv,
+                                           bool& ovf) {
+  constexpr int N = Vec16<T>::N;
+  constexpr int PASS = 32 * R;
+  constexpr T tmax = sizeof(T) == 4 ? (T)3.4028234663852886e38 : (T)1.7976931348623157e308;
+  T yv[R];
+  lane_load<T, R>(yv, yb);
+  const bool full = first_row + PASS <= rows;
+  T part = (T)0;
+#pragma unroll
+  for (int k = 0; k < R; ++k) {
+    const int row = first_row + (k / N) * 32 * N + lane * N + (k % N);
+    const bool act = full || row < rows;
+    const T pv = a[k];
+    const bool bad = ((err >> k) & 1u) || !(m_abs(pv) <= tmax);  // error, NaN or inf
+    const T diff = pv - yv[k];
+    T sq;
+    if (FUSED) {
+      const bool o = !(m_abs(diff) <= Limits<T>::max_diff);  // NaN / inf / > 4e18
+      const T q = mul_rn(diff, diff);
+      const bool o2 = o || !(m_abs(q) <= tmax);
+      ovf = ovf || (act && !bad && o2);
+      sq = (bad || o2) ? (T)0 : q;
+    } else {
+      sq = bad ? (T)0 : mul_rn(diff, diff);
+    }
+    ninv += (act && bad) ? 1 : 0;
+    part += act ? sq : (T)0;
+  }
+  return part;
+}
+
+// Fast per-pass epilogue for a pass whose rows are all inside the chunk, when per-row invalid
+// counts are not requested: squared errors summed in T; validity tracked without branches --
+// fma(pred, 0, acc) turns acc into NaN iff some prediction is NaN or infinite, and for the fused
+// policy fma(diff, 0, .) and max |diff| flag the metric overflow.  Rows that are invalid or
+// overflow only decide the program's class, never a value, so they need no masking here.
+template <typename T, int R, bool FUSED>
+__device__ __forceinline__ T pass_fast(const T (&a)[R], const T* __restrict__ yb, T& nanacc,
+                                       T& ovfacc, T& dmax) {
+  T yv[R];
+  lane_load<T, R>(yv, yb);
+  T part = (T)0;
+#pragma unroll
+  for (int k = 0; k < R; ++k) {
+    const T diff = a[k] - yv[k];
+    part = part + mul_rn(diff, diff);
+    nanacc = fma_rn(a[k], (T)0, nanacc);
+    if (FUSED) {
+      ovfacc = fma_rn(diff, (T)0, ovfacc);
+      dmax = m_max(dmax, m_abs(diff));
+    }
+  }
+  return part;
 }
 
 // Final loss of one program from its combined record.  Classification mirrors the
@@ -281,6 +373,45 @@ __device__ void write_final(const FitParams<T>& P, int64_t p, const PartRec& r) 
   else ((double*)P.out_loss)[p] = out;
 }
 
+// ---- chunk staging: 16-byte asynchronous copies (cp.async) into a shared tile ---------------
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Issues the copy of chunk c (X rows of every variable, then y) into tile `tb` and commits one
+// cp.async group.  With async_stage the copies are 16-byte cp.async (rows of X are 16-byte
+// aligned: D is a multiple of 16/sizeof(T)); otherwise plain loads/stores with zero fill.
+template <typename T>
+__device__ __forceinline__ void stage_chunk(const FitParams<T>& P, int64_t c, T* tb, int tid,
+                                            int nthreads) {
+  constexpr int VE = 16 / (int)sizeof(T);
+  const int64_t row0 = c * P.RC;
+  const int rows = (int)min((int64_t)P.RC, P.D - row0);
+  if (P.async_stage) {
+    const int nvec = rows / VE;
+    for (int v = 0; v <= P.V; ++v) {
+      const T* src = (v < P.V ? P.x + (size_t)v * P.D : P.y) + row0;
+      T* dst = tb + (size_t)v * P.RC;
+      for (int i = tid; i < nvec; i += nthreads) cp_async16(dst + i * VE, src + i * VE);
+    }
+  } else {
+    for (int v = 0; v <= P.V; ++v) {
+      const T* src = (v < P.V ? P.x + (size_t)v * P.D : P.y) + row0;
+      T* dst = tb + (size_t)v * P.RC;
+      for (int r = tid; r < P.RC; r += nthreads) dst[r] = (r < rows) ? src[r] : (T)0;
+    }
+  }
+  cp_async_commit();
+}
+
 template <typename T, int R, bool STRICT>
 __global__ void __launch_bounds__(256) fitness_kernel(const FitParams<T> P) {
   constexpr int N = Vec16<T>::N;
@@ -288,16 +419,18 @@ __global__ void __launch_bounds__(256) fitness_kernel(const FitParams<T> P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int W = blockDim.x >> 5;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  T* xs = reinterpret_cast<T*>(smem_raw);
-  T* ys = xs + (size_t)P.V * P.RC;
-  T* spill = ys + P.RC;
-  Instr<T>* tapes = reinterpret_cast<Instr<T>*>(spill + (size_t)W * P.S * PASS);
-  PartRec* acc_s = reinterpret_cast<PartRec*>(tapes + (size_t)W * P.Lcap);
+  // two tiles of X[:, chunk] and y[chunk] (double-buffered staging), then per-warp spill slots
+  const size_t tile_elems = (size_t)(P.V + 1) * P.RC;
+  T* tiles = reinterpret_cast<T*>(smem_raw);
+  T* spill = tiles + 2 * tile_elems;
+  Instr<T>* tapes = reinterpret_cast<Instr<T>*>(spill + (size_t)W * kSharedSlots * PASS);
+  PartRec* acc_s = reinterpret_cast<PartRec*>(tapes + (size_t)P.PB * P.Lcap);
+  int* meta_s = reinterpret_cast<int*>(acc_s + P.PB);  // per program: n_instr, or -1 if invalid
   __shared__ int64_t s_item;
-  __shared__ int s_next;
 
-  T* sp_w = spill + (size_t)warp * P.S * PASS + lane * N;
-  Instr<T>* tape_w = tapes + (size_t)warp * P.Lcap;
+  T* sp_w = spill + (size_t)warp * kSharedSlots * PASS + lane * N;
+  const int deep = P.S > kSharedSlots ? P.S - kSharedSlots : 0;
+  T* gsp_w = P.gspill + ((size_t)blockIdx.x * W + warp) * (size_t)deep * PASS + lane * N;
   const bool fused_policy = P.policy == WS_POLICY_FUSED;
 
   for (;;) {
@@ -311,69 +444,70 @@ __global__ void __launch_bounds__(256) fitness_kernel(const FitParams<T> P) {
     const int np = (int)min((int64_t)P.PB, P.B - p0);
     const int64_t c0 = (int64_t)split * P.cps;
     const int64_t c1 = min(P.n_chunks, c0 + P.cps);
-    for (int q = threadIdx.x; q < np; q += blockDim.x) acc_s[q] = PartRec{0.0, 0, 0};
+    // stage the block's tapes once for all its chunks (programs arrive sorted by tape length,
+    // so a static warp assignment is balanced)
+    for (int q = warp; q < np; q += W) {
+      const int64_t p = P.perm[p0 + q];
+      const ProgHdr h = P.hdr[p];
+      const Instr<T>* tg = P.tape + p * (int64_t)P.Lcap;
+      for (int i = lane; i < h.n_instr; i += 32) tapes[(size_t)q * P.Lcap + i] = tg[i];
+      if (lane == 0) {
+        meta_s[q] = h.status == PROG_OK ? h.n_instr : -1;
+        acc_s[q] = PartRec{0.0, 0, 0};
+      }
+    }
 
+    int buf = 0;
+    stage_chunk<T>(P, c0, tiles, threadIdx.x, blockDim.x);
     for (int64_t c = c0; c < c1; ++c) {
-      __syncthreads();  // previous chunk fully consumed; accumulators initialised
+      T* xs = tiles + (size_t)buf * tile_elems;
+      T* ys = xs + (size_t)P.V * P.RC;
+      if (c + 1 < c1) {  // the next chunk streams in while this one is evaluated
+        stage_chunk<T>(P, c + 1, tiles + (size_t)(buf ^ 1) * tile_elems, threadIdx.x, blockDim.x);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
       const int64_t row0 = c * P.RC;
       const int rows = (int)min((int64_t)P.RC, P.D - row0);
-      for (int v = 0; v < P.V; ++v) {
-        const T* src = P.x + (size_t)v * P.D + row0;
-        T* dst = xs + (size_t)v * P.RC;
-        for (int r = threadIdx.x; r < P.RC; r += blockDim.x) dst[r] = (r < rows) ? src[r] : (T)0;
+      if (P.async_stage && rows < P.RC) {  // zero the rows past the end of the data
+        for (int v = 0; v <= P.V; ++v)
+          for (int r = rows + threadIdx.x; r < P.RC; r += blockDim.x) xs[(size_t)v * P.RC + r] = (T)0;
       }
-      for (int r = threadIdx.x; r < P.RC; r += blockDim.x) ys[r] = (r < rows) ? P.y[row0 + r] : (T)0;
-      if (threadIdx.x == 0) s_next = 0;
-      __syncthreads();
+      __syncthreads();  // chunk c visible to all warps; tapes and accumulators ready
       const int npass = (rows + PASS - 1) / PASS;
 
-      for (;;) {
-        int q = 0;
-        if (lane == 0) q = atomicAdd(&s_next, 1);
-        q = __shfl_sync(0xFFFFFFFFu, q, 0);
-        if (q >= np) break;
-        const int64_t p = p0 + q;
-        const ProgHdr h = P.hdr[p];
-        if (h.status != PROG_OK) {
+      for (int q = warp; q < np; q += W) {
+        const int n_instr = meta_s[q];
+        if (n_instr < 0) {
           if (lane == 0) acc_s[q].ninv += rows;
           continue;
         }
-        const Instr<T>* tg = P.tape + p * (int64_t)P.Lcap;
-        for (int i = lane; i < h.n_instr; i += 32) tape_w[i] = tg[i];
-        __syncwarp();
+        const Instr<T>* tape_q = tapes + (size_t)q * P.Lcap;
         double sse = 0.0;
         int ninv = 0;
         bool ovf = false;
+        uint32_t errany = 0u;
+        T nanacc = (T)0, ovfacc = (T)0, dmax = (T)0;
         for (int pass = 0; pass < npass; ++pass) {
           T a[R];
           uint32_t err;
-          const T* xp = xs + pass * PASS + lane * N;
-          run_tape<T, R, STRICT>(tape_w, h.n_instr, xp, P.RC, sp_w, a, err);
-          T yv[R];
-          lane_load<T, R>(yv, ys + pass * PASS + lane * N);
-#pragma unroll
-          for (int k = 0; k < R; ++k) {
-            const int row = pass * PASS + (k / N) * 32 * N + lane * N + (k % N);
-            if (row < rows) {
-              const T pv = a[k];
-              if (((err >> k) & 1u) || m_isnan(pv) || m_isinf(pv)) {
-                ninv++;
-              } else {
-                const T diff = pv - yv[k];
-                if (fused_policy) {
-                  const T ad = diff < (T)0 ? -diff : diff;
-                  bool o = m_isnan(diff) || m_isinf(diff) || ad > Limits<T>::max_diff;
-                  const T sq = o ? (T)0 : mul_rn(diff, diff);
-                  o = o || m_isnan(sq) || m_isinf(sq);
-                  if (o) ovf = true;
-                  else sse += (double)sq;
-                } else {
-                  sse += (double)mul_rn(diff, diff);
-                }
-              }
-            }
+          run_tape<T, R, STRICT>(tape_q, n_instr, xs + pass * PASS + lane * N, sp_w, gsp_w, a, err);
+          const T* yb = ys + pass * PASS + lane * N;
+          T part;
+          if (!P.count && (pass + 1) * PASS <= rows) {
+            errany |= err;
+            part = fused_policy ? pass_fast<T, R, true>(a, yb, nanacc, ovfacc, dmax)
+                                : pass_fast<T, R, false>(a, yb, nanacc, ovfacc, dmax);
+          } else {
+            part = fused_policy
+                ? pass_epilogue<T, R, true>(a, err, yb, lane, pass * PASS, rows, ninv, ovf)
+                : pass_epilogue<T, R, false>(a, err, yb, lane, pass * PASS, rows, ninv, ovf);
           }
+          sse += (double)part;
         }
+        if (errany != 0u || m_isnan(nanacc)) ninv += 1;  // only "> 0" matters without counting
+        ovf = ovf || m_isnan(ovfacc) || dmax > Limits<T>::max_diff;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
           sse += __shfl_xor_sync(0xFFFFFFFFu, sse, o);
@@ -385,12 +519,12 @@ __global__ void __launch_bounds__(256) fitness_kernel(const FitParams<T> P) {
           acc_s[q].ninv += ninv;
           acc_s[q].ovf |= any_ovf ? 1 : 0;
         }
-        __syncwarp();
       }
+      __syncthreads();  // every warp is done with this tile before it is refilled
+      buf ^= 1;
     }
-    __syncthreads();
     for (int q = threadIdx.x; q < np; q += blockDim.x) {
-      const int64_t p = p0 + q;
+      const int64_t p = P.perm[p0 + q];
       const PartRec r = acc_s[q];
       if (P.n_splits == 1) {
         write_final<T>(P, p, r);
@@ -412,8 +546,52 @@ __global__ void __launch_bounds__(256) fitness_kernel(const FitParams<T> P) {
         }
       }
     }
-    // the next item's accumulator reset waits on the __syncthreads() at the loop top
+    // the next item's staging waits on the __syncthreads() at the loop top
     __syncthreads();
+  }
+}
+
+// ---- length-sorted schedule: counting sort of programs by tape length (longest first) ------
+constexpr int kSortBins = 258;  // tape lengths 0..256, plus invalid programs
+
+__global__ void __launch_bounds__(256) sort_hist_kernel(const ProgHdr* __restrict__ hdr, int64_t B,
+                                                        unsigned* __restrict__ bins) {
+  __shared__ unsigned h[kSortBins];
+  for (int i = threadIdx.x; i < kSortBins; i += blockDim.x) h[i] = 0u;
+  __syncthreads();
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < B;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const ProgHdr v = hdr[p];
+    const int key = v.status == PROG_OK ? min(v.n_instr, 256) : 257;
+    atomicAdd(&h[key], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kSortBins; i += blockDim.x)
+    if (h[i]) atomicAdd(&bins[i], h[i]);
+}
+
+// Exclusive offsets in descending tape length, invalid programs last (single block).
+__global__ void __launch_bounds__(32) sort_scan_kernel(unsigned* __restrict__ bins) {
+  if (threadIdx.x == 0) {
+    unsigned run = 0u;
+    for (int key = 256; key >= 0; --key) {
+      const unsigned c = bins[key];
+      bins[key] = run;
+      run += c;
+    }
+    bins[257] = run;
+  }
+}
+
+__global__ void __launch_bounds__(256) sort_scatter_kernel(const ProgHdr* __restrict__ hdr,
+                                                           int64_t B, unsigned* __restrict__ bins,
+                                                           int64_t* __restrict__ perm) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < B;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const ProgHdr v = hdr[p];
+    const int key = v.status == PROG_OK ? min(v.n_instr, 256) : 257;
+    const unsigned pos = atomicAdd(&bins[key], 1u);
+    perm[pos] = p;
   }
 }
 
@@ -421,10 +599,28 @@ __global__ void __launch_bounds__(256) fitness_kernel(const FitParams<T> P) {
 // host side
 namespace {
 
-constexpr int kR = 8;       // rows per lane per pass
-constexpr int kW = 8;       // warps per CTA
-constexpr int kPBMax = 64;  // programs per block (upper bound)
-constexpr size_t kSmemBudget = 72 * 1024;
+
+// Compiled schedules: rows per lane per pass (R), warps per CTA (W), shared-memory budget per
+// CTA.  Index 0 = choose automatically; the Python autotuner times the others.
+struct Sched {
+  int R, W, PB;
+  size_t smem_budget;
+};
+constexpr Sched kSched[] = {
+    {16, 8, 32, 72 * 1024},   // 0: auto placeholder (resolved by pick_schedule)
+    {8, 8, 32, 72 * 1024},    // 1
+    {16, 4, 16, 56 * 1024},   // 2
+    {16, 8, 32, 72 * 1024},   // 3
+    {16, 8, 32, 100 * 1024},  // 4
+    {8, 8, 64, 100 * 1024},   // 5
+    {16, 4, 32, 72 * 1024},   // 6
+};
+constexpr int kNumSched = (int)(sizeof(kSched) / sizeof(kSched[0]));
+
+Sched pick_schedule(int idx, int64_t D) {
+  if (idx > 0 && idx < kNumSched) return kSched[idx];
+  return D >= 2048 ? kSched[3] : kSched[1];
+}
 
 // Largest dynamic shared memory the kernel may request (opt-in limit minus its static shared
 // memory); the attribute is raised to it once per device.
@@ -455,12 +651,12 @@ size_t max_dynamic_smem() {
 template <typename T, int R, bool STRICT>
 int occupancy_for(size_t smem, int threads) {
   static std::mutex mu;
-  static std::map<std::pair<int, size_t>, int> cache;
+  static std::map<std::tuple<int, size_t, int>, int> cache;
   int dev = 0;
   cudaGetDevice(&dev);
   if (smem > max_dynamic_smem<T, R, STRICT>()) return 0;
   std::lock_guard<std::mutex> g(mu);
-  auto key = std::make_pair(dev, smem);
+  auto key = std::make_tuple(dev, smem, threads);
   auto it = cache.find(key);
   if (it != cache.end()) return it->second;
   int occ = 0;
@@ -473,8 +669,8 @@ int occupancy_for(size_t smem, int threads) {
   return occ;
 }
 
-template <typename T, bool STRICT>
-ws_status launch_typed(const FitnessRequest& rq) {
+template <typename T, int R, bool STRICT>
+ws_status launch_typed(const FitnessRequest& rq, const Sched& sc) {
   const FitnessWorkspace lay = fitness_workspace_layout(rq.B, rq.L, rq.dtype);
   unsigned char* wsb = static_cast<unsigned char*>(rq.workspace);
   ProgHdr* hdr = reinterpret_cast<ProgHdr*>(wsb + lay.hdr_off);
@@ -485,22 +681,71 @@ ws_status launch_typed(const FitnessRequest& rq) {
   double* yvar = reinterpret_cast<double*>(wsb + lay.misc_off + 16);
 
   const int L = (int)rq.L;
-  const int Lcap = L > 1 ? L : 1;
+  const int Lcap = tape_capacity(L < 256 ? L : 256);  // tape words per program
   const int S = spill_slots_bound(L);
-  const T* consts = static_cast<const T*>(rq.consts);
+  constexpr int PASS = 32 * R;
+  const int W = sc.W;
+  const int threads = W * 32;
 
-  // 1. compile
+  // ---- schedule: chunk rows RC (multiple of the pass), programs per block, splits ----------
+  const size_t szT = sizeof(T);
+  // programs per block: as the schedule says, but the staged tapes stay within 24 KB (long
+  // programs get fewer per block; at least one per warp)
+  int PBmax = sc.PB;
+  {
+    const int fit = (int)((24 * 1024) / ((size_t)Lcap * sizeof(Instr<T>)));
+    if (PBmax > fit) PBmax = fit > W ? fit : W;
+  }
+  const size_t fixed = (size_t)W * kSharedSlots * PASS * szT +
+                       (size_t)PBmax * Lcap * sizeof(Instr<T>) +
+                       (size_t)PBmax * (sizeof(PartRec) + sizeof(int));
+  const size_t per_row = 2 * (size_t)(rq.V + 1) * szT;  // two tiles (double buffering)
+  const size_t optin = max_dynamic_smem<T, R, STRICT>();
+  if (fixed + per_row * PASS > optin) return fail("too many variables for the shared-memory tile");
+  const size_t budget = sc.smem_budget > fixed + per_row * PASS ? sc.smem_budget
+                                                                : fixed + per_row * PASS;
+  int64_t rc = (int64_t)((budget - fixed) / per_row) / PASS * PASS;
+  const int64_t d_pad = (rq.D + PASS - 1) / PASS * PASS;
+  if (rc > d_pad) rc = d_pad;
+  // tape offsets: variable v at v * (RC / PASS) must fit 9 bits
+  const int64_t xmul_cap = rq.V > 0 ? (int64_t)P_OFF_MASK / rq.V : (int64_t)P_OFF_MASK;
+  if (rc / PASS > xmul_cap) rc = xmul_cap * PASS;
+  if (rc < PASS) rc = PASS;
+  const int RC = (int)rc;
+  const int xmul = RC / PASS;
+  const size_t smem = fixed + per_row * (size_t)RC;
+  const int occ = occupancy_for<T, R, STRICT>(smem, threads);
+  if (occ <= 0) return fail("fitness kernel cannot be resident with this tile size");
+  const int64_t n_ctas = (int64_t)occ * device_info().sm_count;
+
+  const T* consts = static_cast<const T*>(rq.consts);
+  int64_t* perm = reinterpret_cast<int64_t*>(wsb + lay.perm_off);
+  unsigned* bins = reinterpret_cast<unsigned*>(wsb + lay.bins_off);
+  T* gspill = reinterpret_cast<T*>(wsb + lay.gspill_off);
+  const int deep = S > kSharedSlots ? S - kSharedSlots : 0;
+  if ((size_t)n_ctas * W * deep * PASS * szT > lay.gspill_bytes)
+    return fail("workspace too small for the spill scratch of this schedule");
+  // 1. compile, then order the programs by tape length
   if (rq.phase != WS_PHASE_EVALUATE) {
-    const int threads = 128;
-    const unsigned grid = (unsigned)((rq.B + threads - 1) / threads);
+    cudaError_t e0 = cudaMemsetAsync(bins, 0, kSortBins * sizeof(unsigned), rq.stream);
+    if (e0 != cudaSuccess) return fail_cuda(e0, "sort-bin reset");
+    const int ct = 128;
+    const unsigned grid = (unsigned)((rq.B + ct - 1) / ct);
     if (L <= 64)
-      compile_kernel<T, STRICT, 64><<<grid, threads, 0, rq.stream>>>(
-          rq.pop, rq.B, L, consts, (int)rq.K, rq.lut, tape, Lcap, hdr, cnt, misc, S);
+      compile_kernel<T, STRICT, 64><<<grid, ct, 0, rq.stream>>>(
+          rq.pop, rq.B, L, consts, (int)rq.K, rq.lut, tape, Lcap, hdr, cnt, misc, S, xmul);
     else
-      compile_kernel<T, STRICT, 256><<<grid, threads, 0, rq.stream>>>(
-          rq.pop, rq.B, L, consts, (int)rq.K, rq.lut, tape, Lcap, hdr, cnt, misc, S);
+      compile_kernel<T, STRICT, 256><<<grid, ct, 0, rq.stream>>>(
+          rq.pop, rq.B, L, consts, (int)rq.K, rq.lut, tape, Lcap, hdr, cnt, misc, S, xmul);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "compile_kernel launch");
+    int sgrid = (int)((rq.B + 255) / 256);
+    if (sgrid > device_info().sm_count * 8) sgrid = device_info().sm_count * 8;
+    sort_hist_kernel<<<sgrid, 256, 0, rq.stream>>>(hdr, rq.B, bins);
+    sort_scan_kernel<<<1, 32, 0, rq.stream>>>(bins);
+    sort_scatter_kernel<<<sgrid, 256, 0, rq.stream>>>(hdr, rq.B, bins, perm);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "sort kernels launch");
   }
   if (rq.phase == WS_PHASE_COMPILE) return WS_OK;
   if (rq.phase == WS_PHASE_EVALUATE) {  // the compile kernel is what resets the queue head
@@ -513,30 +758,9 @@ ws_status launch_typed(const FitnessRequest& rq) {
     if (e != cudaSuccess) return fail_cuda(e, "yvar_kernel launch");
   }
 
-  // 2. schedule
-  constexpr int R = kR;
-  constexpr int PASS = 32 * R;
-  const int W = kW;
-  const int threads = W * 32;
-  const size_t szT = sizeof(T);
-  const size_t fixed = (size_t)W * S * PASS * szT + (size_t)W * Lcap * sizeof(Instr<T>) +
-                       (size_t)kPBMax * sizeof(PartRec);
-  const size_t per_row = (size_t)(rq.V + 1) * szT;
-  const int64_t d_pad = (rq.D + PASS - 1) / PASS * PASS;
-  int64_t rc_cap = kSmemBudget > fixed + per_row * PASS
-                       ? (int64_t)((kSmemBudget - fixed) / per_row) / PASS * PASS
-                       : PASS;
-  const size_t optin = max_dynamic_smem<T, R, STRICT>();
-  if (fixed + per_row * PASS > optin) return fail("too many variables for the shared-memory tile");
-  int RC = (int)(d_pad < rc_cap ? d_pad : rc_cap);
-  if (RC < PASS) RC = PASS;
-  size_t smem = fixed + per_row * (size_t)RC;
-  const int occ = occupancy_for<T, R, STRICT>(smem, threads);
-  if (occ <= 0) return fail("fitness kernel cannot be resident with this tile size");
-  const int64_t n_ctas = (int64_t)occ * device_info().sm_count;
-
+  // 2. evaluate
   const int64_t n_chunks = (rq.D + RC - 1) / RC;
-  int PB = kPBMax;
+  int PB = PBmax;
   int64_t n_blocks = (rq.B + PB - 1) / PB;
   while (PB > W && n_blocks * n_chunks < 2 * n_ctas) {
     PB >>= 1;
@@ -578,6 +802,14 @@ ws_status launch_typed(const FitnessRequest& rq) {
   P.prog_cnt = cnt;
   P.work = misc;
   P.yvar = yvar;
+  P.perm = perm;
+  P.gspill = gspill;
+  P.count = rq.out_ninv != nullptr ? 1 : 0;
+  {
+    constexpr int64_t VE = 16 / (int64_t)sizeof(T);
+    P.async_stage = (rq.D % VE == 0) && (((uintptr_t)rq.x & 15u) == 0) &&
+                    (((uintptr_t)rq.y & 15u) == 0) ? 1 : 0;
+  }
   const int64_t grid = P.n_items < n_ctas ? P.n_items : n_ctas;
   fitness_kernel<T, R, STRICT><<<(unsigned)grid, threads, smem, rq.stream>>>(P);
   cudaError_t e = cudaGetLastError();
@@ -585,12 +817,26 @@ ws_status launch_typed(const FitnessRequest& rq) {
   return WS_OK;
 }
 
+template <typename T, bool STRICT>
+ws_status launch_sched(const FitnessRequest& rq) {
+  Sched sc = pick_schedule(rq.schedule, rq.D);
+  if constexpr (sizeof(T) == 8) {
+    sc.R = 8;  // 16 doubles per operand array would spill registers
+    return launch_typed<T, 8, STRICT>(rq, sc);
+  } else {
+    if (sc.R == 8) return launch_typed<T, 8, STRICT>(rq, sc);
+    return launch_typed<T, 16, STRICT>(rq, sc);
+  }
+}
+
 }  // namespace
+
+int schedule_count() { return kNumSched; }
 
 FitnessWorkspace fitness_workspace_layout(int64_t B, int64_t L, int dtype) {
   FitnessWorkspace w;
   const size_t instr = dtype == WS_F64 ? sizeof(Instr<double>) : sizeof(Instr<float>);
-  const int64_t Lcap = L > 1 ? L : 1;
+  const int64_t Lcap = tape_capacity(L < 0 ? 0 : (L > 256 ? 256 : (int)L));
   size_t off = 0;
   w.hdr_off = off;
   off = align_up(off + (size_t)B * sizeof(ProgHdr), 256);
@@ -603,14 +849,25 @@ FitnessWorkspace fitness_workspace_layout(int64_t B, int64_t L, int dtype) {
   off = align_up(off + (size_t)B * sizeof(unsigned), 256);
   w.misc_off = off;
   off = align_up(off + 256, 256);
+  w.perm_off = off;
+  off = align_up(off + (size_t)B * sizeof(int64_t), 256);
+  w.bins_off = off;
+  off = align_up(off + kSortBins * sizeof(unsigned), 256);
+  // deep spill slots: up to 64 resident warps per SM, one pass of 512 rows per slot
+  const int Lc = L < 0 ? 0 : (L > 256 ? 256 : (int)L);
+  const int deep = spill_slots_bound(Lc) > kSharedSlots ? spill_slots_bound(Lc) - kSharedSlots : 0;
+  const size_t tsz = dtype == WS_F64 ? sizeof(double) : sizeof(float);
+  w.gspill_bytes = (size_t)device_info().sm_count * 64 * (size_t)deep * 512 * tsz;
+  w.gspill_off = off;
+  off = align_up(off + w.gspill_bytes, 256);
   w.total = off;
   return w;
 }
 
 ws_status launch_fitness(const FitnessRequest& rq) {
   if (rq.dtype == WS_F32)
-    return rq.strict ? launch_typed<float, true>(rq) : launch_typed<float, false>(rq);
-  return rq.strict ? launch_typed<double, true>(rq) : launch_typed<double, false>(rq);
+    return rq.strict ? launch_sched<float, true>(rq) : launch_sched<float, false>(rq);
+  return rq.strict ? launch_sched<double, true>(rq) : launch_sched<double, false>(rq);
 }
 
 }  // namespace ws

@@ -35,7 +35,8 @@ const DeviceInfo& device_info();
 
 // Workspace layout of the fitness evaluator for B programs of L tokens.
 struct FitnessWorkspace {
-  size_t hdr_off, tape_off, part_off, cnt_off, misc_off, total;
+  size_t hdr_off, tape_off, part_off, cnt_off, misc_off, perm_off, bins_off, gspill_off;
+  size_t gspill_bytes, total;
   int64_t max_partials;  // partial records available (B * n_splits must not exceed it)
 };
 FitnessWorkspace fitness_workspace_layout(int64_t B, int64_t L, int dtype);
@@ -60,5 +61,8 @@ struct FitnessRequest {
   cudaStream_t stream;
 };
 ws_status launch_fitness(const FitnessRequest& rq);
+
+// Number of evaluator schedules (index 0 = automatic choice).
+int schedule_count();
 
 }  // namespace ws

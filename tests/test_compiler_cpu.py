@@ -19,7 +19,7 @@ def compile_host(g, prog, consts, strict, dtype=np.float32):
     lib = tl.N.lib()
     m = tl.token_map(g)
     L = len(prog)
-    cap = max(L, 1)
+    cap = max(L, 1)  # one tape word per operator
     ctrl = np.zeros(cap, np.uint32)
     imm = np.zeros(cap, np.float64)
     hdr = np.zeros(4, np.int32)
