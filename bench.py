@@ -293,8 +293,12 @@ def run_ours(args):
     alg_bytes = B * (L + 4 * wl.constants.shape[1] + 4) + 4 * (X.shape[0] + 1) * D + 4 * B
     roof = {"bound": "fp32", "achieved": achieved / 1e12, "peak": fp32_peak / 1e12,
             "unit": "T node-evals/s (1 FP32 lane-op per node-eval)", "frac": achieved / fp32_peak,
-            "traffic": traffic_full, "kernel": "fitness_kernel<float,8,false>",
+            "traffic": traffic_full,
+            "traffic_note": "ncu dram read+write of one launch on 65,536 programs, scaled x16 "
+                            "to the full launch (per-program traffic); profiles/fitness_kernel_c2.md",
+            "kernel": "ws::fitness_kernel<float, 16, 0> (evaluate-only launches)",
             "kernel_ms": statistics.mean(kern_ms),
+            "kernel_share_of_step": statistics.mean(kern_ms) / (1e3 * t_total / args.steps),
             "peak_source": "%d SMs x 128 FP32 lanes x sm_max_mhz %.0f (%s MEASURED_PEAKS.json)"
                            % (sms, f_max, peak_src),
             "hbm": {"algorithmic_bytes_per_launch": int(alg_bytes),
