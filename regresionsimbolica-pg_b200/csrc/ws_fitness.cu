@@ -7,14 +7,16 @@
 //
 //   1. compile_kernel  -- one thread per program: tokens -> accumulator-machine tape
 //                         (ws_compile.cuh), constant slots baked, constants folded.
-//   2. fitness_kernel  -- persistent CTAs pull work items (a block of PB programs x a range of
-//                         row chunks).  Per chunk the CTA stages X[:, rows] and y[rows] in shared
-//                         memory once; its warps then take programs of the block one at a time
-//                         and run the program's tape over the chunk in passes of 32*R rows
-//                         (R rows per lane, 16-byte shared loads, conflict-free), accumulating
-//                         squared errors in FP64.  Per-program partials are combined in a fixed
-//                         order, so results do not depend on the schedule or on what else is in
-//                         the batch (up to FP64 rounding of the sum).
+//   2. sort_*_kernel   -- counting sort of the programs by tape length (longest first).
+//   3. fitness_kernel  -- persistent CTAs pull work items (a block of PB length-sorted programs
+//                         x a range of row chunks).  The block's tapes are staged in shared memory
+//                         once; X[:, rows] and y[rows] of each chunk stream into a second shared
+//                         tile (cp.async) while the current one is evaluated.  Warp w runs programs
+//                         w, w+W, ... of the block (balanced: similar lengths) over the chunk in
+//                         passes of 32*R rows (R rows per lane, 16-byte conflict-free shared
+//                         loads), accumulating squared errors in FP64.  Per-program partials are
+//                         combined in a fixed order, so results do not depend on the schedule or
+//                         on what else is in the batch (up to FP64 rounding of the sum).
 //
 // Per-row values are bit-identical to the reference kernels when this file is compiled with
 // the reference's flags (--use_fast_math): same operator code (ws_ops.cuh), same FP32 rounding
@@ -169,16 +171,6 @@ __device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fm
 __device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
 __device__ __forceinline__ float m_max(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ double m_max(double a, double b) { return fmax(a, b); }
-
-// Runs one program tape over one pass of 32*R rows.  xp: X tile at this pass and lane
-// (variable v at xp + v*RC); sp: this warp's spill slots at this lane.
-// Runs one program tape over one pass of 32*R rows.  xb: the X tile at this pass and lane;
-// sb: this warp's spill slots at this lane.  Tape offsets are in units of one pass.
-template <int R, typename F>
-__device__ __forceinline__ void for_rows(F&& f) {
-#pragma unroll
-  for (int k = 0; k < R; ++k) f(k);
-}
 
 // Runs one program tape over one pass of 32*R rows.  xb: the X tile at this pass and lane;
 // sb / gb: this warp's shared / global spill slots at this lane.  Tape offsets are in units
@@ -716,15 +708,18 @@ ws_status launch_typed(const FitnessRequest& rq, const Sched& sc) {
   const size_t smem = fixed + per_row * (size_t)RC;
   const int occ = occupancy_for<T, R, STRICT>(smem, threads);
   if (occ <= 0) return fail("fitness kernel cannot be resident with this tile size");
-  const int64_t n_ctas = (int64_t)occ * device_info().sm_count;
+  int64_t n_ctas = (int64_t)occ * device_info().sm_count;
 
   const T* consts = static_cast<const T*>(rq.consts);
   int64_t* perm = reinterpret_cast<int64_t*>(wsb + lay.perm_off);
   unsigned* bins = reinterpret_cast<unsigned*>(wsb + lay.bins_off);
   T* gspill = reinterpret_cast<T*>(wsb + lay.gspill_off);
   const int deep = S > kSharedSlots ? S - kSharedSlots : 0;
-  if ((size_t)n_ctas * W * deep * PASS * szT > lay.gspill_bytes)
-    return fail("workspace too small for the spill scratch of this schedule");
+  if (deep > 0) {  // one global spill area per resident warp: cap the persistent grid to it
+    const int64_t fit = (int64_t)(lay.gspill_bytes / ((size_t)W * deep * PASS * szT));
+    if (fit < 1) return fail("workspace too small for the spill scratch of this schedule");
+    if (n_ctas > fit) n_ctas = fit;
+  }
   // 1. compile, then order the programs by tape length
   if (rq.phase != WS_PHASE_EVALUATE) {
     cudaError_t e0 = cudaMemsetAsync(bins, 0, kSortBins * sizeof(unsigned), rq.stream);
@@ -853,11 +848,12 @@ FitnessWorkspace fitness_workspace_layout(int64_t B, int64_t L, int dtype) {
   off = align_up(off + (size_t)B * sizeof(int64_t), 256);
   w.bins_off = off;
   off = align_up(off + kSortBins * sizeof(unsigned), 256);
-  // deep spill slots: up to 64 resident warps per SM, one pass of 512 rows per slot
+  // deep spill slots: 32 resident warps per SM (the schedules run at most that many; the
+  // launcher caps its grid otherwise), one pass of 512 rows per slot
   const int Lc = L < 0 ? 0 : (L > 256 ? 256 : (int)L);
   const int deep = spill_slots_bound(Lc) > kSharedSlots ? spill_slots_bound(Lc) - kSharedSlots : 0;
   const size_t tsz = dtype == WS_F64 ? sizeof(double) : sizeof(float);
-  w.gspill_bytes = (size_t)device_info().sm_count * 64 * (size_t)deep * 512 * tsz;
+  w.gspill_bytes = (size_t)device_info().sm_count * 32 * (size_t)deep * 512 * tsz;
   w.gspill_off = off;
   off = align_up(off + w.gspill_bytes, 256);
   w.total = off;
