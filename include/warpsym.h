@@ -146,6 +146,26 @@ size_t ws_fitness_workspace_bytes(int64_t B, int64_t L, int32_t dtype);
 int32_t ws_schedule_count(void);
 
 /*
+ * ws_eval_fitness without a workspace argument.  No counterpart in the reference.  For callers
+ * that cannot allocate device memory at the point of the call -- e.g. a host runtime reaching
+ * this library through a plain C FFI with only device pointers handed over by another framework,
+ * or a loop that must not call cudaMalloc because it synchronises the device.  The scratch is a
+ * static 64 MiB device array inside the library (held by every GPU that loads it until exit);
+ * requests whose ws_fitness_workspace_bytes(B, L, dtype) exceed ws_static_scratch_bytes() are
+ * rejected with an error.  All calls share the array: calls that overlap on the GPU race and must
+ * be serialised.  The first call on a device looks the array's address up; make it before any
+ * stream capture.  Arguments and results are those of ws_eval_fitness.
+ */
+ws_status ws_eval_fitness_static(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
+                                 const void* x, int64_t num_vars, int64_t D,
+                                 const void* constants, int64_t K, const void* y, void* out_loss,
+                                 int32_t* out_ninvalid, const ws_token_map* ids,
+                                 const ws_fitness_opts* opts, void* stream);
+
+/* Size in bytes of the static scratch used by ws_eval_fitness_static. */
+size_t ws_static_scratch_bytes(void);
+
+/*
  * Host-only introspection (no GPU needed; not an evaluation path).  They expose the pieces
  * the evaluator is built from so that they can be verified exactly on a CPU:
  *   ws_debug_token_lut  -- token byte -> internal class / argument table built from the IDs

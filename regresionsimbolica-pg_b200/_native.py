@@ -72,6 +72,9 @@ _SIGS = {
                                  C.POINTER(TokenMap), _I32, _I32, _P, C.c_size_t, _P]),
     "ws_eval_fitness": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P, _P,
                                C.POINTER(TokenMap), C.POINTER(FitnessOpts), _P, C.c_size_t, _P]),
+    "ws_eval_fitness_static": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
+                                      _P, C.POINTER(TokenMap), C.POINTER(FitnessOpts), _P]),
+    "ws_static_scratch_bytes": (C.c_size_t, []),
     "ws_debug_token_lut": (_I32, [C.POINTER(TokenMap), _I64, _I32, _P, _P]),
     "ws_debug_compile": (_I32, [_I32, _P, _I64, _P, _I64, C.POINTER(TokenMap), _I64, _I32, _I32,
                                 _P, _P, _P]),
