@@ -165,6 +165,90 @@ ws_status ws_eval_fitness_static(int32_t dtype, const uint8_t* population, int64
 /* Size in bytes of the static scratch used by ws_eval_fitness_static. */
 size_t ws_static_scratch_bytes(void);
 
+/* ----------------------------------------------------------------------------------------------
+ * Population structure (integer, bit-exact).  Token arrays are [B, L] row-major; the arity table
+ * is int32 [n_arities] indexed by token value (the reference's `token_arities`).
+ */
+
+/* Which of the reference's three stack-validity rules ws_validate_rpn_batch applies. */
+enum {
+  WS_VALIDATE_KERNEL = 0,  /* validate_rpn_batch_kernel, rpn_kernels.cu:850-900: tokens outside
+                              the table have arity 0; PAD-contiguity; depth >= 1 after every
+                              token; final depth == 1                                          */
+  WS_VALIDATE_CLAMPED = 1, /* GPUOperators._validate_rpn_batch torch path, operators.py:551-570
+                              (and _validate_rpn_batch_custom, :660-676): as KERNEL but the arity
+                              lookup clamps the token into [0, n_arities-1]                     */
+  WS_VALIDATE_STACK = 2    /* GPUSymbolicSimplifier._validate_batch_stack,
+                              gpu_simplifier.py:513-579: no contiguity rule (a PAD is a no-op
+                              anywhere), depth >= 1 at EVERY position, final depth == 1, at least
+                              one non-PAD token; clamped lookup                                 */
+};
+
+/*
+ * Per-program stack validity.  Replaces `validate_rpn_batch(population, token_arities,
+ * out_valid, PAD_ID)` (bindings.cpp:462 -> launch_validate_rpn_batch, rpn_kernels.cu:902-925)
+ * for mode WS_VALIDATE_KERNEL, and the two torch fallbacks above for the other modes.
+ * population: token_bytes 1 (uint8, the kernel's layout) or 8 (int64, the simplifier's layout).
+ * out_valid[B]: 1 = valid, 0 = invalid (a torch.bool buffer).
+ */
+ws_status ws_validate_rpn_batch(const void* population, int32_t token_bytes, int64_t B, int64_t L,
+                                const int32_t* token_arities, int64_t n_arities, int32_t pad_id,
+                                int32_t mode, uint8_t* out_valid, void* stream);
+
+/*
+ * Start of the subtree ending at every position.  Replaces `find_subtree_ranges(population,
+ * token_arities, out_starts, PAD_ID, out_lengths=None)` (bindings.cpp:454 ->
+ * launch_find_subtree_ranges, rpn_kernels.cu:506-537; kernel :433-504).  out_starts int64 [B, L]
+ * (-1 for PAD positions and for operators whose operands are missing), identical to the
+ * reference.  out_lengths int64 [B] (optional): position of the first PAD, else L.  On rows that
+ * contain a PAD gap the reference's threads race on this value (every PAD that follows a
+ * non-PAD, and position L-1 when it is not PAD, store their own candidate); the value written
+ * here is always one of those candidates.
+ */
+ws_status ws_find_subtree_ranges(const uint8_t* population, int64_t B, int64_t L,
+                                 const int32_t* token_arities, int64_t n_arities, int32_t pad_id,
+                                 int64_t* out_starts, int64_t* out_lengths, void* stream);
+
+/*
+ * Subtree starts by the simplifier's forward recurrence.  Replaces
+ * `precompute_subtree_starts(population, arities, out_starts)` (bindings.cpp:506 ->
+ * launch_precompute_subtree_starts, simplify_kernels.cu:715-737; kernel :612-661).
+ * population int64 [B, L]; PAD is token 0; positions >= 256 are -1 (the reference's
+ * MAX_FORMULA_LEN).
+ */
+ws_status ws_precompute_subtree_starts(const int64_t* population, int64_t B, int64_t L,
+                                       const int32_t* arities, int64_t n_arities,
+                                       int64_t* out_starts, void* stream);
+
+/*
+ * Tournament selection.  Replaces `tournament_selection(fitness, errors, rand_idx, rand_cases,
+ * selected_idx, lengths, mad_eps=empty)` (bindings.cpp:468 -> launch_tournament_selection,
+ * rpn_kernels.cu:1670-1715; kernel :1535-1601).  fitness f32 [B]; errors f32 [B, n_data] or
+ * NULL; rand_idx int64 [B, tour_size] (global candidate indices); rand_cases int32 [B] or NULL
+ * (lexicase case per slot, < 0 = none); lengths f32 [B] or NULL (parsimony tie-break);
+ * mad_eps f32 [n_data] or NULL.  selected_idx int64 [B].  The winner is the first candidate with
+ * a strictly smaller value; with lengths, a candidate within epsilon (mad_eps[case], else 1e-3
+ * with a case, else 1e-9) that is shorter also wins.  Candidate indices are not range-checked
+ * (as in the reference).
+ */
+ws_status ws_tournament_select(const float* fitness, int64_t B, const float* errors,
+                               int64_t n_data, const int64_t* rand_idx, int64_t tour_size,
+                               const int32_t* rand_cases, const float* lengths,
+                               const float* mad_eps, int64_t* selected_idx, void* stream);
+
+/*
+ * Island tournament on int32 offsets: candidate = base + (offset % span), clamped into [0, B-1],
+ * where base/span are the island of the slot when n_islands > 1 (span = island_size, the last
+ * island truncated), else the whole population.  Replaces launch_tournament_selection_offsets
+ * (rpn_kernels.cu:1717-1760; kernel :1603-1668), the selection step of evolve_generation.
+ */
+ws_status ws_tournament_select_offsets(const float* fitness, int64_t B, const float* errors,
+                                       int64_t n_data, const int32_t* rand_offsets,
+                                       int64_t tour_size, const int32_t* rand_cases,
+                                       const float* lengths, const float* mad_eps,
+                                       int32_t island_size, int32_t n_islands,
+                                       int64_t* selected_idx, void* stream);
+
 /*
  * Host-only introspection (no GPU needed; not an evaluation path).  They expose the pieces
  * the evaluator is built from so that they can be verified exactly on a CPU:

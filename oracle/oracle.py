@@ -6,6 +6,7 @@ Used by tests/ (as the checker), by __graft_entry__.smoke() and by bench.py's CP
 from __future__ import annotations
 
 import ctypes as C
+import glob
 import os
 import subprocess
 
@@ -19,10 +20,10 @@ _lib = None
 
 
 def _build_if_missing():
-    if not os.path.exists(LIB):
+    srcs = sorted(glob.glob(os.path.join(HERE, "*.cpp")))
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(p) for p in srcs):
         subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared",
-                        "-ffp-contract=off", "-fno-fast-math", os.path.join(HERE, "ws_oracle.cpp"),
-                        "-o", LIB], check=True)
+                        "-ffp-contract=off", "-fno-fast-math"] + srcs + ["-o", LIB], check=True)
 
 
 def lib():
@@ -41,6 +42,15 @@ def lib():
                 _P, C.c_int64, C.c_int64, _P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P, C.c_int,
                 C.c_int, C.c_int, C.c_double, _P, _P, C.c_int]
         h.ws_oracle_threads.restype = C.c_int
+        h.ws_oracle_validate.argtypes = [_P, C.c_int32, C.c_int64, C.c_int64, _P, C.c_int64,
+                                         C.c_int32, C.c_int32, _P]
+        h.ws_oracle_subtree_ranges.argtypes = [_P, C.c_int64, C.c_int64, _P, C.c_int64,
+                                               C.c_int32, _P, _P]
+        h.ws_oracle_subtree_length_candidates.argtypes = [_P, C.c_int64, C.c_int64, C.c_int32,
+                                                          _P]
+        h.ws_oracle_subtree_starts.argtypes = [_P, C.c_int64, C.c_int64, _P, C.c_int64, _P]
+        h.ws_oracle_tournament.argtypes = [_P, C.c_int64, _P, C.c_int64, _P, _P, C.c_int64, _P,
+                                           _P, _P, C.c_int32, C.c_int32, _P]
         _lib = h
     return _lib
 
@@ -112,3 +122,71 @@ def fitness(tmap, pop, X, consts, y, strict=0, policy="fused", loss="rmse", inva
         _p(pop), B, L, _p(X), V, D, _p(c), K, _p(y), C.byref(tmap), int(strict), POLICY[policy],
         LOSS[loss], float(invalid_value), _p(out), _p(ninv), int(nthreads or threads()))
     return (out, ninv) if with_ninv else out
+
+
+# ---------------------------------------------------------------------------------------------
+# Population structure (oracle/ws_oracle_structure.cpp).
+
+VALIDATE_MODES = {"kernel": 0, "clamped": 1, "stack": 2}
+
+
+def validate(pop, arities, pad_id=0, mode="kernel"):
+    """bool [B] under the reference rule `mode` (kernel / clamped / stack)."""
+    pop = np.ascontiguousarray(pop)
+    assert pop.dtype in (np.uint8, np.int64)
+    ar = np.ascontiguousarray(arities, dtype=np.int32)
+    B, L = pop.shape
+    out = np.empty(B, dtype=np.uint8)
+    lib().ws_oracle_validate(_p(pop), pop.itemsize, B, L, _p(ar), ar.size, int(pad_id),
+                             VALIDATE_MODES[mode], _p(out))
+    return out.astype(bool)
+
+
+def subtree_ranges(pop, arities, pad_id=0):
+    """(starts int64 [B, L], lengths int64 [B]) by find_subtree_ranges_kernel's backward scan."""
+    pop = np.ascontiguousarray(pop, dtype=np.uint8)
+    ar = np.ascontiguousarray(arities, dtype=np.int32)
+    B, L = pop.shape
+    starts = np.empty((B, L), dtype=np.int64)
+    lengths = np.empty(B, dtype=np.int64)
+    lib().ws_oracle_subtree_ranges(_p(pop), B, L, _p(ar), ar.size, int(pad_id), _p(starts),
+                                   _p(lengths))
+    return starts, lengths
+
+
+def subtree_length_candidates(pop, pad_id=0):
+    """bool [B, L+1]: the values the reference's racing out_lengths stores may leave."""
+    pop = np.ascontiguousarray(pop, dtype=np.uint8)
+    B, L = pop.shape
+    cand = np.empty((B, L + 1), dtype=np.uint8)
+    lib().ws_oracle_subtree_length_candidates(_p(pop), B, L, int(pad_id), _p(cand))
+    return cand.astype(bool)
+
+
+def subtree_starts(pop, arities):
+    """int64 [B, L] by precompute_subtree_starts_kernel's forward recurrence."""
+    pop = np.ascontiguousarray(pop, dtype=np.int64)
+    ar = np.ascontiguousarray(arities, dtype=np.int32)
+    B, L = pop.shape
+    out = np.empty((B, L), dtype=np.int64)
+    lib().ws_oracle_subtree_starts(_p(pop), B, L, _p(ar), ar.size, _p(out))
+    return out
+
+
+def tournament(fitness, cand, errors=None, cases=None, lengths=None, mad_eps=None,
+               island_size=0, n_islands=1):
+    """int64 [B] winners; cand int64 [B, T] indices, or int32 [B, T] island offsets."""
+    fit = np.ascontiguousarray(fitness, dtype=np.float32)
+    cand = np.ascontiguousarray(cand)
+    B, T = cand.shape
+    f32 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float32)  # noqa: E731
+    errors, lengths, mad_eps = f32(errors), f32(lengths), f32(mad_eps)
+    cases = None if cases is None else np.ascontiguousarray(cases, dtype=np.int32)
+    n_data = errors.shape[1] if errors is not None else 0
+    out = np.empty(B, dtype=np.int64)
+    idx = cand if cand.dtype == np.int64 else None
+    off = cand if cand.dtype == np.int32 else None
+    assert idx is not None or off is not None
+    lib().ws_oracle_tournament(_p(fit), B, _p(errors), n_data, _p(idx), _p(off), T, _p(cases),
+                               _p(lengths), _p(mad_eps), int(island_size), int(n_islands), _p(out))
+    return out

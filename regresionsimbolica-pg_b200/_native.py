@@ -16,6 +16,7 @@ WS_OK = 0
 WS_F32, WS_F64 = 0, 1
 WS_POLICY_FUSED, WS_POLICY_CLASSIC = 0, 1
 WS_LOSS_RMSE, WS_LOSS_MSE, WS_LOSS_R2, WS_LOSS_SSE = 0, 1, 2, 3
+WS_VALIDATE_KERNEL, WS_VALIDATE_CLAMPED, WS_VALIDATE_STACK = 0, 1, 2
 
 
 class TokenMap(C.Structure):
@@ -75,6 +76,12 @@ _SIGS = {
     "ws_eval_fitness_static": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
                                       _P, C.POINTER(TokenMap), C.POINTER(FitnessOpts), _P]),
     "ws_static_scratch_bytes": (C.c_size_t, []),
+    "ws_validate_rpn_batch": (_I32, [_P, _I32, _I64, _I64, _P, _I64, _I32, _I32, _P, _P]),
+    "ws_find_subtree_ranges": (_I32, [_P, _I64, _I64, _P, _I64, _I32, _P, _P, _P]),
+    "ws_precompute_subtree_starts": (_I32, [_P, _I64, _I64, _P, _I64, _P, _P]),
+    "ws_tournament_select": (_I32, [_P, _I64, _P, _I64, _P, _I64, _P, _P, _P, _P, _P]),
+    "ws_tournament_select_offsets": (_I32, [_P, _I64, _P, _I64, _P, _I64, _P, _P, _P, _I32, _I32,
+                                            _P, _P]),
     "ws_debug_token_lut": (_I32, [C.POINTER(TokenMap), _I64, _I32, _P, _P]),
     "ws_debug_compile": (_I32, [_I32, _P, _I64, _P, _I64, C.POINTER(TokenMap), _I64, _I32, _I32,
                                 _P, _P, _P]),

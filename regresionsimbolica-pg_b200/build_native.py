@@ -67,11 +67,11 @@ def build_native(verbose: bool = False, jobs: int = 8) -> str:
 
 def build_oracle() -> str:
     """Compiles the CPU oracle (test infrastructure) into oracle/libws_oracle.so."""
-    src = os.path.join(ORACLE_DIR, "ws_oracle.cpp")
-    deps = [src, os.path.join(REPO_DIR, "include", "warpsym.h")]
+    srcs = sorted(glob.glob(os.path.join(ORACLE_DIR, "*.cpp")))
+    deps = srcs + [os.path.join(REPO_DIR, "include", "warpsym.h")]
     if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < _newest(deps):
         _run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off",
-              "-fno-fast-math", src, "-o", ORACLE_LIB])
+              "-fno-fast-math"] + srcs + ["-o", ORACLE_LIB])
     return ORACLE_LIB
 
 

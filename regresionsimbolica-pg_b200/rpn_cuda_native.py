@@ -132,3 +132,87 @@ def eval_rpn_fused(population, x, constants, y_target, out_rmse,
                                   ptr(constants) if K > 0 else None, K, ptr(y_target),
                                   ptr(out_rmse), C.byref(m), int(strict_mode), int(launch_mode),
                                   ptr(ws), nbytes, stream_of(x)))
+
+
+def _optional(t):
+    """The reference treats an empty tensor (numel() == 0) as "not given"."""
+    return None if t is None or (isinstance(t, torch.Tensor) and t.numel() == 0) else t
+
+
+def _expect(t, name, dtype):
+    if t.dtype != dtype:
+        raise RuntimeError("%s: expected scalar type %s but found %s" % (name, dtype, t.dtype))
+
+
+def validate_rpn_batch(population, token_arities, out_valid, PAD_ID):
+    """Stack validity per program (bindings.cpp:462 -> rpn_kernels.cu:850-925): out_valid [B]
+    (torch.bool) written in place."""
+    for t, nm in ((population, "population"), (token_arities, "token_arities"),
+                  (out_valid, "out_valid")):
+        check_cuda(t, nm)
+    _expect(population, "population", torch.uint8)
+    _expect(token_arities, "token_arities", torch.int32)
+    _expect(out_valid, "out_valid", torch.bool)
+    B, L = int(population.size(0)), int(population.size(1))
+    N.check(N.lib().ws_validate_rpn_batch(ptr(population), 1, B, L, ptr(token_arities),
+                                          int(token_arities.size(0)), int(PAD_ID),
+                                          N.WS_VALIDATE_KERNEL, ptr(out_valid),
+                                          stream_of(population)))
+
+
+def find_subtree_ranges(population, token_arities, out_starts, PAD_ID, out_lengths=None):
+    """Subtree start of every position (bindings.cpp:454 -> rpn_kernels.cu:433-537):
+    out_starts [B, L] int64 and, when given, out_lengths [B] int64 written in place."""
+    for t, nm in ((population, "population"), (token_arities, "token_arities"),
+                  (out_starts, "out_starts")):
+        check_cuda(t, nm)
+    out_lengths = _optional(out_lengths)
+    if out_lengths is not None:
+        check_cuda(out_lengths, "out_lengths")
+        _expect(out_lengths, "out_lengths", torch.int64)
+    _expect(population, "population", torch.uint8)
+    _expect(token_arities, "token_arities", torch.int32)
+    _expect(out_starts, "out_starts", torch.int64)
+    B, L = int(population.size(0)), int(population.size(1))
+    N.check(N.lib().ws_find_subtree_ranges(ptr(population), B, L, ptr(token_arities),
+                                           int(token_arities.size(0)), int(PAD_ID),
+                                           ptr(out_starts), ptr(out_lengths),
+                                           stream_of(population)))
+
+
+def precompute_subtree_starts(population, arities, out_starts):
+    """Subtree starts by the simplifier's recurrence (bindings.cpp:506 ->
+    simplify_kernels.cu:612-737): population int64 [B, L], out_starts int64 [B, L]."""
+    for t, nm in ((population, "population"), (arities, "arities"), (out_starts, "out_starts")):
+        check_cuda(t, nm)
+    _expect(population, "population", torch.int64)
+    _expect(arities, "arities", torch.int32)
+    _expect(out_starts, "out_starts", torch.int64)
+    B, L = int(population.size(0)), int(population.size(1))
+    N.check(N.lib().ws_precompute_subtree_starts(ptr(population), B, L, ptr(arities),
+                                                 int(arities.size(0)), ptr(out_starts),
+                                                 stream_of(population)))
+
+
+def tournament_selection(fitness, errors, rand_idx, rand_cases, selected_idx, lengths,
+                         mad_eps=None):
+    """Tournament winners (bindings.cpp:468 -> rpn_kernels.cu:1535-1715): selected_idx [B] int64
+    written in place.  errors / rand_cases / lengths / mad_eps may be empty tensors."""
+    for t, nm in ((fitness, "fitness"), (rand_idx, "rand_idx"), (selected_idx, "selected_idx")):
+        check_cuda(t, nm)
+    errors, rand_cases = _optional(errors), _optional(rand_cases)
+    lengths, mad_eps = _optional(lengths), _optional(mad_eps)
+    for t, nm, dt in ((errors, "errors", torch.float32), (rand_cases, "rand_cases", torch.int32),
+                      (lengths, "lengths", torch.float32), (mad_eps, "mad_eps", torch.float32)):
+        if t is not None:
+            check_cuda(t, nm)
+            _expect(t, nm, dt)
+    _expect(fitness, "fitness", torch.float32)
+    _expect(rand_idx, "rand_idx", torch.int64)
+    _expect(selected_idx, "selected_idx", torch.int64)
+    B = int(fitness.size(0))
+    T = int(rand_idx.size(1))
+    n_data = int(errors.size(1)) if errors is not None else 0
+    N.check(N.lib().ws_tournament_select(ptr(fitness), B, ptr(errors), n_data, ptr(rand_idx), T,
+                                         ptr(rand_cases), ptr(lengths), ptr(mad_eps),
+                                         ptr(selected_idx), stream_of(fitness)))

@@ -16,6 +16,7 @@ import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
+sys.path.insert(0, HERE)
 import refext  # noqa: E402
 import ws_testlib as tl  # noqa: E402
 
@@ -54,6 +55,56 @@ def fused_case(ref, variant, dev, out_dir):
                         rmse=out.cpu().numpy())
 
 
+def structure_case(ref, dev, out_dir):
+    """Integer kernels: validate_rpn_batch, find_subtree_ranges, precompute_subtree_starts,
+    tournament_selection (identical in both builds: no floating-point arithmetic on the path
+    except tournament comparisons, which are exact)."""
+    from make_structure_golden import random_rows
+    rng = np.random.default_rng(4242)
+    g = tl.GPUGrammar(num_variables=3, operators=tl.ALL_OPERATORS)
+    ar = np.zeros(g.vocab_size + 1, dtype=np.int32)
+    ar[:g.vocab_size] = g.arities()
+    rows = random_rows(rng, ar, 3000, 40, 0)
+    pop_u8 = torch.from_numpy(rows.astype(np.uint8)).to(dev)
+    ar_t = torch.from_numpy(ar).to(dev)
+    valid = torch.empty(len(rows), dtype=torch.bool, device=dev)
+    ref.validate_rpn_batch(pop_u8, ar_t, valid, 0)
+    starts = torch.empty(rows.shape, dtype=torch.int64, device=dev)
+    lengths = torch.empty(len(rows), dtype=torch.int64, device=dev)
+    ref.find_subtree_ranges(pop_u8, ar_t, starts, 0, lengths)
+    pre = torch.empty(rows.shape, dtype=torch.int64, device=dev)
+    ref.precompute_subtree_starts(torch.from_numpy(rows).to(dev), ar_t, pre)
+    B, T, n_data = 2048, 5, 37
+    fit = rng.standard_normal(B).astype(np.float32) ** 2
+    fit[::50] = fit[1]
+    errs = np.abs(rng.standard_normal((B, n_data))).astype(np.float32)
+    errs[:, 3] = np.round(errs[:, 3], 1)  # many near-ties on one case
+    cand = rng.integers(0, B, size=(B, T)).astype(np.int64)
+    cases = rng.integers(-1, n_data, size=B).astype(np.int32)
+    lens = rng.integers(3, 40, size=B).astype(np.float32)
+    mad = (rng.random(n_data) * 0.2).astype(np.float32)
+
+    def T_(a):
+        return torch.from_numpy(a).to(dev)
+
+    e0 = torch.empty(0, dtype=torch.float32, device=dev)
+    i0 = torch.empty(0, dtype=torch.int32, device=dev)
+    sel = {}
+    for name, (errors, rc, ln, me) in (
+            ("plain", (e0, i0, e0, e0)), ("lengths", (e0, i0, T_(lens), e0)),
+            ("cases", (T_(errs), T_(cases), e0, e0)),
+            ("cases_lengths", (T_(errs), T_(cases), T_(lens), e0)),
+            ("cases_lengths_mad", (T_(errs), T_(cases), T_(lens), T_(mad)))):
+        out = torch.empty(B, dtype=torch.int64, device=dev)
+        ref.tournament_selection(T_(fit), errors, T_(cand), rc, out, ln, me)
+        sel["sel_" + name] = out.cpu().numpy()
+    np.savez_compressed(os.path.join(out_dir, "ref_structure.npz"),
+                        population=rows.astype(np.uint8), arities=ar, valid=valid.cpu().numpy(),
+                        starts=starts.cpu().numpy(), lengths=lengths.cpu().numpy(),
+                        pre_starts=pre.cpu().numpy(), fitness=fit, errors=errs, cand=cand,
+                        cases=cases, lens=lens, mad_eps=mad, **sel)
+
+
 def main():
     """One process per build variant: both builds export the same symbols, so loading them into
     one process would let the first one's kernels answer for the second."""
@@ -66,6 +117,8 @@ def main():
         for strict in (0, 1):
             rows_case(ref, variant, strict, dev, out_dir)
         fused_case(ref, variant, dev, out_dir)
+        if variant == "fastmath":
+            structure_case(ref, dev, out_dir)
         print("recorded", variant)
         return
     import subprocess
