@@ -165,6 +165,21 @@ ws_status ws_eval_fitness_static(int32_t dtype, const uint8_t* population, int64
 /* Size in bytes of the static scratch used by ws_eval_fitness_static. */
 size_t ws_static_scratch_bytes(void);
 
+/*
+ * Adjoint gradient of program outputs with respect to their constants.  Replaces
+ * `eval_rpn_backward` (bindings.cpp:511 -> run_rpn_backward_cuda, bindings.cpp:108-140 ->
+ * launch_rpn_backward, backward_kernels.cu:286-335; kernel :13-281).
+ *   grad_constants[b, k] += sum over rows d of grad_output[b, d] * d pred[b, d] / d C_k
+ * with the reference's forward and adjoint rules (see ws_backward.cu); the caller zeroes
+ * grad_constants first, as RPNBackwardFunction does (optimization.py:57).  grad_output [B, D] and
+ * grad_constants [B, K] have `dtype`.  L <= 256 (the reference's tapes hold 64 tokens; longer
+ * programs follow the same rules).  Programs whose final stack depth is not 1 contribute nothing.
+ */
+ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
+                               const void* x, int64_t num_vars, int64_t D, const void* constants,
+                               int64_t K, const void* grad_output, void* grad_constants,
+                               const ws_token_map* ids, void* stream);
+
 /* ----------------------------------------------------------------------------------------------
  * Population structure (integer, bit-exact).  Token arrays are [B, L] row-major; the arity table
  * is int32 [n_arities] indexed by token value (the reference's `token_arities`).

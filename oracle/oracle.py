@@ -42,6 +42,10 @@ def lib():
                 _P, C.c_int64, C.c_int64, _P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P, C.c_int,
                 C.c_int, C.c_int, C.c_double, _P, _P, C.c_int]
         h.ws_oracle_threads.restype = C.c_int
+        for suf in ("f32", "f64"):
+            getattr(h, "ws_oracle_backward_" + suf).argtypes = [
+                _P, C.c_int64, C.c_int64, _P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P, _P,
+                _P]
         h.ws_oracle_validate.argtypes = [_P, C.c_int32, C.c_int64, C.c_int64, _P, C.c_int64,
                                          C.c_int32, C.c_int32, _P]
         h.ws_oracle_subtree_ranges.argtypes = [_P, C.c_int64, C.c_int64, _P, C.c_int64,
@@ -122,6 +126,22 @@ def fitness(tmap, pop, X, consts, y, strict=0, policy="fused", loss="rmse", inva
         _p(pop), B, L, _p(X), V, D, _p(c), K, _p(y), C.byref(tmap), int(strict), POLICY[policy],
         LOSS[loss], float(invalid_value), _p(out), _p(ninv), int(nthreads or threads()))
     return (out, ninv) if with_ninv else out
+
+
+def backward(tmap, pop, X, consts, gout):
+    """eval_rpn_backward semantics: (grad [B, K] float64, sum of |terms| [B, K])."""
+    pop = np.ascontiguousarray(pop, dtype=np.uint8)
+    X = np.ascontiguousarray(X)
+    B, L = pop.shape
+    V, D = X.shape
+    c = np.ascontiguousarray(consts, dtype=X.dtype)
+    K = c.shape[1]
+    g = np.ascontiguousarray(gout, dtype=X.dtype).reshape(B, D)
+    grad = np.empty((B, K), dtype=np.float64)
+    absg = np.empty((B, K), dtype=np.float64)
+    getattr(lib(), "ws_oracle_backward_" + _suffix(X.dtype))(
+        _p(pop), B, L, _p(X), V, D, _p(c), K, _p(g), C.byref(tmap), _p(grad), _p(absg))
+    return grad, absg
 
 
 # ---------------------------------------------------------------------------------------------

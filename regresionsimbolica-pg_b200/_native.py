@@ -76,6 +76,8 @@ _SIGS = {
     "ws_eval_fitness_static": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
                                       _P, C.POINTER(TokenMap), C.POINTER(FitnessOpts), _P]),
     "ws_static_scratch_bytes": (C.c_size_t, []),
+    "ws_eval_rpn_backward": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
+                                    C.POINTER(TokenMap), _P]),
     "ws_validate_rpn_batch": (_I32, [_P, _I32, _I64, _I64, _P, _I64, _I32, _I32, _P, _P]),
     "ws_find_subtree_ranges": (_I32, [_P, _I64, _I64, _P, _I64, _I32, _P, _P, _P]),
     "ws_precompute_subtree_starts": (_I32, [_P, _I64, _I64, _P, _I64, _P, _P]),

@@ -1,0 +1,438 @@
+// ws_backward.cu -- adjoint (reverse-mode) gradient of program outputs w.r.t. their constants.
+//
+// Replaces rpn_eval_backward_kernel / launch_rpn_backward (backward_kernels.cu:13-335) behind
+// `eval_rpn_backward`: for every program b and constant slot k,
+//     grad_constants[b, k] += sum_d  dL/dpred[b, d] * dpred[b, d] / dC_k
+// with the reference's own forward rules (its simplified protected operators, the 32-entry
+// index stack, C-slot clamping, unknown tokens acting as unary zero) and its adjoint rules
+// (no gradient through %, tan, abs and the remaining unary operators; guarded div/log/sqrt/pow).
+// Per-row arithmetic follows the reference expression by expression, including its mixed
+// float/double promotions, so per-row adjoints are the reference's bit for bit.
+//
+// B200 layout: one block owns one program for a range of rows.  The program is parsed once per
+// block into a shared-memory plan (operand positions and constant slots), then every thread
+// evaluates rows: forward values and adjoints live in shared memory as [position][thread]
+// (all lanes touch the same position at the same time: conflict-free), and constant adjoints
+// are summed per thread in FP64 accumulators.  The reduction over rows is a fixed-order block
+// sum, written without atomics when one block covers all rows of a program; only programs
+// split across blocks use one atomic per (block, slot) -- the reference issues one atomic per
+// (row, constant node).
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+
+#include "ws_internal.h"
+
+namespace ws {
+namespace {
+
+enum : uint8_t { BK_PAD = 0, BK_VAR, BK_LIT, BK_CONST, BK_BIN, BK_UN };
+// forward operator codes (reference comparison order, backward_kernels.cu:135-188)
+enum : uint8_t { FO_NONE = 0, FO_ADD, FO_SUB, FO_MUL, FO_DIV, FO_POW, FO_MOD,
+                 FO_SIN, FO_COS, FO_TAN, FO_LOG, FO_EXP, FO_SQRT, FO_ABS, FO_NEG };
+// adjoint operator codes (backward_kernels.cu:222-278)
+enum : uint8_t { BO_NONE = 0, BO_ADD, BO_SUB, BO_MUL, BO_DIV, BO_POW,
+                 BO_SIN, BO_COS, BO_LOG, BO_EXP, BO_SQRT, BO_NEG };
+
+struct BwdLut {
+  uint8_t kind[256], arg[256], fop[256], bop[256];
+  double lit[10];
+};
+
+struct BNode {
+  uint8_t kind, fop, bop, pad;
+  uint16_t a;  // left operand position / variable / literal index / constant slot
+  uint16_t r;  // right operand position (binary)
+};
+
+constexpr int kMaxL = 256;
+
+__host__ __device__ constexpr size_t al16(size_t v) { return (v + 15) / 16 * 16; }
+constexpr int kStack = 32;  // STACK_SIZE, backward_kernels.cu:6
+
+template <typename T>
+struct BwdParams {
+  const uint8_t* pop;
+  int64_t B, L;
+  const T* x;
+  int64_t D;
+  const T* consts;
+  int64_t K;
+  const T* gout;
+  T* grad;
+  int64_t n_splits, rows_per_split, n_items;
+  int tape_stride;  // threads per block (row dimension of the tapes)
+};
+
+// Parses program b into the block's plan, as the reference's forward loop walks it
+// (backward_kernels.cu:84-195).  Returns the number of plan entries (root position + 1), or 0
+// when the reference would return early (no root, or final stack depth != 1).
+__device__ int parse_program(const uint8_t* __restrict__ prog, int64_t L, int64_t K,
+                             const uint8_t* s_tab, BNode* plan) {
+  const uint8_t* t_kind = s_tab;
+  const uint8_t* t_fop = s_tab + 256;
+  const uint8_t* t_bop = s_tab + 512;
+  const uint8_t* t_arg = s_tab + 768;
+  int stk[kStack];
+  int sp = 0, root = -1;
+  int64_t c_idx = 0;
+  for (int pc = 0; pc < (int)L; ++pc) {
+    const int tok = prog[pc];
+    const uint8_t kind = t_kind[tok];
+    if (kind == BK_PAD) break;
+    BNode n;
+    n.kind = kind;
+    n.fop = t_fop[tok];
+    n.bop = t_bop[tok];
+    n.pad = 0;
+    n.a = t_arg[tok];
+    n.r = 0xFFFF;
+    if (kind == BK_VAR || kind == BK_LIT || kind == BK_CONST) {
+      if (kind == BK_CONST) {
+        if (K > 0) {
+          n.a = (uint16_t)(c_idx < K ? c_idx : K - 1);
+          c_idx++;
+        } else {
+          n.kind = BK_LIT;  // C without constants pushes 1.0 and takes no gradient
+          n.a = 10;
+        }
+      }
+      plan[pc] = n;
+      if (sp < kStack) stk[sp++] = pc;
+      root = pc;
+      continue;
+    }
+    if (kind == BK_BIN) {
+      if (sp < 2) break;
+      n.r = (uint16_t)stk[--sp];
+      n.a = (uint16_t)stk[--sp];
+    } else {
+      if (sp < 1) break;
+      n.a = (uint16_t)stk[--sp];
+    }
+    plan[pc] = n;
+    stk[sp++] = pc;
+    root = pc;
+  }
+  return (root >= 0 && sp == 1) ? root + 1 : 0;
+}
+
+// ---- forward values (backward_kernels.cu:146-188) ------------------------------------------
+template <typename T>
+__device__ __forceinline__ T fwd_binary(uint8_t op, T op1, T op2) {
+  const T tiny = (T)1e-9;
+  switch (op) {
+    case FO_ADD: return op1 + op2;
+    case FO_SUB: return op1 - op2;
+    case FO_MUL: return op1 * op2;
+    case FO_DIV: return (fabs(op2) < tiny) ? op1 : op1 / op2;
+    case FO_POW: {
+      if (op1 < 0) {
+        const T ib = round(op2);
+        if (fabs(op2 - ib) <= (T)1e-3) op2 = ib;
+        else op1 = fabs(op1);
+      }
+      return pow(op1, op2);
+    }
+    case FO_MOD: return (fabs(op2) < tiny) ? (T)0 : fmod(op1, op2);
+    default: return (T)0;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T fwd_unary(uint8_t op, T op1) {
+  switch (op) {
+    case FO_SIN: return sin(op1);
+    case FO_COS: return cos(op1);
+    case FO_TAN: return tan(op1);
+    case FO_LOG: return log(fabs(op1) + (T)1e-9);
+    case FO_EXP: {
+      T cl = op1;
+      if (cl < -80.0) cl = (T)-80.0;
+      if (cl > 80.0) cl = (T)80.0;
+      return exp(cl);
+    }
+    case FO_SQRT: return sqrt(fabs(op1));
+    case FO_ABS: return fabs(op1);
+    case FO_NEG: return -op1;
+    default: return (T)0;  // operators without a forward rule here evaluate to 0
+  }
+}
+
+// ---- adjoint rules (backward_kernels.cu:222-278) -------------------------------------------
+// The reference writes e.g. `adj_tape[l] += (1.0 / r_val) * adj`: for float that expression is
+// evaluated in double (a double constant promotes it) and the multiply-add contracts into one
+// fused operation before the store rounds back to float.  acc_d / acc_t spell those two shapes.
+template <typename T>
+__device__ __forceinline__ void acc_d(T& dst, double coef, T adj) {
+  dst = (T)fma(coef, (double)adj, (double)dst);
+}
+template <typename T>
+__device__ __forceinline__ void acc_t(T& dst, T coef, T adj) {
+  dst = fma(coef, adj, dst);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) backward_kernel(BwdParams<T> p, BwdLut lut) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int TS = p.tape_stride;
+  BNode* plan = reinterpret_cast<BNode*>(smem);
+  double* cacc = reinterpret_cast<double*>(smem + al16((size_t)kMaxL * sizeof(BNode)));
+  int* touched = reinterpret_cast<int*>(cacc + (size_t)p.K * TS);
+  T* val = reinterpret_cast<T*>(
+      reinterpret_cast<unsigned char*>(touched) + al16((size_t)p.K * sizeof(int)));
+  T* adj = val + (size_t)p.L * TS;
+  __shared__ int s_n;
+  __shared__ int64_t s_prog;
+  __shared__ T s_lit[10];
+  __shared__ uint8_t s_tab[1024];  // kind, forward op, adjoint op, argument per token byte
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) {
+    s_tab[t] = lut.kind[t];
+    s_tab[256 + t] = lut.fop[t];
+    s_tab[512 + t] = lut.bop[t];
+    s_tab[768 + t] = lut.arg[t];
+  }
+  if (threadIdx.x < 10) s_lit[threadIdx.x] = (T)lut.lit[threadIdx.x];
+  if (threadIdx.x == 0) s_prog = -1;
+  const int tid = threadIdx.x;
+
+  for (int64_t item = blockIdx.x; item < p.n_items; item += gridDim.x) {
+    const int64_t b = item / p.n_splits;
+    const int64_t split = item - b * p.n_splits;
+    __syncthreads();
+    if (tid == 0 && s_prog != b) {
+      s_n = parse_program(p.pop + b * p.L, p.L, p.K, s_tab, plan);
+      s_prog = b;
+    }
+    for (int64_t k = tid; k < p.K; k += blockDim.x) touched[k] = 0;
+    for (int64_t k = 0; k < p.K; ++k) cacc[k * TS + tid] = 0.0;
+    __syncthreads();
+    const int n = s_n;
+    if (n == 0) continue;
+
+    const int64_t d_begin = split * p.rows_per_split;
+    int64_t d_end = d_begin + p.rows_per_split;
+    if (d_end > p.D) d_end = p.D;
+    const T* xcol = p.x;
+    const T* cst = p.consts + b * p.K;
+    for (int64_t d = d_begin + tid; d < d_end; d += blockDim.x) {
+      // forward
+      for (int pc = 0; pc < n; ++pc) {
+        const BNode nd = plan[pc];
+        T v;
+        switch (nd.kind) {
+          case BK_VAR: v = xcol[(int64_t)nd.a * p.D + d]; break;
+          case BK_LIT: v = nd.a < 10 ? s_lit[nd.a] : (T)1.0; break;
+          case BK_CONST: v = cst[nd.a]; break;
+          case BK_BIN: v = fwd_binary<T>(nd.fop, val[(size_t)nd.a * TS + tid],
+                                          val[(size_t)nd.r * TS + tid]); break;
+          default: v = fwd_unary<T>(nd.fop, val[(size_t)nd.a * TS + tid]); break;
+        }
+        val[(size_t)pc * TS + tid] = v;
+        adj[(size_t)pc * TS + tid] = (T)0;
+      }
+      adj[(size_t)(n - 1) * TS + tid] = p.gout[b * p.D + d];
+      // reverse
+      for (int pc = n - 1; pc >= 0; --pc) {
+        const T g = adj[(size_t)pc * TS + tid];
+        if (g == (T)0) continue;
+        const BNode nd = plan[pc];
+        if (nd.kind == BK_CONST) {
+          cacc[(size_t)nd.a * TS + tid] += (double)g;
+          touched[nd.a] = 1;
+          continue;
+        }
+        if (nd.kind != BK_BIN && nd.kind != BK_UN) continue;
+        T& al = adj[(size_t)nd.a * TS + tid];
+        const T l_val = val[(size_t)nd.a * TS + tid];
+        if (nd.kind == BK_BIN) {
+          T& ar = adj[(size_t)nd.r * TS + tid];
+          const T r_val = val[(size_t)nd.r * TS + tid];
+          switch (nd.bop) {
+            case BO_ADD: al += g; ar += g; break;
+            case BO_SUB: al += g; ar -= g; break;
+            case BO_MUL: acc_t(al, r_val, g); acc_t(ar, l_val, g); break;
+            case BO_DIV:
+              if (fabs(r_val) >= (T)1e-9) {
+                acc_d(al, 1.0 / r_val, g);
+                acc_t(ar, -(l_val / (r_val * r_val)), g);
+              }
+              break;
+            case BO_POW:
+              if (l_val > 0) {
+                const T out_val = val[(size_t)pc * TS + tid];
+                acc_d(al, (double)r_val * pow((double)l_val, (double)r_val - 1.0), g);
+                acc_t(ar, out_val * log(l_val), g);
+              }
+              break;
+            default: break;
+          }
+        } else {
+          switch (nd.bop) {
+            case BO_SIN: acc_t(al, cos(l_val), g); break;
+            case BO_COS: acc_t(al, -sin(l_val), g); break;
+            case BO_LOG:
+              if (fabs(l_val) > (T)1e-9) acc_d(al, 1.0 / l_val, g);
+              break;
+            case BO_EXP: acc_t(al, val[(size_t)pc * TS + tid], g); break;
+            case BO_SQRT:
+              if (l_val > (T)1e-9) acc_d(al, 0.5 / sqrt(l_val), g);
+              break;
+            case BO_NEG: al += -g; break;
+            default: break;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // fixed-order reduction over the block's threads, one thread per slot
+    for (int64_t k = tid; k < p.K; k += blockDim.x) {
+      if (!touched[k]) continue;
+      double s = 0.0;
+      for (int t = 0; t < (int)blockDim.x; ++t) s += cacc[k * TS + t];
+      T* dst = p.grad + b * p.K + k;
+      if (p.n_splits == 1) *dst = *dst + (T)s;
+      else atomicAdd(dst, (T)s);
+    }
+  }
+}
+
+BwdLut build_bwd_lut(const ws_token_map& m, int64_t num_vars) {
+  BwdLut lut;
+  const int lit_ids[10] = {m.id_0, m.id_1, m.id_2, m.id_3, m.id_4,
+                           m.id_5, m.id_6, m.id_10, m.id_pi, m.id_e};
+  const double lit_val[10] = {0.0, 1.0, 2.0, 3.0, 4.0, 5.0, 6.0, 10.0, m.pi_val, m.e_val};
+  for (int i = 0; i < 10; ++i) lut.lit[i] = lit_val[i];
+  const int bin_ids[6] = {m.op_add, m.op_sub, m.op_mul, m.op_div, m.op_pow, m.op_mod};
+  const uint8_t bin_f[6] = {FO_ADD, FO_SUB, FO_MUL, FO_DIV, FO_POW, FO_MOD};
+  const uint8_t bin_b[6] = {BO_ADD, BO_SUB, BO_MUL, BO_DIV, BO_POW, BO_NONE};
+  const int un_f_ids[8] = {m.op_sin, m.op_cos, m.op_tan, m.op_log,
+                           m.op_exp, m.op_sqrt, m.op_abs, m.op_neg};
+  const uint8_t un_f[8] = {FO_SIN, FO_COS, FO_TAN, FO_LOG, FO_EXP, FO_SQRT, FO_ABS, FO_NEG};
+  const int un_b_ids[6] = {m.op_sin, m.op_cos, m.op_log, m.op_exp, m.op_sqrt, m.op_neg};
+  const uint8_t un_b[6] = {BO_SIN, BO_COS, BO_LOG, BO_EXP, BO_SQRT, BO_NEG};
+  for (int t = 0; t < 256; ++t) {
+    uint8_t kind = BK_UN, arg = 0, fo = FO_NONE, bo = BO_NONE;
+    bool lit = false;
+    if (t == m.pad_id) {
+      kind = BK_PAD;
+    } else if ((int64_t)t >= (int64_t)m.id_x_start &&
+               (int64_t)t < (int64_t)m.id_x_start + num_vars) {
+      kind = BK_VAR;
+      arg = (uint8_t)(t - m.id_x_start);
+    } else {
+      for (int i = 0; i < 10 && !lit; ++i)
+        if (t == lit_ids[i]) { kind = BK_LIT; arg = (uint8_t)i; lit = true; }
+      if (!lit) {
+        if (t == m.id_C) {
+          kind = BK_CONST;
+        } else {
+          int bi = -1;
+          for (int i = 0; i < 6 && bi < 0; ++i)
+            if (t == bin_ids[i]) bi = i;
+          if (bi >= 0) {
+            kind = BK_BIN;
+            fo = bin_f[bi];
+            // the adjoint pass compares add, sub, mul, div, pow in that order
+            for (int i = 0; i < 5; ++i)
+              if (t == bin_ids[i]) { bo = bin_b[i]; break; }
+          } else {
+            kind = BK_UN;
+            for (int i = 0; i < 8; ++i)
+              if (t == un_f_ids[i]) { fo = un_f[i]; break; }
+            for (int i = 0; i < 6; ++i)
+              if (t == un_b_ids[i]) { bo = un_b[i]; break; }
+          }
+        }
+      }
+    }
+    lut.kind[t] = kind;
+    lut.arg[t] = arg;
+    lut.fop[t] = fo;
+    lut.bop[t] = bo;
+  }
+  return lut;
+}
+
+template <typename T>
+size_t backward_smem(int64_t L, int64_t K, int threads) {
+  return al16((size_t)kMaxL * sizeof(BNode)) + (size_t)K * threads * sizeof(double) +
+         al16((size_t)K * sizeof(int)) + 2 * (size_t)L * threads * sizeof(T);
+}
+
+template <typename T>
+ws_status launch_backward_typed(const uint8_t* pop, int64_t B, int64_t L, const void* x,
+                                int64_t D, const void* consts, int64_t K, const void* gout,
+                                void* grad, const BwdLut& lut, cudaStream_t stream) {
+  const DeviceInfo& dev = device_info();
+  const size_t budget = dev.smem_optin < (size_t)200 * 1024 ? dev.smem_optin : 200 * 1024;
+  int threads = 128;
+  while (threads > 32 && backward_smem<T>(L, K, threads) > budget / 2) threads /= 2;
+  const size_t smem = backward_smem<T>(L, K, threads);
+  if (smem > budget)
+    return fail("backward: " + std::to_string(K) + " constants and " + std::to_string(L) +
+                " tokens need more shared memory than a block has");
+  auto kern = backward_kernel<T>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
+  if (per_sm < 1) return fail("backward kernel cannot be resident");
+  const int64_t slots = (int64_t)dev.sm_count * per_sm;
+  // split rows only when there are too few programs to fill the GPU
+  int64_t n_splits = (2 * slots + B - 1) / B;
+  const int64_t max_splits = (D + threads - 1) / threads;
+  if (n_splits > max_splits) n_splits = max_splits;
+  if (n_splits < 1) n_splits = 1;
+  int64_t rows = (D + n_splits - 1) / n_splits;
+  rows = (rows + threads - 1) / threads * threads;
+  n_splits = (D + rows - 1) / rows;
+  BwdParams<T> prm;
+  prm.pop = pop;
+  prm.B = B;
+  prm.L = L;
+  prm.x = static_cast<const T*>(x);
+  prm.D = D;
+  prm.consts = static_cast<const T*>(consts);
+  prm.K = K;
+  prm.gout = static_cast<const T*>(gout);
+  prm.grad = static_cast<T*>(grad);
+  prm.n_splits = n_splits;
+  prm.rows_per_split = rows;
+  prm.n_items = B * n_splits;
+  prm.tape_stride = threads;
+  const int64_t grid = prm.n_items < slots ? prm.n_items : slots;
+  kern<<<(unsigned)grid, threads, smem, stream>>>(prm, lut);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? WS_OK : fail_cuda(e, "eval_rpn_backward");
+}
+
+}  // namespace
+}  // namespace ws
+
+extern "C" ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* population, int64_t B,
+                                          int64_t L, const void* x, int64_t num_vars, int64_t D,
+                                          const void* constants, int64_t K,
+                                          const void* grad_output, void* grad_constants,
+                                          const ws_token_map* ids, void* stream) {
+  using namespace ws;
+  clear_error();
+  if (dtype != WS_F32 && dtype != WS_F64) return fail("x must be float32 or float64");
+  if (!ids) return fail("token map is required");
+  if (B < 0 || L < 0 || D < 0 || K < 0 || num_vars < 0) return fail("negative dimension");
+  if (L > kMaxL) return fail("backward supports programs of at most 256 tokens");
+  if (K > 0xFFFF) return fail("backward supports at most 65535 constants per program");
+  if (num_vars > 255) return fail("at most 255 variables are addressable by uint8 tokens");
+  if (B == 0 || D == 0 || K == 0 || L == 0) return WS_OK;  // nothing to accumulate
+  if (!population || !constants || !grad_output || !grad_constants || (num_vars > 0 && !x))
+    return fail("null tensor pointer");
+  const BwdLut lut = build_bwd_lut(*ids, num_vars);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (dtype == WS_F32)
+    return launch_backward_typed<float>(population, B, L, x, D, constants, K, grad_output,
+                                        grad_constants, lut, s);
+  return launch_backward_typed<double>(population, B, L, x, D, constants, K, grad_output,
+                                       grad_constants, lut, s);
+}

@@ -216,3 +216,37 @@ def tournament_selection(fitness, errors, rand_idx, rand_cases, selected_idx, le
     N.check(N.lib().ws_tournament_select(ptr(fitness), B, ptr(errors), n_data, ptr(rand_idx), T,
                                          ptr(rand_cases), ptr(lengths), ptr(mad_eps),
                                          ptr(selected_idx), stream_of(fitness)))
+
+
+def eval_rpn_backward(population, x, constants, grad_output, grad_constants,
+                      PAD_ID, id_x_start, id_C, id_pi, id_e,
+                      id_0, id_1, id_2, id_3, id_4, id_5, id_6, id_10,
+                      op_add, op_sub, op_mul, op_div, op_pow, op_mod,
+                      op_sin, op_cos, op_tan, op_log, op_exp,
+                      op_sqrt, op_abs, op_neg,
+                      op_fact, op_floor, op_ceil, op_sign,
+                      op_gamma, op_lgamma, op_asin, op_acos, op_atan,
+                      pi_val, e_val):
+    """Adjoint of the program outputs w.r.t. the constants (bindings.cpp:511 ->
+    backward_kernels.cu:13-335): grad_constants [B, K] += sum_d grad_output[b, d] * dpred/dC."""
+    for t, nm in ((population, "population"), (x, "x"), (constants, "constants"),
+                  (grad_output, "grad_output"), (grad_constants, "grad_constants")):
+        check_cuda(t, nm)
+    _expect(population, "population", torch.uint8)
+    B, L = int(population.size(0)), int(population.size(1))
+    V, D = int(x.size(0)), int(x.size(1))
+    K = int(constants.size(1)) if constants.dim() > 1 else 0
+    for t, nm in ((constants, "constants"), (grad_output, "grad_output"),
+                  (grad_constants, "grad_constants")):
+        _expect(t, nm, x.dtype)
+    if grad_output.numel() != B * D:
+        raise RuntimeError("grad_output must have B*D elements")
+    if grad_constants.numel() != B * K:
+        raise RuntimeError("grad_constants must have B*K elements")
+    m = _token_map((PAD_ID, id_x_start, id_C, id_pi, id_e, id_0, id_1, id_2, id_3, id_4, id_5,
+                    id_6, id_10, op_add, op_sub, op_mul, op_div, op_pow, op_mod, op_sin, op_cos,
+                    op_tan, op_log, op_exp, op_sqrt, op_abs, op_neg, op_fact, op_floor, op_ceil,
+                    op_sign, op_gamma, op_lgamma, op_asin, op_acos, op_atan), pi_val, e_val)
+    N.check(N.lib().ws_eval_rpn_backward(dtype_code(x.dtype), ptr(population), B, L, ptr(x), V, D,
+                                         ptr(constants), K, ptr(grad_output),
+                                         ptr(grad_constants), C.byref(m), stream_of(x)))
