@@ -180,6 +180,21 @@ ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* population, int64_t
                                int64_t K, const void* grad_output, void* grad_constants,
                                const ws_token_map* ids, void* stream);
 
+/*
+ * RPN -> infix text (host only: HOST pointers, no GPU work).  Replaces `decode_rpn(population,
+ * constants, vocab, arities, PAD_ID, precision=4)` (bindings.cpp:450 -> decoder.cpp:32-152)
+ * with the same text, character for character.  population uint8 [B, L] and constants [B, K]
+ * (const_dtype WS_F32 / WS_F64) are host arrays; vocab[n_vocab] are the token strings by ID,
+ * arities[n_arities] the arity by ID.  Writes B NUL-terminated strings into out, string b at
+ * offsets[b] (offsets has B + 1 entries, offsets[B] = bytes used).  When out is NULL or
+ * out_bytes is too small, returns WS_ERR_WORKSPACE with *needed_bytes set (call again).
+ */
+ws_status ws_decode_rpn(const uint8_t* population, int64_t B, int64_t L, const void* constants,
+                        int32_t const_dtype, int64_t K, const char* const* vocab, int64_t n_vocab,
+                        const int32_t* arities, int64_t n_arities, int32_t pad_id,
+                        int32_t precision, char* out, size_t out_bytes, int64_t* offsets,
+                        size_t* needed_bytes);
+
 /* ----------------------------------------------------------------------------------------------
  * Population structure (integer, bit-exact).  Token arrays are [B, L] row-major; the arity table
  * is int32 [n_arities] indexed by token value (the reference's `token_arities`).

@@ -78,6 +78,8 @@ _SIGS = {
     "ws_static_scratch_bytes": (C.c_size_t, []),
     "ws_eval_rpn_backward": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
                                     C.POINTER(TokenMap), _P]),
+    "ws_decode_rpn": (_I32, [_P, _I64, _I64, _P, _I32, _I64, C.POINTER(C.c_char_p), _I64, _P,
+                             _I64, _I32, _I32, _P, C.c_size_t, _P, C.POINTER(C.c_size_t)]),
     "ws_validate_rpn_batch": (_I32, [_P, _I32, _I64, _I64, _P, _I64, _I32, _I32, _P, _P]),
     "ws_find_subtree_ranges": (_I32, [_P, _I64, _I64, _P, _I64, _I32, _P, _P, _P]),
     "ws_precompute_subtree_starts": (_I32, [_P, _I64, _I64, _P, _I64, _P, _P]),

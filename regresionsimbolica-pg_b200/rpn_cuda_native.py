@@ -250,3 +250,34 @@ def eval_rpn_backward(population, x, constants, grad_output, grad_constants,
     N.check(N.lib().ws_eval_rpn_backward(dtype_code(x.dtype), ptr(population), B, L, ptr(x), V, D,
                                          ptr(constants), K, ptr(grad_output),
                                          ptr(grad_constants), C.byref(m), stream_of(x)))
+
+
+def decode_rpn(population, constants, vocab, arities, PAD_ID, precision=4):
+    """RPN -> infix strings (bindings.cpp:450 -> decoder.cpp:32-152), on the host like the
+    reference: population uint8 [B, L], constants float32/float64 [B, K] on any device."""
+    import numpy as np
+    pop = population.detach().cpu()
+    if pop.dtype != torch.uint8:
+        raise RuntimeError("population: expected scalar type Byte but found %s" % pop.dtype)
+    pop = pop.contiguous()
+    cst = constants.detach().cpu().contiguous()
+    if cst.dtype not in (torch.float32, torch.float64):
+        raise RuntimeError("constants: expected scalar type Double but found %s" % cst.dtype)
+    B, L = int(pop.size(0)), int(pop.size(1))
+    K = int(cst.size(1))
+    voc = (C.c_char_p * max(len(vocab), 1))(*[str(v).encode("utf-8") for v in vocab])
+    ar = np.ascontiguousarray(np.asarray(list(arities), dtype=np.int64).astype(np.int32))
+    offsets = np.zeros(B + 1, dtype=np.int64)
+    need = C.c_size_t(0)
+    lib = N.lib()
+    args = (C.c_void_p(pop.data_ptr()), B, L, C.c_void_p(cst.data_ptr()),
+            N.WS_F32 if cst.dtype == torch.float32 else N.WS_F64, K, voc, len(vocab),
+            C.c_void_p(ar.ctypes.data), ar.size, int(PAD_ID), int(precision))
+    st = lib.ws_decode_rpn(*args, None, 0, C.c_void_p(offsets.ctypes.data), C.byref(need))
+    if st not in (N.WS_OK, 3):
+        N.check(st)
+    buf = C.create_string_buffer(max(int(need.value), 1))
+    N.check(lib.ws_decode_rpn(*args, buf, int(need.value), C.c_void_p(offsets.ctypes.data),
+                              C.byref(need)))
+    raw = buf.raw
+    return [raw[offsets[i]:offsets[i + 1] - 1].decode("utf-8") for i in range(B)]
