@@ -180,6 +180,70 @@ ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* population, int64_t
                                int64_t K, const void* grad_output, void* grad_constants,
                                const ws_token_map* ids, void* stream);
 
+/* ----------------------------------------------------------------------------------------------
+ * Particle-swarm constant fitting.
+ */
+
+/*
+ * Velocity / position step of every particle.  Replaces `pso_update(pos, vel, pbest, gbest, r1,
+ * r2, w, c1, c2)` (bindings.cpp:470 -> launch_pso_update, pso_kernels.cu:155-187; kernel
+ * :29-70):  vel = w vel + c1 r1 (pbest - pos) + c2 r2 (gbest[b] - pos);  pos += vel,
+ * bit-identical.  pos, vel, pbest, r1, r2: [B, P, K]; gbest: [B, K]; all `dtype`.
+ */
+ws_status ws_pso_update(int32_t dtype, void* pos, void* vel, const void* pbest,
+                        const void* gbest, const void* r1, const void* r2, float w, float c1,
+                        float c2, int64_t B, int64_t P, int64_t K, void* stream);
+
+/*
+ * Personal and swarm bests.  Replaces `pso_update_bests(current_err, pbest_err, pbest_pos,
+ * current_pos, gbest_err, gbest_pos)` (bindings.cpp:471 -> launch_pso_update_bests,
+ * pso_kernels.cu:189-233; kernels :74-153) with its tie rules: a particle improves on a strictly
+ * smaller error; the swarm best is replaced by the strict minimum of the personal bests, found
+ * as the reference finds it (first minimum of each lane's 32-strided particles, then a
+ * shuffle-down tree that takes a partner's value only when strictly smaller, which settles
+ * ties); errors at or above 1e30 and NaN never win.  current_err, pbest_err: [B, P]; positions [B, P, K];
+ * gbest_err [B]; gbest_pos [B, K].
+ */
+ws_status ws_pso_update_bests(int32_t dtype, const void* current_err, void* pbest_err,
+                              void* pbest_pos, const void* current_pos, void* gbest_err,
+                              void* gbest_pos, int64_t B, int64_t P, int64_t K, void* stream);
+
+/*
+ * The whole PSO loop in one launch.  Replaces `fused_pso(population, init_consts, x, y_target,
+ * out_gbest_pos, out_gbest_err, num_particles, num_steps, w, c1, c2, const_min, const_max, <ids>,
+ * pi_val, e_val, rng_seed)` (bindings.cpp:510 -> launch_fused_pso, fused_pso_kernels.cu:431-515;
+ * kernel :208-427) with the same limits and messages (L <= 256, K <= 16, D <= 1024, particles
+ * <= 64, float32 only) and the same results for the same seed: particle p of program b draws
+ * curand XORWOW stream seed + b * num_particles + p; particle 0 starts at init_consts, the others
+ * jittered by N(0, (0.15 range)^2) and clamped; velocities N(0, (0.02 range)^2); inertia decays
+ * linearly from w to 0.4; the fitness is the RMSE under the reference PSO evaluator's rules
+ * (fused_pso_kernels.cu:57-197).  Writes out_gbest_pos [B, K] and out_gbest_err [B].
+ * K == 0 with a C token evaluates C as 1.0 (the reference reads outside its arrays there).
+ */
+ws_status ws_fused_pso(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
+                       const void* init_consts, int64_t K, const void* x, int64_t num_vars,
+                       int64_t D, const void* y_target, void* out_gbest_pos, void* out_gbest_err,
+                       int32_t num_particles, int32_t num_steps, float w, float c1, float c2,
+                       float const_min, float const_max, const ws_token_map* ids,
+                       uint64_t rng_seed, void* stream);
+
+/*
+ * Constant fitting with the reference's L-BFGS kernel.  Replaces `lbfgs_optimize(population,
+ * constants, x, y_target, out_rmse, max_iter=20, history_size=10, gtol=1e-7, const_min=-25,
+ * const_max=25, <ids>, pi_val, e_val)` (bindings.cpp:542-563 -> launch_lbfgs_optimize,
+ * lbfgs_kernels.cu:624-694; kernel :214-621) with its limits and messages (L <= 256, K <= 32,
+ * D <= 1024).  constants [B, K] are updated in place; out_rmse [B] receives the final fitness.
+ * The fitness, the finite-difference gradient and the iteration are the reference kernel's (see
+ * ws_lbfgs.cu): its curvature history never admits a pair, and the history slots it reads
+ * without writing are taken as zero.  history_size is accepted and, as in the reference,
+ * unused.  K == 0 with a C token evaluates C as 1.0 (the reference reads outside its arrays).
+ */
+ws_status ws_lbfgs_optimize(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
+                            void* constants, int64_t K, const void* x, int64_t num_vars,
+                            int64_t D, const void* y_target, void* out_rmse, int32_t max_iter,
+                            int32_t history_size, float gtol, float const_min, float const_max,
+                            const ws_token_map* ids, void* stream);
+
 /*
  * RPN -> infix text (host only: HOST pointers, no GPU work).  Replaces `decode_rpn(population,
  * constants, vocab, arities, PAD_ID, precision=4)` (bindings.cpp:450 -> decoder.cpp:32-152)

@@ -46,6 +46,18 @@ def lib():
             getattr(h, "ws_oracle_backward_" + suf).argtypes = [
                 _P, C.c_int64, C.c_int64, _P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P, _P,
                 _P]
+        for suf in ("f32", "f64"):
+            getattr(h, "ws_oracle_pso_update_" + suf).argtypes = [
+                _P, _P, _P, _P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_int64, C.c_int64,
+                C.c_int64]
+            getattr(h, "ws_oracle_pso_bests_" + suf).argtypes = [
+                _P, _P, _P, _P, _P, _P, C.c_int64, C.c_int64, C.c_int64]
+        h.ws_oracle_pso_rmse.argtypes = [_P, C.c_int64, C.c_int64, _P, C.c_int64, C.c_int64, _P,
+                                         C.c_int64, _P, _P, _P]
+        for suf in ("f32", "f64"):
+            getattr(h, "ws_oracle_lbfgs_" + suf).argtypes = [
+                _P, C.c_int64, C.c_int64, _P, C.c_int64, _P, C.c_int64, C.c_int64, _P, _P,
+                C.c_int, C.c_float, C.c_float, C.c_float, _P]
         h.ws_oracle_validate.argtypes = [_P, C.c_int32, C.c_int64, C.c_int64, _P, C.c_int64,
                                          C.c_int32, C.c_int32, _P]
         h.ws_oracle_subtree_ranges.argtypes = [_P, C.c_int64, C.c_int64, _P, C.c_int64,
@@ -210,3 +222,60 @@ def tournament(fitness, cand, errors=None, cases=None, lengths=None, mad_eps=Non
     lib().ws_oracle_tournament(_p(fit), B, _p(errors), n_data, _p(idx), _p(off), T, _p(cases),
                                _p(lengths), _p(mad_eps), int(island_size), int(n_islands), _p(out))
     return out
+
+
+# ---------------------------------------------------------------------------------------------
+# Particle swarm (oracle/ws_oracle_pso.cpp).
+
+def pso_update(pos, vel, pbest, gbest, r1, r2, w, c1, c2):
+    """Returns updated (pos, vel) copies; arrays [B, P, K], gbest [B, K]."""
+    pos, vel = np.array(pos, copy=True, order="C"), np.array(vel, copy=True, order="C")
+    B, P, K = pos.shape
+    arr = [np.ascontiguousarray(a, dtype=pos.dtype) for a in (pbest, gbest, r1, r2)]
+    getattr(lib(), "ws_oracle_pso_update_" + _suffix(pos.dtype))(
+        _p(pos), _p(vel), *[_p(a) for a in arr], float(w), float(c1), float(c2), B, P, K)
+    return pos, vel
+
+
+def pso_update_bests(cur_err, pb_err, pb_pos, cur_pos, gb_err, gb_pos):
+    """Returns updated (pb_err, pb_pos, gb_err, gb_pos) copies."""
+    out = [np.array(a, copy=True, order="C") for a in (pb_err, pb_pos, gb_err, gb_pos)]
+    ce = np.ascontiguousarray(cur_err, dtype=out[0].dtype)
+    cp = np.ascontiguousarray(cur_pos, dtype=out[0].dtype)
+    B, P = out[0].shape
+    K = out[1].shape[2]
+    getattr(lib(), "ws_oracle_pso_bests_" + _suffix(out[0].dtype))(
+        _p(ce), _p(out[0]), _p(out[1]), _p(cp), _p(out[2]), _p(out[3]), B, P, K)
+    return tuple(out)
+
+
+def pso_rmse(tmap, pop, X, consts, y):
+    """RMSE [B] under the fused PSO's evaluator (float32; 1e30 when a row fails)."""
+    pop = np.ascontiguousarray(pop, dtype=np.uint8)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    c = np.ascontiguousarray(consts, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    B, L = pop.shape
+    V, D = X.shape
+    out = np.empty(B, dtype=np.float32)
+    lib().ws_oracle_pso_rmse(_p(pop), B, L, _p(X), V, D, _p(c), c.shape[1], _p(y),
+                             C.byref(tmap), _p(out))
+    return out
+
+
+# ---------------------------------------------------------------------------------------------
+# L-BFGS kernel semantics (oracle/ws_oracle_lbfgs.cpp).
+
+def lbfgs(tmap, pop, X, consts, y, max_iter=20, gtol=1e-7, cmin=-25.0, cmax=25.0):
+    """Returns (constants [B, K] after fitting, rmse [B])."""
+    pop = np.ascontiguousarray(pop, dtype=np.uint8)
+    X = np.ascontiguousarray(X)
+    c = np.array(consts, dtype=X.dtype, copy=True, order="C")
+    y = np.ascontiguousarray(y, dtype=X.dtype)
+    B, L = pop.shape
+    V, D = X.shape
+    out = np.empty(B, dtype=X.dtype)
+    getattr(lib(), "ws_oracle_lbfgs_" + _suffix(X.dtype))(
+        _p(pop), B, L, _p(c), c.shape[1], _p(X), V, D, _p(y), _p(out), int(max_iter),
+        float(gtol), float(cmin), float(cmax), C.byref(tmap))
+    return c, out

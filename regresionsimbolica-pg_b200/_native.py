@@ -80,6 +80,14 @@ _SIGS = {
                                     C.POINTER(TokenMap), _P]),
     "ws_decode_rpn": (_I32, [_P, _I64, _I64, _P, _I32, _I64, C.POINTER(C.c_char_p), _I64, _P,
                              _I64, _I32, _I32, _P, C.c_size_t, _P, C.POINTER(C.c_size_t)]),
+    "ws_pso_update": (_I32, [_I32, _P, _P, _P, _P, _P, _P, C.c_float, C.c_float, C.c_float,
+                             _I64, _I64, _I64, _P]),
+    "ws_pso_update_bests": (_I32, [_I32, _P, _P, _P, _P, _P, _P, _I64, _I64, _I64, _P]),
+    "ws_fused_pso": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _P, _I64, _I64, _P, _P, _P, _I32,
+                            _I32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                            C.POINTER(TokenMap), C.c_uint64, _P]),
+    "ws_lbfgs_optimize": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _P, _I64, _I64, _P, _P, _I32,
+                                 _I32, C.c_float, C.c_float, C.c_float, C.POINTER(TokenMap), _P]),
     "ws_validate_rpn_batch": (_I32, [_P, _I32, _I64, _I64, _P, _I64, _I32, _I32, _P, _P]),
     "ws_find_subtree_ranges": (_I32, [_P, _I64, _I64, _P, _I64, _I32, _P, _P, _P]),
     "ws_precompute_subtree_starts": (_I32, [_P, _I64, _I64, _P, _I64, _P, _P]),

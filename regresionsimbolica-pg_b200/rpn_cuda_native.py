@@ -281,3 +281,99 @@ def decode_rpn(population, constants, vocab, arities, PAD_ID, precision=4):
                               C.byref(need)))
     raw = buf.raw
     return [raw[offsets[i]:offsets[i + 1] - 1].decode("utf-8") for i in range(B)]
+
+
+def pso_update(pos, vel, pbest, gbest, r1, r2, w, c1, c2):
+    """PSO velocity / position step (bindings.cpp:470 -> pso_kernels.cu:29-187), in place on
+    pos and vel [B, P, K]."""
+    check_cuda(pos, "pos")
+    check_cuda(vel, "vel")
+    B, P, K = (int(v) for v in pos.shape)
+    for t, nm in ((vel, "vel"), (pbest, "pbest"), (gbest, "gbest"), (r1, "r1"), (r2, "r2")):
+        check_cuda(t, nm)
+        _expect(t, nm, pos.dtype)
+    N.check(N.lib().ws_pso_update(dtype_code(pos.dtype), ptr(pos), ptr(vel), ptr(pbest),
+                                  ptr(gbest), ptr(r1), ptr(r2), float(w), float(c1), float(c2),
+                                  B, P, K, stream_of(pos)))
+
+
+def pso_update_bests(current_err, pbest_err, pbest_pos, current_pos, gbest_err, gbest_pos):
+    """Personal / swarm bests (bindings.cpp:471 -> pso_kernels.cu:74-233), in place."""
+    for t, nm in ((current_err, "current_err"), (pbest_err, "pbest_err"),
+                  (pbest_pos, "pbest_pos"), (current_pos, "current_pos"),
+                  (gbest_err, "gbest_err"), (gbest_pos, "gbest_pos")):
+        check_cuda(t, nm)
+        _expect(t, nm, pbest_err.dtype)
+    B, P = int(pbest_err.size(0)), int(pbest_err.size(1))
+    K = int(pbest_pos.size(2))
+    N.check(N.lib().ws_pso_update_bests(dtype_code(pbest_err.dtype), ptr(current_err),
+                                        ptr(pbest_err), ptr(pbest_pos), ptr(current_pos),
+                                        ptr(gbest_err), ptr(gbest_pos), B, P, K,
+                                        stream_of(pbest_err)))
+
+
+def fused_pso(population, init_consts, x, y_target, out_gbest_pos, out_gbest_err,
+              num_particles, num_steps, w, c1, c2, const_min, const_max,
+              PAD_ID, id_x_start, id_C, id_pi, id_e,
+              id_0, id_1, id_2, id_3, id_4, id_5, id_6, id_10,
+              op_add, op_sub, op_mul, op_div, op_pow, op_mod,
+              op_sin, op_cos, op_tan, op_log, op_exp,
+              op_sqrt, op_abs, op_neg,
+              op_fact, op_floor, op_ceil, op_sign,
+              op_gamma, op_lgamma, op_asin, op_acos, op_atan,
+              pi_val, e_val, rng_seed):
+    """The whole PSO loop in one launch (bindings.cpp:510 -> fused_pso_kernels.cu:208-515):
+    writes out_gbest_pos [B, K] and out_gbest_err [B]."""
+    for t, nm in ((population, "population"), (init_consts, "init_consts"), (x, "x"),
+                  (y_target, "y_target")):
+        check_cuda(t, nm)
+    B, L = int(population.size(0)), int(population.size(1))
+    K = int(init_consts.size(1))
+    V, D = int(x.size(0)), int(x.size(1))
+    m = _token_map((PAD_ID, id_x_start, id_C, id_pi, id_e, id_0, id_1, id_2, id_3, id_4, id_5,
+                    id_6, id_10, op_add, op_sub, op_mul, op_div, op_pow, op_mod, op_sin, op_cos,
+                    op_tan, op_log, op_exp, op_sqrt, op_abs, op_neg, op_fact, op_floor, op_ceil,
+                    op_sign, op_gamma, op_lgamma, op_asin, op_acos, op_atan), pi_val, e_val)
+    lib = N.lib()
+    if x.dtype == torch.float32:
+        for t, nm in ((init_consts, "init_consts"), (y_target, "y_target"),
+                      (out_gbest_pos, "out_gbest_pos"), (out_gbest_err, "out_gbest_err")):
+            if t.dtype != x.dtype:
+                raise RuntimeError("%s dtype must match x" % nm)
+    code = N.WS_F32 if x.dtype == torch.float32 else N.WS_F64
+    N.check(lib.ws_fused_pso(code, ptr(population), B, L, ptr(init_consts), K, ptr(x), V, D,
+                             ptr(y_target), ptr(out_gbest_pos), ptr(out_gbest_err),
+                             int(num_particles), int(num_steps), float(w), float(c1), float(c2),
+                             float(const_min), float(const_max), C.byref(m),
+                             int(rng_seed) & 0xFFFFFFFFFFFFFFFF, stream_of(x)))
+
+
+def lbfgs_optimize(population, constants, x, y_target, out_rmse, max_iter=20, history_size=10,
+                   gtol=1e-7, const_min=-25.0, const_max=25.0, PAD_ID=None, id_x_start=None,
+                   id_C=None, id_pi=None, id_e=None, id_0=None, id_1=None, id_2=None, id_3=None,
+                   id_4=None, id_5=None, id_6=None, id_10=None, op_add=None, op_sub=None,
+                   op_mul=None, op_div=None, op_pow=None, op_mod=None, op_sin=None, op_cos=None,
+                   op_tan=None, op_log=None, op_exp=None, op_sqrt=None, op_abs=None,
+                   op_neg=None, op_fact=None, op_floor=None, op_ceil=None, op_sign=None,
+                   op_gamma=None, op_lgamma=None, op_asin=None, op_acos=None, op_atan=None,
+                   pi_val=None, e_val=None):
+    """Constant fitting with the reference's L-BFGS kernel (bindings.cpp:542-563 ->
+    lbfgs_kernels.cu:214-694): constants [B, K] updated in place, out_rmse [B] written."""
+    ids = (PAD_ID, id_x_start, id_C, id_pi, id_e, id_0, id_1, id_2, id_3, id_4, id_5, id_6,
+           id_10, op_add, op_sub, op_mul, op_div, op_pow, op_mod, op_sin, op_cos, op_tan,
+           op_log, op_exp, op_sqrt, op_abs, op_neg, op_fact, op_floor, op_ceil, op_sign,
+           op_gamma, op_lgamma, op_asin, op_acos, op_atan)
+    if any(v is None for v in ids) or pi_val is None or e_val is None:
+        raise TypeError("lbfgs_optimize: the token IDs, pi_val and e_val are required")
+    for t, nm in ((population, "population"), (constants, "constants"), (x, "x"),
+                  (y_target, "y_target"), (out_rmse, "out_rmse")):
+        check_cuda(t, nm)
+    B, L = int(population.size(0)), int(population.size(1))
+    K = int(constants.size(1))
+    V, D = int(x.size(0)), int(x.size(1))
+    m = _token_map(ids, pi_val, e_val)
+    N.check(N.lib().ws_lbfgs_optimize(dtype_code(x.dtype), ptr(population), B, L, ptr(constants),
+                                      K, ptr(x), V, D, ptr(y_target), ptr(out_rmse),
+                                      int(max_iter), int(history_size), float(gtol),
+                                      float(const_min), float(const_max), C.byref(m),
+                                      stream_of(x)))

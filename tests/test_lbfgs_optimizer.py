@@ -1,0 +1,173 @@
+"""Constant fitting: the L-BFGS kernel (bit-exact against the reference extension, close to the
+CPU oracle that restates the reference kernel literally, trial gradients included) and the
+GPUOptimizer mirror (PSO in both paths, L-BFGS in both paths)."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import refext
+import ws_testlib as tl
+
+O = tl.oracle
+gpu = pytest.mark.gpu
+needs_ref = pytest.mark.skipif(refext.path("fastmath") is None,
+                               reason="reference extension not built (oracle/build_ref.sh)")
+DEV = torch.device("cuda:0") if torch.cuda.is_available() else None
+BIN_OPS = ('+', '-', '*', '/', 'pow', '%')
+
+
+def T(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
+
+
+def tmap(g):
+    return tl.N.TokenMap.from_args(*g.scalar_ids(), pi_val=math.pi, e_val=math.e)
+
+
+def _case(seed, B, L, K, D, dtype, ops=BIN_OPS, V=2):
+    rng = np.random.default_rng(seed)
+    g = tl.GPUGrammar(num_variables=V, operators=ops)
+    pop = tl.synthetic.random_programs(g, B, 3, L, L, rng, max_consts=K, use_literals=True)
+    consts = rng.uniform(-3, 3, size=(B, K)).astype(dtype)
+    X = rng.uniform(0.2, 3, size=(V, D)).astype(dtype)
+    y = (2.5 * X[0] + 0.7 * X[-1] ** 2 - 1.0).astype(dtype)
+    return g, pop, consts, X, y
+
+
+def test_oracle_fits_a_line():
+    """The restated kernel descends from its start: 'C x0 * C +' towards y = 2.5 x + 0.7."""
+    g = tl.GPUGrammar(num_variables=1, operators=BIN_OPS)
+    X = np.linspace(-2, 2, 50)[None, :]
+    y = 2.5 * X[0] + 0.7
+    pop = np.array([g.encode(["C", "x0", "*", "C", "+"], 8)], np.uint8)
+    c0 = np.array([[1.0, 0.0]])
+    start = np.sqrt(np.mean((c0[0, 0] * X[0] + c0[0, 1] - y) ** 2))
+    for dt in (np.float32, np.float64):
+        c, r = O.lbfgs(tmap(g), pop, X.astype(dt), c0, y.astype(dt), max_iter=30)
+        assert r[0] < 0.25 * start
+        assert abs(float(np.sqrt(np.mean((c[0, 0] * X[0] + c[0, 1] - y) ** 2))) - r[0]) < 1e-5
+
+
+def _run(mod, g, pop, consts, X, y, max_iter=20, cmin=-25.0, cmax=25.0):
+    c = T(consts)
+    out = torch.empty(len(pop), dtype=c.dtype, device=DEV)
+    mod.lbfgs_optimize(T(pop), c, T(X), T(y), out, max_iter, 10, 1e-7, cmin, cmax,
+                       *g.scalar_ids(), math.pi, math.e)
+    torch.cuda.synchronize()
+    return c.cpu().numpy(), out.cpu().numpy()
+
+
+@gpu
+@needs_ref
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("B,L,K,D,ops", [(64, 20, 4, 200, BIN_OPS), (50, 40, 8, 1024, BIN_OPS),
+                                         (64, 16, 3, 77, tl.C1_OPERATORS)])
+def test_lbfgs_bit_exact_against_reference(dtype, B, L, K, D, ops):
+    ref = refext.load("fastmath")
+    from warpsymbolic_b200 import rpn_cuda_native as ours
+    g, pop, consts, X, y = _case(B + L + K, B, L, K, D, dtype, ops=ops)
+    rc, rr = _run(ref, g, pop, consts, X, y)
+    oc, orr = _run(ours, g, pop, consts, X, y)
+    assert np.array_equal(rr, orr, equal_nan=True), np.nonzero(rr != orr)[0][:5]
+    assert np.array_equal(rc, oc, equal_nan=True)
+    if ops is BIN_OPS:
+        assert (orr < 1e29).mean() > 0.5
+
+
+@gpu
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_lbfgs_close_to_oracle(dtype):
+    from warpsymbolic_b200 import rpn_cuda_native as ours
+    g, pop, consts, X, y = _case(7, 64, 20, 4, 300, dtype)
+    oc, orr = _run(ours, g, pop, consts, X, y)
+    wc, wr = O.lbfgs(tmap(g), pop, X, consts, y, max_iter=20)
+    # fast-math powf / division on the GPU against host libm: line-search decisions can differ
+    close = (np.abs(orr - wr) <= 1e-3 * np.abs(wr) + 1e-6) | ((orr >= 1e29) & (wr >= 1e29))
+    assert close.mean() > 0.9
+    start = O.lbfgs(tmap(g), pop, X, consts, y, max_iter=0)[1]
+    assert (orr <= start * (1 + 1e-5) + 1e-6).all()
+
+
+@gpu
+def test_lbfgs_argument_checks():
+    from warpsymbolic_b200 import rpn_cuda_native as ours
+    g, pop, consts, X, y = _case(1, 4, 10, 3, 50, np.float32)
+    with pytest.raises(RuntimeError, match="Formula length exceeds LBFGS_MAX_L"):
+        _run(ours, g, np.zeros((4, 300), np.uint8), consts, X, y)
+    with pytest.raises(RuntimeError, match="Constants exceed LBFGS_MAX_K"):
+        _run(ours, g, pop, np.zeros((4, 33), np.float32), X, y)
+    with pytest.raises(RuntimeError, match="Data samples exceed LBFGS_MAX_D"):
+        _run(ours, g, pop, consts, np.zeros((2, 1025), np.float32), np.zeros(1025, np.float32))
+
+
+# ---- GPUOptimizer mirror --------------------------------------------------------------------
+
+def _optimizer(g, dtype=torch.float64):
+    from warpsymbolic_b200.evaluation import GPUEvaluator
+    from warpsymbolic_b200.optimization import GPUOptimizer
+    ev = GPUEvaluator(g, DEV, dtype=dtype)
+    return ev, GPUOptimizer(ev, DEV, dtype=dtype)
+
+
+def _pso_case(seed, B, D, dtype):
+    rng = np.random.default_rng(seed)
+    g = tl.GPUGrammar(num_variables=2, operators=tl.C1_OPERATORS)
+    pop = tl.synthetic.random_programs(g, B, 3, 20, 20, rng, max_consts=4)
+    consts = rng.uniform(-2, 2, size=(B, 4))
+    X = rng.uniform(-3, 3, size=(2, D))
+    y = 1.7 * X[0] * X[1] - 0.5 * np.sin(X[1]) + 0.3
+    return g, pop, T(consts.astype(dtype)), T(X.astype(dtype)), T(y.astype(dtype))
+
+
+@gpu
+@pytest.mark.parametrize("path", ["fused", "multi_kernel_f64", "multi_kernel_rows"])
+def test_nano_pso_never_worse_and_improves(path):
+    """Both PSO paths keep particle 0 at the starting constants, so the swarm best is never worse
+    than the start; on this target most programs improve (the reference tests PSO the same way,
+    statistically: tests/gpu/test_pso_fixes.py)."""
+    dtype = np.float32 if path == "fused" else np.float64
+    D = 2000 if path == "multi_kernel_rows" else 256
+    g, pop, c, X, y = _pso_case(3, 300, D, dtype)
+    ev, opt = _optimizer(g, dtype=torch.float32 if dtype == np.float32 else torch.float64)
+    P = T(pop)
+    fused = path == "fused"
+    assert opt._can_use_fused_pso(P, c, X, y, 20) == fused
+
+    def fitness(consts):
+        # the fused loop scores with its own evaluator's rules, the multi-kernel one with the
+        # batch evaluator's
+        if fused:
+            return torch.from_numpy(O.pso_rmse(tmap(g), pop, X.cpu().numpy(),
+                                               consts.cpu().numpy(), y.cpu().numpy())).double().to(DEV)
+        return ev.evaluate_batch(P, X, y, consts).double()
+
+    start = fitness(c)
+    torch.manual_seed(0)
+    gpos, gerr = opt.nano_pso(P, c, X, y, steps=20, num_particles=20)
+    gerr = gerr.double()
+    again = fitness(gpos.to(c.dtype))
+    fin = torch.isfinite(start) & (start < 1e14)
+    assert bool((gerr[fin] <= start[fin] * (1 + 1e-4) + 1e-6).all())
+    assert float((gerr[fin] < start[fin] * 0.999).float().mean()) > 0.5
+    ok = torch.isfinite(gerr) & (gerr < 1e14)
+    # the reported error is the evaluator's fitness of the reported constants
+    torch.testing.assert_close(again[ok], gerr[ok], rtol=2e-3, atol=1e-5)
+
+
+@gpu
+@pytest.mark.parametrize("n_programs,D", [(40, 300), (100, 300), (30, 3000)])
+def test_lbfgs_top_k_paths(n_programs, D):
+    """<= 64 programs and <= 1024 rows: the L-BFGS kernel; otherwise torch's L-BFGS over
+    RPNBackwardFunction.  Either way only improvements are accepted."""
+    g, pop, c, X, y = _pso_case(5, n_programs, D, np.float64)
+    ev, opt = _optimizer(g)
+    P = T(pop)
+    start = ev.evaluate_batch(P, X, y, c)
+    res_c, res_e = opt.lbfgs_optimize_top_k(P, c, X, y, top_k=n_programs, max_iter=10)
+    assert res_c.shape == c.shape
+    fin = torch.isfinite(start)
+    assert bool((res_e[fin] <= start[fin] + 1e-12).all())
+    now = ev.evaluate_batch(P, X, y, res_c)
+    torch.testing.assert_close(now[fin], res_e[fin], rtol=1e-9, atol=1e-12)
