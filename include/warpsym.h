@@ -259,6 +259,30 @@ ws_status ws_decode_rpn(const uint8_t* population, int64_t B, int64_t L, const v
                         int32_t precision, char* out, size_t out_bytes, int64_t* offsets,
                         size_t* needed_bytes);
 
+/* Operator / literal IDs of the simplifier, in the reference's argument order
+ * (simplify_kernels.cu:665-678); absent ones are -1. */
+typedef struct ws_simplify_ids {
+  int32_t op_plus, op_minus, op_mult, op_div, op_neg, op_mod, op_pow;
+  int32_t op_sin, op_cos, op_tan, op_asin, op_acos, op_atan;
+  int32_t op_log, op_exp, op_sqrt, op_abs, op_gamma, op_lgamma, op_floor, op_ceil, op_sign;
+  int32_t id_0, id_1, id_2, id_3, id_4, id_5, id_6;
+} ws_simplify_ids;
+
+/*
+ * Rule-based simplification of programs in place.  Replaces `simplify_batch(population,
+ * arities, val_table, literal_ids, literal_vals, max_passes, <ids>)` (bindings.cpp:505 ->
+ * launch_simplify_batch, simplify_kernels.cu:665-713; kernel :100-601) with identical output
+ * programs: the same rules in the same order, the same in-place editing and compaction, the
+ * same nearest-literal folding (see ws_simplify.cu).  population int64 [B, L] (PAD = 0; only
+ * the first 256 positions are rewritten, as in the reference); arities int32 [max_id];
+ * val_table float32 [max_id] (the literal's value, NaN for other tokens); literal_ids int64 /
+ * literal_vals float32 [n_literals] (the first 64 are used).
+ */
+ws_status ws_simplify_batch(int64_t* population, int64_t B, int64_t L, const int32_t* arities,
+                            int64_t max_id, const float* val_table, const int64_t* literal_ids,
+                            const float* literal_vals, int64_t n_literals, int32_t max_passes,
+                            const ws_simplify_ids* ids, void* stream);
+
 /* ----------------------------------------------------------------------------------------------
  * Population structure (integer, bit-exact).  Token arrays are [B, L] row-major; the arity table
  * is int32 [n_arities] indexed by token value (the reference's `token_arities`).

@@ -58,6 +58,8 @@ def lib():
             getattr(h, "ws_oracle_lbfgs_" + suf).argtypes = [
                 _P, C.c_int64, C.c_int64, _P, C.c_int64, _P, C.c_int64, C.c_int64, _P, _P,
                 C.c_int, C.c_float, C.c_float, C.c_float, _P]
+        h.ws_oracle_simplify.argtypes = [_P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P, _P,
+                                         C.c_int64, C.c_int32, _P]
         h.ws_oracle_validate.argtypes = [_P, C.c_int32, C.c_int64, C.c_int64, _P, C.c_int64,
                                          C.c_int32, C.c_int32, _P]
         h.ws_oracle_subtree_ranges.argtypes = [_P, C.c_int64, C.c_int64, _P, C.c_int64,
@@ -279,3 +281,22 @@ def lbfgs(tmap, pop, X, consts, y, max_iter=20, gtol=1e-7, cmin=-25.0, cmax=25.0
         _p(pop), B, L, _p(c), c.shape[1], _p(X), V, D, _p(y), _p(out), int(max_iter),
         float(gtol), float(cmin), float(cmax), C.byref(tmap))
     return c, out
+
+
+# ---------------------------------------------------------------------------------------------
+# Simplifier (oracle/ws_oracle_simplify.cpp).
+
+def simplify(pop, arities, val_table, lit_ids, lit_vals, max_passes, ids29):
+    """Returns the simplified copy of int64 pop [B, L]; ids29: the 29 operator / literal IDs in
+    the kernel's argument order."""
+    out = np.array(pop, dtype=np.int64, copy=True, order="C")
+    ar = np.ascontiguousarray(arities, dtype=np.int32)
+    vt = np.ascontiguousarray(val_table, dtype=np.float32)
+    li = np.ascontiguousarray(lit_ids, dtype=np.int64)
+    lv = np.ascontiguousarray(lit_vals, dtype=np.float32)
+    idv = np.ascontiguousarray(ids29, dtype=np.int32)
+    assert idv.size == 29
+    B, L = out.shape
+    lib().ws_oracle_simplify(_p(out), B, L, _p(ar), ar.size, _p(vt), _p(li), _p(lv), li.size,
+                             int(max_passes), _p(idv))
+    return out

@@ -53,6 +53,17 @@ class TokenMap(C.Structure):
 WS_PHASE_ALL, WS_PHASE_COMPILE, WS_PHASE_EVALUATE = 0, 1, 2
 
 
+class SimplifyIds(C.Structure):
+    """Mirror of ws_simplify_ids: the simplifier's operator / literal IDs (argument order of
+    simplify_kernels.cu:665-678)."""
+
+    _fields_ = [(n, C.c_int32) for n in (
+        "op_plus", "op_minus", "op_mult", "op_div", "op_neg", "op_mod", "op_pow",
+        "op_sin", "op_cos", "op_tan", "op_asin", "op_acos", "op_atan",
+        "op_log", "op_exp", "op_sqrt", "op_abs", "op_gamma", "op_lgamma", "op_floor", "op_ceil",
+        "op_sign", "id_0", "id_1", "id_2", "id_3", "id_4", "id_5", "id_6")]
+
+
 class FitnessOpts(C.Structure):
     _fields_ = [("strict_mode", C.c_int32), ("policy", C.c_int32), ("loss", C.c_int32),
                 ("schedule", C.c_int32), ("invalid_value", C.c_double), ("phase", C.c_int32),
@@ -88,6 +99,8 @@ _SIGS = {
                             C.POINTER(TokenMap), C.c_uint64, _P]),
     "ws_lbfgs_optimize": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _P, _I64, _I64, _P, _P, _I32,
                                  _I32, C.c_float, C.c_float, C.c_float, C.POINTER(TokenMap), _P]),
+    "ws_simplify_batch": (_I32, [_P, _I64, _I64, _P, _I64, _P, _P, _P, _I64, _I32,
+                                 C.POINTER(SimplifyIds), _P]),
     "ws_validate_rpn_batch": (_I32, [_P, _I32, _I64, _I64, _P, _I64, _I32, _I32, _P, _P]),
     "ws_find_subtree_ranges": (_I32, [_P, _I64, _I64, _P, _I64, _I32, _P, _P, _P]),
     "ws_precompute_subtree_starts": (_I32, [_P, _I64, _I64, _P, _I64, _P, _P]),

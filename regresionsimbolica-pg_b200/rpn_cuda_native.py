@@ -377,3 +377,30 @@ def lbfgs_optimize(population, constants, x, y_target, out_rmse, max_iter=20, hi
                                       int(max_iter), int(history_size), float(gtol),
                                       float(const_min), float(const_max), C.byref(m),
                                       stream_of(x)))
+
+
+def simplify_batch(population, arities, val_table, literal_ids, literal_vals, max_passes,
+                   op_plus, op_minus, op_mult, op_div, op_neg, op_mod, op_pow,
+                   op_sin, op_cos, op_tan, op_asin, op_acos, op_atan,
+                   op_log, op_exp, op_sqrt, op_abs, op_gamma, op_lgamma,
+                   op_floor, op_ceil, op_sign,
+                   id_0, id_1, id_2, id_3, id_4, id_5, id_6):
+    """Rule-based simplification in place (bindings.cpp:505 -> simplify_kernels.cu:100-713):
+    population int64 [B, L] is rewritten."""
+    for t, nm in ((population, "population"), (arities, "arities"), (val_table, "val_table"),
+                  (literal_ids, "literal_ids"), (literal_vals, "literal_vals")):
+        check_cuda(t, nm)
+    _expect(population, "population", torch.int64)
+    _expect(arities, "arities", torch.int32)
+    _expect(val_table, "val_table", torch.float32)
+    _expect(literal_ids, "literal_ids", torch.int64)
+    _expect(literal_vals, "literal_vals", torch.float32)
+    ids = N.SimplifyIds(*[int(v) for v in (
+        op_plus, op_minus, op_mult, op_div, op_neg, op_mod, op_pow, op_sin, op_cos, op_tan,
+        op_asin, op_acos, op_atan, op_log, op_exp, op_sqrt, op_abs, op_gamma, op_lgamma,
+        op_floor, op_ceil, op_sign, id_0, id_1, id_2, id_3, id_4, id_5, id_6)])
+    B, L = int(population.size(0)), int(population.size(1))
+    N.check(N.lib().ws_simplify_batch(ptr(population), B, L, ptr(arities), int(arities.size(0)),
+                                      ptr(val_table), ptr(literal_ids), ptr(literal_vals),
+                                      int(literal_ids.size(0)), int(max_passes), C.byref(ids),
+                                      stream_of(population)))

@@ -105,6 +105,22 @@ def structure_case(ref, dev, out_dir):
                         cases=cases, lens=lens, mad_eps=mad, **sel)
 
 
+def simplify_case(ref, dev, out_dir):
+    """simplify_batch on literal-rich programs (rules fire often), one and three passes."""
+    from test_simplify import _tables, literal_rich
+    g = tl.GPUGrammar(num_variables=3, operators=tl.ALL_OPERATORS)
+    pop = literal_rich(g, 3000, 48, 4343)
+    ar, vt, li, lv, ids = _tables(g)
+    args = [torch.from_numpy(a).to(dev) for a in (ar, vt, li, lv)]
+    outs = {}
+    for passes in (1, 3):
+        t = torch.from_numpy(pop.copy()).to(dev)
+        ref.simplify_batch(t, *args, passes, *[int(v) for v in ids])
+        outs["out_p%d" % passes] = t.cpu().numpy()
+    np.savez_compressed(os.path.join(out_dir, "ref_simplify.npz"), population=pop, arities=ar,
+                        val_table=vt, literal_ids=li, literal_vals=lv, ids=ids, **outs)
+
+
 def main():
     """One process per build variant: both builds export the same symbols, so loading them into
     one process would let the first one's kernels answer for the second."""
@@ -119,6 +135,7 @@ def main():
         fused_case(ref, variant, dev, out_dir)
         if variant == "fastmath":
             structure_case(ref, dev, out_dir)
+            simplify_case(ref, dev, out_dir)
         print("recorded", variant)
         return
     import subprocess
