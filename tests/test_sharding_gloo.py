@@ -1,0 +1,95 @@
+"""Multi-process (N > 1) host logic on CPU: world_size-2 gloo process groups.
+
+Each rank scores its own contiguous shard with the CPU oracle standing in for the GPU evaluator
+(no GPU here); the gathered fitness must equal a single-process evaluation of the whole
+population, for populations that do not divide evenly and for fewer programs than ranks; the
+timing reduction takes the maximum over ranks."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import ws_testlib as tl
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _case():
+    rng = np.random.default_rng(11)
+    g = tl.GPUGrammar(num_variables=2, operators=tl.C1_OPERATORS)
+    pop, consts = tl.random_population(g, 257, 24, 4, rng, valid_only=False)
+    X = rng.uniform(-3, 3, size=(2, 64)).astype(np.float32)
+    y = (X[0] * X[1]).astype(np.float32)
+    return g, pop, consts, X, y
+
+
+def _worker(rank, world, port, n_programs, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from warpsymbolic_b200.sharding import ShardedEvaluator, max_over_ranks, shard_bounds
+        g, pop, consts, X, y = _case()
+        pop, consts = pop[:n_programs], consts[:n_programs]
+        tm = tl.token_map(g)
+
+        def score(p, c):
+            if len(p) == 0:
+                return torch.empty(0, dtype=torch.float32)
+            return torch.from_numpy(tl.oracle.fitness(tm, p.numpy(), X, c.numpy(), y,
+                                                      policy="classic", loss="rmse"))
+
+        ev = ShardedEvaluator(score)
+        full = ev.evaluate(torch.from_numpy(pop), torch.from_numpy(consts))
+        local, (s, e) = ev.evaluate_local(torch.from_numpy(pop), torch.from_numpy(consts))
+        t = max_over_ranks(0.5 + rank)
+        q.put((rank, full.numpy(), (s, e), shard_bounds(n_programs, world, rank), t))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("n_programs", [257, 1])
+def test_two_rank_sharded_evaluation_matches_single_process(n_programs):
+    g, pop, consts, X, y = _case()
+    want = tl.oracle.fitness(tl.token_map(g), pop[:n_programs], X, consts[:n_programs], y,
+                             policy="classic", loss="rmse")
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, n_programs, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    bounds = {}
+    for rank, full, se, sb, t in res:
+        np.testing.assert_array_equal(full, want)
+        assert se == sb
+        bounds[rank] = se
+        assert t == 1.5
+    assert bounds[0][0] == 0 and bounds[0][1] == bounds[1][0] and bounds[1][1] == n_programs
+
+
+def test_shard_bounds_partition():
+    from warpsymbolic_b200.sharding import shard_bounds
+    for n in (0, 1, 7, 1 << 20):
+        for world in (1, 2, 3, 8):
+            b = [shard_bounds(n, world, r) for r in range(world)]
+            assert b[0][0] == 0 and b[-1][1] == n
+            assert all(b[i][1] == b[i + 1][0] for i in range(world - 1))
+            sizes = [e - s for s, e in b]
+            assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(ValueError):
+        shard_bounds(10, 2, 2)
