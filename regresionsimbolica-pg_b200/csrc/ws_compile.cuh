@@ -100,10 +100,12 @@ struct Frame {
 
 // ---- evaluator tape word (the lowering of the logical fields above) ---------------------
 //   [0:6)   dense case: 0 = NOP, 1..17 unary (cls - T_SIN + 1), 18..41 binary
-//           (18 + 4*(cls-T_ADD) + form)
+//           (18 + 4*(cls-T_ADD) + form); the binary forms AV and VA read a vector operand V
 //   [6]     SPILL: store ACC into spill slot [7:10) first
 //   [10]    LOADA_X: ACC <- X row at offset [12:21); [11] LOADA_S: ACC <- immediate
-//   [21]    FETCH: V <- shared row at offset [23:32), from a spill slot when [22] is set
+//   [21]    SLOW: any of SPILL, LOADA_X, LOADA_S, or V in a deep (global) spill slot -- the
+//           evaluator tests this one bit and skips all of them on the common path
+//   [22]    V is the spill slot [23:32) (else the X row at offset [23:32))
 // Offsets are in units of one pass (32*R rows): variable v of a chunk of RC rows sits at
 // v * (RC / pass), spill slot s at s.  Scalar operands are the immediate.  `xmul` = RC / pass
 // is fixed by the schedule before compiling.  Spill slots below kSharedSlots live in shared
@@ -115,13 +117,18 @@ enum : uint32_t {
   P_LOADA_X = 1u << 10,
   P_LOADA_S = 1u << 11,
   P_SH_LA = 12,
-  P_FETCH = 1u << 21,
+  P_SLOW = 1u << 21,
   P_FETCH_SLOT = 1u << 22,
   P_SH_V = 23,
   P_OFF_MASK = 0x1FFu,
 };
 enum { PCASE_NOP = 0, PCASE_UNARY0 = 1, PCASE_BIN = 18, PCASE_COUNT = 42 };
 constexpr int kSharedSlots = 2;
+
+// True for the cases that read the vector operand V (binary forms AV and VA).
+WS_HD bool pcase_fetches(uint32_t cs) {
+  return cs >= PCASE_BIN && ((cs - PCASE_BIN) & 3u) <= (uint32_t)FORM_VA;
+}
 
 WS_HD uint32_t lower_case(uint32_t logical) {
   const uint32_t c = logical & CASE_MASK;
@@ -139,14 +146,14 @@ struct Emitter {
   bool ok = true;  // false if an operand is not representable in the tape word
   WS_HD void put(uint32_t c, T imm) {
     uint32_t w = lower_case(c);
-    if (c & F_SPILL) w |= P_SPILL | (((c >> SH_SLOT) & 7u) << P_SH_SLOT);
+    if (c & F_SPILL) w |= P_SLOW | P_SPILL | (((c >> SH_SLOT) & 7u) << P_SH_SLOT);
     const uint32_t la = (c >> SH_LA) & 3u, lai = (c >> SH_LA_IDX) & 63u;
     if (la == LA_X) {
       const uint32_t off = lai * (uint32_t)xmul;
       ok = ok && off <= P_OFF_MASK;
-      w |= P_LOADA_X | ((off & P_OFF_MASK) << P_SH_LA);
+      w |= P_SLOW | P_LOADA_X | ((off & P_OFF_MASK) << P_SH_LA);
     } else if (la == LA_IMM) {
-      w |= P_LOADA_S;
+      w |= P_SLOW | P_LOADA_S;
     } else if (la == LA_PARAM) {
       ok = false;  // parameters are baked into immediates for this tape
     }
@@ -154,9 +161,10 @@ struct Emitter {
     if (opk == OK_X) {
       const uint32_t off = oi * (uint32_t)xmul;
       ok = ok && off <= P_OFF_MASK;
-      w |= P_FETCH | ((off & P_OFF_MASK) << P_SH_V);
+      w |= (off & P_OFF_MASK) << P_SH_V;
     } else if (opk == OK_SLOT) {
-      w |= P_FETCH | P_FETCH_SLOT | (oi << P_SH_V);
+      w |= P_FETCH_SLOT | (oi << P_SH_V);
+      if (oi >= (uint32_t)kSharedSlots) w |= P_SLOW;
     } else if (opk == OK_SCALAR && (c & F_OP_PARAM)) {
       ok = false;
     }

@@ -47,11 +47,11 @@ void run_host(const uint32_t* ctrl, const double* imm, int n, const T* x, int64_
       if (c & P_LOADA_X) acc = x[((c >> P_SH_LA) & P_OFF_MASK) * D + d];
       else if (c & P_LOADA_S) acc = im;
       T v = im;
-      if (c & P_FETCH) {
+      const uint32_t cs = c & P_CASE_MASK;
+      if (pcase_fetches(cs)) {
         const uint32_t off = c >> P_SH_V;
         v = (c & P_FETCH_SLOT) ? slots[off & 31u] : x[off * D + d];
       }
-      const uint32_t cs = c & P_CASE_MASK;
       bool e = false;
       if (cs == PCASE_NOP) {
       } else if (cs >= PCASE_BIN) {

@@ -172,49 +172,119 @@ __device__ __forceinline__ double fma_rn(double a, double b, double c) { return 
 __device__ __forceinline__ float m_max(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ double m_max(double a, double b) { return fmax(a, b); }
 
+// Paired FP32 arithmetic (sm_100 f32x2): two rows per instruction, each lane rounded exactly as
+// the scalar add / sub / mul of this translation unit (round to nearest, subnormals flushed, as
+// --use_fast_math compiles them), so pairing changes instruction counts, not results.
+#define WS_PAIR_ASM(OP)                                                                   \
+  asm("{\n .reg .b64 p, q;\n mov.b64 p, {%0, %1};\n mov.b64 q, {%2, %3};\n " OP      \
+      " p, p, q;\n mov.b64 {%0, %1}, p;\n}"                                             \
+      : "+f"(a0), "+f"(a1)                                                                \
+      : "f"(b0), "f"(b1))
+__device__ __forceinline__ void pair_add(float& a0, float& a1, float b0, float b1) {
+  WS_PAIR_ASM("add.rn.ftz.f32x2");
+}
+__device__ __forceinline__ void pair_sub(float& a0, float& a1, float b0, float b1) {
+  WS_PAIR_ASM("sub.rn.ftz.f32x2");
+}
+__device__ __forceinline__ void pair_mul(float& a0, float& a1, float b0, float b1) {
+  WS_PAIR_ASM("mul.rn.ftz.f32x2");
+}
+#undef WS_PAIR_ASM
+
+// a = a OP b (REV: a = b OP a) for rows k, k+1; OPK 0 add, 1 sub, 2 mul.
+template <int OPK, bool REV>
+__device__ __forceinline__ void pair_apply(float& a0, float& a1, float b0, float b1) {
+  if (OPK == 0) {
+    pair_add(a0, a1, b0, b1);
+  } else if (OPK == 2) {
+    pair_mul(a0, a1, b0, b1);
+  } else if (!REV) {
+    pair_sub(a0, a1, b0, b1);
+  } else {
+    float t0 = b0, t1 = b1;
+    pair_sub(t0, t1, a0, a1);
+    a0 = t0;
+    a1 = t1;
+  }
+}
+
 // Runs one program tape over one pass of 32*R rows.  xb: the X tile at this pass and lane;
 // sb / gb: this warp's shared / global spill slots at this lane.  Tape offsets are in units
-// of one pass.
+// of one pass.  A fetched operand is read group by group inside its case (16-byte loads), so
+// only one group of it is live at a time: registers go to the R accumulators instead.
 template <typename T, int R, bool STRICT>
 __device__ __forceinline__ void run_tape(const Instr<T>* __restrict__ tp, int n,
                                          const T* __restrict__ xb, T* __restrict__ sb,
                                          T* __restrict__ gb, T (&acc)[R], uint32_t& err) {
   constexpr int PASS = 32 * R;
+  constexpr int N = Vec16<T>::N;
+  constexpr bool PAIR = sizeof(T) == 4;
   err = 0u;
-  // The next tape word is loaded while the current one executes.
+  // The next tape word is loaded while the current one executes (reading one word past the end
+  // of a tape stays inside the block's shared memory and is never used).
   Instr<T> nxt = tp[0];
 #pragma unroll 1
   for (int i = 0; i < n; ++i) {
     const Instr<T> ins = nxt;
-    nxt = tp[i + 1 < n ? i + 1 : i];
+    nxt = tp[i + 1];
     const uint32_t c = ins.ctrl;
-    if (c & P_SPILL) {
-      const uint32_t sl = (c >> P_SH_SLOT) & 7u;
-      if (sl < (uint32_t)kSharedSlots) lane_store<T, R>(sb + sl * PASS, acc);
-      else lane_store<T, R>(gb + (sl - kSharedSlots) * PASS, acc);
-    }
-    if (c & P_LOADA_X) {
-      lane_load<T, R>(acc, xb + ((c >> P_SH_LA) & P_OFF_MASK) * PASS);
-    } else if (c & P_LOADA_S) {
+    // vector operand: an X row of the tile or a shared spill slot (dereferenced only by the
+    // cases that read it)
+    const T* vp = ((c & P_FETCH_SLOT) ? sb : xb) + (c >> P_SH_V) * PASS;
+    if (c & P_SLOW) {  // spill, accumulator load, deep spill slot: rare
+      if (c & P_SPILL) {
+        const uint32_t sl = (c >> P_SH_SLOT) & 7u;
+        if (sl < (uint32_t)kSharedSlots) lane_store<T, R>(sb + sl * PASS, acc);
+        else lane_store<T, R>(gb + (sl - kSharedSlots) * PASS, acc);
+      }
+      if (c & P_LOADA_X) {
+        lane_load<T, R>(acc, xb + ((c >> P_SH_LA) & P_OFF_MASK) * PASS);
+      } else if (c & P_LOADA_S) {
 #pragma unroll
-      for (int k = 0; k < R; ++k) acc[k] = ins.imm;
-    }
-    T v[R];
-    if (c & P_FETCH) {
+        for (int k = 0; k < R; ++k) acc[k] = ins.imm;
+      }
       const uint32_t off = c >> P_SH_V;
-      if (!(c & P_FETCH_SLOT)) lane_load<T, R>(v, xb + off * PASS);
-      else if (off < (uint32_t)kSharedSlots) lane_load<T, R>(v, sb + off * PASS);
-      else lane_load<T, R>(v, gb + (off - kSharedSlots) * PASS);
+      if ((c & P_FETCH_SLOT) && off >= (uint32_t)kSharedSlots) vp = gb + (off - kSharedSlots) * PASS;
     }
     const T s = ins.imm;
 
 #define WS_ROWS(BODY) _Pragma("unroll") for (int k = 0; k < R; ++k) { BODY; } break
+// rows with a fetched operand: group g of the operand is loaded, then used as v[q]
+#define WS_ROWS_V(BODY)                                                        \
+  _Pragma("unroll") for (int g = 0; g < R / N; ++g) {                          \
+    T v[N];                                                                    \
+    Vec16<T>::load(v, vp + g * 32 * N);                                        \
+    _Pragma("unroll") for (int q = 0; q < N; ++q) { const int k = g * N + q; BODY; } \
+  }                                                                            \
+  break
+#define WS_PAIRS_V(OPK, REV)                                                   \
+  _Pragma("unroll") for (int g = 0; g < R / N; ++g) {                          \
+    float v[N];                                                                \
+    Vec16<float>::load(v, (const float*)vp + g * 32 * N);                      \
+    _Pragma("unroll") for (int q = 0; q < N; q += 2)                           \
+      pair_apply<OPK, REV>(*(float*)&acc[g * N + q], *(float*)&acc[g * N + q + 1], v[q], v[q + 1]); \
+  }                                                                            \
+  break
+#define WS_PAIRS_S(OPK, REV)                                                   \
+  _Pragma("unroll") for (int k = 0; k < R; k += 2)                             \
+    pair_apply<OPK, REV>(*(float*)&acc[k], *(float*)&acc[k + 1], (float)s, (float)s); \
+  break
 #define WS_ERR(EXPR) { bool e_ = false; acc[k] = (EXPR); err |= (uint32_t)e_ << k; }
 #define WS_BIN4(CLS, F)                                                          \
-  case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_AV: WS_ROWS(F(acc[k], v[k]));        \
-  case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_VA: WS_ROWS(F(v[k], acc[k]));        \
+  case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_AV: WS_ROWS_V(F(acc[k], v[q]));      \
+  case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_VA: WS_ROWS_V(F(v[q], acc[k]));      \
   case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_AS: WS_ROWS(F(acc[k], s));           \
   case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_SA: WS_ROWS(F(s, acc[k]));
+// + - *: paired when T is float
+#define WS_BIN4P(CLS, F, OPK)                                                    \
+  case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_AV:                                  \
+    if (PAIR) { WS_PAIRS_V(OPK, false); } else { WS_ROWS_V(F(acc[k], v[q])); }   \
+  case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_VA:                                  \
+    if (PAIR) { WS_PAIRS_V(OPK, true); } else { WS_ROWS_V(F(v[q], acc[k])); }    \
+  case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_AS:                                  \
+    if (PAIR) { WS_PAIRS_S(OPK, false); } else { WS_ROWS(F(acc[k], s)); }        \
+  case PCASE_BIN + 4 * (CLS - T_ADD) + FORM_SA:                                  \
+    if (PAIR) { WS_PAIRS_S(OPK, true); } else { WS_ROWS(F(s, acc[k])); }
 #define F_ADD(a, b) acc[k] = (a) + (b)
 #define F_SUB(a, b) acc[k] = (a) - (b)
 #define F_MUL(a, b) acc[k] = (a) * (b)
@@ -224,9 +294,9 @@ __device__ __forceinline__ void run_tape(const Instr<T>* __restrict__ tp, int n,
 #define U_(CLS) (PCASE_UNARY0 + (CLS - T_SIN))
     switch (c & P_CASE_MASK) {
       case PCASE_NOP: break;
-      WS_BIN4(T_ADD, F_ADD)
-      WS_BIN4(T_SUB, F_SUB)
-      WS_BIN4(T_MUL, F_MUL)
+      WS_BIN4P(T_ADD, F_ADD, 0)
+      WS_BIN4P(T_SUB, F_SUB, 1)
+      WS_BIN4P(T_MUL, F_MUL, 2)
       WS_BIN4(T_DIV, F_DIV)
       WS_BIN4(T_POW, F_POW)
       WS_BIN4(T_MOD, F_MOD)
@@ -257,7 +327,11 @@ __device__ __forceinline__ void run_tape(const Instr<T>* __restrict__ tp, int n,
 #undef F_POW
 #undef F_MOD
 #undef WS_BIN4
+#undef WS_BIN4P
+#undef WS_PAIRS_V
+#undef WS_PAIRS_S
 #undef WS_ERR
+#undef WS_ROWS_V
 #undef WS_ROWS
   }
 }
@@ -606,6 +680,9 @@ constexpr Sched kSched[] = {
     {16, 8, 32, 100 * 1024},  // 4
     {8, 8, 64, 100 * 1024},   // 5
     {16, 4, 32, 72 * 1024},   // 6
+    {32, 8, 32, 100 * 1024},  // 7
+    {32, 4, 16, 100 * 1024},  // 8
+    {32, 8, 32, 140 * 1024},  // 9
 };
 constexpr int kNumSched = (int)(sizeof(kSched) / sizeof(kSched[0]));
 
@@ -820,6 +897,10 @@ ws_status launch_sched(const FitnessRequest& rq) {
     return launch_typed<T, 8, STRICT>(rq, sc);
   } else {
     if (sc.R == 8) return launch_typed<T, 8, STRICT>(rq, sc);
+    if constexpr (!STRICT) {
+      if (sc.R == 32) return launch_typed<T, 32, STRICT>(rq, sc);
+    }
+    sc.R = 16;  // 32-row passes are compiled for the protected operators only
     return launch_typed<T, 16, STRICT>(rq, sc);
   }
 }
