@@ -14,15 +14,19 @@
 //                         tile (cp.async) while the current one is evaluated.  Warp w runs programs
 //                         w, w+W, ... of the block (balanced: similar lengths) over the chunk in
 //                         passes of 32*R rows (R rows per lane, 16-byte conflict-free shared
-//                         loads), accumulating squared errors in FP64.  Per-program partials are
-//                         combined in a fixed order, so results do not depend on the schedule or
-//                         on what else is in the batch (up to FP64 rounding of the sum).
+//                         loads), accumulating squared errors in FP64 per lane.  Per-lane
+//                         partials live in shared memory across chunks and are combined once per
+//                         block in a fixed order, so results do not depend on the schedule or on
+//                         what else is in the batch (up to FP64 rounding of the sum).
+//                         Programs whose spill slots all fit in shared memory (all but ~0.2% of
+//                         random 64-token programs) run an FP32 interpreter that addresses its
+//                         operands, spill slots and tape words as 32-bit shared addresses.
 //
 // Per-row values are bit-identical to the reference kernels when this file is compiled with
 // the reference's flags (--use_fast_math): same operator code (ws_ops.cuh), same FP32 rounding
 // of pred - y and of its square.  Only the order of the sum differs: each lane sums the R
-// squared errors of a pass in T, passes and lanes are combined in FP64 (the reference sums in
-// FP32 warp butterflies).
+// squared errors of a pass in T (two interleaved partial sums for FP32), passes and lanes are
+// combined in FP64 (the reference sums in FP32 warp butterflies).
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
@@ -41,6 +45,11 @@ struct alignas(16) PartRec {
   int32_t ninv;
   int32_t ovf;
 };
+// per-program per-lane partial sums: row stride of 33 doubles (conflict-free column reads)
+constexpr int kLaneStride = 33;
+// shared meta word of a staged program: tape length, and a flag for global spill slots
+constexpr int kMetaLenMask = 0xFFFF;
+constexpr int kMetaGlobalSpill = 1 << 16;
 
 // ---------------------------------------------------------------------------------------
 // 1. compile
@@ -208,61 +217,62 @@ __device__ __forceinline__ void pair_apply(float& a0, float& a1, float b0, float
   }
 }
 
-// Runs one program tape over one pass of 32*R rows.  xb: the X tile at this pass and lane;
-// sb / gb: this warp's shared / global spill slots at this lane.  Tape offsets are in units
-// of one pass.  A fetched operand is read group by group inside its case (16-byte loads), so
-// only one group of it is live at a time: registers go to the R accumulators instead.
-template <typename T, int R, bool STRICT>
-__device__ __forceinline__ void run_tape(const Instr<T>* __restrict__ tp, int n,
-                                         const T* __restrict__ xb, T* __restrict__ sb,
-                                         T* __restrict__ gb, T (&acc)[R], uint32_t& err) {
-  constexpr int PASS = 32 * R;
+// ---- shared-memory access by 32-bit address ------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void lds4(float (&d)[4], uint32_t a) {
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+               : "r"(a));
+}
+__device__ __forceinline__ void sts4(uint32_t a, float d0, float d1, float d2, float d3) {
+  asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(a), "f"(d0), "f"(d1), "f"(d2),
+               "f"(d3)
+               : "memory");
+}
+__device__ __forceinline__ void lds_word(uint32_t& c, uint32_t& imm, uint32_t a) {
+  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(c), "=r"(imm) : "r"(a));
+}
+
+// Vector-operand loaders: group g (16 bytes) of this lane's rows of operand V.
+template <typename T>
+struct GenericOperand {  // V anywhere (shared X tile, shared or global spill slot)
+  const T* vp;
+  __device__ __forceinline__ void load(T (&v)[Vec16<T>::N], int g) const {
+    Vec16<T>::load(v, vp + g * 32 * Vec16<T>::N);
+  }
+};
+struct SharedOperand {  // V in shared memory at a 32-bit address (FP32)
+  uint32_t va;
+  __device__ __forceinline__ void load(float (&v)[4], int g) const { lds4(v, va + g * 512); }
+};
+
+// One tape instruction's operator over this lane's R rows: ACC = ACC o V / V o ACC / ACC o s /
+// s o ACC for binary cases, ACC = f(ACC) for unary ones.  A fetched operand is read group by
+// group inside its case (16-byte loads), so only one group of it is live at a time: registers
+// go to the R accumulators instead.
+template <typename T, int R, bool STRICT, class LD>
+__device__ __forceinline__ void exec_case(uint32_t cs, T s, const LD& ld, T (&acc)[R],
+                                          uint32_t& err) {
   constexpr int N = Vec16<T>::N;
   constexpr bool PAIR = sizeof(T) == 4;
-  err = 0u;
-  // The next tape word is loaded while the current one executes (reading one word past the end
-  // of a tape stays inside the block's shared memory and is never used).
-  Instr<T> nxt = tp[0];
-#pragma unroll 1
-  for (int i = 0; i < n; ++i) {
-    const Instr<T> ins = nxt;
-    nxt = tp[i + 1];
-    const uint32_t c = ins.ctrl;
-    // vector operand: an X row of the tile or a shared spill slot (dereferenced only by the
-    // cases that read it)
-    const T* vp = ((c & P_FETCH_SLOT) ? sb : xb) + (c >> P_SH_V) * PASS;
-    if (c & P_SLOW) {  // spill, accumulator load, deep spill slot: rare
-      if (c & P_SPILL) {
-        const uint32_t sl = (c >> P_SH_SLOT) & 7u;
-        if (sl < (uint32_t)kSharedSlots) lane_store<T, R>(sb + sl * PASS, acc);
-        else lane_store<T, R>(gb + (sl - kSharedSlots) * PASS, acc);
-      }
-      if (c & P_LOADA_X) {
-        lane_load<T, R>(acc, xb + ((c >> P_SH_LA) & P_OFF_MASK) * PASS);
-      } else if (c & P_LOADA_S) {
-#pragma unroll
-        for (int k = 0; k < R; ++k) acc[k] = ins.imm;
-      }
-      const uint32_t off = c >> P_SH_V;
-      if ((c & P_FETCH_SLOT) && off >= (uint32_t)kSharedSlots) vp = gb + (off - kSharedSlots) * PASS;
-    }
-    const T s = ins.imm;
-
 #define WS_ROWS(BODY) _Pragma("unroll") for (int k = 0; k < R; ++k) { BODY; } break
 // rows with a fetched operand: group g of the operand is loaded, then used as v[q]
 #define WS_ROWS_V(BODY)                                                        \
   _Pragma("unroll") for (int g = 0; g < R / N; ++g) {                          \
     T v[N];                                                                    \
-    Vec16<T>::load(v, vp + g * 32 * N);                                        \
+    ld.load(v, g);                                                             \
     _Pragma("unroll") for (int q = 0; q < N; ++q) { const int k = g * N + q; BODY; } \
   }                                                                            \
   break
 #define WS_PAIRS_V(OPK, REV)                                                   \
   _Pragma("unroll") for (int g = 0; g < R / N; ++g) {                          \
-    float v[N];                                                                \
-    Vec16<float>::load(v, (const float*)vp + g * 32 * N);                      \
+    T v[N];                                                                    \
+    ld.load(v, g);                                                             \
     _Pragma("unroll") for (int q = 0; q < N; q += 2)                           \
-      pair_apply<OPK, REV>(*(float*)&acc[g * N + q], *(float*)&acc[g * N + q + 1], v[q], v[q + 1]); \
+      pair_apply<OPK, REV>(*(float*)&acc[g * N + q], *(float*)&acc[g * N + q + 1], \
+                           *(float*)&v[q], *(float*)&v[q + 1]);                \
   }                                                                            \
   break
 #define WS_PAIRS_S(OPK, REV)                                                   \
@@ -292,33 +302,34 @@ __device__ __forceinline__ void run_tape(const Instr<T>* __restrict__ tp, int n,
 #define F_POW(a, b) WS_ERR((op_pow<T, STRICT>((a), (b), e_)))
 #define F_MOD(a, b) WS_ERR((op_mod<T, STRICT>((a), (b), e_)))
 #define U_(CLS) (PCASE_UNARY0 + (CLS - T_SIN))
-    switch (c & P_CASE_MASK) {
-      case PCASE_NOP: break;
-      WS_BIN4P(T_ADD, F_ADD, 0)
-      WS_BIN4P(T_SUB, F_SUB, 1)
-      WS_BIN4P(T_MUL, F_MUL, 2)
-      WS_BIN4(T_DIV, F_DIV)
-      WS_BIN4(T_POW, F_POW)
-      WS_BIN4(T_MOD, F_MOD)
-      case U_(T_SIN): WS_ROWS(acc[k] = m_sin(acc[k]));
-      case U_(T_COS): WS_ROWS(acc[k] = m_cos(acc[k]));
-      case U_(T_TAN): WS_ROWS(acc[k] = m_tan(acc[k]));
-      case U_(T_LOG): WS_ROWS(WS_ERR((op_log<T, STRICT>(acc[k], e_))));
-      case U_(T_EXP): WS_ROWS(WS_ERR((op_exp<T, STRICT>(acc[k], e_))));
-      case U_(T_SQRT): WS_ROWS(WS_ERR((op_sqrt<T, STRICT>(acc[k], e_))));
-      case U_(T_ABS): WS_ROWS(acc[k] = m_abs(acc[k]));
-      case U_(T_NEG): WS_ROWS(acc[k] = -acc[k]);
-      case U_(T_FACT): WS_ROWS(WS_ERR((op_tgamma<T, STRICT>(acc[k] + (T)1.0, e_))));
-      case U_(T_FLOOR): WS_ROWS(acc[k] = m_floor(acc[k]));
-      case U_(T_CEIL): WS_ROWS(acc[k] = m_ceil(acc[k]));
-      case U_(T_SIGN): WS_ROWS(acc[k] = op_sign<T>(acc[k]));
-      case U_(T_GAMMA): WS_ROWS(WS_ERR((op_tgamma<T, STRICT>(acc[k], e_))));
-      case U_(T_LGAMMA): WS_ROWS(WS_ERR((op_lgamma<T, STRICT>(acc[k], e_))));
-      case U_(T_ASIN): WS_ROWS(WS_ERR((op_asin<T, STRICT>(acc[k], e_))));
-      case U_(T_ACOS): WS_ROWS(WS_ERR((op_acos<T, STRICT>(acc[k], e_))));
-      case U_(T_ATAN): WS_ROWS(acc[k] = m_atan(acc[k]));
-      default: err = 0xFFFFFFFFu; break;  // malformed tape: every row invalid
-    }
+  switch (cs) {
+    case PCASE_NOP: break;
+    WS_BIN4P(T_ADD, F_ADD, 0)
+    WS_BIN4P(T_SUB, F_SUB, 1)
+    WS_BIN4P(T_MUL, F_MUL, 2)
+    WS_BIN4(T_DIV, F_DIV)
+    WS_BIN4(T_POW, F_POW)
+    WS_BIN4(T_MOD, F_MOD)
+    case U_(T_SIN): WS_ROWS(acc[k] = m_sin(acc[k]));
+    case U_(T_COS): WS_ROWS(acc[k] = m_cos(acc[k]));
+    case U_(T_TAN): WS_ROWS(acc[k] = m_tan(acc[k]));
+    case U_(T_LOG): WS_ROWS(WS_ERR((op_log<T, STRICT>(acc[k], e_))));
+    case U_(T_EXP): WS_ROWS(WS_ERR((op_exp<T, STRICT>(acc[k], e_))));
+    case U_(T_SQRT): WS_ROWS(WS_ERR((op_sqrt<T, STRICT>(acc[k], e_))));
+    case U_(T_ABS): WS_ROWS(acc[k] = m_abs(acc[k]));
+    case U_(T_NEG): WS_ROWS(acc[k] = -acc[k]);
+    case U_(T_FACT): WS_ROWS(WS_ERR((op_tgamma<T, STRICT>(acc[k] + (T)1.0, e_))));
+    case U_(T_FLOOR): WS_ROWS(acc[k] = m_floor(acc[k]));
+    case U_(T_CEIL): WS_ROWS(acc[k] = m_ceil(acc[k]));
+    case U_(T_SIGN): WS_ROWS(acc[k] = op_sign<T>(acc[k]));
+    case U_(T_GAMMA): WS_ROWS(WS_ERR((op_tgamma<T, STRICT>(acc[k], e_))));
+    case U_(T_LGAMMA): WS_ROWS(WS_ERR((op_lgamma<T, STRICT>(acc[k], e_))));
+    case U_(T_ASIN): WS_ROWS(WS_ERR((op_asin<T, STRICT>(acc[k], e_))));
+    case U_(T_ACOS): WS_ROWS(WS_ERR((op_acos<T, STRICT>(acc[k], e_))));
+    case U_(T_ATAN): WS_ROWS(acc[k] = m_atan(acc[k]));
+    // the compiler emits only the cases above (the tape's case field is 6 bits; 42..63 unused)
+    default: __builtin_unreachable();
+  }
 #undef U_
 #undef F_ADD
 #undef F_SUB
@@ -333,6 +344,96 @@ __device__ __forceinline__ void run_tape(const Instr<T>* __restrict__ tp, int n,
 #undef WS_ERR
 #undef WS_ROWS_V
 #undef WS_ROWS
+}
+
+// Runs one program tape over one pass of 32*R rows (any T, any spill depth).  xb: the X tile
+// at this pass and lane; sb / gb: this warp's shared / global spill slots at this lane.  Tape
+// offsets are in units of one pass.
+template <typename T, int R, bool STRICT>
+__device__ __forceinline__ void run_tape(const Instr<T>* __restrict__ tp, int n,
+                                         const T* __restrict__ xb, T* __restrict__ sb,
+                                         T* __restrict__ gb, T (&acc)[R], uint32_t& err) {
+  constexpr int PASS = 32 * R;
+  err = 0u;
+  // The next tape word is loaded while the current one executes (reading one word past the end
+  // of a tape stays inside the block's shared memory and is never used).
+  Instr<T> nxt = tp[0];
+#pragma unroll 1
+  for (int i = 0; i < n; ++i) {
+    const Instr<T> ins = nxt;
+    nxt = tp[i + 1];
+    const uint32_t c = __shfl_sync(0xFFFFFFFFu, ins.ctrl, 0);  // warp-uniform by construction
+    // vector operand: an X row of the tile or a shared spill slot (dereferenced only by the
+    // cases that read it)
+    const T* vp = ((c & P_FETCH_SLOT) ? sb : xb) + (c >> P_SH_V) * PASS;
+    if (c & P_SLOW) {  // spill, accumulator load, deep spill slot: rare
+      if (c & P_SPILL) {
+        const uint32_t sl = (c >> P_SH_SLOT) & 7u;
+        if (sl < (uint32_t)kSharedSlots) lane_store<T, R>(sb + sl * PASS, acc);
+        else lane_store<T, R>(gb + (sl - kSharedSlots) * PASS, acc);
+      }
+      if (c & P_LOADA_X) {
+        lane_load<T, R>(acc, xb + ((c >> P_SH_LA) & P_OFF_MASK) * PASS);
+      } else if (c & P_LOADA_S) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) acc[k] = ins.imm;
+      }
+      const uint32_t off = c >> P_SH_V;
+      if ((c & P_FETCH_SLOT) && off >= (uint32_t)kSharedSlots) vp = gb + (off - kSharedSlots) * PASS;
+    }
+    exec_case<T, R, STRICT>(c & P_CASE_MASK, ins.imm, GenericOperand<T>{vp}, acc, err);
+  }
+}
+
+// The FP32 interpreter for programs whose spill slots are all in shared memory (every program
+// but the deepest 0.2%): operands, spill slots and tape words are addressed as 32-bit shared
+// addresses.  xa: X tile at this pass and lane; sa: this warp's spill slot 0 at this lane; ta:
+// the tape.  One pass is 32*R rows = PASS*4 bytes = 1 << PSH.
+template <int R, bool STRICT>
+__device__ __forceinline__ void run_tape_shared(uint32_t ta, int n, uint32_t xa, uint32_t sa,
+                                                float (&acc)[R], uint32_t& err) {
+  static_assert(R == 8 || R == 16 || R == 32, "pass size");
+  constexpr int PSH = R == 8 ? 10 : (R == 16 ? 11 : 12);
+  err = 0u;
+  // software-pipelined decode: the next word is broadcast and its operand address computed
+  // while the current case executes; the word after it is already in flight
+  uint32_t nc, ni, c1, n1;
+  lds_word(c1, n1, ta);
+  lds_word(nc, ni, ta + 8u);
+  uint32_t cn = __shfl_sync(0xFFFFFFFFu, c1, 0);  // warp-uniform by construction
+  float sn = __uint_as_float(n1);
+  uint32_t van = ((cn & P_FETCH_SLOT) ? sa : xa) + ((cn >> P_SH_V) << PSH);
+#pragma unroll 1
+  for (int i = 0; i < n; ++i) {
+    const uint32_t c = cn;
+    const float s = sn;
+    const uint32_t va = van;
+    cn = __shfl_sync(0xFFFFFFFFu, nc, 0);
+    sn = __uint_as_float(ni);
+    van = ((cn & P_FETCH_SLOT) ? sa : xa) + ((cn >> P_SH_V) << PSH);
+    ta += 8u;
+    lds_word(nc, ni, ta + 8u);  // up to two words past the end: inside the block's smem
+    if (c & P_SLOW) {  // spill, accumulator load: rare
+      if (c & P_SPILL) {
+        const uint32_t a = sa + (((c >> P_SH_SLOT) & 7u) << PSH);
+#pragma unroll
+        for (int g = 0; g < R / 4; ++g)
+          sts4(a + g * 512, acc[4 * g], acc[4 * g + 1], acc[4 * g + 2], acc[4 * g + 3]);
+      }
+      if (c & P_LOADA_X) {
+        const uint32_t a = xa + (((c >> P_SH_LA) & P_OFF_MASK) << PSH);
+#pragma unroll
+        for (int g = 0; g < R / 4; ++g) {
+          float v[4];
+          lds4(v, a + g * 512);
+          acc[4 * g] = v[0]; acc[4 * g + 1] = v[1]; acc[4 * g + 2] = v[2]; acc[4 * g + 3] = v[3];
+        }
+      } else if (c & P_LOADA_S) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) acc[k] = s;
+      }
+    }
+    exec_case<float, R, STRICT>(c & P_CASE_MASK, s, SharedOperand{va}, acc, err);
   }
 }
 
@@ -392,6 +493,30 @@ __device__ __forceinline__ T pass_fast(const T (&a)[R], const T* __restrict__ yb
       ovfacc = fma_rn(diff, (T)0, ovfacc);
       dmax = m_max(dmax, m_abs(diff));
     }
+  }
+  return part;
+}
+
+// Paired fast epilogue (FP32, classic policy): diff, square and the running sums two rows per
+// instruction, each row rounded as the scalar code rounds it.  A non-finite prediction makes
+// the pass sum non-finite (NaN, or +inf: squares are >= 0), so rows are only re-examined then.
+template <int R>
+__device__ __forceinline__ float pass_fast_pairs(const float (&a)[R], const float* __restrict__ yb,
+                                                 bool& bad) {
+  float yv[R];
+  lane_load<float, R>(yv, yb);
+  float p0 = 0.f, p1 = 0.f;
+#pragma unroll
+  for (int k = 0; k < R; k += 2) {
+    float d0 = a[k], d1 = a[k + 1];
+    pair_sub(d0, d1, yv[k], yv[k + 1]);
+    pair_mul(d0, d1, d0, d1);
+    pair_add(p0, p1, d0, d1);
+  }
+  const float part = p0 + p1;
+  if (!(part <= 3.4028234663852886e38f)) {
+#pragma unroll
+    for (int k = 0; k < R; ++k) bad = bad || !(fabsf(a[k]) <= 3.4028234663852886e38f);
   }
   return part;
 }
@@ -479,19 +604,25 @@ __device__ __forceinline__ void stage_chunk(const FitParams<T>& P, int64_t c, T*
 }
 
 template <typename T, int R, bool STRICT>
-__global__ void __launch_bounds__(256) fitness_kernel(const FitParams<T> P) {
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2) fitness_kernel(const FitParams<T> P) {
   constexpr int N = Vec16<T>::N;
   constexpr int PASS = 32 * R;
+  constexpr bool F32 = sizeof(T) == 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int W = blockDim.x >> 5;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // two tiles of X[:, chunk] and y[chunk] (double-buffered staging), then per-warp spill slots
+  // warp index broadcast from lane 0: the compiler then treats it (and the tape addresses
+  // derived from it) as warp-uniform
+  const int warp = __shfl_sync(0xFFFFFFFFu, (int)(threadIdx.x >> 5), 0);
+  const int lane = threadIdx.x & 31;
+  // two tiles of X[:, chunk] and y[chunk] (double-buffered staging), per-warp spill slots, the
+  // block's tapes, per-program records, per-program per-lane FP64 partial sums
   const size_t tile_elems = (size_t)(P.V + 1) * P.RC;
   T* tiles = reinterpret_cast<T*>(smem_raw);
   T* spill = tiles + 2 * tile_elems;
   Instr<T>* tapes = reinterpret_cast<Instr<T>*>(spill + (size_t)W * kSharedSlots * PASS);
   PartRec* acc_s = reinterpret_cast<PartRec*>(tapes + (size_t)P.PB * P.Lcap);
-  int* meta_s = reinterpret_cast<int*>(acc_s + P.PB);  // per program: n_instr, or -1 if invalid
+  double* lane_sse = reinterpret_cast<double*>(acc_s + P.PB);  // [PB][kLaneStride]
+  int* meta_s = reinterpret_cast<int*>(lane_sse + (size_t)P.PB * kLaneStride);
   __shared__ int64_t s_item;
 
   T* sp_w = spill + (size_t)warp * kSharedSlots * PASS + lane * N;
@@ -517,8 +648,12 @@ __global__ void __launch_bounds__(256) fitness_kernel(const FitParams<T> P) {
       const ProgHdr h = P.hdr[p];
       const Instr<T>* tg = P.tape + p * (int64_t)P.Lcap;
       for (int i = lane; i < h.n_instr; i += 32) tapes[(size_t)q * P.Lcap + i] = tg[i];
+      lane_sse[q * kLaneStride + lane] = 0.0;
       if (lane == 0) {
-        meta_s[q] = h.status == PROG_OK ? h.n_instr : -1;
+        // n_instr, kMetaGlobalSpill if a spill slot lives in global memory; -1: invalid
+        meta_s[q] = h.status == PROG_OK
+                        ? (h.n_instr | (h.n_slots > kSharedSlots ? kMetaGlobalSpill : 0))
+                        : -1;
         acc_s[q] = PartRec{0.0, 0, 0};
       }
     }
@@ -544,27 +679,46 @@ __global__ void __launch_bounds__(256) fitness_kernel(const FitParams<T> P) {
       const int npass = (rows + PASS - 1) / PASS;
 
       for (int q = warp; q < np; q += W) {
-        const int n_instr = meta_s[q];
-        if (n_instr < 0) {
+        const int meta = meta_s[q];
+        if (meta < 0) {
           if (lane == 0) acc_s[q].ninv += rows;
           continue;
         }
+        const int n_instr = meta & kMetaLenMask;
+        const bool shared_only = F32 && !(meta & kMetaGlobalSpill);
         const Instr<T>* tape_q = tapes + (size_t)q * P.Lcap;
         double sse = 0.0;
         int ninv = 0;
-        bool ovf = false;
+        bool ovf = false, nonfinite = false;
         uint32_t errany = 0u;
         T nanacc = (T)0, ovfacc = (T)0, dmax = (T)0;
         for (int pass = 0; pass < npass; ++pass) {
           T a[R];
           uint32_t err;
-          run_tape<T, R, STRICT>(tape_q, n_instr, xs + pass * PASS + lane * N, sp_w, gsp_w, a, err);
+          if constexpr (F32) {
+            if (shared_only)
+              run_tape_shared<R, STRICT>(smem_u32(tape_q), n_instr,
+                                         smem_u32(xs + pass * PASS + lane * N), smem_u32(sp_w),
+                                         *reinterpret_cast<float(*)[R]>(&a), err);
+            else
+              run_tape<T, R, STRICT>(tape_q, n_instr, xs + pass * PASS + lane * N, sp_w, gsp_w,
+                                     a, err);
+          } else {
+            run_tape<T, R, STRICT>(tape_q, n_instr, xs + pass * PASS + lane * N, sp_w, gsp_w, a,
+                                   err);
+          }
           const T* yb = ys + pass * PASS + lane * N;
           T part;
           if (!P.count && (pass + 1) * PASS <= rows) {
             errany |= err;
-            part = fused_policy ? pass_fast<T, R, true>(a, yb, nanacc, ovfacc, dmax)
-                                : pass_fast<T, R, false>(a, yb, nanacc, ovfacc, dmax);
+            if (fused_policy) {
+              part = pass_fast<T, R, true>(a, yb, nanacc, ovfacc, dmax);
+            } else if constexpr (F32) {
+              part = pass_fast_pairs<R>(*reinterpret_cast<const float(*)[R]>(&a),
+                                        reinterpret_cast<const float*>(yb), nonfinite);
+            } else {
+              part = pass_fast<T, R, false>(a, yb, nanacc, ovfacc, dmax);
+            }
           } else {
             part = fused_policy
                 ? pass_epilogue<T, R, true>(a, err, yb, lane, pass * PASS, rows, ninv, ovf)
@@ -572,18 +726,19 @@ __global__ void __launch_bounds__(256) fitness_kernel(const FitParams<T> P) {
           }
           sse += (double)part;
         }
-        if (errany != 0u || m_isnan(nanacc)) ninv += 1;  // only "> 0" matters without counting
-        ovf = ovf || m_isnan(ovfacc) || dmax > Limits<T>::max_diff;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          sse += __shfl_xor_sync(0xFFFFFFFFu, sse, o);
-          ninv += __shfl_xor_sync(0xFFFFFFFFu, ninv, o);
+        // this lane's partial sum of the program, in a fixed per-lane order across chunks
+        lane_sse[q * kLaneStride + lane] += sse;
+        // without per-row counts only "ninv > 0" matters
+        if (errany != 0u || nonfinite || m_isnan(nanacc)) ninv += 1;
+        if (P.count) {
+          const unsigned tot = __reduce_add_sync(0xFFFFFFFFu, (unsigned)ninv);
+          if (lane == 0 && tot) acc_s[q].ninv += (int)tot;
+        } else if (__any_sync(0xFFFFFFFFu, ninv > 0)) {
+          if (lane == 0) acc_s[q].ninv += 1;
         }
-        const bool any_ovf = __any_sync(0xFFFFFFFFu, ovf);
-        if (lane == 0) {
-          acc_s[q].sse += sse;
-          acc_s[q].ninv += ninv;
-          acc_s[q].ovf |= any_ovf ? 1 : 0;
+        if (fused_policy) {
+          ovf = ovf || m_isnan(ovfacc) || dmax > Limits<T>::max_diff;
+          if (__any_sync(0xFFFFFFFFu, ovf) && lane == 0) acc_s[q].ovf = 1;
         }
       }
       __syncthreads();  // every warp is done with this tile before it is refilled
@@ -591,7 +746,10 @@ __global__ void __launch_bounds__(256) fitness_kernel(const FitParams<T> P) {
     }
     for (int q = threadIdx.x; q < np; q += blockDim.x) {
       const int64_t p = P.perm[p0 + q];
-      const PartRec r = acc_s[q];
+      PartRec r = acc_s[q];
+      double t = 0.0;  // lanes combined in a fixed order
+      for (int l = 0; l < 32; ++l) t += lane_sse[q * kLaneStride + l];
+      r.sse = t;
       if (P.n_splits == 1) {
         write_final<T>(P, p, r);
       } else {
@@ -600,14 +758,14 @@ __global__ void __launch_bounds__(256) fitness_kernel(const FitParams<T> P) {
         const unsigned done = atomicAdd(&P.prog_cnt[p], 1u);
         if (done == (unsigned)P.n_splits - 1u) {
           __threadfence();
-          PartRec t{0.0, 0, 0};
+          PartRec t2{0.0, 0, 0};
           for (int s2 = 0; s2 < P.n_splits; ++s2) {
             const PartRec* pr = &P.part[p * P.n_splits + s2];
-            t.sse += __ldcg(&pr->sse);
-            t.ninv += __ldcg(&pr->ninv);
-            t.ovf |= __ldcg(&pr->ovf);
+            t2.sse += __ldcg(&pr->sse);
+            t2.ninv += __ldcg(&pr->ninv);
+            t2.ovf |= __ldcg(&pr->ovf);
           }
-          write_final<T>(P, p, t);
+          write_final<T>(P, p, t2);
           P.prog_cnt[p] = 0u;  // ready for an evaluate-only rerun on the same tape
         }
       }
@@ -673,16 +831,18 @@ struct Sched {
   size_t smem_budget;
 };
 constexpr Sched kSched[] = {
-    {16, 8, 32, 72 * 1024},   // 0: auto placeholder (resolved by pick_schedule)
+    {16, 8, 24, 72 * 1024},   // 0: auto placeholder (resolved by pick_schedule)
     {8, 8, 32, 72 * 1024},    // 1
     {16, 4, 16, 56 * 1024},   // 2
-    {16, 8, 32, 72 * 1024},   // 3
+    {16, 8, 24, 72 * 1024},   // 3
     {16, 8, 32, 100 * 1024},  // 4
     {8, 8, 64, 100 * 1024},   // 5
     {16, 4, 32, 72 * 1024},   // 6
     {32, 8, 32, 100 * 1024},  // 7
     {32, 4, 16, 100 * 1024},  // 8
     {32, 8, 32, 140 * 1024},  // 9
+    {16, 8, 16, 72 * 1024},   // 10
+    {16, 8, 16, 100 * 1024},  // 11
 };
 constexpr int kNumSched = (int)(sizeof(kSched) / sizeof(kSched[0]));
 
@@ -767,7 +927,7 @@ ws_status launch_typed(const FitnessRequest& rq, const Sched& sc) {
   }
   const size_t fixed = (size_t)W * kSharedSlots * PASS * szT +
                        (size_t)PBmax * Lcap * sizeof(Instr<T>) +
-                       (size_t)PBmax * (sizeof(PartRec) + sizeof(int));
+                       (size_t)PBmax * (sizeof(PartRec) + sizeof(int) + kLaneStride * sizeof(double));
   const size_t per_row = 2 * (size_t)(rq.V + 1) * szT;  // two tiles (double buffering)
   const size_t optin = max_dynamic_smem<T, R, STRICT>();
   if (fixed + per_row * PASS > optin) return fail("too many variables for the shared-memory tile");
