@@ -166,6 +166,53 @@ ws_status ws_eval_fitness_static(int32_t dtype, const uint8_t* population, int64
 size_t ws_static_scratch_bytes(void);
 
 /*
+ * Batched fitness: many independent problems -- each with its own population, constants, data
+ * set (rows and variable count), vocabulary and outputs -- scored by ONE launch sequence (one
+ * compile kernel, one length sort, one persistent evaluator launch) instead of one
+ * `evaluate_batch` call per problem (evaluation.py:45-198, called per dataset by
+ * TensorGeneticEngine, engine.py:956,1136).  Results per problem are those of ws_eval_fitness on
+ * that problem alone (same values, same classes), whatever else is in the batch.
+ *
+ *   ws_batch_workspace_bytes  size of the device workspace the batch needs
+ *   ws_batch_create           plans the batch (chunk sizes per problem, programs per block, row
+ *                             splits, heaviest work first) and uploads the problem descriptors
+ *                             into the workspace (synchronous copy: call it outside any stream
+ *                             capture, once per set of problems)
+ *   ws_batch_eval             compile + sort + evaluate on `stream`: kernels and memsets only,
+ *                             no host synchronisation or allocation, so a CUDA graph can capture
+ *                             it and replay it after the populations / constants are rewritten
+ *                             in place (their pointers and shapes are fixed by the plan)
+ *   ws_batch_info             plan facts: 0 work items, 1 rows per lane, 2 programs per block,
+ *                             3 dynamic shared memory per CTA, 4 resident CTAs, 5 programs
+ *
+ * All problems share dtype, program width L (<= 256), strict_mode, policy, loss, schedule and
+ * invalid_value (from opts); opts->phase is ignored here (ws_batch_eval takes the phase).
+ */
+typedef struct ws_problem {
+  const uint8_t* population;  /* [B, L] uint8                                              */
+  int64_t B;
+  const void* x;              /* [num_vars, D] of dtype                                    */
+  int64_t num_vars, D;
+  const void* constants;      /* [B, K] of dtype, or NULL with K = 0                        */
+  int64_t K;
+  const void* y;              /* [D] of dtype                                              */
+  void* out_loss;             /* [B] of dtype (double for WS_LOSS_SSE)                     */
+  int32_t* out_ninvalid;      /* [B] invalid-row counts, or NULL                           */
+  const ws_token_map* ids;    /* this problem's token IDs                                  */
+} ws_problem;
+
+typedef struct ws_batch ws_batch;
+
+ws_status ws_batch_workspace_bytes(int32_t dtype, const ws_problem* problems, int32_t n_problems,
+                                   int64_t L, const ws_fitness_opts* opts, size_t* out_bytes);
+ws_status ws_batch_create(int32_t dtype, const ws_problem* problems, int32_t n_problems, int64_t L,
+                          const ws_fitness_opts* opts, void* workspace, size_t workspace_bytes,
+                          ws_batch** out_batch);
+ws_status ws_batch_eval(ws_batch* batch, int32_t phase, void* stream);
+int64_t ws_batch_info(const ws_batch* batch, int32_t what);
+void ws_batch_destroy(ws_batch* batch);
+
+/*
  * Adjoint gradient of program outputs with respect to their constants.  Replaces
  * `eval_rpn_backward` (bindings.cpp:511 -> run_rpn_backward_cuda, bindings.cpp:108-140 ->
  * launch_rpn_backward, backward_kernels.cu:286-335; kernel :13-281).

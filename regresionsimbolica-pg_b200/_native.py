@@ -70,6 +70,14 @@ class FitnessOpts(C.Structure):
                 ("reserved", C.c_int32)]
 
 
+class Problem(C.Structure):
+    """ws_problem: one problem of a batched fitness call (device pointers)."""
+    _fields_ = [("population", C.c_void_p), ("B", C.c_int64), ("x", C.c_void_p),
+                ("num_vars", C.c_int64), ("D", C.c_int64), ("constants", C.c_void_p),
+                ("K", C.c_int64), ("y", C.c_void_p), ("out_loss", C.c_void_p),
+                ("out_ninvalid", C.c_void_p), ("ids", C.POINTER(TokenMap))]
+
+
 _P = C.c_void_p
 _I64 = C.c_int64
 _I32 = C.c_int32
@@ -87,6 +95,13 @@ _SIGS = {
     "ws_eval_fitness_static": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
                                       _P, C.POINTER(TokenMap), C.POINTER(FitnessOpts), _P]),
     "ws_static_scratch_bytes": (C.c_size_t, []),
+    "ws_batch_workspace_bytes": (_I32, [_I32, _P, _I32, _I64, C.POINTER(FitnessOpts),
+                                        C.POINTER(C.c_size_t)]),
+    "ws_batch_create": (_I32, [_I32, _P, _I32, _I64, C.POINTER(FitnessOpts), _P, C.c_size_t,
+                               C.POINTER(_P)]),
+    "ws_batch_eval": (_I32, [_P, _I32, _P]),
+    "ws_batch_info": (_I64, [_P, _I32]),
+    "ws_batch_destroy": (None, [_P]),
     "ws_eval_rpn_backward": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
                                     C.POINTER(TokenMap), _P]),
     "ws_decode_rpn": (_I32, [_P, _I64, _I64, _P, _I32, _I64, C.POINTER(C.c_char_p), _I64, _P,

@@ -4,6 +4,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "ws_internal.h"
 
@@ -247,6 +248,89 @@ ws_status ws_eval_fitness(int32_t dtype, const uint8_t* population, int64_t B, i
   rq.workspace_bytes = workspace_bytes;
   rq.stream = (cudaStream_t)stream;
   return launch_fitness(rq);
+}
+
+static ws_status batch_requests(int32_t dtype, const ws_problem* problems, int32_t n,
+                                int64_t L, const ws_fitness_opts* opts,
+                                std::vector<ProblemRequest>& out) {
+  if (dtype != WS_F32 && dtype != WS_F64) return fail("x must be float32 or float64");
+  if (!opts) return fail("options are required");
+  if (n < 0 || (n > 0 && !problems)) return fail("problem list is null");
+  if (L < 1 || L > 256) return fail("program length must be in 1..256");
+  if (opts->policy != WS_POLICY_FUSED && opts->policy != WS_POLICY_CLASSIC)
+    return fail("unknown policy");
+  if (opts->loss < WS_LOSS_RMSE || opts->loss > WS_LOSS_SSE) return fail("unknown loss");
+  if (opts->schedule < 0 || opts->schedule >= ws_schedule_count())
+    return fail("schedule index out of range");
+  out.clear();
+  for (int32_t i = 0; i < n; ++i) {
+    const ws_problem& q = problems[i];
+    const std::string at = "problem " + std::to_string(i) + ": ";
+    if (!q.ids) return fail(at + "token map is required");
+    if (q.B < 0 || q.K < 0) return fail(at + "negative dimension");
+    if (q.num_vars < 0 || q.num_vars > 64) return fail(at + "supports 0..64 variables");
+    if (q.D < 1 || q.D > (int64_t)INT32_MAX) return fail(at + "supports 1..2^31-1 samples");
+    if (q.B > 0 && (!q.population || (!q.x && q.num_vars > 0) || !q.y || !q.out_loss ||
+                    (q.K > 0 && !q.constants)))
+      return fail(at + "null tensor pointer");
+    ProblemRequest r;
+    r.pop = q.population;
+    r.B = q.B;
+    r.x = q.x;
+    r.V = q.num_vars;
+    r.D = q.D;
+    r.consts = q.K > 0 ? q.constants : nullptr;
+    r.K = q.K;
+    r.y = q.y;
+    r.out_loss = q.out_loss;
+    r.out_ninv = q.out_ninvalid;
+    r.lut = build_lut(*q.ids, q.num_vars, opts->policy == WS_POLICY_FUSED);
+    out.push_back(r);
+  }
+  return WS_OK;
+}
+
+ws_status ws_batch_workspace_bytes(int32_t dtype, const ws_problem* problems, int32_t n_problems,
+                                   int64_t L, const ws_fitness_opts* opts, size_t* out_bytes) {
+  clear_error();
+  if (!out_bytes) return fail("out_bytes is null");
+  std::vector<ProblemRequest> rq;
+  ws_status st = batch_requests(dtype, problems, n_problems, L, opts, rq);
+  if (st != WS_OK) return st;
+  return batch_workspace_bytes(dtype, rq.data(), (int)rq.size(), L, opts->strict_mode ? 1 : 0,
+                               opts->schedule, out_bytes);
+}
+
+ws_status ws_batch_create(int32_t dtype, const ws_problem* problems, int32_t n_problems, int64_t L,
+                          const ws_fitness_opts* opts, void* workspace, size_t workspace_bytes,
+                          ws_batch** out_batch) {
+  clear_error();
+  if (!out_batch) return fail("out_batch is null");
+  *out_batch = nullptr;
+  std::vector<ProblemRequest> rq;
+  ws_status st = batch_requests(dtype, problems, n_problems, L, opts, rq);
+  if (st != WS_OK) return st;
+  void* h = nullptr;
+  st = batch_create(dtype, rq.data(), (int)rq.size(), L, opts->strict_mode ? 1 : 0, opts->policy,
+                    opts->loss, opts->schedule, opts->invalid_value, workspace, workspace_bytes, &h);
+  if (st == WS_OK) *out_batch = static_cast<ws_batch*>(h);
+  return st;
+}
+
+ws_status ws_batch_eval(ws_batch* batch, int32_t phase, void* stream) {
+  clear_error();
+  if (!batch) return fail("batch is null");
+  if (phase < WS_PHASE_ALL || phase > WS_PHASE_EVALUATE) return fail("unknown phase");
+  return batch_eval(batch, phase, (cudaStream_t)stream);
+}
+
+int64_t ws_batch_info(const ws_batch* batch, int32_t what) {
+  if (!batch) return -1;
+  return batch_info(const_cast<ws_batch*>(batch), what);
+}
+
+void ws_batch_destroy(ws_batch* batch) {
+  if (batch) batch_destroy(batch);
 }
 
 }  // extern "C"

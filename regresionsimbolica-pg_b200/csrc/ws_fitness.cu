@@ -34,6 +34,11 @@
 #include <mutex>
 #include <map>
 #include <tuple>
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <type_traits>
+#include <vector>
 
 #include "ws_internal.h"
 #include "ws_compile.cuh"
@@ -52,38 +57,88 @@ constexpr int kMetaLenMask = 0xFFFF;
 constexpr int kMetaGlobalSpill = 1 << 16;
 
 // ---------------------------------------------------------------------------------------
-// 1. compile
+// Problem descriptors.  One launch evaluates the programs of one or many problems (each with
+// its own population, constants, data set, token map and outputs).  The programs of all
+// problems form one index space [0, sum of B): problem p owns [prog0, prog0 + B); its work
+// items (blocks of PB programs x ranges of row chunks) are [item0, item0 + n_blocks * n_splits).
+template <typename T>
+struct ProbDesc {
+  const uint8_t* pop;   // [B, L]
+  const T* consts;      // [B, K] or null
+  const T* x;           // [V, D]
+  const T* y;           // [D]
+  void* out_loss;       // [B]
+  int32_t* out_ninv;    // [B] or null
+  int64_t B, D, prog0, item0, n_chunks, cps, part0;
+  int V, K, RC, xmul, n_splits, count, async_stage, pad;
+};
+
+// Index of the problem whose range [start, next start) holds `i` (starts ascending, n >= 1).
+template <typename T>
+__device__ __forceinline__ int find_problem(const ProbDesc<T>* __restrict__ d, int n, int64_t i,
+                                            bool by_item) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const int64_t st = by_item ? d[mid].item0 : d[mid].prog0;
+    if (st <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// ---------------------------------------------------------------------------------------
+// 1. compile (one thread per program of any problem)
 template <typename T, bool STRICT, int LMAX>
-__global__ void __launch_bounds__(128) compile_kernel(const uint8_t* __restrict__ pop, int64_t B,
-                                                      int L, const T* __restrict__ consts, int K,
-                                                      TokenLut lut, Instr<T>* __restrict__ tape,
-                                                      int Lcap, ProgHdr* __restrict__ hdr,
+__global__ void __launch_bounds__(128) compile_kernel(const ProbDesc<T>* __restrict__ desc,
+                                                      int n_prob, const TokenLut* __restrict__ luts,
+                                                      int64_t total_B, int L,
+                                                      Instr<T>* __restrict__ tape, int Lcap,
+                                                      ProgHdr* __restrict__ hdr,
+                                                      int32_t* __restrict__ prob_of,
                                                       unsigned* __restrict__ prog_cnt,
-                                                      unsigned* __restrict__ misc, int S,
-                                                      int xmul) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p == 0) misc[0] = 0u;  // work-queue head of the evaluator launch that follows
-  if (p >= B) return;
-  ProgHdr h = compile_program<T, STRICT, true, LMAX>(pop + p * (int64_t)L, L,
-                                                      K > 0 ? consts + p * (int64_t)K : nullptr,
-                                                      K, lut, tape + p * (int64_t)Lcap, xmul);
+                                                      unsigned* __restrict__ misc, int S) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g == 0) misc[0] = 0u;  // work-queue head of the evaluator launch that follows
+  if (g >= total_B) return;
+  const int pi = find_problem(desc, n_prob, g, false);
+  const ProbDesc<T>& d = desc[pi];
+  const int64_t p = g - d.prog0;
+  ProgHdr h = compile_program<T, STRICT, true, LMAX>(
+      d.pop + p * (int64_t)L, L, d.K > 0 ? d.consts + p * (int64_t)d.K : nullptr, d.K, luts[pi],
+      tape + g * (int64_t)Lcap, d.xmul);
   // Neither can happen (Sethi-Ullman bound; chunk size chosen for the offsets): guard anyway.
   if ((h.status == PROG_OK && h.n_slots > S) || h.status == PROG_UNREPRESENTABLE) {
     h.status = PROG_INVALID;
     atomicAdd(&misc[1], 1u);
   }
-  hdr[p] = h;
-  prog_cnt[p] = 0u;
+  hdr[g] = h;
+  prob_of[g] = pi;
+  prog_cnt[g] = 0u;
 }
 
-// FP64 variance of y (population variance, same rows as the loss) for WS_LOSS_R2.
+// Copies one problem's descriptor and token table into device memory: the single-problem entry
+// points write their descriptor this way (a kernel argument), so their launch sequence stays a
+// pure sequence of kernels and memsets that a CUDA graph can capture.
 template <typename T>
-__global__ void __launch_bounds__(256) yvar_kernel(const T* __restrict__ y, int64_t D,
+__global__ void write_desc_kernel(const ProbDesc<T> d, const TokenLut lut, ProbDesc<T>* dst,
+                                  TokenLut* lut_dst) {
+  if (threadIdx.x == 0) *dst = d;
+  const unsigned* s = reinterpret_cast<const unsigned*>(&lut);
+  unsigned* o = reinterpret_cast<unsigned*>(lut_dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(TokenLut) / 4); i += blockDim.x) o[i] = s[i];
+}
+
+// FP64 variance of y (population variance, same rows as the loss) for WS_LOSS_R2; one block per
+// problem.
+template <typename T>
+__global__ void __launch_bounds__(256) yvar_kernel(const ProbDesc<T>* __restrict__ desc,
                                                    double* __restrict__ out) {
   __shared__ double s1[256], s2[256];
+  const ProbDesc<T>& d = desc[blockIdx.x];
   double a = 0.0, b = 0.0;
-  for (int64_t i = threadIdx.x; i < D; i += blockDim.x) {
-    const double v = (double)y[i];
+  for (int64_t i = threadIdx.x; i < d.D; i += blockDim.x) {
+    const double v = (double)d.y[i];
     a += v;
     b += v * v;
   }
@@ -98,9 +153,9 @@ __global__ void __launch_bounds__(256) yvar_kernel(const T* __restrict__ y, int6
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    const double m = s1[0] / (double)D;
-    double v = s2[0] / (double)D - m * m;
-    out[0] = v > 0.0 ? v : 0.0;
+    const double m = s1[0] / (double)d.D;
+    double v = s2[0] / (double)d.D - m * m;
+    out[blockIdx.x] = v > 0.0 ? v : 0.0;
   }
 }
 
@@ -108,34 +163,23 @@ __global__ void __launch_bounds__(256) yvar_kernel(const T* __restrict__ y, int6
 // 2. evaluate
 template <typename T>
 struct FitParams {
-  const Instr<T>* tape;
-  const ProgHdr* hdr;
+  const ProbDesc<T>* desc;  // problems, ascending item0 / prog0
+  int n_prob;
+  const Instr<T>* tape;     // [sum B, Lcap]
+  const ProgHdr* hdr;       // [sum B]
   int Lcap;
-  const T* x;
-  const T* y;
-  int V;
-  int64_t D;
-  int64_t B;
-  int RC;            // rows per chunk (multiple of 32*R)
-  int64_t n_chunks;
-  int PB;            // programs per block
-  int64_t n_blocks;
-  int n_splits;      // chunk ranges per block
-  int64_t cps;       // chunks per split
+  int PB;                   // programs per block
   int64_t n_items;
-  int S;             // spill slots per warp
+  int64_t tile_cap;         // elements of one staging tile: max over problems of (V+1) * RC
+  int S;                    // spill slots per warp
   int policy, loss;
   double invalid_value;
-  void* out_loss;
-  int32_t* out_ninv;
   PartRec* part;
   unsigned* prog_cnt;
   unsigned* work;
-  const double* yvar;
-  const int64_t* perm;  // programs in evaluation order (sorted by tape length)
-  T* gspill;            // per-warp scratch for spill slots beyond the shared ones
-  int count;            // 1: exact per-row invalid counts (out_ninv requested)
-  int async_stage;      // 1: chunk rows are 16-byte aligned -> cp.async staging
+  const double* yvar;       // [n_prob] (WS_LOSS_R2)
+  const int64_t* perm;      // programs in evaluation order: by problem, then tape length
+  T* gspill;                // per-warp scratch for spill slots beyond the shared ones
 };
 
 template <typename T> struct Vec16;
@@ -529,11 +573,12 @@ __device__ __forceinline__ float pass_fast_pairs(const float (&a)[R], const floa
 // An FP64 sum above the T range stands for the overflow of the reference's T accumulator.
 // MSE uses the same classification (any overflow -> iv); R2 writes -iv for both.
 template <typename T>
-__device__ void write_final(const FitParams<T>& P, int64_t p, const PartRec& r) {
-  if (P.out_ninv) P.out_ninv[p] = r.ninv;
+__device__ void write_final(const FitParams<T>& P, const ProbDesc<T>& d, double yvar, int64_t p,
+                            const PartRec& r) {
+  if (d.out_ninv) d.out_ninv[p] = r.ninv;
   const double tmax = (double)(sizeof(T) == 4 ? FLT_MAX : DBL_MAX);
   if (P.loss == WS_LOSS_SSE) {
-    ((double*)P.out_loss)[p] = (r.ninv > 0) ? P.invalid_value : r.sse;
+    ((double*)d.out_loss)[p] = (r.ninv > 0) ? P.invalid_value : r.sse;
     return;
   }
   const bool fused = P.policy == WS_POLICY_FUSED;
@@ -548,7 +593,7 @@ __device__ void write_final(const FitParams<T>& P, int64_t p, const PartRec& r) 
     if (P.loss == WS_LOSS_RMSE) out = (fused && !row_ovf) ? (double)iv : (double)m_sqrt(iv);
     else out = (P.loss == WS_LOSS_MSE) ? P.invalid_value : -P.invalid_value;
   } else {
-    const double mse = r.sse / (double)P.D;
+    const double mse = r.sse / (double)d.D;
     const T mse_t = (T)mse;
     if (P.loss == WS_LOSS_RMSE) {
       const T q = m_sqrt(mse_t);
@@ -556,12 +601,11 @@ __device__ void write_final(const FitParams<T>& P, int64_t p, const PartRec& r) 
     } else if (P.loss == WS_LOSS_MSE) {
       out = (double)mse_t;
     } else {
-      const double vy = *P.yvar;
-      out = vy > 0.0 ? 1.0 - mse / vy : (mse == 0.0 ? 1.0 : -P.invalid_value);
+      out = yvar > 0.0 ? 1.0 - mse / yvar : (mse == 0.0 ? 1.0 : -P.invalid_value);
     }
   }
-  if (sizeof(T) == 4) ((float*)P.out_loss)[p] = (float)out;
-  else ((double*)P.out_loss)[p] = out;
+  if (sizeof(T) == 4) ((float*)d.out_loss)[p] = (float)out;
+  else ((double*)d.out_loss)[p] = out;
 }
 
 // ---- chunk staging: 16-byte asynchronous copies (cp.async) into a shared tile ---------------
@@ -581,30 +625,31 @@ __device__ __forceinline__ void cp_async_wait() {
 // cp.async group.  With async_stage the copies are 16-byte cp.async (rows of X are 16-byte
 // aligned: D is a multiple of 16/sizeof(T)); otherwise plain loads/stores with zero fill.
 template <typename T>
-__device__ __forceinline__ void stage_chunk(const FitParams<T>& P, int64_t c, T* tb, int tid,
+__device__ __forceinline__ void stage_chunk(const ProbDesc<T>& d, int64_t c, T* tb, int tid,
                                             int nthreads) {
   constexpr int VE = 16 / (int)sizeof(T);
-  const int64_t row0 = c * P.RC;
-  const int rows = (int)min((int64_t)P.RC, P.D - row0);
-  if (P.async_stage) {
+  const int64_t row0 = c * d.RC;
+  const int rows = (int)min((int64_t)d.RC, d.D - row0);
+  if (d.async_stage) {
     const int nvec = rows / VE;
-    for (int v = 0; v <= P.V; ++v) {
-      const T* src = (v < P.V ? P.x + (size_t)v * P.D : P.y) + row0;
-      T* dst = tb + (size_t)v * P.RC;
+    for (int v = 0; v <= d.V; ++v) {
+      const T* src = (v < d.V ? d.x + (size_t)v * d.D : d.y) + row0;
+      T* dst = tb + (size_t)v * d.RC;
       for (int i = tid; i < nvec; i += nthreads) cp_async16(dst + i * VE, src + i * VE);
     }
   } else {
-    for (int v = 0; v <= P.V; ++v) {
-      const T* src = (v < P.V ? P.x + (size_t)v * P.D : P.y) + row0;
-      T* dst = tb + (size_t)v * P.RC;
-      for (int r = tid; r < P.RC; r += nthreads) dst[r] = (r < rows) ? src[r] : (T)0;
+    for (int v = 0; v <= d.V; ++v) {
+      const T* src = (v < d.V ? d.x + (size_t)v * d.D : d.y) + row0;
+      T* dst = tb + (size_t)v * d.RC;
+      for (int r = tid; r < d.RC; r += nthreads) dst[r] = (r < rows) ? src[r] : (T)0;
     }
   }
   cp_async_commit();
 }
 
 template <typename T, int R, bool STRICT>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2) fitness_kernel(const FitParams<T> P) {
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2)
+    fitness_kernel(const FitParams<T> P) {
   constexpr int N = Vec16<T>::N;
   constexpr int PASS = 32 * R;
   constexpr bool F32 = sizeof(T) == 4;
@@ -616,14 +661,15 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2) fitn
   const int lane = threadIdx.x & 31;
   // two tiles of X[:, chunk] and y[chunk] (double-buffered staging), per-warp spill slots, the
   // block's tapes, per-program records, per-program per-lane FP64 partial sums
-  const size_t tile_elems = (size_t)(P.V + 1) * P.RC;
   T* tiles = reinterpret_cast<T*>(smem_raw);
-  T* spill = tiles + 2 * tile_elems;
+  T* spill = tiles + 2 * P.tile_cap;
   Instr<T>* tapes = reinterpret_cast<Instr<T>*>(spill + (size_t)W * kSharedSlots * PASS);
   PartRec* acc_s = reinterpret_cast<PartRec*>(tapes + (size_t)P.PB * P.Lcap);
   double* lane_sse = reinterpret_cast<double*>(acc_s + P.PB);  // [PB][kLaneStride]
   int* meta_s = reinterpret_cast<int*>(lane_sse + (size_t)P.PB * kLaneStride);
   __shared__ int64_t s_item;
+  __shared__ ProbDesc<T> s_desc;
+  __shared__ double s_yvar;
 
   T* sp_w = spill + (size_t)warp * kSharedSlots * PASS + lane * N;
   const int deep = P.S > kSharedSlots ? P.S - kSharedSlots : 0;
@@ -631,22 +677,33 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2) fitn
   const bool fused_policy = P.policy == WS_POLICY_FUSED;
 
   for (;;) {
-    if (threadIdx.x == 0) s_item = (int64_t)atomicAdd(P.work, 1u);
+    if (threadIdx.x == 0) {
+      const int64_t it = (int64_t)atomicAdd(P.work, 1u);
+      s_item = it;
+      if (it < P.n_items) {
+        const int pi = find_problem(P.desc, P.n_prob, it, true);
+        s_desc = P.desc[pi];
+        s_yvar = P.yvar ? P.yvar[pi] : 0.0;
+      }
+    }
     __syncthreads();
     const int64_t item = s_item;
     if (item >= P.n_items) break;
-    const int64_t blk = item / P.n_splits;
-    const int split = (int)(item % P.n_splits);
-    const int64_t p0 = blk * P.PB;
-    const int np = (int)min((int64_t)P.PB, P.B - p0);
-    const int64_t c0 = (int64_t)split * P.cps;
-    const int64_t c1 = min(P.n_chunks, c0 + P.cps);
+    const ProbDesc<T>& d = s_desc;
+    const int64_t local = item - d.item0;
+    const int64_t blk = local / d.n_splits;
+    const int split = (int)(local % d.n_splits);
+    const int64_t p0 = d.prog0 + blk * P.PB;  // position in perm
+    const int np = (int)min((int64_t)P.PB, d.B - blk * P.PB);
+    const int64_t c0 = (int64_t)split * d.cps;
+    const int64_t c1 = min(d.n_chunks, c0 + d.cps);
+    const size_t tile_elems = (size_t)(d.V + 1) * d.RC;
     // stage the block's tapes once for all its chunks (programs arrive sorted by tape length,
     // so a static warp assignment is balanced)
     for (int q = warp; q < np; q += W) {
-      const int64_t p = P.perm[p0 + q];
-      const ProgHdr h = P.hdr[p];
-      const Instr<T>* tg = P.tape + p * (int64_t)P.Lcap;
+      const int64_t g = P.perm[p0 + q];
+      const ProgHdr h = P.hdr[g];
+      const Instr<T>* tg = P.tape + g * (int64_t)P.Lcap;
       for (int i = lane; i < h.n_instr; i += 32) tapes[(size_t)q * P.Lcap + i] = tg[i];
       lane_sse[q * kLaneStride + lane] = 0.0;
       if (lane == 0) {
@@ -659,24 +716,25 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2) fitn
     }
 
     int buf = 0;
-    stage_chunk<T>(P, c0, tiles, threadIdx.x, blockDim.x);
+    stage_chunk<T>(d, c0, tiles, threadIdx.x, blockDim.x);
     for (int64_t c = c0; c < c1; ++c) {
-      T* xs = tiles + (size_t)buf * tile_elems;
-      T* ys = xs + (size_t)P.V * P.RC;
+      T* xs = tiles + (size_t)buf * P.tile_cap;
+      T* ys = xs + (size_t)d.V * d.RC;
       if (c + 1 < c1) {  // the next chunk streams in while this one is evaluated
-        stage_chunk<T>(P, c + 1, tiles + (size_t)(buf ^ 1) * tile_elems, threadIdx.x, blockDim.x);
+        stage_chunk<T>(d, c + 1, tiles + (size_t)(buf ^ 1) * P.tile_cap, threadIdx.x, blockDim.x);
         cp_async_wait<1>();
       } else {
         cp_async_wait<0>();
       }
-      const int64_t row0 = c * P.RC;
-      const int rows = (int)min((int64_t)P.RC, P.D - row0);
-      if (P.async_stage && rows < P.RC) {  // zero the rows past the end of the data
-        for (int v = 0; v <= P.V; ++v)
-          for (int r = rows + threadIdx.x; r < P.RC; r += blockDim.x) xs[(size_t)v * P.RC + r] = (T)0;
+      const int64_t row0 = c * d.RC;
+      const int rows = (int)min((int64_t)d.RC, d.D - row0);
+      if (d.async_stage && rows < d.RC) {  // zero the rows past the end of the data
+        for (int v = 0; v <= d.V; ++v)
+          for (int r = rows + threadIdx.x; r < d.RC; r += blockDim.x) xs[(size_t)v * d.RC + r] = (T)0;
       }
       __syncthreads();  // chunk c visible to all warps; tapes and accumulators ready
       const int npass = (rows + PASS - 1) / PASS;
+      const bool count = d.count != 0;
 
       for (int q = warp; q < np; q += W) {
         const int meta = meta_s[q];
@@ -709,7 +767,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2) fitn
           }
           const T* yb = ys + pass * PASS + lane * N;
           T part;
-          if (!P.count && (pass + 1) * PASS <= rows) {
+          if (!count && (pass + 1) * PASS <= rows) {
             errany |= err;
             if (fused_policy) {
               part = pass_fast<T, R, true>(a, yb, nanacc, ovfacc, dmax);
@@ -730,7 +788,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2) fitn
         lane_sse[q * kLaneStride + lane] += sse;
         // without per-row counts only "ninv > 0" matters
         if (errany != 0u || nonfinite || m_isnan(nanacc)) ninv += 1;
-        if (P.count) {
+        if (count) {
           const unsigned tot = __reduce_add_sync(0xFFFFFFFFu, (unsigned)ninv);
           if (lane == 0 && tot) acc_s[q].ninv += (int)tot;
         } else if (__any_sync(0xFFFFFFFFu, ninv > 0)) {
@@ -745,77 +803,123 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2) fitn
       buf ^= 1;
     }
     for (int q = threadIdx.x; q < np; q += blockDim.x) {
-      const int64_t p = P.perm[p0 + q];
+      const int64_t g = P.perm[p0 + q];
+      const int64_t pl = g - d.prog0;  // index within the problem
       PartRec r = acc_s[q];
       double t = 0.0;  // lanes combined in a fixed order
       for (int l = 0; l < 32; ++l) t += lane_sse[q * kLaneStride + l];
       r.sse = t;
-      if (P.n_splits == 1) {
-        write_final<T>(P, p, r);
+      if (d.n_splits == 1) {
+        write_final<T>(P, d, s_yvar, pl, r);
       } else {
-        P.part[p * P.n_splits + split] = r;
+        PartRec* pr0 = P.part + d.part0 + pl * d.n_splits;
+        pr0[split] = r;
         __threadfence();
-        const unsigned done = atomicAdd(&P.prog_cnt[p], 1u);
-        if (done == (unsigned)P.n_splits - 1u) {
+        const unsigned done = atomicAdd(&P.prog_cnt[g], 1u);
+        if (done == (unsigned)d.n_splits - 1u) {
           __threadfence();
           PartRec t2{0.0, 0, 0};
-          for (int s2 = 0; s2 < P.n_splits; ++s2) {
-            const PartRec* pr = &P.part[p * P.n_splits + s2];
-            t2.sse += __ldcg(&pr->sse);
-            t2.ninv += __ldcg(&pr->ninv);
-            t2.ovf |= __ldcg(&pr->ovf);
+          for (int s2 = 0; s2 < d.n_splits; ++s2) {
+            t2.sse += __ldcg(&pr0[s2].sse);
+            t2.ninv += __ldcg(&pr0[s2].ninv);
+            t2.ovf |= __ldcg(&pr0[s2].ovf);
           }
-          write_final<T>(P, p, t2);
-          P.prog_cnt[p] = 0u;  // ready for an evaluate-only rerun on the same tape
+          write_final<T>(P, d, s_yvar, pl, t2);
+          P.prog_cnt[g] = 0u;  // ready for an evaluate-only rerun on the same tape
         }
       }
     }
-    // the next item's staging waits on the __syncthreads() at the loop top
+    // the next item's staging (and the descriptor) waits on the __syncthreads() at the loop top
     __syncthreads();
   }
 }
 
-// ---- length-sorted schedule: counting sort of programs by tape length (longest first) ------
+// ---- length-sorted schedule: counting sort of programs by (problem, tape length) -----------
+// Bins are problem-major; within a problem tape lengths descend and invalid programs come last,
+// so problem p's programs occupy perm[prog0, prog0 + B) longest first.
 constexpr int kSortBins = 258;  // tape lengths 0..256, plus invalid programs
 
-__global__ void __launch_bounds__(256) sort_hist_kernel(const ProgHdr* __restrict__ hdr, int64_t B,
+__device__ __forceinline__ int sort_key(const ProgHdr& v) {
+  return v.status == PROG_OK ? min(v.n_instr, 256) : 257;
+}
+
+// Each block counts a contiguous range of programs; counts of the problem that opens the range
+// go through a shared-memory histogram, the (rare) others straight to global memory.
+__global__ void __launch_bounds__(256) sort_hist_kernel(const ProgHdr* __restrict__ hdr,
+                                                        const int32_t* __restrict__ prob_of,
+                                                        int64_t total_B, int64_t per_block,
                                                         unsigned* __restrict__ bins) {
   __shared__ unsigned h[kSortBins];
   for (int i = threadIdx.x; i < kSortBins; i += blockDim.x) h[i] = 0u;
+  const int64_t g0 = (int64_t)blockIdx.x * per_block;
+  const int64_t g1 = min(total_B, g0 + per_block);
+  const int pb = g0 < total_B ? prob_of[g0] : 0;
   __syncthreads();
-  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < B;
-       p += (int64_t)gridDim.x * blockDim.x) {
-    const ProgHdr v = hdr[p];
-    const int key = v.status == PROG_OK ? min(v.n_instr, 256) : 257;
-    atomicAdd(&h[key], 1u);
+  for (int64_t g = g0 + threadIdx.x; g < g1; g += blockDim.x) {
+    const int key = sort_key(hdr[g]);
+    const int pi = prob_of[g];
+    if (pi == pb) atomicAdd(&h[key], 1u);
+    else atomicAdd(&bins[(size_t)pi * kSortBins + key], 1u);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < kSortBins; i += blockDim.x)
-    if (h[i]) atomicAdd(&bins[i], h[i]);
+    if (h[i]) atomicAdd(&bins[(size_t)pb * kSortBins + i], h[i]);
 }
 
-// Exclusive offsets in descending tape length, invalid programs last (single block).
-__global__ void __launch_bounds__(32) sort_scan_kernel(unsigned* __restrict__ bins) {
-  if (threadIdx.x == 0) {
-    unsigned run = 0u;
-    for (int key = 256; key >= 0; --key) {
-      const unsigned c = bins[key];
-      bins[key] = run;
-      run += c;
+// Exclusive offsets over all bins in evaluation order (problem ascending; within a problem tape
+// length descending, invalid last).  One block of 1024 threads.
+__device__ __forceinline__ int sort_bin_at(int j) {
+  const int p = j / kSortBins, r = j - p * kSortBins;
+  return p * kSortBins + (r < 257 ? 256 - r : 257);
+}
+__global__ void __launch_bounds__(1024) sort_scan_kernel(unsigned* __restrict__ bins, int n_prob) {
+  __shared__ unsigned wsum[32];
+  const int n = n_prob * kSortBins;
+  const int per = (n + (int)blockDim.x - 1) / (int)blockDim.x;
+  const int j0 = min(n, (int)threadIdx.x * per), j1 = min(n, j0 + per);
+  unsigned sum = 0u;
+  for (int j = j0; j < j1; ++j) sum += bins[sort_bin_at(j)];
+  // block exclusive scan of the per-thread sums
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = (int)blockDim.x >> 5;
+    unsigned v = lane < nw ? wsum[lane] : 0u;
+    unsigned iv = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xFFFFFFFFu, iv, o);
+      if (lane >= o) iv += t;
     }
-    bins[257] = run;
+    if (lane < nw) wsum[lane] = iv - v;  // exclusive warp offsets
+  }
+  __syncthreads();
+  unsigned run = wsum[warp] + (incl - sum);
+  for (int j = j0; j < j1; ++j) {
+    const int b = sort_bin_at(j);
+    const unsigned c = bins[b];
+    bins[b] = run;
+    run += c;
   }
 }
 
 __global__ void __launch_bounds__(256) sort_scatter_kernel(const ProgHdr* __restrict__ hdr,
-                                                           int64_t B, unsigned* __restrict__ bins,
+                                                           const int32_t* __restrict__ prob_of,
+                                                           int64_t total_B,
+                                                           unsigned* __restrict__ bins,
                                                            int64_t* __restrict__ perm) {
-  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < B;
-       p += (int64_t)gridDim.x * blockDim.x) {
-    const ProgHdr v = hdr[p];
-    const int key = v.status == PROG_OK ? min(v.n_instr, 256) : 257;
-    const unsigned pos = atomicAdd(&bins[key], 1u);
-    perm[pos] = p;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total_B;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int key = sort_key(hdr[g]);
+    const unsigned pos = atomicAdd(&bins[(size_t)prob_of[g] * kSortBins + key], 1u);
+    perm[pos] = g;
   }
 }
 
@@ -898,197 +1002,324 @@ int occupancy_for(size_t smem, int threads) {
   return occ;
 }
 
+// ---- plans -----------------------------------------------------------------------------
+// A plan fixes, for one schedule and one set of problems, the chunk size of every problem, the
+// programs per block, the row splits and the order of the work items (heaviest items first, so
+// that the persistent CTAs finish together).
+struct ProbPlan {
+  int RC = 0, xmul = 0, n_splits = 1, async_stage = 0;
+  int64_t n_chunks = 0, cps = 0, n_blocks = 0, item0 = 0, prog0 = 0, part0 = 0;
+};
+struct Plan {
+  int R = 16, W = 8, PB = 8, S = 0, Lcap = 1;
+  size_t smem = 0;
+  int64_t n_ctas = 0, n_items = 0, total_B = 0, n_part = 0, tile_cap = 0;
+  std::vector<int> order;    // descriptor index -> problem index (problems with B > 0 only)
+  std::vector<ProbPlan> pp;  // by problem index
+};
+
 template <typename T, int R, bool STRICT>
-ws_status launch_typed(const FitnessRequest& rq, const Sched& sc) {
-  const FitnessWorkspace lay = fitness_workspace_layout(rq.B, rq.L, rq.dtype);
-  unsigned char* wsb = static_cast<unsigned char*>(rq.workspace);
+ws_status make_plan(const ProblemRequest* probs, int n, int64_t L, const Sched& sc,
+                    int64_t part_cap, size_t gspill_bytes, Plan& pl) {
+  constexpr int PASS = 32 * R;
+  constexpr int64_t VE = 16 / (int64_t)sizeof(T);
+  const size_t szT = sizeof(T);
+  pl.R = R;
+  pl.W = sc.W;
+  pl.Lcap = tape_capacity(L < 256 ? (int)L : 256);
+  pl.S = spill_slots_bound((int)L);
+  const int threads = pl.W * 32;
+  // programs per block: as the schedule says, but the staged tapes stay within 24 KB (long
+  // programs get fewer per block; at least one per warp)
+  int PBmax = sc.PB;
+  {
+    const int fit = (int)((24 * 1024) / ((size_t)pl.Lcap * sizeof(Instr<T>)));
+    if (PBmax > fit) PBmax = fit > pl.W ? fit : pl.W;
+  }
+  const size_t fixed = (size_t)pl.W * kSharedSlots * PASS * szT +
+                       (size_t)PBmax * pl.Lcap * sizeof(Instr<T>) +
+                       (size_t)PBmax * (sizeof(PartRec) + sizeof(int) + kLaneStride * sizeof(double));
+  int64_t vmax = 0;
+  for (int i = 0; i < n; ++i) vmax = probs[i].V > vmax ? probs[i].V : vmax;
+  const size_t per_row_max = 2 * (size_t)(vmax + 1) * szT;  // two tiles (double buffering)
+  const size_t optin = max_dynamic_smem<T, R, STRICT>();
+  if (fixed + per_row_max * PASS > optin) return fail("too many variables for the shared-memory tile");
+  const size_t budget = sc.smem_budget > fixed + per_row_max * PASS ? sc.smem_budget
+                                                                    : fixed + per_row_max * PASS;
+  const size_t avail = budget - fixed;
+  pl.pp.assign(n, ProbPlan());
+  pl.tile_cap = 0;
+  for (int i = 0; i < n; ++i) {
+    const ProblemRequest& q = probs[i];
+    ProbPlan& pp = pl.pp[i];
+    const size_t per_row = 2 * (size_t)(q.V + 1) * szT;
+    int64_t rc = (int64_t)(avail / per_row) / PASS * PASS;
+    const int64_t d_pad = (q.D + PASS - 1) / PASS * PASS;
+    if (rc > d_pad) rc = d_pad;
+    // tape offsets: variable v at v * (RC / PASS) must fit 9 bits
+    const int64_t xmul_cap = q.V > 0 ? (int64_t)P_OFF_MASK / q.V : (int64_t)P_OFF_MASK;
+    if (rc / PASS > xmul_cap) rc = xmul_cap * PASS;
+    if (rc < PASS) rc = PASS;
+    pp.RC = (int)rc;
+    pp.xmul = (int)(rc / PASS);
+    pp.n_chunks = (q.D + rc - 1) / rc;
+    const int64_t tile = (q.V + 1) * rc;
+    if (tile > pl.tile_cap) pl.tile_cap = tile;
+    pp.async_stage = (q.D % VE == 0) && (((uintptr_t)q.x & 15u) == 0) &&
+                     (((uintptr_t)q.y & 15u) == 0) ? 1 : 0;
+  }
+  pl.smem = fixed + 2 * (size_t)pl.tile_cap * szT;
+  const int occ = occupancy_for<T, R, STRICT>(pl.smem, threads);
+  if (occ <= 0) return fail("fitness kernel cannot be resident with this tile size");
+  pl.n_ctas = (int64_t)occ * device_info().sm_count;
+  const int deep = pl.S > kSharedSlots ? pl.S - kSharedSlots : 0;
+  if (deep > 0) {  // one global spill area per resident warp: cap the persistent grid to it
+    const int64_t fit = (int64_t)(gspill_bytes / ((size_t)pl.W * deep * PASS * szT));
+    if (fit < 1) return fail("workspace too small for the spill scratch of this schedule");
+    if (pl.n_ctas > fit) pl.n_ctas = fit;
+  }
+  // programs per block: halve while the whole launch has fewer than two units per CTA
+  auto units = [&](int pb) {
+    int64_t u = 0;
+    for (int i = 0; i < n; ++i) u += (probs[i].B + pb - 1) / pb * pl.pp[i].n_chunks;
+    return u;
+  };
+  int PB = PBmax;
+  while (PB > pl.W && units(PB) < 2 * pl.n_ctas) PB >>= 1;
+  pl.PB = PB;
+  // row splits: aim at >= 4 work items per CTA, items of similar size
+  double work = 0.0;
+  for (int i = 0; i < n; ++i) work += (double)probs[i].B * (double)pl.pp[i].n_chunks;
+  const double target = work / (4.0 * (double)pl.n_ctas) > 1.0 ? work / (4.0 * (double)pl.n_ctas)
+                                                                : 1.0;
+  for (int i = 0; i < n; ++i) {
+    ProbPlan& pp = pl.pp[i];
+    const int64_t B = probs[i].B;
+    pp.n_blocks = (B + PB - 1) / PB;
+    const double bw = (double)(B < PB ? B : PB) * (double)pp.n_chunks;
+    int64_t ns = (int64_t)std::ceil(bw / target);
+    if (ns < 1) ns = 1;
+    if (ns > pp.n_chunks) ns = pp.n_chunks;
+    if (part_cap >= 0 && ns > 1 && B * ns > part_cap) ns = B > 0 && part_cap / B > 1 ? part_cap / B : 1;
+    pp.cps = (pp.n_chunks + ns - 1) / ns;
+    pp.n_splits = (int)((pp.n_chunks + pp.cps - 1) / pp.cps);
+  }
+  // evaluation order: heaviest work items first
+  pl.order.clear();
+  for (int i = 0; i < n; ++i)
+    if (probs[i].B > 0) pl.order.push_back(i);
+  auto cost = [&](int i) {
+    const ProbPlan& pp = pl.pp[i];
+    return (double)(probs[i].B < pl.PB ? probs[i].B : pl.PB) * (double)pp.cps * (double)pp.RC;
+  };
+  std::stable_sort(pl.order.begin(), pl.order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+  pl.total_B = pl.n_items = pl.n_part = 0;
+  for (int i : pl.order) {
+    ProbPlan& pp = pl.pp[i];
+    pp.prog0 = pl.total_B;
+    pp.item0 = pl.n_items;
+    pp.part0 = pl.n_part;
+    pl.total_B += probs[i].B;
+    pl.n_items += pp.n_blocks * pp.n_splits;
+    if (pp.n_splits > 1) pl.n_part += probs[i].B * pp.n_splits;
+  }
+  if (part_cap >= 0 && pl.n_part > part_cap) return fail("partial-record area too small");
+  return WS_OK;
+}
+
+template <typename T>
+ProbDesc<T> make_desc(const ProblemRequest& q, const ProbPlan& pp) {
+  ProbDesc<T> d;
+  d.pop = q.pop;
+  d.consts = static_cast<const T*>(q.consts);
+  d.x = static_cast<const T*>(q.x);
+  d.y = static_cast<const T*>(q.y);
+  d.out_loss = q.out_loss;
+  d.out_ninv = q.out_ninv;
+  d.B = q.B;
+  d.D = q.D;
+  d.prog0 = pp.prog0;
+  d.item0 = pp.item0;
+  d.n_chunks = pp.n_chunks;
+  d.cps = pp.cps;
+  d.part0 = pp.part0;
+  d.V = (int)q.V;
+  d.K = q.consts ? (int)q.K : 0;
+  d.RC = pp.RC;
+  d.xmul = pp.xmul;
+  d.n_splits = pp.n_splits;
+  d.count = q.out_ninv != nullptr ? 1 : 0;
+  d.async_stage = pp.async_stage;
+  d.pad = 0;
+  return d;
+}
+
+struct RunArgs {
+  int64_t L;
+  int n_desc;
+  int phase, policy, loss;
+  double invalid_value;
+  cudaStream_t stream;
+};
+
+// The launch sequence of a plan whose descriptors and token tables are in the workspace:
+// compile + length sort (unless evaluate-only), then the evaluator.  Kernels and memsets only,
+// so a CUDA graph can capture it.
+template <typename T, int R, bool STRICT>
+ws_status run_plan(const Plan& pl, const FitnessWorkspace& lay, unsigned char* wsb,
+                   const RunArgs& a) {
   ProgHdr* hdr = reinterpret_cast<ProgHdr*>(wsb + lay.hdr_off);
   Instr<T>* tape = reinterpret_cast<Instr<T>*>(wsb + lay.tape_off);
   PartRec* part = reinterpret_cast<PartRec*>(wsb + lay.part_off);
   unsigned* cnt = reinterpret_cast<unsigned*>(wsb + lay.cnt_off);
   unsigned* misc = reinterpret_cast<unsigned*>(wsb + lay.misc_off);
-  double* yvar = reinterpret_cast<double*>(wsb + lay.misc_off + 16);
-
-  const int L = (int)rq.L;
-  const int Lcap = tape_capacity(L < 256 ? L : 256);  // tape words per program
-  const int S = spill_slots_bound(L);
-  constexpr int PASS = 32 * R;
-  const int W = sc.W;
-  const int threads = W * 32;
-
-  // ---- schedule: chunk rows RC (multiple of the pass), programs per block, splits ----------
-  const size_t szT = sizeof(T);
-  // programs per block: as the schedule says, but the staged tapes stay within 24 KB (long
-  // programs get fewer per block; at least one per warp)
-  int PBmax = sc.PB;
-  {
-    const int fit = (int)((24 * 1024) / ((size_t)Lcap * sizeof(Instr<T>)));
-    if (PBmax > fit) PBmax = fit > W ? fit : W;
-  }
-  const size_t fixed = (size_t)W * kSharedSlots * PASS * szT +
-                       (size_t)PBmax * Lcap * sizeof(Instr<T>) +
-                       (size_t)PBmax * (sizeof(PartRec) + sizeof(int) + kLaneStride * sizeof(double));
-  const size_t per_row = 2 * (size_t)(rq.V + 1) * szT;  // two tiles (double buffering)
-  const size_t optin = max_dynamic_smem<T, R, STRICT>();
-  if (fixed + per_row * PASS > optin) return fail("too many variables for the shared-memory tile");
-  const size_t budget = sc.smem_budget > fixed + per_row * PASS ? sc.smem_budget
-                                                                : fixed + per_row * PASS;
-  int64_t rc = (int64_t)((budget - fixed) / per_row) / PASS * PASS;
-  const int64_t d_pad = (rq.D + PASS - 1) / PASS * PASS;
-  if (rc > d_pad) rc = d_pad;
-  // tape offsets: variable v at v * (RC / PASS) must fit 9 bits
-  const int64_t xmul_cap = rq.V > 0 ? (int64_t)P_OFF_MASK / rq.V : (int64_t)P_OFF_MASK;
-  if (rc / PASS > xmul_cap) rc = xmul_cap * PASS;
-  if (rc < PASS) rc = PASS;
-  const int RC = (int)rc;
-  const int xmul = RC / PASS;
-  const size_t smem = fixed + per_row * (size_t)RC;
-  const int occ = occupancy_for<T, R, STRICT>(smem, threads);
-  if (occ <= 0) return fail("fitness kernel cannot be resident with this tile size");
-  int64_t n_ctas = (int64_t)occ * device_info().sm_count;
-
-  const T* consts = static_cast<const T*>(rq.consts);
   int64_t* perm = reinterpret_cast<int64_t*>(wsb + lay.perm_off);
   unsigned* bins = reinterpret_cast<unsigned*>(wsb + lay.bins_off);
   T* gspill = reinterpret_cast<T*>(wsb + lay.gspill_off);
-  const int deep = S > kSharedSlots ? S - kSharedSlots : 0;
-  if (deep > 0) {  // one global spill area per resident warp: cap the persistent grid to it
-    const int64_t fit = (int64_t)(lay.gspill_bytes / ((size_t)W * deep * PASS * szT));
-    if (fit < 1) return fail("workspace too small for the spill scratch of this schedule");
-    if (n_ctas > fit) n_ctas = fit;
-  }
-  // 1. compile, then order the programs by tape length
-  if (rq.phase != WS_PHASE_EVALUATE) {
-    cudaError_t e0 = cudaMemsetAsync(bins, 0, kSortBins * sizeof(unsigned), rq.stream);
+  const ProbDesc<T>* desc = reinterpret_cast<const ProbDesc<T>*>(wsb + lay.desc_off);
+  const TokenLut* luts = reinterpret_cast<const TokenLut*>(wsb + lay.lut_off);
+  double* yvar = reinterpret_cast<double*>(wsb + lay.yvar_off);
+  int32_t* prob_of = reinterpret_cast<int32_t*>(wsb + lay.probof_off);
+  if (pl.total_B == 0) return WS_OK;
+
+  // 1. compile, then order the programs by (problem, tape length)
+  if (a.phase != WS_PHASE_EVALUATE) {
+    cudaError_t e0 = cudaMemsetAsync(bins, 0, (size_t)a.n_desc * kSortBins * sizeof(unsigned),
+                                     a.stream);
     if (e0 != cudaSuccess) return fail_cuda(e0, "sort-bin reset");
     const int ct = 128;
-    const unsigned grid = (unsigned)((rq.B + ct - 1) / ct);
-    if (L <= 64)
-      compile_kernel<T, STRICT, 64><<<grid, ct, 0, rq.stream>>>(
-          rq.pop, rq.B, L, consts, (int)rq.K, rq.lut, tape, Lcap, hdr, cnt, misc, S, xmul);
+    const unsigned grid = (unsigned)((pl.total_B + ct - 1) / ct);
+    if (a.L <= 64)
+      compile_kernel<T, STRICT, 64><<<grid, ct, 0, a.stream>>>(
+          desc, a.n_desc, luts, pl.total_B, (int)a.L, tape, pl.Lcap, hdr, prob_of, cnt, misc, pl.S);
     else
-      compile_kernel<T, STRICT, 256><<<grid, ct, 0, rq.stream>>>(
-          rq.pop, rq.B, L, consts, (int)rq.K, rq.lut, tape, Lcap, hdr, cnt, misc, S, xmul);
+      compile_kernel<T, STRICT, 256><<<grid, ct, 0, a.stream>>>(
+          desc, a.n_desc, luts, pl.total_B, (int)a.L, tape, pl.Lcap, hdr, prob_of, cnt, misc, pl.S);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "compile_kernel launch");
-    int sgrid = (int)((rq.B + 255) / 256);
+    int64_t hgrid = (pl.total_B + 4095) / 4096;
+    if (hgrid < 1) hgrid = 1;
+    if (hgrid > (int64_t)device_info().sm_count * 8) hgrid = (int64_t)device_info().sm_count * 8;
+    const int64_t per_block = (pl.total_B + hgrid - 1) / hgrid;
+    sort_hist_kernel<<<(unsigned)hgrid, 256, 0, a.stream>>>(hdr, prob_of, pl.total_B, per_block,
+                                                            bins);
+    sort_scan_kernel<<<1, 1024, 0, a.stream>>>(bins, a.n_desc);
+    int sgrid = (int)((pl.total_B + 255) / 256);
     if (sgrid > device_info().sm_count * 8) sgrid = device_info().sm_count * 8;
-    sort_hist_kernel<<<sgrid, 256, 0, rq.stream>>>(hdr, rq.B, bins);
-    sort_scan_kernel<<<1, 32, 0, rq.stream>>>(bins);
-    sort_scatter_kernel<<<sgrid, 256, 0, rq.stream>>>(hdr, rq.B, bins, perm);
+    sort_scatter_kernel<<<sgrid, 256, 0, a.stream>>>(hdr, prob_of, pl.total_B, bins, perm);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "sort kernels launch");
   }
-  if (rq.phase == WS_PHASE_COMPILE) return WS_OK;
-  if (rq.phase == WS_PHASE_EVALUATE) {  // the compile kernel is what resets the queue head
-    cudaError_t e = cudaMemsetAsync(misc, 0, 16, rq.stream);
+  if (a.phase == WS_PHASE_COMPILE) return WS_OK;
+  if (a.phase == WS_PHASE_EVALUATE) {  // the compile kernel is what resets the queue head
+    cudaError_t e = cudaMemsetAsync(misc, 0, 16, a.stream);
     if (e != cudaSuccess) return fail_cuda(e, "work-queue reset");
   }
-  if (rq.loss == WS_LOSS_R2) {
-    yvar_kernel<T><<<1, 256, 0, rq.stream>>>(static_cast<const T*>(rq.y), rq.D, yvar);
+  if (a.loss == WS_LOSS_R2) {
+    yvar_kernel<T><<<a.n_desc, 256, 0, a.stream>>>(desc, yvar);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "yvar_kernel launch");
   }
 
   // 2. evaluate
-  const int64_t n_chunks = (rq.D + RC - 1) / RC;
-  int PB = PBmax;
-  int64_t n_blocks = (rq.B + PB - 1) / PB;
-  while (PB > W && n_blocks * n_chunks < 2 * n_ctas) {
-    PB >>= 1;
-    n_blocks = (rq.B + PB - 1) / PB;
-  }
-  int64_t n_splits = 1;
-  if (n_blocks < 2 * n_ctas) {
-    n_splits = (2 * n_ctas + n_blocks - 1) / n_blocks;
-    if (n_splits > n_chunks) n_splits = n_chunks;
-    const int64_t cap = lay.max_partials / (rq.B > 0 ? rq.B : 1);
-    if (n_splits > cap) n_splits = cap > 0 ? cap : 1;
-  }
-  const int64_t cps = (n_chunks + n_splits - 1) / n_splits;
-  n_splits = (n_chunks + cps - 1) / cps;
-
   FitParams<T> P;
+  P.desc = desc;
+  P.n_prob = a.n_desc;
   P.tape = tape;
   P.hdr = hdr;
-  P.Lcap = Lcap;
-  P.x = static_cast<const T*>(rq.x);
-  P.y = static_cast<const T*>(rq.y);
-  P.V = (int)rq.V;
-  P.D = rq.D;
-  P.B = rq.B;
-  P.RC = RC;
-  P.n_chunks = n_chunks;
-  P.PB = PB;
-  P.n_blocks = n_blocks;
-  P.n_splits = (int)n_splits;
-  P.cps = cps;
-  P.n_items = n_blocks * n_splits;
-  P.S = S;
-  P.policy = rq.policy;
-  P.loss = rq.loss;
-  P.invalid_value = rq.invalid_value;
-  P.out_loss = rq.out_loss;
-  P.out_ninv = rq.out_ninv;
+  P.Lcap = pl.Lcap;
+  P.PB = pl.PB;
+  P.n_items = pl.n_items;
+  P.tile_cap = pl.tile_cap;
+  P.S = pl.S;
+  P.policy = a.policy;
+  P.loss = a.loss;
+  P.invalid_value = a.invalid_value;
   P.part = part;
   P.prog_cnt = cnt;
   P.work = misc;
-  P.yvar = yvar;
+  P.yvar = a.loss == WS_LOSS_R2 ? yvar : nullptr;
   P.perm = perm;
   P.gspill = gspill;
-  P.count = rq.out_ninv != nullptr ? 1 : 0;
-  {
-    constexpr int64_t VE = 16 / (int64_t)sizeof(T);
-    P.async_stage = (rq.D % VE == 0) && (((uintptr_t)rq.x & 15u) == 0) &&
-                    (((uintptr_t)rq.y & 15u) == 0) ? 1 : 0;
-  }
-  const int64_t grid = P.n_items < n_ctas ? P.n_items : n_ctas;
-  fitness_kernel<T, R, STRICT><<<(unsigned)grid, threads, smem, rq.stream>>>(P);
+  const int64_t grid = pl.n_items < pl.n_ctas ? pl.n_items : pl.n_ctas;
+  if (grid <= 0) return WS_OK;
+  fitness_kernel<T, R, STRICT><<<(unsigned)grid, pl.W * 32, pl.smem, a.stream>>>(P);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail_cuda(e, "fitness_kernel launch");
   return WS_OK;
 }
 
-template <typename T, bool STRICT>
-ws_status launch_sched(const FitnessRequest& rq) {
-  Sched sc = pick_schedule(rq.schedule, rq.D);
-  if constexpr (sizeof(T) == 8) {
-    sc.R = 8;  // 16 doubles per operand array would spill registers
-    return launch_typed<T, 8, STRICT>(rq, sc);
-  } else {
-    if (sc.R == 8) return launch_typed<T, 8, STRICT>(rq, sc);
-    if constexpr (!STRICT) {
-      if (sc.R == 32) return launch_typed<T, 32, STRICT>(rq, sc);
-    }
-    sc.R = 16;  // 32-row passes are compiled for the protected operators only
-    return launch_typed<T, 16, STRICT>(rq, sc);
+// Calls f(TypeTag<T>, integral_constant<int, R>, integral_constant<bool, STRICT>) for the
+// element type, operator mode and rows per lane of a request.  FP64 runs R = 8 (16 doubles per
+// operand array would spill registers); 32-row passes are compiled for the protected operators
+// only.
+template <class T> struct TypeTag { using type = T; };
+template <int R> using RowsTag = std::integral_constant<int, R>;
+template <class F>
+ws_status dispatch(int dtype, bool strict, const Sched& sc, F&& f) {
+  if (dtype == WS_F64) {
+    if (strict) return f(TypeTag<double>(), RowsTag<8>(), std::true_type());
+    return f(TypeTag<double>(), RowsTag<8>(), std::false_type());
   }
+  if (strict) {
+    if (sc.R == 8) return f(TypeTag<float>(), RowsTag<8>(), std::true_type());
+    return f(TypeTag<float>(), RowsTag<16>(), std::true_type());
+  }
+  if (sc.R == 8) return f(TypeTag<float>(), RowsTag<8>(), std::false_type());
+  if (sc.R == 32) return f(TypeTag<float>(), RowsTag<32>(), std::false_type());
+  return f(TypeTag<float>(), RowsTag<16>(), std::false_type());
 }
+#define WS_DISPATCH_TYPES                        \
+  using T = typename decltype(tt_)::type;        \
+  constexpr int R = decltype(rr_)::value;        \
+  constexpr bool S = decltype(ss_)::value;
+
+// Opaque batch handle behind the ws_batch_* entry points.
+struct BatchState {
+  int dtype = WS_F32, strict = 0, n_desc = 0;
+  int policy = WS_POLICY_CLASSIC, loss = WS_LOSS_MSE;
+  double invalid_value = 0.0;
+  int64_t L = 0;
+  Sched sc{};
+  Plan plan;
+  FitnessWorkspace lay{};
+  unsigned char* wsb = nullptr;
+};
 
 }  // namespace
 
 int schedule_count() { return kNumSched; }
 
-FitnessWorkspace fitness_workspace_layout(int64_t B, int64_t L, int dtype) {
+FitnessWorkspace fitness_workspace_layout(int64_t total_B, int64_t L, int dtype, int64_t n_prob,
+                                          int64_t n_part) {
   FitnessWorkspace w;
   const size_t instr = dtype == WS_F64 ? sizeof(Instr<double>) : sizeof(Instr<float>);
   const int64_t Lcap = tape_capacity(L < 0 ? 0 : (L > 256 ? 256 : (int)L));
+  if (n_prob < 1) n_prob = 1;
   size_t off = 0;
   w.hdr_off = off;
-  off = align_up(off + (size_t)B * sizeof(ProgHdr), 256);
+  off = align_up(off + (size_t)total_B * sizeof(ProgHdr), 256);
   w.tape_off = off;
-  off = align_up(off + (size_t)B * Lcap * instr, 256);
-  w.max_partials = B > 65536 ? B : 65536;
+  off = align_up(off + (size_t)total_B * Lcap * instr, 256);
+  w.max_partials = n_part;
   w.part_off = off;
-  off = align_up(off + (size_t)w.max_partials * sizeof(PartRec), 256);
+  off = align_up(off + (size_t)n_part * sizeof(PartRec), 256);
   w.cnt_off = off;
-  off = align_up(off + (size_t)B * sizeof(unsigned), 256);
+  off = align_up(off + (size_t)total_B * sizeof(unsigned), 256);
   w.misc_off = off;
   off = align_up(off + 256, 256);
   w.perm_off = off;
-  off = align_up(off + (size_t)B * sizeof(int64_t), 256);
+  off = align_up(off + (size_t)total_B * sizeof(int64_t), 256);
   w.bins_off = off;
-  off = align_up(off + kSortBins * sizeof(unsigned), 256);
+  off = align_up(off + (size_t)n_prob * kSortBins * sizeof(unsigned), 256);
+  w.probof_off = off;
+  off = align_up(off + (size_t)total_B * sizeof(int32_t), 256);
+  w.desc_off = off;
+  off = align_up(off + (size_t)n_prob * sizeof(ProbDesc<double>), 256);
+  w.lut_off = off;
+  off = align_up(off + (size_t)n_prob * sizeof(TokenLut), 256);
+  w.yvar_off = off;
+  off = align_up(off + (size_t)n_prob * sizeof(double), 256);
   // deep spill slots: 32 resident warps per SM (the schedules run at most that many; the
   // launcher caps its grid otherwise), one pass of 512 rows per slot
   const int Lc = L < 0 ? 0 : (L > 256 ? 256 : (int)L);
@@ -1101,10 +1332,143 @@ FitnessWorkspace fitness_workspace_layout(int64_t B, int64_t L, int dtype) {
   return w;
 }
 
+FitnessWorkspace fitness_workspace_layout(int64_t B, int64_t L, int dtype) {
+  return fitness_workspace_layout(B, L, dtype, 1, B > 65536 ? B : 65536);
+}
+
 ws_status launch_fitness(const FitnessRequest& rq) {
-  if (rq.dtype == WS_F32)
-    return rq.strict ? launch_sched<float, true>(rq) : launch_sched<float, false>(rq);
-  return rq.strict ? launch_sched<double, true>(rq) : launch_sched<double, false>(rq);
+  const FitnessWorkspace lay = fitness_workspace_layout(rq.B, rq.L, rq.dtype);
+  ProblemRequest pr;
+  pr.pop = rq.pop;
+  pr.B = rq.B;
+  pr.x = rq.x;
+  pr.V = rq.V;
+  pr.D = rq.D;
+  pr.consts = rq.consts;
+  pr.K = rq.K;
+  pr.y = rq.y;
+  pr.out_loss = rq.out_loss;
+  pr.out_ninv = rq.out_ninv;
+  pr.lut = rq.lut;
+  const Sched sc = pick_schedule(rq.schedule, rq.D);
+  unsigned char* wsb = static_cast<unsigned char*>(rq.workspace);
+  return dispatch(rq.dtype, rq.strict != 0, sc, [&](auto tt_, auto rr_, auto ss_) -> ws_status {
+    WS_DISPATCH_TYPES
+    Plan pl;
+    ws_status st = make_plan<T, R, S>(&pr, 1, rq.L, sc, lay.max_partials, lay.gspill_bytes, pl);
+    if (st != WS_OK) return st;
+    const ProbDesc<T> d = make_desc<T>(pr, pl.pp[0]);
+    write_desc_kernel<T><<<1, 128, 0, rq.stream>>>(
+        d, pr.lut, reinterpret_cast<ProbDesc<T>*>(wsb + lay.desc_off),
+        reinterpret_cast<TokenLut*>(wsb + lay.lut_off));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "descriptor write");
+    RunArgs a{rq.L, 1, rq.phase, rq.policy, rq.loss, rq.invalid_value, rq.stream};
+    return run_plan<T, R, S>(pl, lay, wsb, a);
+  });
+}
+
+// ---- batches of problems (one launch sequence for all of them) --------------------------------
+static Sched batch_schedule(const ProblemRequest* probs, int n, int schedule) {
+  int64_t dmax = 0;
+  for (int i = 0; i < n; ++i) dmax = probs[i].D > dmax ? probs[i].D : dmax;
+  return pick_schedule(schedule, dmax);
+}
+
+ws_status batch_workspace_bytes(int dtype, const ProblemRequest* probs, int n, int64_t L,
+                                int strict, int schedule, size_t* out) {
+  const Sched sc = batch_schedule(probs, n, schedule);
+  return dispatch(dtype, strict != 0, sc, [&](auto tt_, auto rr_, auto ss_) -> ws_status {
+    WS_DISPATCH_TYPES
+    int64_t tb = 0;
+    for (int i = 0; i < n; ++i) tb += probs[i].B;
+    // the spill scratch does not depend on the plan: size it first, then plan against it
+    const FitnessWorkspace probe = fitness_workspace_layout(tb, L, dtype, n, 0);
+    Plan pl;
+    ws_status st = make_plan<T, R, S>(probs, n, L, sc, -1, probe.gspill_bytes, pl);
+    if (st != WS_OK) return st;
+    *out = fitness_workspace_layout(tb, L, dtype, n, pl.n_part).total;
+    return WS_OK;
+  });
+}
+
+ws_status batch_create(int dtype, const ProblemRequest* probs, int n, int64_t L, int strict,
+                       int policy, int loss, int schedule, double invalid_value, void* workspace,
+                       size_t workspace_bytes, void** out) {
+  const Sched sc = batch_schedule(probs, n, schedule);
+  BatchState* bs = new BatchState();
+  bs->dtype = dtype;
+  bs->strict = strict;
+  bs->policy = policy;
+  bs->loss = loss;
+  bs->invalid_value = invalid_value;
+  bs->L = L;
+  bs->sc = sc;
+  bs->wsb = static_cast<unsigned char*>(workspace);
+  ws_status st = dispatch(dtype, strict != 0, sc, [&](auto tt_, auto rr_, auto ss_) -> ws_status {
+    WS_DISPATCH_TYPES
+    int64_t tb = 0;
+    for (int i = 0; i < n; ++i) tb += probs[i].B;
+    const FitnessWorkspace probe = fitness_workspace_layout(tb, L, dtype, n, 0);
+    ws_status s2 = make_plan<T, R, S>(probs, n, L, sc, -1, probe.gspill_bytes, bs->plan);
+    if (s2 != WS_OK) return s2;
+    bs->n_desc = (int)bs->plan.order.size();
+    bs->lay = fitness_workspace_layout(tb, L, dtype, n, bs->plan.n_part);
+    if (!workspace || workspace_bytes < bs->lay.total) {
+      set_error("workspace of " + std::to_string(bs->lay.total) + " bytes required (got " +
+                std::to_string(workspace_bytes) + ")");
+      return WS_ERR_WORKSPACE;
+    }
+    if (((uintptr_t)workspace & 255u) != 0) {
+      set_error("workspace must be 256-byte aligned");
+      return WS_ERR_WORKSPACE;
+    }
+    std::vector<ProbDesc<T>> descs;
+    std::vector<TokenLut> luts;
+    for (int i : bs->plan.order) {
+      descs.push_back(make_desc<T>(probs[i], bs->plan.pp[i]));
+      luts.push_back(probs[i].lut);
+    }
+    if (!descs.empty()) {
+      cudaError_t e = cudaMemcpy(bs->wsb + bs->lay.desc_off, descs.data(),
+                                 descs.size() * sizeof(ProbDesc<T>), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess)
+        e = cudaMemcpy(bs->wsb + bs->lay.lut_off, luts.data(), luts.size() * sizeof(TokenLut),
+                       cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return fail_cuda(e, "batch descriptor upload");
+    }
+    return WS_OK;
+  });
+  if (st != WS_OK) {
+    delete bs;
+    return st;
+  }
+  *out = bs;
+  return WS_OK;
+}
+
+ws_status batch_eval(void* handle, int phase, cudaStream_t stream) {
+  BatchState* bs = static_cast<BatchState*>(handle);
+  return dispatch(bs->dtype, bs->strict != 0, bs->sc, [&](auto tt_, auto rr_, auto ss_) -> ws_status {
+    WS_DISPATCH_TYPES
+    RunArgs a{bs->L, bs->n_desc, phase, bs->policy, bs->loss, bs->invalid_value, stream};
+    return run_plan<T, R, S>(bs->plan, bs->lay, bs->wsb, a);
+  });
+}
+
+void batch_destroy(void* handle) { delete static_cast<BatchState*>(handle); }
+
+int64_t batch_info(void* handle, int what) {
+  const BatchState* bs = static_cast<const BatchState*>(handle);
+  switch (what) {
+    case 0: return bs->plan.n_items;
+    case 1: return bs->plan.R;
+    case 2: return bs->plan.PB;
+    case 3: return (int64_t)bs->plan.smem;
+    case 4: return bs->plan.n_ctas;
+    case 5: return bs->plan.total_B;
+    default: return -1;
+  }
 }
 
 }  // namespace ws

@@ -36,10 +36,39 @@ const DeviceInfo& device_info();
 // Workspace layout of the fitness evaluator for B programs of L tokens.
 struct FitnessWorkspace {
   size_t hdr_off, tape_off, part_off, cnt_off, misc_off, perm_off, bins_off, gspill_off;
+  size_t probof_off, desc_off, lut_off, yvar_off;
   size_t gspill_bytes, total;
   int64_t max_partials;  // partial records available (B * n_splits must not exceed it)
 };
+// One problem (single-problem calls) with the default partial-record area.
 FitnessWorkspace fitness_workspace_layout(int64_t B, int64_t L, int dtype);
+// Programs of n_prob problems (total_B in all) with n_part partial records.
+FitnessWorkspace fitness_workspace_layout(int64_t total_B, int64_t L, int dtype, int64_t n_prob,
+                                          int64_t n_part);
+
+// One problem of a (possibly batched) fitness launch.
+struct ProblemRequest {
+  const uint8_t* pop;
+  int64_t B;
+  const void* x;
+  int64_t V, D;
+  const void* consts;
+  int64_t K;
+  const void* y;
+  void* out_loss;
+  int32_t* out_ninv;
+  TokenLut lut;
+};
+// Batches of problems evaluated by one launch sequence (ws_fitness.cu): the handle holds the
+// plan; descriptors live in the caller's workspace.
+ws_status batch_workspace_bytes(int dtype, const ProblemRequest* probs, int n, int64_t L,
+                                int strict, int schedule, size_t* out);
+ws_status batch_create(int dtype, const ProblemRequest* probs, int n, int64_t L, int strict,
+                       int policy, int loss, int schedule, double invalid_value, void* workspace,
+                       size_t workspace_bytes, void** out);
+ws_status batch_eval(void* handle, int phase, cudaStream_t stream);
+void batch_destroy(void* handle);
+int64_t batch_info(void* handle, int what);
 
 // Launch of the compile + evaluate pipeline (ws_fitness.cu).
 struct FitnessRequest {

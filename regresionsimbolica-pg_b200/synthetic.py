@@ -178,3 +178,39 @@ def eval_scale_workload(seed: int = 0, n_programs: int = 1_048_576, n_rows: int 
     X = rng.uniform(*x_range, size=(n_vars, n_rows)).astype(np.float32)
     y, _ = random_target(rng, X, target_depth)
     return EvalWorkload(g, pop, consts, X, y)
+
+
+@dataclass
+class BatchWorkload:
+    """Independent regression problems, each an EvalWorkload with its own grammar (variable
+    count), rows, population and target."""
+    problems: list
+
+    def n_node_evals(self) -> float:
+        return float(sum(float(p.n_tokens().sum()) * p.X.shape[1] for p in self.problems))
+
+
+def batched_workload(seed: int = 0, n_problems: int = 256, programs: int = 2048,
+                     rows=(100, 100_000), n_vars=(1, 10), L: int = 64, len_low: int = 3,
+                     len_high: int = 64, K: int = 8, const_range=(-2.0, 2.0),
+                     x_range=(-4.0, 4.0), depth=(3, 6), noise_rel: float = 0.01,
+                     operators: Optional[Sequence[str]] = None) -> BatchWorkload:
+    """Batched uneven instances: rows log-uniform in [rows], features uniform in [n_vars],
+    X ~ U[x_range], targets from random depth-U{depth} trees with multiplicative relative noise
+    y * (1 + noise_rel * N(0, 1)), `programs` random valid programs of lengths U{len_low..len_high}
+    per problem."""
+    rng = np.random.default_rng(seed)
+    ops = BENCH_OPERATORS if operators is None else operators
+    lo, hi = np.log10(rows[0]), np.log10(rows[1])
+    out = []
+    for _ in range(n_problems):
+        D = int(np.floor(10.0 ** rng.uniform(lo, hi)))
+        V = int(rng.integers(n_vars[0], n_vars[1] + 1))
+        g = GPUGrammar(num_variables=V, operators=ops)
+        pop = random_programs(g, programs, len_low, len_high, L, rng, max_consts=K)
+        consts = rng.uniform(*const_range, size=(programs, K)).astype(np.float32)
+        X = rng.uniform(*x_range, size=(V, D)).astype(np.float32)
+        y, _ = random_target(rng, X, int(rng.integers(depth[0], depth[1] + 1)))
+        y = (y.astype(np.float64) * (1.0 + noise_rel * rng.standard_normal(D))).astype(np.float32)
+        out.append(EvalWorkload(g, pop, consts, X, y))
+    return BatchWorkload(out)
