@@ -65,8 +65,14 @@ class BatchedFitness:
                                    float(invalid_value), 0, 0)
         arr = (N.Problem * len(self.problems))()
         self._keep: List[object] = []   # tensors and token maps referenced by the descriptors
+        # outputs of all problems are views of one flat buffer (one copy reads them all back)
+        total = sum(int(p.population.shape[0]) for p in self.problems)
+        self.flat_out = torch.empty(max(total, 1), dtype=out_dtype, device=self.device)
+        self.flat_ninvalid = (torch.empty(max(total, 1), dtype=torch.int32, device=self.device)
+                              if count_invalid else None)
         self.outputs: List[torch.Tensor] = []
         self.ninvalid: List[Optional[torch.Tensor]] = []
+        off = 0
         for i, p in enumerate(self.problems):
             pop, x, y = p.population, p.x, p.y.reshape(-1)
             for t, nm in ((pop, "population"), (x, "x"), (y, "y")):
@@ -86,8 +92,9 @@ class BatchedFitness:
                 if c.dtype != dtype or c.dim() != 2 or int(c.shape[0]) != B:
                     raise RuntimeError("problem %d: constants must be %s [B, K]" % (i, dtype))
                 K = int(c.shape[1])
-            out = torch.empty(B, dtype=out_dtype, device=self.device)
-            nin = torch.empty(B, dtype=torch.int32, device=self.device) if count_invalid else None
+            out = self.flat_out[off:off + B]
+            nin = self.flat_ninvalid[off:off + B] if count_invalid else None
+            off += B
             tmap = N.TokenMap.from_args(*p.grammar.scalar_ids(), pi_val=PI_VAL, e_val=E_VAL)
             self._keep += [pop, x, y, c, out, nin, tmap]
             self.outputs.append(out)

@@ -70,7 +70,8 @@ struct ProbDesc {
   void* out_loss;       // [B]
   int32_t* out_ninv;    // [B] or null
   int64_t B, D, prog0, item0, n_chunks, cps, part0;
-  int V, K, RC, xmul, n_splits, count, async_stage, pad;
+  int V, K, RC, xmul, n_splits, count, async_stage;
+  int single;  // 1: one staging tile spanning both buffers (many variables), no prefetch
 };
 
 // Index of the problem whose range [start, next start) holds `i` (starts ascending, n >= 1).
@@ -170,7 +171,7 @@ struct FitParams {
   int Lcap;
   int PB;                   // programs per block
   int64_t n_items;
-  int64_t tile_cap;         // elements of one staging tile: max over problems of (V+1) * RC
+  int64_t tile_cap;         // elements per staging buffer (a single-buffered tile spans two)
   int S;                    // spill slots per warp
   int policy, loss;
   double invalid_value;
@@ -716,11 +717,12 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2)
     }
 
     int buf = 0;
+    const bool single = d.single != 0;
     stage_chunk<T>(d, c0, tiles, threadIdx.x, blockDim.x);
     for (int64_t c = c0; c < c1; ++c) {
       T* xs = tiles + (size_t)buf * P.tile_cap;
       T* ys = xs + (size_t)d.V * d.RC;
-      if (c + 1 < c1) {  // the next chunk streams in while this one is evaluated
+      if (!single && c + 1 < c1) {  // the next chunk streams in while this one is evaluated
         stage_chunk<T>(d, c + 1, tiles + (size_t)(buf ^ 1) * P.tile_cap, threadIdx.x, blockDim.x);
         cp_async_wait<1>();
       } else {
@@ -800,7 +802,11 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2)
         }
       }
       __syncthreads();  // every warp is done with this tile before it is refilled
-      buf ^= 1;
+      if (single) {
+        if (c + 1 < c1) stage_chunk<T>(d, c + 1, tiles, threadIdx.x, blockDim.x);
+      } else {
+        buf ^= 1;
+      }
     }
     for (int q = threadIdx.x; q < np; q += blockDim.x) {
       const int64_t g = P.perm[p0 + q];
@@ -935,10 +941,10 @@ struct Sched {
   size_t smem_budget;
 };
 constexpr Sched kSched[] = {
-    {16, 8, 24, 72 * 1024},   // 0: auto placeholder (resolved by pick_schedule)
+    {16, 8, 24, 75 * 1024},   // 0: auto placeholder (resolved by pick_schedule)
     {8, 8, 32, 72 * 1024},    // 1
     {16, 4, 16, 56 * 1024},   // 2
-    {16, 8, 24, 72 * 1024},   // 3
+    {16, 8, 24, 75 * 1024},   // 3
     {16, 8, 32, 100 * 1024},  // 4
     {8, 8, 64, 100 * 1024},   // 5
     {16, 4, 32, 72 * 1024},   // 6
@@ -1007,7 +1013,7 @@ int occupancy_for(size_t smem, int threads) {
 // programs per block, the row splits and the order of the work items (heaviest items first, so
 // that the persistent CTAs finish together).
 struct ProbPlan {
-  int RC = 0, xmul = 0, n_splits = 1, async_stage = 0;
+  int RC = 0, xmul = 0, n_splits = 1, async_stage = 0, single = 0;
   int64_t n_chunks = 0, cps = 0, n_blocks = 0, item0 = 0, prog0 = 0, part0 = 0;
 };
 struct Plan {
@@ -1039,20 +1045,25 @@ ws_status make_plan(const ProblemRequest* probs, int n, int64_t L, const Sched& 
   const size_t fixed = (size_t)pl.W * kSharedSlots * PASS * szT +
                        (size_t)PBmax * pl.Lcap * sizeof(Instr<T>) +
                        (size_t)PBmax * (sizeof(PartRec) + sizeof(int) + kLaneStride * sizeof(double));
+  // Staging tiles: a problem whose two tiles of one pass fit the schedule's budget is
+  // double-buffered; one with more variables gets a single tile spanning both buffers (staged
+  // after each chunk instead of during it), so that it does not force the whole launch to a
+  // larger tile and a lower occupancy.
   int64_t vmax = 0;
   for (int i = 0; i < n; ++i) vmax = probs[i].V > vmax ? probs[i].V : vmax;
-  const size_t per_row_max = 2 * (size_t)(vmax + 1) * szT;  // two tiles (double buffering)
+  const size_t single_max = (size_t)(vmax + 1) * PASS * szT;
   const size_t optin = max_dynamic_smem<T, R, STRICT>();
-  if (fixed + per_row_max * PASS > optin) return fail("too many variables for the shared-memory tile");
-  const size_t budget = sc.smem_budget > fixed + per_row_max * PASS ? sc.smem_budget
-                                                                    : fixed + per_row_max * PASS;
-  const size_t avail = budget - fixed;
+  if (fixed + single_max > optin) return fail("too many variables for the shared-memory tile");
+  size_t avail = sc.smem_budget > fixed ? sc.smem_budget - fixed : 0;
+  if (avail < single_max) avail = single_max;
   pl.pp.assign(n, ProbPlan());
   pl.tile_cap = 0;
+  int64_t region = 0;  // elements of the staging region (both buffers)
   for (int i = 0; i < n; ++i) {
     const ProblemRequest& q = probs[i];
     ProbPlan& pp = pl.pp[i];
-    const size_t per_row = 2 * (size_t)(q.V + 1) * szT;
+    pp.single = 2 * (size_t)(q.V + 1) * PASS * szT > avail ? 1 : 0;
+    const size_t per_row = (pp.single ? 1 : 2) * (size_t)(q.V + 1) * szT;
     int64_t rc = (int64_t)(avail / per_row) / PASS * PASS;
     const int64_t d_pad = (q.D + PASS - 1) / PASS * PASS;
     if (rc > d_pad) rc = d_pad;
@@ -1064,10 +1075,12 @@ ws_status make_plan(const ProblemRequest* probs, int n, int64_t L, const Sched& 
     pp.xmul = (int)(rc / PASS);
     pp.n_chunks = (q.D + rc - 1) / rc;
     const int64_t tile = (q.V + 1) * rc;
-    if (tile > pl.tile_cap) pl.tile_cap = tile;
+    const int64_t need = pp.single ? tile : 2 * tile;
+    if (need > region) region = need;
     pp.async_stage = (q.D % VE == 0) && (((uintptr_t)q.x & 15u) == 0) &&
                      (((uintptr_t)q.y & 15u) == 0) ? 1 : 0;
   }
+  pl.tile_cap = ((region + 1) / 2 + 3) / 4 * 4;  // per-buffer stride (16-byte aligned)
   pl.smem = fixed + 2 * (size_t)pl.tile_cap * szT;
   const int occ = occupancy_for<T, R, STRICT>(pl.smem, threads);
   if (occ <= 0) return fail("fitness kernel cannot be resident with this tile size");
@@ -1150,7 +1163,7 @@ ProbDesc<T> make_desc(const ProblemRequest& q, const ProbPlan& pp) {
   d.n_splits = pp.n_splits;
   d.count = q.out_ninv != nullptr ? 1 : 0;
   d.async_stage = pp.async_stage;
-  d.pad = 0;
+  d.single = pp.single;
   return d;
 }
 
