@@ -213,6 +213,50 @@ int64_t ws_batch_info(const ws_batch* batch, int32_t what);
 void ws_batch_destroy(ws_batch* batch);
 
 /*
+ * One genetic-programming generation, in place, for many problems at once.  Replaces the
+ * breeding half of `evolve_generation` (rpn_kernels.cu:1810-2237: tournament K16, elitism
+ * :1905-1907, subtree crossover K5/K6/K10, same-arity point mutation K7/K11, constant
+ * recombination / perturbation K12/K15) with three launches per generation (elite, children,
+ * copy-back) and a counter-based generator keyed by (problem seed, generation, child): a
+ * problem's offspring are the same alone or batched with others, and graph replays advance the
+ * device-side generation counter.  Semantics per child are stated in csrc/ws_gp.cu.
+ *   fitness: [B] of dtype, lower is better (e.g. the MSE written by ws_batch_eval)
+ *   population / constants: rewritten in place with the next generation
+ */
+typedef struct ws_gp_problem {
+  uint8_t* population;       /* [B, L]                                                   */
+  int64_t B;
+  void* constants;           /* [B, K] of dtype, or NULL with K = 0 (K <= 64)            */
+  int64_t K;
+  const void* fitness;       /* [B] of dtype                                             */
+  int64_t num_vars;
+  const ws_token_map* ids;   /* this problem's token IDs                                 */
+  uint64_t seed;             /* this problem's random stream                             */
+} ws_gp_problem;
+
+typedef struct ws_gp_opts {
+  int32_t tournament_size;    /* uniform draws per tournament, >= 1                       */
+  int32_t elitism;            /* 1: child 0 is the generation's best program              */
+  float crossover_rate;       /* probability that a child splices a second parent's subtree */
+  float mutation_rate;        /* per-token probability of a same-arity replacement        */
+  float const_mutation_rate;  /* per-constant probability of multiplicative noise         */
+  float const_sigma;          /* relative standard deviation of that noise                */
+  float parsimony_eps;        /* fitness ties within eps go to the shorter program        */
+  int32_t reserved;
+} ws_gp_opts;
+
+typedef struct ws_gp ws_gp;
+
+ws_status ws_gp_workspace_bytes(int32_t dtype, const ws_gp_problem* problems, int32_t n_problems,
+                                int64_t L, size_t* out_bytes);
+ws_status ws_gp_create(int32_t dtype, const ws_gp_problem* problems, int32_t n_problems, int64_t L,
+                       const ws_gp_opts* opts, void* workspace, size_t workspace_bytes,
+                       ws_gp** out);
+ws_status ws_gp_step(ws_gp* gp, void* stream);
+ws_status ws_gp_set_generation(ws_gp* gp, uint64_t generation, void* stream);
+void ws_gp_destroy(ws_gp* gp);
+
+/*
  * Adjoint gradient of program outputs with respect to their constants.  Replaces
  * `eval_rpn_backward` (bindings.cpp:511 -> run_rpn_backward_cuda, bindings.cpp:108-140 ->
  * launch_rpn_backward, backward_kernels.cu:286-335; kernel :13-281).

@@ -60,6 +60,11 @@ def lib():
                 C.c_int, C.c_float, C.c_float, C.c_float, _P]
         h.ws_oracle_simplify.argtypes = [_P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P, _P,
                                          C.c_int64, C.c_int32, _P]
+        for suf in ("f32", "f64"):
+            getattr(h, "ws_oracle_gp_step_" + suf).argtypes = [
+                _P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P, _P, _P, C.c_int, _P, C.c_int, _P,
+                C.c_int, C.c_uint64, C.c_uint64, C.c_int, C.c_int, C.c_float, C.c_float,
+                C.c_float, C.c_float, C.c_float, _P, _P]
         h.ws_oracle_validate.argtypes = [_P, C.c_int32, C.c_int64, C.c_int64, _P, C.c_int64,
                                          C.c_int32, C.c_int32, _P]
         h.ws_oracle_subtree_ranges.argtypes = [_P, C.c_int64, C.c_int64, _P, C.c_int64,
@@ -300,3 +305,51 @@ def simplify(pop, arities, val_table, lit_ids, lit_vals, max_passes, ids29):
     lib().ws_oracle_simplify(_p(out), B, L, _p(ar), ar.size, _p(vt), _p(li), _p(lv), li.size,
                              int(max_passes), _p(idv))
     return out
+
+
+def gp_tables(grammar):
+    """(arity[256], kind[256], variables, unary ops, binary ops) of a GPUGrammar, as the GP step
+    classifies tokens: arity 0 leaf / 1 unary / 2 binary / 3 PAD / 4 other; kind 1 variable,
+    2 C, 3 operator, 4 literal, 0 other; the lists in ascending token ID."""
+    arity = np.full(256, 4, dtype=np.uint8)
+    kind = np.zeros(256, dtype=np.uint8)
+    arity[0] = 3
+    for tok, i in grammar.token_to_id.items():
+        if i == 0:
+            continue
+        a = grammar.token_arity.get(tok, 0)
+        arity[i] = a
+        if tok in grammar.active_variables:
+            kind[i] = 1
+        elif tok == "C":
+            kind[i] = 2
+        elif a == 0:
+            kind[i] = 4
+        else:
+            kind[i] = 3
+    ids = np.arange(256)
+    vars_ = ids[kind == 1].astype(np.uint8)
+    uns = ids[(kind == 3) & (arity == 1)].astype(np.uint8)
+    bins = ids[(kind == 3) & (arity == 2)].astype(np.uint8)
+    return arity, kind, vars_, uns, bins
+
+
+def gp_step(grammar, pop, consts, fitness, seed, generation, tournament_size=3, elitism=1,
+            crossover_rate=0.7, mutation_rate=0.05, const_mutation_rate=0.1, const_sigma=0.1,
+            parsimony_eps=1e-9):
+    """One generation of the B200 GP step on the CPU: (next population, next constants)."""
+    pop = np.ascontiguousarray(pop, dtype=np.uint8)
+    B, L = pop.shape
+    dt = np.float64 if consts.dtype == np.float64 else np.float32
+    consts = np.ascontiguousarray(consts, dtype=dt)
+    fitness = np.ascontiguousarray(fitness, dtype=dt)
+    K = consts.shape[1]
+    arity, kind, vars_, uns, bins = gp_tables(grammar)
+    out_p = np.zeros_like(pop)
+    out_c = np.zeros_like(consts)
+    getattr(lib(), "ws_oracle_gp_step_" + _suffix(dt))(
+        _p(pop), B, L, _p(consts), K, _p(fitness), _p(arity), _p(kind), _p(vars_), len(vars_),
+        _p(uns), len(uns), _p(bins), len(bins), seed, generation, tournament_size, elitism,
+        crossover_rate, mutation_rate, const_mutation_rate, const_sigma, parsimony_eps,
+        _p(out_p), _p(out_c))
+    return out_p, out_c

@@ -78,6 +78,20 @@ class Problem(C.Structure):
                 ("out_ninvalid", C.c_void_p), ("ids", C.POINTER(TokenMap))]
 
 
+class GpProblem(C.Structure):
+    """ws_gp_problem: one problem of a batched GP generation (device pointers)."""
+    _fields_ = [("population", C.c_void_p), ("B", C.c_int64), ("constants", C.c_void_p),
+                ("K", C.c_int64), ("fitness", C.c_void_p), ("num_vars", C.c_int64),
+                ("ids", C.POINTER(TokenMap)), ("seed", C.c_uint64)]
+
+
+class GpOpts(C.Structure):
+    _fields_ = [("tournament_size", C.c_int32), ("elitism", C.c_int32),
+                ("crossover_rate", C.c_float), ("mutation_rate", C.c_float),
+                ("const_mutation_rate", C.c_float), ("const_sigma", C.c_float),
+                ("parsimony_eps", C.c_float), ("reserved", C.c_int32)]
+
+
 _P = C.c_void_p
 _I64 = C.c_int64
 _I32 = C.c_int32
@@ -102,6 +116,12 @@ _SIGS = {
     "ws_batch_eval": (_I32, [_P, _I32, _P]),
     "ws_batch_info": (_I64, [_P, _I32]),
     "ws_batch_destroy": (None, [_P]),
+    "ws_gp_workspace_bytes": (_I32, [_I32, _P, _I32, _I64, C.POINTER(C.c_size_t)]),
+    "ws_gp_create": (_I32, [_I32, _P, _I32, _I64, C.POINTER(GpOpts), _P, C.c_size_t,
+                            C.POINTER(_P)]),
+    "ws_gp_step": (_I32, [_P, _P]),
+    "ws_gp_set_generation": (_I32, [_P, C.c_uint64, _P]),
+    "ws_gp_destroy": (None, [_P]),
     "ws_eval_rpn_backward": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
                                     C.POINTER(TokenMap), _P]),
     "ws_decode_rpn": (_I32, [_P, _I64, _I64, _P, _I32, _I64, C.POINTER(C.c_char_p), _I64, _P,
