@@ -454,6 +454,50 @@ def run_batched(args):
     same = all(torch.allclose(o, bf.outputs[i], rtol=1e-6, atol=0, equal_nan=True)
                for i, o in enumerate(outs))
 
+    # the fit loop: every generation = evaluate + breed (device GP step), one graph replay
+    from warpsymbolic_b200.gp import GPStep
+    init = [(p.population.clone(), p.constants.clone()) for p in probs]
+    gp = GPStep(probs, bf.outputs, [args.seed * 1000 + i for i in range(len(probs))])
+    fit_graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(stream)
+    with torch.cuda.stream(side):  # warm-up outside capture, then restore and rewind
+        bf.evaluate(stream=side)
+        gp.step(stream=side)
+        for p, (ip, ic) in zip(probs, init):
+            p.population.copy_(ip)
+            p.constants.copy_(ic)
+        gp.set_generation(0, stream=side)
+    stream.wait_stream(side)
+    with torch.cuda.graph(fit_graph):
+        bf.evaluate()
+        gp.step()
+    bf.evaluate()
+    torch.cuda.synchronize()
+    best0 = float(np.median([float(o.min()) for o in bf.outputs]))
+    f_ms = timed(fit_graph.replay, args.generations)
+    bf.evaluate()
+    torch.cuda.synchronize()
+    best_end = float(np.median([float(o.min()) for o in bf.outputs]))
+    fit_evals = sum(float((p.population != 0).sum()) * p.x.shape[1] for p in probs)
+
+    # plain fit: one evaluation launch sequence and one GP step per problem, per generation
+    gps = [GPStep([p], [o], [i]) for i, (p, o) in enumerate(zip(probs, outs))]
+
+    def plain_fit():
+        for vm, p, o, g in zip(vms, probs, outs, gps):
+            vm.eval_fitness(p.population, p.x, p.constants, p.y, policy="classic", loss="mse",
+                            out=o)
+            g.step()
+    plain_fit()
+    torch.cuda.synchronize()
+    pf_ms = timed(plain_fit, 3)
+    for p, (ip, ic) in zip(probs, init):
+        p.population.copy_(ip)
+        p.constants.copy_(ic)
+    bf.evaluate()
+    torch.cuda.synchronize()
+
     # end to end: host populations/constants in, all losses out, every generation
     h_out = torch.empty(bf.flat_out.numel(), dtype=torch.float32).pin_memory()
 
@@ -491,10 +535,22 @@ def run_batched(args):
                     "h2d_bytes_per_step": int(h_pop.numel() + 4 * h_c.numel()),
                     "d2h_bytes_per_step": int(4 * h_out.numel()),
                     "ms_per_step": statistics.mean(e_ms)},
+            "fit": {"what": "evaluate + device GP step (tournament 3, elitism, subtree "
+                            "crossover 0.7, point mutation 0.05, constant noise) per generation, "
+                            "one graph replay each",
+                    "generations": args.generations,
+                    "ms_per_generation": statistics.mean(f_ms),
+                    "node_evals_per_s": fit_evals / (statistics.mean(f_ms) / 1e3),
+                    "median_best_mse_start": best0, "median_best_mse_end": best_end,
+                    "plain_ms_per_generation": statistics.mean(pf_ms),
+                    "plain_launch_sequences_per_generation": 2 * len(probs)},
             "clocks": clk.summary(),
             "gpu_launches": 6 * args.generations}
     print(json.dumps(line), flush=True)
-    del graph
+    del graph, fit_graph
+    gp.close()
+    for g in gps:
+        g.close()
     bf.close()
 
 

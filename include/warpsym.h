@@ -170,8 +170,9 @@ size_t ws_static_scratch_bytes(void);
  * set (rows and variable count), vocabulary and outputs -- scored by ONE launch sequence (one
  * compile kernel, one length sort, one persistent evaluator launch) instead of one
  * `evaluate_batch` call per problem (evaluation.py:45-198, called per dataset by
- * TensorGeneticEngine, engine.py:956,1136).  Results per problem are those of ws_eval_fitness on
- * that problem alone (same values, same classes), whatever else is in the batch.
+ * TensorGeneticEngine, engine.py:956,1136).  A problem's results are those of ws_eval_fitness on
+ * that problem alone with the same schedule, bit for bit, whatever else is in the batch (chunk
+ * sizes and row splits depend on the problem's own shape only).
  *
  *   ws_batch_workspace_bytes  size of the device workspace the batch needs
  *   ws_batch_create           plans the batch (chunk sizes per problem, programs per block, row

@@ -1100,17 +1100,17 @@ ws_status make_plan(const ProblemRequest* probs, int n, int64_t L, const Sched& 
   int PB = PBmax;
   while (PB > pl.W && units(PB) < 2 * pl.n_ctas) PB >>= 1;
   pl.PB = PB;
-  // row splits: aim at >= 4 work items per CTA, items of similar size
-  double work = 0.0;
-  for (int i = 0; i < n; ++i) work += (double)probs[i].B * (double)pl.pp[i].n_chunks;
-  const double target = work / (4.0 * (double)pl.n_ctas) > 1.0 ? work / (4.0 * (double)pl.n_ctas)
-                                                                : 1.0;
+  // Row splits per problem, from the problem's own shape only (its programs per block at the
+  // schedule's PB and a nominal three CTAs per SM, as if it ran alone): the summation order of a
+  // program's loss -- and so the loss, bit for bit -- does not depend on what else shares the
+  // launch.  Small problems are cut into enough items to fill the GPU by themselves.
+  const int64_t nominal_ctas = 3 * (int64_t)device_info().sm_count;
   for (int i = 0; i < n; ++i) {
     ProbPlan& pp = pl.pp[i];
     const int64_t B = probs[i].B;
     pp.n_blocks = (B + PB - 1) / PB;
-    const double bw = (double)(B < PB ? B : PB) * (double)pp.n_chunks;
-    int64_t ns = (int64_t)std::ceil(bw / target);
+    const int64_t own_blocks = (B + PBmax - 1) / PBmax;
+    int64_t ns = own_blocks > 0 ? (2 * nominal_ctas + own_blocks - 1) / own_blocks : 1;
     if (ns < 1) ns = 1;
     if (ns > pp.n_chunks) ns = pp.n_chunks;
     if (part_cap >= 0 && ns > 1 && B * ns > part_cap) ns = B > 0 && part_cap / B > 1 ? part_cap / B : 1;
