@@ -48,9 +48,13 @@ def parse():
                     help="target CPU time of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--config", default="eval-scale", choices=["eval-scale", "batched"],
+    ap.add_argument("--config", default="eval-scale", choices=["eval-scale", "batched", "serving"],
                     help="eval-scale: the evaluation-only scale test (default); batched: 256 "
-                         "uneven problems scored by one graph-replayed launch per generation")
+                         "uneven problems scored by one graph-replayed launch per generation; "
+                         "serving: a Poisson stream of fit/evaluate requests, continuously "
+                         "batched, against one request at a time")
+    ap.add_argument("--requests", type=int, default=8)
+    ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
     ap.add_argument("--problems", type=int, default=256)
     ap.add_argument("--generations", type=int, default=50)
     return ap.parse_args()
@@ -554,8 +558,81 @@ def run_batched(args):
     bf.close()
 
 
+def run_serving(args):
+    """Serving stream: `--requests` requests arriving as a Poisson process at `--rate`/s (20 by
+    default), half fits
+    (population 4,096, 30 generations) and half evaluations (4,096 programs), rows log-uniform in
+    [1,000, 200,000], 1..8 variables, X ~ U[-3,3], targets from depth 3-6 trees with noise
+    0.01 * std(y).  Served by the continuous-batching loop (one batched evaluation and one batched
+    GP generation per tick for all admitted requests), then by the plain path (one request at a
+    time, one launch sequence per evaluation and per generation) on the same stream; every
+    request's result is checked to be identical on both."""
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    entry.load_package()
+    from warpsymbolic_b200 import synthetic
+    from warpsymbolic_b200.serving import (ContinuousBatchingServer, serve_plain,
+                                           latency_summary)
+    warm = synthetic.serving_stream(seed=99, n_requests=4, rate=1e6, rows=(1000, 3000),
+                                    population=512, generations=2)
+    ContinuousBatchingServer(dev).serve(warm, realtime=False)
+    serve_plain(warm, dev, realtime=False)
+    reqs = synthetic.serving_stream(seed=args.seed, n_requests=args.requests, rate=args.rate)
+    evals = 0.0
+    for r in reqs:
+        n_tok = float((r.population != 0).sum())
+        evals += n_tok * r.X.shape[1] * ((r.generations + 1) if r.kind == "fit" else 1)
+    torch.cuda.synchronize()
+    srv = ContinuousBatchingServer(dev)
+    with ClockSampler(0) as clk:
+        batched = srv.serve(reqs, realtime=True)
+    mk_b = max(r.done for r in batched) - min(r.arrival for r in batched)
+    plain = serve_plain(reqs, dev, realtime=True)
+    mk_p = max(r.done for r in plain) - min(r.arrival for r in plain)
+    same = True
+    for a, b in zip(batched, plain):
+        if a.kind == "evaluate":
+            same &= bool(np.array_equal(a.losses, b.losses, equal_nan=True))
+        else:
+            same &= a.best_loss == b.best_loss and bool(np.array_equal(a.best_program, b.best_program))
+    sb, sp = latency_summary(batched, mk_b), latency_summary(plain, mk_p)
+    by_kind = {k: {"batched_p50_s": float(np.median([r.latency for r in batched if r.kind == k])),
+                   "plain_p50_s": float(np.median([r.latency for r in plain if r.kind == k]))}
+               for k in ("fit", "evaluate") if any(r.kind == k for r in batched)}
+    line = {"metric": "served-fit p50/p99 latency and throughput vs plain", "value": sb["p99_s"],
+            "unit": "s (p99 latency)", "n_gpus": 1, "steps": len(reqs), "warmup": 1,
+            "ms_per_step": 1e3 * mk_b / len(reqs), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Poisson stream with the serving config's distributions)",
+            "config": {"workload": "serving stream: %d requests, Poisson %g/s, fit:evaluate 1:1, "
+                                   "population 4096, 30 generations, rows log-U[1e3,2e5], vars "
+                                   "U{1..8}" % (len(reqs), args.rate),
+                       "fits": sum(r.kind == "fit" for r in reqs), "schedule": 3},
+            "batched": sb, "plain": sp, "by_kind": by_kind,
+            "p99_speedup": sp["p99_s"] / sb["p99_s"], "p50_speedup": sp["p50_s"] / sb["p50_s"],
+            "throughput_speedup": sb["throughput_req_s"] / sp["throughput_req_s"],
+            "node_evals_per_s_batched": evals / mk_b, "node_evals_per_s_plain": evals / mk_p,
+            "identical_results": same, "server": srv.stats, "clocks": clk.summary(),
+            "e2e": {"value": sb["p99_s"], "unit": "s (p99 latency, host arrays in and results "
+                                                    "out per request)",
+                    "h2d_bytes_per_step": int(np.mean([r.population.nbytes + r.constants.nbytes
+                                                       + r.X.nbytes + r.y.nbytes for r in reqs])),
+                    "d2h_bytes_per_step": int(np.mean([4 * r.population.shape[0] for r in reqs]))},
+            "gpu_launches": int(srv.stats.get("ticks", 0)) * 8}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.config == "serving":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "config": "serving",
+                              "unavailable": "the reference has no serving loop; the plain "
+                                             "one-request-at-a-time path is timed beside ours"}))
+            return
+        run_serving(args)
+        return
     if args.config == "batched":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "config": "batched",

@@ -176,9 +176,9 @@ size_t ws_static_scratch_bytes(void);
  *
  *   ws_batch_workspace_bytes  size of the device workspace the batch needs
  *   ws_batch_create           plans the batch (chunk sizes per problem, programs per block, row
- *                             splits, heaviest work first) and uploads the problem descriptors
- *                             into the workspace (synchronous copy: call it outside any stream
- *                             capture, once per set of problems)
+ *                             splits, heaviest work first) and writes the problem descriptors
+ *                             into the workspace with kernels on `stream` (stream-ordered; no
+ *                             host synchronisation), once per set of problems
  *   ws_batch_eval             compile + sort + evaluate on `stream`: kernels and memsets only,
  *                             no host synchronisation or allocation, so a CUDA graph can capture
  *                             it and replay it after the populations / constants are rewritten
@@ -208,7 +208,7 @@ ws_status ws_batch_workspace_bytes(int32_t dtype, const ws_problem* problems, in
                                    int64_t L, const ws_fitness_opts* opts, size_t* out_bytes);
 ws_status ws_batch_create(int32_t dtype, const ws_problem* problems, int32_t n_problems, int64_t L,
                           const ws_fitness_opts* opts, void* workspace, size_t workspace_bytes,
-                          ws_batch** out_batch);
+                          void* stream, ws_batch** out_batch);
 ws_status ws_batch_eval(ws_batch* batch, int32_t phase, void* stream);
 int64_t ws_batch_info(const ws_batch* batch, int32_t what);
 void ws_batch_destroy(ws_batch* batch);
@@ -219,8 +219,8 @@ void ws_batch_destroy(ws_batch* batch);
  * :1905-1907, subtree crossover K5/K6/K10, same-arity point mutation K7/K11, constant
  * recombination / perturbation K12/K15) with three launches per generation (elite, children,
  * copy-back) and a counter-based generator keyed by (problem seed, generation, child): a
- * problem's offspring are the same alone or batched with others, and graph replays advance the
- * device-side generation counter.  Semantics per child are stated in csrc/ws_gp.cu.
+ * problem's offspring are the same alone or batched with others, and graph replays advance each
+ * problem's device-side generation counter (ws_gp_set_generation sets them all).  Semantics per child are stated in csrc/ws_gp.cu.
  *   fitness: [B] of dtype, lower is better (e.g. the MSE written by ws_batch_eval)
  *   population / constants: rewritten in place with the next generation
  */
@@ -233,6 +233,8 @@ typedef struct ws_gp_problem {
   int64_t num_vars;
   const ws_token_map* ids;   /* this problem's token IDs                                 */
   uint64_t seed;             /* this problem's random stream                             */
+  uint64_t generation;       /* this problem's next generation number (0 for a new run);
+                                the device counter advances by one per ws_gp_step        */
 } ws_gp_problem;
 
 typedef struct ws_gp_opts {
@@ -252,7 +254,7 @@ ws_status ws_gp_workspace_bytes(int32_t dtype, const ws_gp_problem* problems, in
                                 int64_t L, size_t* out_bytes);
 ws_status ws_gp_create(int32_t dtype, const ws_gp_problem* problems, int32_t n_problems, int64_t L,
                        const ws_gp_opts* opts, void* workspace, size_t workspace_bytes,
-                       ws_gp** out);
+                       void* stream, ws_gp** out);
 ws_status ws_gp_step(ws_gp* gp, void* stream);
 ws_status ws_gp_set_generation(ws_gp* gp, uint64_t generation, void* stream);
 void ws_gp_destroy(ws_gp* gp);

@@ -82,7 +82,7 @@ class GpProblem(C.Structure):
     """ws_gp_problem: one problem of a batched GP generation (device pointers)."""
     _fields_ = [("population", C.c_void_p), ("B", C.c_int64), ("constants", C.c_void_p),
                 ("K", C.c_int64), ("fitness", C.c_void_p), ("num_vars", C.c_int64),
-                ("ids", C.POINTER(TokenMap)), ("seed", C.c_uint64)]
+                ("ids", C.POINTER(TokenMap)), ("seed", C.c_uint64), ("generation", C.c_uint64)]
 
 
 class GpOpts(C.Structure):
@@ -112,12 +112,12 @@ _SIGS = {
     "ws_batch_workspace_bytes": (_I32, [_I32, _P, _I32, _I64, C.POINTER(FitnessOpts),
                                         C.POINTER(C.c_size_t)]),
     "ws_batch_create": (_I32, [_I32, _P, _I32, _I64, C.POINTER(FitnessOpts), _P, C.c_size_t,
-                               C.POINTER(_P)]),
+                               _P, C.POINTER(_P)]),
     "ws_batch_eval": (_I32, [_P, _I32, _P]),
     "ws_batch_info": (_I64, [_P, _I32]),
     "ws_batch_destroy": (None, [_P]),
     "ws_gp_workspace_bytes": (_I32, [_I32, _P, _I32, _I64, C.POINTER(C.c_size_t)]),
-    "ws_gp_create": (_I32, [_I32, _P, _I32, _I64, C.POINTER(GpOpts), _P, C.c_size_t,
+    "ws_gp_create": (_I32, [_I32, _P, _I32, _I64, C.POINTER(GpOpts), _P, C.c_size_t, _P,
                             C.POINTER(_P)]),
     "ws_gp_step": (_I32, [_P, _P]),
     "ws_gp_set_generation": (_I32, [_P, C.c_uint64, _P]),

@@ -44,8 +44,8 @@ class BatchProblem:
 
 class BatchedFitness:
     """Per-program losses of many problems from one launch sequence.  The plan (and the
-    device descriptors it uploads) fixes every tensor's address and shape: rewrite populations
-    and constants in place between calls, never reallocate them."""
+    device descriptors it writes on the current stream) fixes every tensor's address and shape:
+    rewrite populations and constants in place between calls, never reallocate them."""
 
     def __init__(self, problems: Sequence[BatchProblem], *, loss: str = "mse",
                  policy: str = "classic", strict_mode: int = 0, schedule: int = 0,
@@ -111,7 +111,8 @@ class BatchedFitness:
         h = C.c_void_p()
         N.check(lib.ws_batch_create(code, C.cast(arr, C.c_void_p), len(arr), L,
                                     C.byref(self._opts), ptr(self.workspace),
-                                    int(self.workspace.numel()), C.byref(h)))
+                                    int(self.workspace.numel()), stream_of(self.workspace),
+                                    C.byref(h)))
         self._h = h
         self.L = L
 

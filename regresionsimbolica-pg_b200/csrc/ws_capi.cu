@@ -303,7 +303,7 @@ ws_status ws_batch_workspace_bytes(int32_t dtype, const ws_problem* problems, in
 
 ws_status ws_batch_create(int32_t dtype, const ws_problem* problems, int32_t n_problems, int64_t L,
                           const ws_fitness_opts* opts, void* workspace, size_t workspace_bytes,
-                          ws_batch** out_batch) {
+                          void* stream, ws_batch** out_batch) {
   clear_error();
   if (!out_batch) return fail("out_batch is null");
   *out_batch = nullptr;
@@ -312,7 +312,8 @@ ws_status ws_batch_create(int32_t dtype, const ws_problem* problems, int32_t n_p
   if (st != WS_OK) return st;
   void* h = nullptr;
   st = batch_create(dtype, rq.data(), (int)rq.size(), L, opts->strict_mode ? 1 : 0, opts->policy,
-                    opts->loss, opts->schedule, opts->invalid_value, workspace, workspace_bytes, &h);
+                    opts->loss, opts->schedule, opts->invalid_value, workspace, workspace_bytes,
+                    (cudaStream_t)stream, &h);
   if (st == WS_OK) *out_batch = static_cast<ws_batch*>(h);
   return st;
 }

@@ -30,6 +30,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <cstring>
 #include <cfloat>
 #include <mutex>
 #include <map>
@@ -128,6 +129,29 @@ __global__ void write_desc_kernel(const ProbDesc<T> d, const TokenLut lut, ProbD
   const unsigned* s = reinterpret_cast<const unsigned*>(&lut);
   unsigned* o = reinterpret_cast<unsigned*>(lut_dst);
   for (int i = threadIdx.x; i < (int)(sizeof(TokenLut) / 4); i += blockDim.x) o[i] = s[i];
+}
+
+// Up to kUploadChunk descriptors and token tables of a batch, passed as one kernel argument and
+// copied into the workspace: batch plans reach the device in stream order, without a host-side
+// copy that would wait for the work already queued.
+constexpr int kUploadChunk = 16;
+template <typename T>
+struct DescChunk {
+  int n, base;
+  ProbDesc<T> d[kUploadChunk];
+  TokenLut lut[kUploadChunk];
+};
+template <typename T>
+__global__ void __launch_bounds__(128) upload_desc_kernel(const DescChunk<T> c,
+                                                          ProbDesc<T>* __restrict__ dst,
+                                                          TokenLut* __restrict__ lut_dst) {
+  const int nd = c.n * (int)(sizeof(ProbDesc<T>) / 4), nl = c.n * (int)(sizeof(TokenLut) / 4);
+  const unsigned* sd = reinterpret_cast<const unsigned*>(c.d);
+  const unsigned* sl = reinterpret_cast<const unsigned*>(c.lut);
+  unsigned* od = reinterpret_cast<unsigned*>(dst + c.base);
+  unsigned* ol = reinterpret_cast<unsigned*>(lut_dst + c.base);
+  for (int i = threadIdx.x; i < nd; i += blockDim.x) od[i] = sd[i];
+  for (int i = threadIdx.x; i < nl; i += blockDim.x) ol[i] = sl[i];
 }
 
 // FP64 variance of y (population variance, same rows as the loss) for WS_LOSS_R2; one block per
@@ -1407,7 +1431,7 @@ ws_status batch_workspace_bytes(int dtype, const ProblemRequest* probs, int n, i
 
 ws_status batch_create(int dtype, const ProblemRequest* probs, int n, int64_t L, int strict,
                        int policy, int loss, int schedule, double invalid_value, void* workspace,
-                       size_t workspace_bytes, void** out) {
+                       size_t workspace_bytes, cudaStream_t stream, void** out) {
   const Sched sc = batch_schedule(probs, n, schedule);
   BatchState* bs = new BatchState();
   bs->dtype = dtype;
@@ -1442,12 +1466,19 @@ ws_status batch_create(int dtype, const ProblemRequest* probs, int n, int64_t L,
       descs.push_back(make_desc<T>(probs[i], bs->plan.pp[i]));
       luts.push_back(probs[i].lut);
     }
-    if (!descs.empty()) {
-      cudaError_t e = cudaMemcpy(bs->wsb + bs->lay.desc_off, descs.data(),
-                                 descs.size() * sizeof(ProbDesc<T>), cudaMemcpyHostToDevice);
-      if (e == cudaSuccess)
-        e = cudaMemcpy(bs->wsb + bs->lay.lut_off, luts.data(), luts.size() * sizeof(TokenLut),
-                       cudaMemcpyHostToDevice);
+    for (size_t b0 = 0; b0 < descs.size(); b0 += kUploadChunk) {
+      DescChunk<T> ch;
+      std::memset(&ch, 0, sizeof(ch));
+      ch.base = (int)b0;
+      ch.n = (int)std::min(descs.size() - b0, (size_t)kUploadChunk);
+      for (int j = 0; j < ch.n; ++j) {
+        ch.d[j] = descs[b0 + j];
+        ch.lut[j] = luts[b0 + j];
+      }
+      upload_desc_kernel<T><<<1, 128, 0, stream>>>(
+          ch, reinterpret_cast<ProbDesc<T>*>(bs->wsb + bs->lay.desc_off),
+          reinterpret_cast<TokenLut*>(bs->wsb + bs->lay.lut_off));
+      cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return fail_cuda(e, "batch descriptor upload");
     }
     return WS_OK;

@@ -8,7 +8,7 @@
 // generation of every problem is three launches (elite argmin, children, copy-back), with a
 // counter-based generator (SplitMix64, Steele-Lea-Flood 2014) keyed by (problem seed,
 // generation, child), so a problem's offspring do not depend on what else shares the launch and
-// the step is graph-capturable (the generation counter lives on the device).
+// the step is graph-capturable (each problem's generation counter lives on the device).
 //
 // Per child c of a problem with B programs of width L (draws in this order):
 //   c == 0 with elitism: the best program (lowest fitness, NaN last, lowest index) unchanged.
@@ -27,6 +27,7 @@
 #include <cstdint>
 #include <cstring>
 #include <cmath>
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -183,7 +184,7 @@ __global__ void __launch_bounds__(128) gp_child_kernel(const GpDesc<T>* __restri
     return;
   }
   Rng r;
-  r.s = sm_mix(d.seed + 0x9E3779B97F4A7C15ull * (*generation + 1ull)) ^
+  r.s = sm_mix(d.seed + 0x9E3779B97F4A7C15ull * (generation[pi] + 1ull)) ^
         sm_mix((uint64_t)c + 0x632BE59BD9B4E019ull);
   const int64_t a = tournament(d, r, P.tournament_size, P.parsimony_eps, L);
   const uint8_t* ra = d.pop + a * L;
@@ -262,7 +263,8 @@ __global__ void __launch_bounds__(128) gp_child_kernel(const GpDesc<T>* __restri
   }
 }
 
-// Next generation back into the problems' own tensors; thread 0 then advances the counter.
+// Next generation back into the problems' own tensors; child 0 of every problem advances its
+// problem's counter (the child kernel that read the counters has completed).
 template <typename T>
 __global__ void __launch_bounds__(128) gp_copyback_kernel(const GpDesc<T>* __restrict__ desc, int n,
                                                           int64_t total, int L, int Kmax,
@@ -270,16 +272,37 @@ __global__ void __launch_bounds__(128) gp_copyback_kernel(const GpDesc<T>* __res
                                                           const T* __restrict__ consts_s,
                                                           uint64_t* __restrict__ generation) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g == 0) *generation += 1ull;
   if (g >= total) return;
   const int pi = find_gp_problem(desc, n, g);
   const GpDesc<T>& d = desc[pi];
   const int64_t c = g - d.child0;
+  if (c == 0) generation[pi] += 1ull;
   for (int j = 0; j < L; ++j) d.pop[c * L + j] = pop_s[g * (int64_t)L + j];
   for (int k = 0; k < d.K; ++k) d.consts[c * d.K + k] = consts_s[g * (int64_t)Kmax + k];
 }
 
-__global__ void gp_set_generation_kernel(uint64_t* generation, uint64_t v) { *generation = v; }
+__global__ void gp_set_generation_kernel(uint64_t* generation, int n, uint64_t v) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) generation[i] = v;
+}
+
+// Up to kGpUploadChunk descriptors (and starting generations) as one kernel argument, copied
+// into the workspace in stream order.
+constexpr int kGpUploadChunk = 16;
+template <typename T>
+struct GpChunk {
+  int n, base;
+  GpDesc<T> d[kGpUploadChunk];
+  uint64_t gen[kGpUploadChunk];
+};
+template <typename T>
+__global__ void __launch_bounds__(128) gp_upload_kernel(const GpChunk<T> c, GpDesc<T>* dst,
+                                                        uint64_t* gen_dst) {
+  const int nd = c.n * (int)(sizeof(GpDesc<T>) / 4);
+  const unsigned* sd = reinterpret_cast<const unsigned*>(c.d);
+  unsigned* od = reinterpret_cast<unsigned*>(dst + c.base);
+  for (int i = threadIdx.x; i < nd; i += blockDim.x) od[i] = sd[i];
+  for (int i = threadIdx.x; i < c.n; i += blockDim.x) gen_dst[c.base + i] = c.gen[i];
+}
 
 struct GpLayout {
   size_t desc, elite, gen, pop_s, consts_s, total;
@@ -293,7 +316,7 @@ GpLayout gp_layout(int n, int64_t total, int64_t L, int Kmax, size_t tsz, size_t
   w.elite = off;
   off = align_up(off + (size_t)n * sizeof(int64_t), 256);
   w.gen = off;
-  off = align_up(off + 16, 256);
+  off = align_up(off + (size_t)(n > 0 ? n : 1) * sizeof(uint64_t), 256);
   w.pop_s = off;
   off = align_up(off + (size_t)total * L, 256);
   w.consts_s = off;
@@ -395,7 +418,7 @@ ws_status ws_gp_workspace_bytes(int32_t dtype, const ws_gp_problem* problems, in
 
 ws_status ws_gp_create(int32_t dtype, const ws_gp_problem* problems, int32_t n_problems, int64_t L,
                        const ws_gp_opts* opts, void* workspace, size_t workspace_bytes,
-                       ws_gp** out) {
+                       void* stream, ws_gp** out) {
   clear_error();
   if (!out || !opts) return fail("options and output handle are required");
   *out = nullptr;
@@ -414,6 +437,9 @@ ws_status ws_gp_create(int32_t dtype, const ws_gp_problem* problems, int32_t n_p
   auto upload = [&](auto tag) -> ws_status {
     using T = decltype(tag);
     std::vector<GpDesc<T>> descs;
+    std::vector<uint64_t> gens;  // each problem's starting generation, in descriptor order
+    for (int i = 0; i < n_problems; ++i)
+      if (problems[i].B > 0) gens.push_back(problems[i].generation);
     ws_status s2 = gp_build<T>(*gs, problems, n_problems, descs);
     if (s2 != WS_OK) return s2;
     gs->n = (int)descs.size();
@@ -423,12 +449,21 @@ ws_status ws_gp_create(int32_t dtype, const ws_gp_problem* problems, int32_t n_p
                 " bytes (256-byte aligned) required (got " + std::to_string(workspace_bytes) + ")");
       return WS_ERR_WORKSPACE;
     }
-    cudaError_t e = cudaSuccess;
-    if (!descs.empty())
-      e = cudaMemcpy(gs->wsb + gs->lay.desc, descs.data(), descs.size() * sizeof(GpDesc<T>),
-                     cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(gs->wsb + gs->lay.gen, 0, 16);
-    if (e != cudaSuccess) return fail_cuda(e, "GP descriptor upload");
+    for (size_t b0 = 0; b0 < descs.size(); b0 += kGpUploadChunk) {
+      GpChunk<T> ch;
+      std::memset(&ch, 0, sizeof(ch));
+      ch.base = (int)b0;
+      ch.n = (int)std::min(descs.size() - b0, (size_t)kGpUploadChunk);
+      for (int j = 0; j < ch.n; ++j) {
+        ch.d[j] = descs[b0 + j];
+        ch.gen[j] = gens[b0 + j];
+      }
+      gp_upload_kernel<T><<<1, 128, 0, (cudaStream_t)stream>>>(
+          ch, reinterpret_cast<GpDesc<T>*>(gs->wsb + gs->lay.desc),
+          reinterpret_cast<uint64_t*>(gs->wsb + gs->lay.gen));
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return fail_cuda(e, "GP descriptor upload");
+    }
     return WS_OK;
   };
   st = dtype == WS_F64 ? upload(double()) : upload(float());
@@ -471,8 +506,9 @@ ws_status ws_gp_set_generation(ws_gp* handle, uint64_t generation, void* stream)
   clear_error();
   if (!handle) return fail("handle is null");
   GpState* gs = reinterpret_cast<GpState*>(handle);
-  gp_set_generation_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(
-      reinterpret_cast<uint64_t*>(gs->wsb + gs->lay.gen), generation);
+  if (gs->n == 0) return WS_OK;
+  gp_set_generation_kernel<<<1, 128, 0, (cudaStream_t)stream>>>(
+      reinterpret_cast<uint64_t*>(gs->wsb + gs->lay.gen), gs->n, generation);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? WS_OK : fail_cuda(e, "generation write");
 }

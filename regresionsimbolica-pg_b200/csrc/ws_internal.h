@@ -65,7 +65,7 @@ ws_status batch_workspace_bytes(int dtype, const ProblemRequest* probs, int n, i
                                 int strict, int schedule, size_t* out);
 ws_status batch_create(int dtype, const ProblemRequest* probs, int n, int64_t L, int strict,
                        int policy, int loss, int schedule, double invalid_value, void* workspace,
-                       size_t workspace_bytes, void** out);
+                       size_t workspace_bytes, cudaStream_t stream, void** out);
 ws_status batch_eval(void* handle, int phase, cudaStream_t stream);
 void batch_destroy(void* handle);
 int64_t batch_info(void* handle, int what);

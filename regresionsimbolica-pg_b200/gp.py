@@ -6,15 +6,16 @@
 `problems` are the same BatchProblem records the batched evaluator uses (their population and
 constants tensors are rewritten in place, so a BatchedFitness over them sees every new
 generation without re-planning); `fitness[p]` is problem p's [B] loss tensor (lower is better),
-e.g. BatchedFitness.outputs.  A generation is three launches; the generation counter lives on
-the device, so evaluate + step can be captured once as a CUDA graph and replayed per generation.
+e.g. BatchedFitness.outputs.  A generation is three launches; the generation counters live on
+the device (one per problem, starting at `generations[p]`), so evaluate + step can be captured
+once as a CUDA graph and replayed per generation.
 Offspring of a problem depend only on its seed, the generation and its own population and
 fitness -- never on the other problems of the launch.
 """
 from __future__ import annotations
 
 import ctypes as C
-from typing import List, Sequence
+from typing import List, Optional, Sequence
 
 import torch
 
@@ -25,13 +26,18 @@ from .grammar import PI_VAL, E_VAL
 
 class GPStep:
     def __init__(self, problems: Sequence, fitness: Sequence[torch.Tensor], seeds: Sequence[int],
-                 *, tournament_size: int = 3, elitism: bool = True, crossover_rate: float = 0.7,
+                 *, generations: Optional[Sequence[int]] = None, tournament_size: int = 3,
+                 elitism: bool = True, crossover_rate: float = 0.7,
                  mutation_rate: float = 0.05, const_mutation_rate: float = 0.1,
                  const_sigma: float = 0.1, parsimony_eps: float = 1e-9):
         if not problems:
             raise ValueError("no problems")
         if len(fitness) != len(problems) or len(seeds) != len(problems):
             raise ValueError("one fitness tensor and one seed per problem")
+        if generations is None:
+            generations = [0] * len(problems)
+        if len(generations) != len(problems):
+            raise ValueError("one starting generation per problem")
         L = int(problems[0].population.shape[1])
         dtype = fitness[0].dtype
         code = dtype_code(dtype)
@@ -56,7 +62,7 @@ class GPStep:
             self._keep += [p.population, c, f, tmap]
             arr[i] = N.GpProblem(ptr(p.population), B, ptr(c) if K > 0 else None, K, ptr(f),
                                  len(p.grammar.active_variables), C.pointer(tmap),
-                                 int(s) & 0xFFFFFFFFFFFFFFFF)
+                                 int(s) & 0xFFFFFFFFFFFFFFFF, int(generations[i]))
         self._arr = arr
         self._opts = N.GpOpts(int(tournament_size), 1 if elitism else 0, float(crossover_rate),
                               float(mutation_rate), float(const_mutation_rate), float(const_sigma),
@@ -68,7 +74,8 @@ class GPStep:
         self.workspace = torch.empty(max(int(need.value), 256), dtype=torch.uint8, device=self.device)
         h = C.c_void_p()
         N.check(lib.ws_gp_create(code, C.cast(arr, C.c_void_p), len(arr), L, C.byref(self._opts),
-                                 ptr(self.workspace), int(self.workspace.numel()), C.byref(h)))
+                                 ptr(self.workspace), int(self.workspace.numel()),
+                                 stream_of(self.workspace), C.byref(h)))
         self._h = h
 
     def step(self, stream=None) -> None:

@@ -214,3 +214,33 @@ def batched_workload(seed: int = 0, n_problems: int = 256, programs: int = 2048,
         y = (y.astype(np.float64) * (1.0 + noise_rel * rng.standard_normal(D))).astype(np.float32)
         out.append(EvalWorkload(g, pop, consts, X, y))
     return BatchWorkload(out)
+
+
+def serving_stream(seed: int = 0, n_requests: int = 8, rate: float = 20.0,
+                   fit_fraction: float = 0.5, rows=(1_000, 200_000), n_vars=(1, 8),
+                   population: int = 4096, generations: int = 30, L: int = 64, K: int = 8,
+                   x_range=(-3.0, 3.0), depth=(3, 6), noise: float = 0.01,
+                   operators: Optional[Sequence[str]] = None) -> list:
+    """Serving stream: Poisson arrivals at `rate` per second of fit and evaluate requests; rows
+    log-uniform in [rows], features uniform in [n_vars], X ~ U[x_range], targets from random
+    depth-U{depth} trees plus N(0, (noise * std y)^2); every request carries `population`
+    random programs (the initial population of a fit, or the programs an evaluate scores)."""
+    from .serving import Request
+    rng = np.random.default_rng(seed)
+    ops = BENCH_OPERATORS if operators is None else operators
+    lo, hi = np.log10(rows[0]), np.log10(rows[1])
+    t = 0.0
+    out = []
+    for rid in range(n_requests):
+        t += float(rng.exponential(1.0 / rate))
+        D = int(np.floor(10.0 ** rng.uniform(lo, hi)))
+        V = int(rng.integers(n_vars[0], n_vars[1] + 1))
+        g = GPUGrammar(num_variables=V, operators=ops)
+        pop = random_programs(g, population, 3, L, L, rng, max_consts=K)
+        consts = rng.uniform(-2.0, 2.0, size=(population, K)).astype(np.float32)
+        X = rng.uniform(*x_range, size=(V, D)).astype(np.float32)
+        y, _ = random_target(rng, X, int(rng.integers(depth[0], depth[1] + 1)), noise_rel=noise)
+        kind = "fit" if rng.random() < fit_fraction else "evaluate"
+        out.append(Request(rid, kind, g, X, y, pop, consts,
+                           generations if kind == "fit" else 0, seed * 100_003 + rid, t))
+    return out
