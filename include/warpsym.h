@@ -214,6 +214,58 @@ int64_t ws_batch_info(const ws_batch* batch, int32_t what);
 void ws_batch_destroy(ws_batch* batch);
 
 /*
+ * The reference extension's genetic-operator and tracker exports, same inputs -> same outputs.
+ *
+ * ws_mutate_population replaces `mutate_population` (bindings.cpp:457 -> launch_mutation_kernel,
+ *   rpn_kernels.cu:772-845): each non-PAD token with rand_floats[i] < mutation_rate becomes
+ *   arity_k_ids[rand_ints[i] % n_k] of its own arity k (token_arities[tok], 0 outside the table).
+ * ws_crossover_splicing replaces `crossover_splicing` (bindings.cpp:458 ->
+ *   rpn_kernels.cu:927-1016,1266-1300): child1 = p1[0:s1] + p2[s2:e2+1] + p1[e1+1:], child2 the
+ *   mirror image, PAD where a source index leaves the row; pairs whose cx_mask byte is 0 copy
+ *   their parents (cx_mask may be NULL).
+ * ws_constant_perturbation replaces `constant_perturbation` (bindings.cpp:463 ->
+ *   rpn_kernels.cu:1455-1535): hash-seeded rows get Box-Muller multiplicative noise, clamped.
+ * ws_generate_random_rpn replaces `generate_random_rpn` (bindings.cpp:507 ->
+ *   genrand_kernels.cu:70-210): one valid program per row from a per-row xorshift64 stream.
+ * ws_update_best / ws_check_improvement / ws_batch_update_best replace `update_best`,
+ *   `check_improvement`, `batch_update_best` (bindings.cpp:565-590 ->
+ *   best_tracker_kernels.cu:47-340).  The reference's update_best and check_improvement let
+ *   several blocks update one result without ordering (best_tracker_kernels.cu:104-135,
+ *   :168-172); here one block reduces all programs -- the reference's result whenever it is
+ *   deterministic (B <= 256), otherwise the global minimum with its tie rules.
+ */
+ws_status ws_mutate_population(uint8_t* population, int64_t B, int64_t L, const float* rand_floats,
+                               const int64_t* rand_ints, const int32_t* token_arities,
+                               int64_t vocab_size, const uint8_t* arity0_ids, int64_t n0,
+                               const uint8_t* arity1_ids, int64_t n1, const uint8_t* arity2_ids,
+                               int64_t n2, float mutation_rate, int32_t pad_id, void* stream);
+ws_status ws_crossover_splicing(const uint8_t* parent1, const uint8_t* parent2, int64_t N,
+                                int64_t L, const int64_t* starts1, const int64_t* ends1,
+                                const int64_t* starts2, const int64_t* ends2, uint8_t* child1,
+                                uint8_t* child2, int32_t pad_id, const uint8_t* cx_mask,
+                                void* stream);
+ws_status ws_constant_perturbation(int32_t dtype, void* constants, int64_t B, int64_t K,
+                                   float rate, float sigma, float c_min, float c_max,
+                                   uint32_t seed, void* stream);
+ws_status ws_generate_random_rpn(uint8_t* population, int64_t B, int64_t L,
+                                 const uint8_t* terminal_ids, int64_t n_terminals,
+                                 const uint8_t* unary_ids, int64_t n_unary,
+                                 const uint8_t* binary_ids, int64_t n_binary, uint64_t seed,
+                                 float term_weight, float unary_weight, float bin_weight,
+                                 void* stream);
+ws_status ws_update_best(const int64_t* population, int64_t B, int64_t L, const float* constants,
+                         int64_t K, const float* fitness, int64_t* tracker_rpn,
+                         float* tracker_consts, float* tracker_rmse, int32_t* tracker_idx,
+                         int32_t* tracker_gen, int32_t* tracker_len, int32_t* tracker_updated,
+                         int32_t current_generation, float tolerance, void* stream);
+ws_status ws_check_improvement(const float* fitness, int64_t B, const float* tracked_rmse,
+                               int32_t* improved, float tolerance, void* stream);
+ws_status ws_batch_update_best(const uint8_t* population, int64_t B, int64_t L,
+                               const float* constants, int64_t K, const float* fitness,
+                               uint8_t* best_rpn, float* best_consts, float* best_rmse,
+                               int32_t* best_idx, float tolerance, void* stream);
+
+/*
  * One genetic-programming generation, in place, for many problems at once.  Replaces the
  * breeding half of `evolve_generation` (rpn_kernels.cu:1810-2237: tournament K16, elitism
  * :1905-1907, subtree crossover K5/K6/K10, same-arity point mutation K7/K11, constant

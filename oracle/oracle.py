@@ -65,6 +65,14 @@ def lib():
                 _P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P, _P, _P, C.c_int, _P, C.c_int, _P,
                 C.c_int, C.c_uint64, C.c_uint64, C.c_int, C.c_int, C.c_float, C.c_float,
                 C.c_float, C.c_float, C.c_float, _P, _P]
+        h.ws_oracle_mutate.argtypes = [_P, C.c_int64, _P, _P, _P, C.c_int, _P, C.c_int, _P,
+                                       C.c_int, _P, C.c_int, C.c_float, C.c_int]
+        h.ws_oracle_splice.argtypes = [_P, _P, C.c_int64, C.c_int64, _P, _P, _P, _P, _P, _P, _P,
+                                       C.c_int]
+        h.ws_oracle_genrand.argtypes = [_P, C.c_int64, C.c_int, _P, C.c_int, _P, C.c_int, _P,
+                                        C.c_int, C.c_uint64, C.c_float, C.c_float, C.c_float]
+        h.ws_oracle_batch_best.argtypes = [_P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P, _P,
+                                           _P, _P, C.c_float]
         h.ws_oracle_validate.argtypes = [_P, C.c_int32, C.c_int64, C.c_int64, _P, C.c_int64,
                                          C.c_int32, C.c_int32, _P]
         h.ws_oracle_subtree_ranges.argtypes = [_P, C.c_int64, C.c_int64, _P, C.c_int64,
@@ -353,3 +361,51 @@ def gp_step(grammar, pop, consts, fitness, seed, generation, tournament_size=3, 
         crossover_rate, mutation_rate, const_mutation_rate, const_sigma, parsimony_eps,
         _p(out_p), _p(out_c))
     return out_p, out_c
+
+
+def mutate(pop, rand_floats, rand_ints, arities, a0, a1, a2, rate, pad=0):
+    out = np.ascontiguousarray(pop, dtype=np.uint8).copy()
+    rf = np.ascontiguousarray(rand_floats, dtype=np.float32)
+    ri = np.ascontiguousarray(rand_ints, dtype=np.int64)
+    ar = np.ascontiguousarray(arities, dtype=np.int32)
+    a0, a1, a2 = (np.ascontiguousarray(a, dtype=np.uint8) for a in (a0, a1, a2))
+    lib().ws_oracle_mutate(_p(out), out.size, _p(rf), _p(ri), _p(ar), len(ar), _p(a0), len(a0),
+                           _p(a1), len(a1), _p(a2), len(a2), rate, pad)
+    return out
+
+
+def splice(p1, p2, s1, e1, s2, e2, mask=None, pad=0):
+    p1 = np.ascontiguousarray(p1, dtype=np.uint8)
+    p2 = np.ascontiguousarray(p2, dtype=np.uint8)
+    N, L = p1.shape
+    ss = [np.ascontiguousarray(a, dtype=np.int64) for a in (s1, e1, s2, e2)]
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    c1, c2 = np.zeros_like(p1), np.zeros_like(p2)
+    lib().ws_oracle_splice(_p(p1), _p(p2), N, L, *[_p(a) for a in ss], _p(m) if m is not None else None,
+                           _p(c1), _p(c2), pad)
+    return c1, c2
+
+
+def genrand(B, L, term, un, binr, seed, wt, wu, wb):
+    term, un, binr = (np.ascontiguousarray(a, dtype=np.uint8) for a in (term, un, binr))
+    out = np.zeros((B, L), dtype=np.uint8)
+    lib().ws_oracle_genrand(_p(out), B, L, _p(term), len(term), _p(un), len(un), _p(binr),
+                            len(binr), seed, wt, wu, wb)
+    return out
+
+
+def batch_best(pop, consts, fit, best_rmse, tol=1e-9):
+    """(best_rpn [L], best_consts [K], best_rmse, best_idx) after one single-block update from
+    an empty tracker with `best_rmse`."""
+    pop = np.ascontiguousarray(pop, dtype=np.uint8)
+    consts = np.ascontiguousarray(consts, dtype=np.float32)
+    fit = np.ascontiguousarray(fit, dtype=np.float32)
+    B, L = pop.shape
+    K = consts.shape[1]
+    rpn = np.zeros(L, np.uint8)
+    bc = np.zeros(max(K, 1), np.float32)
+    br = np.array([best_rmse], np.float32)
+    bi = np.array([-1], np.int32)
+    lib().ws_oracle_batch_best(_p(pop), B, L, _p(consts), K, _p(fit), _p(rpn), _p(bc), _p(br),
+                               _p(bi), tol)
+    return rpn, bc[:K], float(br[0]), int(bi[0])

@@ -122,6 +122,17 @@ _SIGS = {
     "ws_gp_step": (_I32, [_P, _P]),
     "ws_gp_set_generation": (_I32, [_P, C.c_uint64, _P]),
     "ws_gp_destroy": (None, [_P]),
+    "ws_mutate_population": (_I32, [_P, _I64, _I64, _P, _P, _P, _I64, _P, _I64, _P, _I64, _P,
+                                    _I64, C.c_float, _I32, _P]),
+    "ws_crossover_splicing": (_I32, [_P, _P, _I64, _I64, _P, _P, _P, _P, _P, _P, _I32, _P, _P]),
+    "ws_constant_perturbation": (_I32, [_I32, _P, _I64, _I64, C.c_float, C.c_float, C.c_float,
+                                        C.c_float, C.c_uint32, _P]),
+    "ws_generate_random_rpn": (_I32, [_P, _I64, _I64, _P, _I64, _P, _I64, _P, _I64, C.c_uint64,
+                                      C.c_float, C.c_float, C.c_float, _P]),
+    "ws_update_best": (_I32, [_P, _I64, _I64, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _I32,
+                              C.c_float, _P]),
+    "ws_check_improvement": (_I32, [_P, _I64, _P, _P, C.c_float, _P]),
+    "ws_batch_update_best": (_I32, [_P, _I64, _I64, _P, _I64, _P, _P, _P, _P, _P, C.c_float, _P]),
     "ws_eval_rpn_backward": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
                                     C.POINTER(TokenMap), _P]),
     "ws_decode_rpn": (_I32, [_P, _I64, _I64, _P, _I32, _I64, C.POINTER(C.c_char_p), _I64, _P,

@@ -404,3 +404,128 @@ def simplify_batch(population, arities, val_table, literal_ids, literal_vals, ma
                                       ptr(val_table), ptr(literal_ids), ptr(literal_vals),
                                       int(literal_ids.size(0)), int(max_passes), C.byref(ids),
                                       stream_of(population)))
+
+
+# ---- genetic operators and best tracking (next-tier exports of bindings.cpp) -----------------
+def _u8_ptr_n(t, name):
+    check_cuda(t, name)
+    _expect(t, name, torch.uint8)
+    return ptr(t) if t.numel() > 0 else None, int(t.numel())
+
+
+def mutate_population(population, rand_floats, rand_ints, token_arities, arity_0_ids,
+                      arity_1_ids, arity_2_ids, mutation_rate, PAD_ID):
+    """Point mutation from pre-drawn randoms, in place (bindings.cpp:457 ->
+    rpn_kernels.cu:772-845)."""
+    for t, nm in ((population, "population"), (rand_floats, "rand_floats"),
+                  (rand_ints, "rand_ints"), (token_arities, "token_arities")):
+        check_cuda(t, nm)
+    _expect(population, "population", torch.uint8)
+    _expect(rand_floats, "rand_floats", torch.float32)
+    _expect(rand_ints, "rand_ints", torch.int64)
+    _expect(token_arities, "token_arities", torch.int32)
+    B, L = int(population.size(0)), int(population.size(1))
+    if rand_floats.numel() < B * L or rand_ints.numel() < B * L:
+        raise RuntimeError("rand_floats and rand_ints must hold [B, L] values")
+    a0, n0 = _u8_ptr_n(arity_0_ids, "arity_0_ids")
+    a1, n1 = _u8_ptr_n(arity_1_ids, "arity_1_ids")
+    a2, n2 = _u8_ptr_n(arity_2_ids, "arity_2_ids")
+    N.check(N.lib().ws_mutate_population(ptr(population), B, L, ptr(rand_floats), ptr(rand_ints),
+                                         ptr(token_arities), int(token_arities.size(0)), a0, n0,
+                                         a1, n1, a2, n2, float(mutation_rate), int(PAD_ID),
+                                         stream_of(population)))
+
+
+def crossover_splicing(parent1, parent2, starts1, ends1, starts2, ends2, child1, child2, PAD_ID,
+                       cx_mask=None):
+    """Subtree splicing of parent pairs into children (bindings.cpp:458 ->
+    rpn_kernels.cu:927-1016,1266-1300)."""
+    for t, nm in ((parent1, "parent1"), (parent2, "parent2"), (child1, "child1"),
+                  (child2, "child2")):
+        check_cuda(t, nm)
+        _expect(t, nm, torch.uint8)
+    for t, nm in ((starts1, "starts1"), (ends1, "ends1"), (starts2, "starts2"), (ends2, "ends2")):
+        check_cuda(t, nm)
+        _expect(t, nm, torch.int64)
+    N_, L = int(parent1.size(0)), int(parent1.size(1))
+    mask = _optional(cx_mask)
+    if mask is not None:
+        check_cuda(mask, "cx_mask")
+        _expect(mask, "cx_mask", torch.bool)
+    N.check(N.lib().ws_crossover_splicing(ptr(parent1), ptr(parent2), N_, L, ptr(starts1),
+                                          ptr(ends1), ptr(starts2), ptr(ends2), ptr(child1),
+                                          ptr(child2), int(PAD_ID), ptr(mask),
+                                          stream_of(parent1)))
+
+
+def constant_perturbation(constants, rate, sigma, c_min, c_max, seed):
+    """In-place multiplicative constant noise (bindings.cpp:463 -> rpn_kernels.cu:1455-1535)."""
+    check_cuda(constants, "constants")
+    if constants.numel() == 0 or rate <= 0.0 or sigma <= 0.0:
+        return
+    B, K = int(constants.size(0)), int(constants.size(1))
+    N.check(N.lib().ws_constant_perturbation(dtype_code(constants.dtype), ptr(constants), B, K,
+                                             float(rate), float(sigma), float(c_min),
+                                             float(c_max), int(seed) & 0xFFFFFFFF,
+                                             stream_of(constants)))
+
+
+def generate_random_rpn(population, terminal_ids, unary_ids, binary_ids, seed, term_weight,
+                        unary_weight, bin_weight):
+    """Valid random programs, one per row (bindings.cpp:507 -> genrand_kernels.cu:70-210)."""
+    check_cuda(population, "population")
+    _expect(population, "population", torch.uint8)
+    t, nt = _u8_ptr_n(terminal_ids, "terminal_ids")
+    if nt <= 0:
+        raise RuntimeError("Must have at least one terminal token")
+    u, nu = _u8_ptr_n(unary_ids, "unary_ids")
+    b, nb = _u8_ptr_n(binary_ids, "binary_ids")
+    B, L = int(population.size(0)), int(population.size(1))
+    N.check(N.lib().ws_generate_random_rpn(ptr(population), B, L, t, nt, u, nu, b, nb,
+                                           int(seed) & 0xFFFFFFFFFFFFFFFF, float(term_weight),
+                                           float(unary_weight), float(bin_weight),
+                                           stream_of(population)))
+
+
+def update_best(population, constants, fitness, tracker_rpn, tracker_consts, tracker_rmse,
+                tracker_idx, tracker_gen, tracker_len, tracker_updated, current_generation,
+                tolerance=1e-9):
+    """Device-side best tracker (bindings.cpp:565 -> best_tracker_kernels.cu:47-136,238-282);
+    one block reduces every program (see include/warpsym.h on the reference's block race)."""
+    for t, nm in ((population, "population"), (constants, "constants"), (fitness, "fitness")):
+        check_cuda(t, nm)
+    _expect(population, "population", torch.int64)
+    _expect(constants, "constants", torch.float32)
+    _expect(fitness, "fitness", torch.float32)
+    B, L = int(population.size(0)), int(population.size(1))
+    K = int(constants.size(1))
+    N.check(N.lib().ws_update_best(ptr(population), B, L, ptr(constants), K, ptr(fitness),
+                                   ptr(tracker_rpn), ptr(tracker_consts), ptr(tracker_rmse),
+                                   ptr(tracker_idx), ptr(tracker_gen), ptr(tracker_len),
+                                   ptr(tracker_updated), int(current_generation), float(tolerance),
+                                   stream_of(fitness)))
+
+
+def check_improvement(fitness, tracked_rmse, improved, tolerance=1e-9):
+    """improved[0] = min(fitness) < tracked_rmse[0] - tolerance, without a host sync
+    (bindings.cpp:572 -> best_tracker_kernels.cu:141-173,284-305)."""
+    check_cuda(fitness, "fitness")
+    _expect(fitness, "fitness", torch.float32)
+    N.check(N.lib().ws_check_improvement(ptr(fitness), int(fitness.size(0)), ptr(tracked_rmse),
+                                         ptr(improved), float(tolerance), stream_of(fitness)))
+
+
+def batch_update_best(population, constants, fitness, best_rpn, best_consts, best_rmse, best_idx,
+                      tolerance=1e-9):
+    """Single-block best update used by the generation loop (bindings.cpp:576 ->
+    best_tracker_kernels.cu:178-231,307-340)."""
+    for t, nm in ((population, "population"), (constants, "constants"), (fitness, "fitness")):
+        check_cuda(t, nm)
+    _expect(population, "population", torch.uint8)
+    _expect(constants, "constants", torch.float32)
+    _expect(fitness, "fitness", torch.float32)
+    B, L = int(population.size(0)), int(population.size(1))
+    K = int(constants.size(1))
+    N.check(N.lib().ws_batch_update_best(ptr(population), B, L, ptr(constants), K, ptr(fitness),
+                                         ptr(best_rpn), ptr(best_consts), ptr(best_rmse),
+                                         ptr(best_idx), float(tolerance), stream_of(fitness)))
