@@ -48,11 +48,15 @@ def parse():
                     help="target CPU time of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--config", default="eval-scale", choices=["eval-scale", "batched", "serving"],
+    ap.add_argument("--config", default="eval-scale",
+                    choices=["eval-scale", "batched", "serving", "kernels"],
                     help="eval-scale: the evaluation-only scale test (default); batched: 256 "
                          "uneven problems scored by one graph-replayed launch per generation; "
                          "serving: a Poisson stream of fit/evaluate requests, continuously "
-                         "batched, against one request at a time")
+                         "batched, against one request at a time; kernels: every other kernel "
+                         "of the library on its own workload, timed against its roofline")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="kernels: fraction of the default sizes (smaller cases for profiling)")
     ap.add_argument("--requests", type=int, default=8)
     ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
     ap.add_argument("--problems", type=int, default=256)
@@ -623,8 +627,185 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def run_kernels(args):
+    """Every kernel beside the fitness evaluator on a workload of the benchmark configs' shapes,
+    timed with CUDA events (median of 5 after 3 warm-ups, L2 flushed before each), one JSON line
+    per kernel with its algorithmic bytes (HBM-bound kernels: GB/s against the measured copy
+    bandwidth) or node-evals (evaluating kernels: against 1 FP32 lane-op per node-eval)."""
+    import math
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    entry.load_package()
+    from warpsymbolic_b200 import synthetic, rpn_cuda_native as R
+    from warpsymbolic_b200.grammar import GPUGrammar, PI_VAL, E_VAL
+    from warpsymbolic_b200.simplifier import GPUSymbolicSimplifier
+    from warpsymbolic_b200.batch import BatchProblem
+    from warpsymbolic_b200.gp import GPStep
+    peaks, _ = measured_peaks()
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    fp32 = sms * 128 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    rng = np.random.default_rng(args.seed)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    sc = lambda n: max(1, int(n * args.scale))
+    out = []
+
+    def timed(name, fn, nbytes=None, evals=None, note=""):
+        for _ in range(3):
+            fn()
+        ms = []
+        for _ in range(5):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        t = statistics.median(ms) / 1e3
+        line = {"kernel": name, "ms": t * 1e3, "note": note}
+        if nbytes is not None:
+            line.update({"bound": "hbm", "algorithmic_bytes": int(nbytes),
+                         "achieved_gbs": nbytes / t / 1e9, "peak_gbs": hbm,
+                         "frac": nbytes / t / 1e9 / hbm})
+        if evals is not None:
+            line.update({"node_evals_per_s": evals / t, "fp32_lane_op_frac": evals / t / fp32})
+        out.append(line)
+        print(json.dumps(line), flush=True)
+
+    g = GPUGrammar(num_variables=5, operators=synthetic.BENCH_OPERATORS)
+    ids = g.scalar_ids()
+    B1, L = sc(1_048_576), 64
+    pop = synthetic.random_programs(g, B1, 3, 64, L, rng, max_consts=8)
+    dpop = T(pop)
+    ar = T(np.array(g.arities() + [0] * (256 - g.vocab_size), dtype=np.int32)[:g.vocab_size])
+    valid = torch.empty(B1, dtype=torch.bool, device=dev)
+    timed("validate_rpn_batch", lambda: R.validate_rpn_batch(dpop, ar, valid, 0),
+          nbytes=B1 * L + B1, note="%d x %d uint8" % (B1, L))
+    starts = torch.empty((B1, L), dtype=torch.int64, device=dev)
+    lens = torch.empty(B1, dtype=torch.int64, device=dev)
+    timed("find_subtree_ranges", lambda: R.find_subtree_ranges(dpop, ar, starts, 0, lens),
+          nbytes=B1 * L * 9 + B1 * 8, note="%d x %d -> int64 starts + lengths" % (B1, L))
+    pop64 = dpop.to(torch.int64)
+    timed("precompute_subtree_starts", lambda: R.precompute_subtree_starts(pop64, ar, starts),
+          nbytes=B1 * L * 16, note="%d x %d int64 -> int64" % (B1, L))
+    fit = T(rng.uniform(0, 10, size=B1).astype(np.float32))
+    ridx = T(rng.integers(0, B1, size=(B1, 4)))
+    lengths = T(rng.integers(3, 64, size=B1).astype(np.float32))
+    sel = torch.empty(B1, dtype=torch.int64, device=dev)
+    empty = torch.empty(0, device=dev)
+    timed("tournament_selection", lambda: R.tournament_selection(
+        fit, empty, ridx, torch.empty(0, dtype=torch.int32, device=dev), sel, lengths),
+        nbytes=B1 * (4 + 32 + 4 + 8), note="%d programs, tournament 4, parsimony lengths" % B1)
+    # genetic operators
+    arn = np.array(g.arities(), dtype=np.int32)
+    idsv = np.arange(g.vocab_size)
+    a0 = T(idsv[(arn == 0) & (idsv != 0)].astype(np.uint8))
+    a1 = T(idsv[arn == 1].astype(np.uint8))
+    a2 = T(idsv[arn == 2].astype(np.uint8))
+    rf = T(rng.random((B1, L), dtype=np.float32))
+    ri = T(rng.integers(0, 2**62, size=(B1, L)))
+    mp = dpop.clone()
+    timed("mutate_population", lambda: R.mutate_population(mp, rf, ri, ar, a0, a1, a2, 0.05, 0),
+          nbytes=B1 * L * (1 + 4 + 8 + 1), note="%d x %d, rate 0.05" % (B1, L))
+    Np = B1 // 2
+    s1 = T(rng.integers(0, 30, size=Np))
+    e1 = s1 + T(rng.integers(0, 20, size=Np))
+    s2 = T(rng.integers(0, 30, size=Np))
+    e2 = s2 + T(rng.integers(0, 20, size=Np))
+    c1 = torch.empty((Np, L), dtype=torch.uint8, device=dev)
+    c2 = torch.empty_like(c1)
+    timed("crossover_splicing", lambda: R.crossover_splicing(dpop[:Np], dpop[Np:2 * Np], s1, e1,
+                                                             s2, e2, c1, c2, 0),
+          nbytes=Np * (4 * L + 32), note="%d pairs x %d" % (Np, L))
+    cst = T(rng.uniform(-5, 5, size=(B1, 8)).astype(np.float32))
+    timed("constant_perturbation", lambda: R.constant_perturbation(cst, 0.3, 0.1, -25.0, 25.0, 7),
+          nbytes=B1 * 8 * 4 * 2, note="%d x 8 float32, rate 0.3" % B1)
+    gp = torch.empty((B1, L), dtype=torch.uint8, device=dev)
+    timed("generate_random_rpn", lambda: R.generate_random_rpn(gp, a0, a1, a2, 11, 0.4, 0.2, 0.4),
+          nbytes=B1 * L, note="%d x %d" % (B1, L))
+    brpn = torch.zeros(L, dtype=torch.uint8, device=dev)
+    bc = torch.zeros(8, dtype=torch.float32, device=dev)
+    br = torch.full((1,), 1e30, dtype=torch.float32, device=dev)
+    bi = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def bub():
+        br.fill_(1e30)
+        R.batch_update_best(dpop, cst, fit, brpn, bc, br, bi)
+    timed("batch_update_best", bub, nbytes=B1 * 4, note="%d programs (one block, as the "
+                                                      "reference)" % B1)
+    # simplifier
+    simp = GPUSymbolicSimplifier(g, dev)
+    Bs = sc(262_144)
+    sp = synthetic.random_programs(g, Bs, 3, 64, L, rng, max_consts=0)
+    spt = T(sp)
+    timed("simplify_batch", lambda: simp.simplify_batch(spt.clone(), None, max_passes=3),
+          nbytes=Bs * L * 16, note="%d x %d, 3 passes (int64 round trip)" % (Bs, L))
+    # constant fitting and gradients (constant-optimisation config shapes)
+    g3 = GPUGrammar(num_variables=3, operators=synthetic.BENCH_OPERATORS)
+    ids3 = g3.scalar_ids()
+    B3, L3, K3, D3 = sc(65_536), 40, 8, 16_384
+    p3 = synthetic.random_programs(g3, B3, 5, 40, L3, rng, max_consts=K3)
+    X3 = T(rng.standard_normal((3, D3)).astype(np.float32))
+    y3 = T(rng.standard_normal(D3).astype(np.float32))
+    c3 = T(rng.uniform(-3, 3, size=(B3, K3)).astype(np.float32))
+    dp3 = T(p3)
+    gout = T(rng.standard_normal((B3, D3)).astype(np.float32))
+    gc = torch.zeros((B3, K3), dtype=torch.float32, device=dev)
+    tok3 = float((p3 != 0).sum())
+    timed("eval_rpn_backward", lambda: R.eval_rpn_backward(dp3, X3, c3, gout, gc, *ids3, PI_VAL,
+                                                           E_VAL),
+          nbytes=4 * B3 * D3, evals=tok3 * D3,
+          note="%d programs x %d rows, K=%d (bytes: grad_output)" % (B3, D3, K3))
+    Bp, Dp = sc(8192), 1024
+    Xp, yp = X3[:, :Dp].contiguous(), y3[:Dp].contiguous()
+    gpos = torch.empty((Bp, K3), dtype=torch.float32, device=dev)
+    gerr = torch.empty(Bp, dtype=torch.float32, device=dev)
+    tokp = float((p3[:Bp] != 0).sum())
+    timed("fused_pso", lambda: R.fused_pso(dp3[:Bp], c3[:Bp], Xp, yp, gpos, gerr, 32, 20, 0.7,
+                                           1.5, 1.5, -25.0, 25.0, *ids3, PI_VAL, E_VAL, 3),
+          evals=tokp * Dp * 32 * 21, note="%d programs, 32 particles x 20 steps, %d rows" % (Bp, Dp))
+    gb = synthetic.random_programs(g3, 64, 5, 39, L3, rng, max_consts=K3,
+                                   cat_weights=(0.55, 0.0, 0.45))  # the kernel's binary-only set
+    gbin = T(gb)
+    cl = c3[:64].clone()
+    rm = torch.empty(64, dtype=torch.float32, device=dev)
+
+    def lb():
+        cl.copy_(c3[:64])
+        R.lbfgs_optimize(gbin, cl, Xp, yp, rm, 10, 5, 1e-7, -25.0, 25.0, *ids3, PI_VAL, E_VAL)
+    timed("lbfgs_optimize", lb, note="64 programs (the kernel's envelope), %d rows, 10 "
+                                     "iterations" % Dp)
+    # classic per-row interpreter (outputs every row)
+    Bc, Dc = sc(4096), 100_000
+    X5 = T(rng.uniform(-3, 3, size=(5, Dc)).astype(np.float32))
+    cc = T(rng.uniform(-5, 5, size=(Bc, 8)).astype(np.float32))
+    preds = torch.empty((Bc, Dc), dtype=torch.float32, device=dev)
+    spv = torch.empty((Bc, Dc), dtype=torch.int32, device=dev)
+    err = torch.empty((Bc, Dc), dtype=torch.uint8, device=dev)
+    timed("eval_rpn", lambda: R.eval_rpn(dpop[:Bc], X5, cc, preds, spv, err, *ids, PI_VAL, E_VAL, 0),
+          nbytes=9 * Bc * Dc, evals=float((pop[:Bc] != 0).sum()) * Dc,
+          note="%d programs x %d rows (bytes: preds, sp, error outputs)" % (Bc, Dc))
+    # device GP generation (batched instances config)
+    wl = synthetic.batched_workload(seed=1, n_problems=sc(256), programs=2048, rows=(100, 200))
+    probs = [BatchProblem(T(p.population), T(p.X), T(p.y), T(p.constants), p.grammar)
+             for p in wl.problems]
+    fits = [T(rng.uniform(0, 10, size=p.population.shape[0]).astype(np.float32)) for p in wl.problems]
+    gps = GPStep(probs, fits, list(range(len(probs))))
+    nch = sum(p.population.shape[0] for p in wl.problems)
+    timed("gp_generation", gps.step, nbytes=nch * (L + 8 * 4) * 3,
+          note="%d problems x 2048 children (3 launches)" % len(probs))
+    gps.close()
+    print(json.dumps({"config": "kernels", "kernels": len(out)}), flush=True)
+
+
 def main():
     args = parse()
+    if args.config == "kernels":
+        run_kernels(args)
+        return
     if args.config == "serving":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "config": "serving",

@@ -10,10 +10,14 @@
 // float/double promotions, so per-row adjoints are the reference's bit for bit.
 //
 // B200 layout: one block owns one program for a range of rows.  The program is parsed once per
-// block into a shared-memory plan (operand positions and constant slots), then every thread
-// evaluates rows: forward values and adjoints live in shared memory as [position][thread]
-// (all lanes touch the same position at the same time: conflict-free), and constant adjoints
-// are summed per thread in FP64 accumulators.  The reduction over rows is a fixed-order block
+// block into a shared-memory tape of its OPERATORS only, each naming its operands (an earlier
+// operator, a variable, a literal or a constant slot) and whether its value reaches the root;
+// terminals are read where they are used.  Every thread evaluates rows: operator values and
+// adjoints live in shared memory as [operator][thread] (all lanes touch the same operator at the
+// same time: conflict-free).  The program is a tree, so each node receives exactly one adjoint
+// contribution: a child's slot is written with the value the reference's `+=` leaves in it
+// (`0 + contribution`, or 0 where the reference adds nothing), and constant adjoints go straight
+// into per-thread FP64 accumulators.  The reduction over rows is a fixed-order block
 // sum, written without atomics when one block covers all rows of a program; only programs
 // split across blocks use one atomic per (block, slot) -- the reference issues one atomic per
 // (row, constant node).
@@ -39,10 +43,22 @@ struct BwdLut {
   double lit[10];
 };
 
-struct BNode {
-  uint8_t kind, fop, bop, pad;
-  uint16_t a;  // left operand position / variable / literal index / constant slot
-  uint16_t r;  // right operand position (binary)
+// Operand kinds of a tape operator.
+enum : uint8_t { OPD_OP = 0, OPD_VAR, OPD_LIT, OPD_CONST };
+
+struct BOp {
+  uint8_t fop, bop;   // forward and adjoint operator codes
+  uint8_t ka, kb;     // operand kinds (kb unused for unary operators)
+  uint16_t a, b;      // operand: operator index, variable, literal index (10 = 1.0), constant slot
+  uint8_t binary, reach;  // reach: the value flows into the root
+  uint16_t pad;
+};
+
+struct BRoot {
+  int n_ops;          // operators in the tape (0: the program is one terminal)
+  uint8_t kind;       // root operand kind (OPD_OP: the last operator)
+  uint16_t idx;
+  int valid;          // the reference's forward pass yields a root (final depth 1)
 };
 
 constexpr int kMaxL = 256;
@@ -64,57 +80,86 @@ struct BwdParams {
   int tape_stride;  // threads per block (row dimension of the tapes)
 };
 
-// Parses program b into the block's plan, as the reference's forward loop walks it
-// (backward_kernels.cu:84-195).  Returns the number of plan entries (root position + 1), or 0
-// when the reference would return early (no root, or final stack depth != 1).
-__device__ int parse_program(const uint8_t* __restrict__ prog, int64_t L, int64_t K,
-                             const uint8_t* s_tab, BNode* plan) {
+// Walks program b as the reference's forward loop does (backward_kernels.cu:84-195): PAD ends
+// it, an operator that finds too few operands ends it (the prefix is the program), pushes beyond
+// depth 32 are dropped, C takes slot min(c_idx, K-1) (1.0 without constants).  Operands are kept
+// on the stack as (kind, index) pairs, so terminals never enter the tape.
+__device__ BRoot parse_program(const uint8_t* __restrict__ prog, int64_t L, int64_t K,
+                               const uint8_t* s_tab, BOp* ops) {
   const uint8_t* t_kind = s_tab;
   const uint8_t* t_fop = s_tab + 256;
   const uint8_t* t_bop = s_tab + 512;
   const uint8_t* t_arg = s_tab + 768;
-  int stk[kStack];
-  int sp = 0, root = -1;
+  uint8_t sk[kStack];
+  uint16_t si[kStack];
+  int sp = 0, n_ops = 0;
   int64_t c_idx = 0;
   for (int pc = 0; pc < (int)L; ++pc) {
     const int tok = prog[pc];
     const uint8_t kind = t_kind[tok];
     if (kind == BK_PAD) break;
-    BNode n;
-    n.kind = kind;
-    n.fop = t_fop[tok];
-    n.bop = t_bop[tok];
-    n.pad = 0;
-    n.a = t_arg[tok];
-    n.r = 0xFFFF;
     if (kind == BK_VAR || kind == BK_LIT || kind == BK_CONST) {
+      uint8_t k = kind == BK_VAR ? OPD_VAR : OPD_LIT;
+      uint16_t ix = t_arg[tok];
       if (kind == BK_CONST) {
         if (K > 0) {
-          n.a = (uint16_t)(c_idx < K ? c_idx : K - 1);
+          k = OPD_CONST;
+          ix = (uint16_t)(c_idx < K ? c_idx : K - 1);
           c_idx++;
         } else {
-          n.kind = BK_LIT;  // C without constants pushes 1.0 and takes no gradient
-          n.a = 10;
+          ix = 10;  // C without constants pushes 1.0 and takes no gradient
         }
       }
-      plan[pc] = n;
-      if (sp < kStack) stk[sp++] = pc;
-      root = pc;
+      if (sp < kStack) {
+        sk[sp] = k;
+        si[sp] = ix;
+        ++sp;
+      }
       continue;
     }
+    BOp o;
+    o.fop = t_fop[tok];
+    o.bop = t_bop[tok];
+    o.reach = 0;
+    o.pad = 0;
+    o.kb = OPD_LIT;
+    o.b = 0;
     if (kind == BK_BIN) {
       if (sp < 2) break;
-      n.r = (uint16_t)stk[--sp];
-      n.a = (uint16_t)stk[--sp];
+      --sp;
+      o.kb = sk[sp];
+      o.b = si[sp];
+      --sp;
+      o.ka = sk[sp];
+      o.a = si[sp];
+      o.binary = 1;
     } else {
       if (sp < 1) break;
-      n.a = (uint16_t)stk[--sp];
+      --sp;
+      o.ka = sk[sp];
+      o.a = si[sp];
+      o.binary = 0;
     }
-    plan[pc] = n;
-    stk[sp++] = pc;
-    root = pc;
+    ops[n_ops] = o;
+    sk[sp] = OPD_OP;  // an operator always finds room: it just freed one or two slots
+    si[sp] = (uint16_t)n_ops;
+    ++sp;
+    ++n_ops;
   }
-  return (root >= 0 && sp == 1) ? root + 1 : 0;
+  BRoot r;
+  r.n_ops = n_ops;
+  r.valid = sp == 1 ? 1 : 0;
+  r.kind = sp >= 1 ? sk[0] : OPD_LIT;
+  r.idx = sp >= 1 ? si[0] : 0;
+  if (r.valid && r.kind == OPD_OP) {  // mark the operators whose value reaches the root
+    ops[r.idx].reach = 1;
+    for (int o = r.idx; o >= 0; --o) {
+      if (!ops[o].reach) continue;
+      if (ops[o].ka == OPD_OP) ops[ops[o].a].reach = 1;
+      if (ops[o].binary && ops[o].kb == OPD_OP) ops[ops[o].b].reach = 1;
+    }
+  }
+  return r;
 }
 
 // ---- forward values (backward_kernels.cu:146-188) ------------------------------------------
@@ -172,17 +217,44 @@ __device__ __forceinline__ void acc_t(T& dst, T coef, T adj) {
   dst = fma(coef, adj, dst);
 }
 
+// One operand of a tape operator for this thread's row.
+template <typename T>
+__device__ __forceinline__ T operand(uint8_t k, uint16_t i, const T* val, int TS, int tid,
+                                     const T* x, int64_t D, int64_t d, const T* s_lit,
+                                     const T* cst) {
+  switch (k) {
+    case OPD_OP: return val[(size_t)i * TS + tid];
+    case OPD_VAR: return x[(int64_t)i * D + d];
+    case OPD_CONST: return cst[i];
+    default: return i < 10 ? s_lit[i] : (T)1.0;
+  }
+}
+
+// Hands an adjoint contribution to an operand: an operator's slot is written (the value the
+// reference's `+=` leaves in a zero slot); a constant slot accumulates it when nonzero (the
+// reference skips zero adjoints); variables and literals take none.
+template <typename T>
+__device__ __forceinline__ void deliver(uint8_t k, uint16_t i, T c, T* adj, int TS, int tid,
+                                        double* cacc, int* touched) {
+  if (k == OPD_OP) {
+    adj[(size_t)i * TS + tid] = c;
+  } else if (k == OPD_CONST && c != (T)0) {
+    cacc[(size_t)i * TS + tid] += (double)c;
+    touched[i] = 1;
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(128) backward_kernel(BwdParams<T> p, BwdLut lut) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int TS = p.tape_stride;
-  BNode* plan = reinterpret_cast<BNode*>(smem);
-  double* cacc = reinterpret_cast<double*>(smem + al16((size_t)kMaxL * sizeof(BNode)));
+  BOp* ops = reinterpret_cast<BOp*>(smem);
+  double* cacc = reinterpret_cast<double*>(smem + al16((size_t)kMaxL * sizeof(BOp)));
   int* touched = reinterpret_cast<int*>(cacc + (size_t)p.K * TS);
   T* val = reinterpret_cast<T*>(
       reinterpret_cast<unsigned char*>(touched) + al16((size_t)p.K * sizeof(int)));
   T* adj = val + (size_t)p.L * TS;
-  __shared__ int s_n;
+  __shared__ BRoot s_root;
   __shared__ int64_t s_prog;
   __shared__ T s_lit[10];
   __shared__ uint8_t s_tab[1024];  // kind, forward op, adjoint op, argument per token byte
@@ -201,87 +273,90 @@ __global__ void __launch_bounds__(128) backward_kernel(BwdParams<T> p, BwdLut lu
     const int64_t split = item - b * p.n_splits;
     __syncthreads();
     if (tid == 0 && s_prog != b) {
-      s_n = parse_program(p.pop + b * p.L, p.L, p.K, s_tab, plan);
+      s_root = parse_program(p.pop + b * p.L, p.L, p.K, s_tab, ops);
       s_prog = b;
     }
     for (int64_t k = tid; k < p.K; k += blockDim.x) touched[k] = 0;
     for (int64_t k = 0; k < p.K; ++k) cacc[k * TS + tid] = 0.0;
     __syncthreads();
-    const int n = s_n;
-    if (n == 0) continue;
+    const BRoot rt = s_root;
+    if (!rt.valid) continue;
 
     const int64_t d_begin = split * p.rows_per_split;
     int64_t d_end = d_begin + p.rows_per_split;
     if (d_end > p.D) d_end = p.D;
     const T* xcol = p.x;
     const T* cst = p.consts + b * p.K;
+    const int n = rt.n_ops;
     for (int64_t d = d_begin + tid; d < d_end; d += blockDim.x) {
-      // forward
-      for (int pc = 0; pc < n; ++pc) {
-        const BNode nd = plan[pc];
-        T v;
-        switch (nd.kind) {
-          case BK_VAR: v = xcol[(int64_t)nd.a * p.D + d]; break;
-          case BK_LIT: v = nd.a < 10 ? s_lit[nd.a] : (T)1.0; break;
-          case BK_CONST: v = cst[nd.a]; break;
-          case BK_BIN: v = fwd_binary<T>(nd.fop, val[(size_t)nd.a * TS + tid],
-                                          val[(size_t)nd.r * TS + tid]); break;
-          default: v = fwd_unary<T>(nd.fop, val[(size_t)nd.a * TS + tid]); break;
-        }
-        val[(size_t)pc * TS + tid] = v;
-        adj[(size_t)pc * TS + tid] = (T)0;
+      const T g_root = p.gout[b * p.D + d];
+      if (rt.kind != OPD_OP) {  // a one-terminal program
+        deliver<T>(rt.kind, rt.idx, g_root, adj, TS, tid, cacc, touched);
+        continue;
       }
-      adj[(size_t)(n - 1) * TS + tid] = p.gout[b * p.D + d];
-      // reverse
-      for (int pc = n - 1; pc >= 0; --pc) {
-        const T g = adj[(size_t)pc * TS + tid];
-        if (g == (T)0) continue;
-        const BNode nd = plan[pc];
-        if (nd.kind == BK_CONST) {
-          cacc[(size_t)nd.a * TS + tid] += (double)g;
-          touched[nd.a] = 1;
-          continue;
-        }
-        if (nd.kind != BK_BIN && nd.kind != BK_UN) continue;
-        T& al = adj[(size_t)nd.a * TS + tid];
-        const T l_val = val[(size_t)nd.a * TS + tid];
-        if (nd.kind == BK_BIN) {
-          T& ar = adj[(size_t)nd.r * TS + tid];
-          const T r_val = val[(size_t)nd.r * TS + tid];
-          switch (nd.bop) {
-            case BO_ADD: al += g; ar += g; break;
-            case BO_SUB: al += g; ar -= g; break;
-            case BO_MUL: acc_t(al, r_val, g); acc_t(ar, l_val, g); break;
-            case BO_DIV:
-              if (fabs(r_val) >= (T)1e-9) {
-                acc_d(al, 1.0 / r_val, g);
-                acc_t(ar, -(l_val / (r_val * r_val)), g);
-              }
-              break;
-            case BO_POW:
-              if (l_val > 0) {
-                const T out_val = val[(size_t)pc * TS + tid];
-                acc_d(al, (double)r_val * pow((double)l_val, (double)r_val - 1.0), g);
-                acc_t(ar, out_val * log(l_val), g);
-              }
-              break;
-            default: break;
-          }
+      // forward: operator values
+      for (int o = 0; o < n; ++o) {
+        const BOp op = ops[o];
+        const T v1 = operand<T>(op.ka, op.a, val, TS, tid, xcol, p.D, d, s_lit, cst);
+        T v;
+        if (op.binary) {
+          const T v2 = operand<T>(op.kb, op.b, val, TS, tid, xcol, p.D, d, s_lit, cst);
+          v = fwd_binary<T>(op.fop, v1, v2);
         } else {
-          switch (nd.bop) {
-            case BO_SIN: acc_t(al, cos(l_val), g); break;
-            case BO_COS: acc_t(al, -sin(l_val), g); break;
-            case BO_LOG:
-              if (fabs(l_val) > (T)1e-9) acc_d(al, 1.0 / l_val, g);
-              break;
-            case BO_EXP: acc_t(al, val[(size_t)pc * TS + tid], g); break;
-            case BO_SQRT:
-              if (l_val > (T)1e-9) acc_d(al, 0.5 / sqrt(l_val), g);
-              break;
-            case BO_NEG: al += -g; break;
-            default: break;
+          v = fwd_unary<T>(op.fop, v1);
+        }
+        val[(size_t)o * TS + tid] = v;
+      }
+      // reverse: each operator hands its adjoint to its operands
+      adj[(size_t)rt.idx * TS + tid] = g_root;
+      for (int o = n - 1; o >= 0; --o) {
+        const BOp op = ops[o];
+        if (!op.reach) continue;
+        const T g = adj[(size_t)o * TS + tid];
+        T ca = (T)0, cb = (T)0;  // the operands' slots, as the reference leaves them
+        if (g != (T)0) {
+          const T l_val = operand<T>(op.ka, op.a, val, TS, tid, xcol, p.D, d, s_lit, cst);
+          if (op.binary) {
+            const T r_val = operand<T>(op.kb, op.b, val, TS, tid, xcol, p.D, d, s_lit, cst);
+            switch (op.bop) {
+              case BO_ADD: ca += g; cb += g; break;
+              case BO_SUB: ca += g; cb -= g; break;
+              case BO_MUL: acc_t(ca, r_val, g); acc_t(cb, l_val, g); break;
+              case BO_DIV:
+                if (fabs(r_val) >= (T)1e-9) {
+                  acc_d(ca, 1.0 / r_val, g);
+                  acc_t(cb, -(l_val / (r_val * r_val)), g);
+                }
+                break;
+              case BO_POW:
+                if (l_val > 0) {
+                  const T out_val = val[(size_t)o * TS + tid];
+                  acc_d(ca, (double)r_val * pow((double)l_val, (double)r_val - 1.0), g);
+                  acc_t(cb, out_val * log(l_val), g);
+                }
+                break;
+              default: break;
+            }
+          } else {
+            switch (op.bop) {
+              case BO_SIN: acc_t(ca, cos(l_val), g); break;
+              case BO_COS: acc_t(ca, -sin(l_val), g); break;
+              case BO_LOG:
+                if (fabs(l_val) > (T)1e-9) acc_d(ca, 1.0 / l_val, g);
+                break;
+              case BO_EXP: acc_t(ca, val[(size_t)o * TS + tid], g); break;
+              case BO_SQRT:
+                if (l_val > (T)1e-9) acc_d(ca, 0.5 / sqrt(l_val), g);
+                break;
+              case BO_NEG: ca += -g; break;
+              default: break;
+            }
           }
         }
+        // the right operand sits later in the program: its constants first, as the reference's
+        // reverse walk meets them
+        if (op.binary) deliver<T>(op.kb, op.b, cb, adj, TS, tid, cacc, touched);
+        deliver<T>(op.ka, op.a, ca, adj, TS, tid, cacc, touched);
       }
     }
     __syncthreads();
@@ -356,7 +431,7 @@ BwdLut build_bwd_lut(const ws_token_map& m, int64_t num_vars) {
 
 template <typename T>
 size_t backward_smem(int64_t L, int64_t K, int threads) {
-  return al16((size_t)kMaxL * sizeof(BNode)) + (size_t)K * threads * sizeof(double) +
+  return al16((size_t)kMaxL * sizeof(BOp)) + (size_t)K * threads * sizeof(double) +
          al16((size_t)K * sizeof(int)) + 2 * (size_t)L * threads * sizeof(T);
 }
 
