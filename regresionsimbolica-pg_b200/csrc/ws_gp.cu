@@ -208,7 +208,10 @@ __global__ void __launch_bounds__(128) gp_child_kernel(const GpDesc<T>* __restri
     }
   }
   const uint8_t* rb = d.pop + b * L;
-  // assemble; the k-th C token of the child takes its constant from (parent, slot)
+  // assemble in a thread-local row (written out 16 bytes at a time below); the k-th C token of
+  // the child takes its constant from (parent, slot)
+  uint4 rowbuf[16];  // 256 bytes: the longest program
+  uint8_t* crow = reinterpret_cast<uint8_t*>(rowbuf);
   T cval[kGpMaxConsts];
   const int K = d.K;
   int n_out = 0, nc = 0, ca = 0;
@@ -219,7 +222,7 @@ __global__ void __launch_bounds__(128) gp_child_kernel(const GpDesc<T>* __restri
       ++nc;
       ++ca;
     }
-    orow[n_out++] = t;
+    crow[n_out++] = t;
   }
   if (eb >= sb) {
     int cb = 0;
@@ -231,7 +234,7 @@ __global__ void __launch_bounds__(128) gp_child_kernel(const GpDesc<T>* __restri
         ++nc;
         ++cb;
       }
-      orow[n_out++] = t;
+      crow[n_out++] = t;
     }
     for (int j = sa; j <= ea; ++j) ca += d.kind[ra[j]] == 2 ? 1 : 0;  // skipped part of a
     for (int j = ea + 1; j < la; ++j) {
@@ -241,19 +244,24 @@ __global__ void __launch_bounds__(128) gp_child_kernel(const GpDesc<T>* __restri
         ++nc;
         ++ca;
       }
-      orow[n_out++] = t;
+      crow[n_out++] = t;
     }
   }
-  for (int j = n_out; j < L; ++j) orow[j] = 0;
+  for (int j = n_out; j < L; ++j) crow[j] = 0;
   // point mutation: operators within their arity, variables among the variables
   for (int j = 0; j < n_out; ++j) {
     if (r.uniform() < P.mutation_rate) {
-      const uint8_t t = orow[j];
+      const uint8_t t = crow[j];
       const int kd = d.kind[t], ar = d.arity[t];
-      if (kd == 3 && ar == 2 && d.n_bin > 0) orow[j] = d.bin_ids[r.randint(d.n_bin)];
-      else if (kd == 3 && ar == 1 && d.n_un > 0) orow[j] = d.un_ids[r.randint(d.n_un)];
-      else if (kd == 1 && d.n_var > 0) orow[j] = d.var_ids[r.randint(d.n_var)];
+      if (kd == 3 && ar == 2 && d.n_bin > 0) crow[j] = d.bin_ids[r.randint(d.n_bin)];
+      else if (kd == 3 && ar == 1 && d.n_un > 0) crow[j] = d.un_ids[r.randint(d.n_un)];
+      else if (kd == 1 && d.n_var > 0) crow[j] = d.var_ids[r.randint(d.n_var)];
     }
+  }
+  if (((L & 15) == 0) && ((((uintptr_t)orow) & 15u) == 0)) {
+    for (int j = 0; j < L; j += 16) *reinterpret_cast<uint4*>(orow + j) = rowbuf[j >> 4];
+  } else {
+    for (int j = 0; j < L; ++j) orow[j] = crow[j];
   }
   // constants, then their perturbation
   for (int k = 0; k < K; ++k) {
@@ -264,7 +272,8 @@ __global__ void __launch_bounds__(128) gp_child_kernel(const GpDesc<T>* __restri
 }
 
 // Next generation back into the problems' own tensors; child 0 of every problem advances its
-// problem's counter (the child kernel that read the counters has completed).
+// problem's counter (the child kernel that read the counters has completed).  Rows are copied
+// 16 bytes per load/store when both sides allow it.
 template <typename T>
 __global__ void __launch_bounds__(128) gp_copyback_kernel(const GpDesc<T>* __restrict__ desc, int n,
                                                           int64_t total, int L, int Kmax,
@@ -277,7 +286,14 @@ __global__ void __launch_bounds__(128) gp_copyback_kernel(const GpDesc<T>* __res
   const GpDesc<T>& d = desc[pi];
   const int64_t c = g - d.child0;
   if (c == 0) generation[pi] += 1ull;
-  for (int j = 0; j < L; ++j) d.pop[c * L + j] = pop_s[g * (int64_t)L + j];
+  const uint8_t* src = pop_s + g * (int64_t)L;
+  uint8_t* dst = d.pop + c * L;
+  if (((L & 15) == 0) && ((((uintptr_t)src) | ((uintptr_t)dst)) & 15u) == 0) {
+    for (int j = 0; j < L; j += 16)
+      *reinterpret_cast<uint4*>(dst + j) = *reinterpret_cast<const uint4*>(src + j);
+  } else {
+    for (int j = 0; j < L; ++j) dst[j] = src[j];
+  }
   for (int k = 0; k < d.K; ++k) d.consts[c * d.K + k] = consts_s[g * (int64_t)Kmax + k];
 }
 

@@ -74,9 +74,18 @@ __global__ void __launch_bounds__(256) splice_kernel(
     const uint8_t* __restrict__ mask, uint8_t* __restrict__ c1, uint8_t* __restrict__ c2,
     int pad) {
   const int64_t total = N * L;
+  const bool narrow = total < ((int64_t)1 << 31);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t n = i / L, t = i - n * L;
+    int64_t n, t;
+    if (narrow) {  // 32-bit division: the 64-bit one costs more than the copy
+      const uint32_t q = (uint32_t)i / (uint32_t)L;
+      n = q;
+      t = (int64_t)((uint32_t)i - q * (uint32_t)L);
+    } else {
+      n = i / L;
+      t = i - n * L;
+    }
     const uint8_t* a = p1 + n * L;
     const uint8_t* b = p2 + n * L;
     if (mask && !mask[n]) {
@@ -112,7 +121,7 @@ __global__ void __launch_bounds__(256) perturb_kernel(T* __restrict__ c, int64_t
   const int64_t total = B * K;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const int row = (int)(i / K);
+    const int row = total < ((int64_t)1 << 31) ? (int)((uint32_t)i / (uint32_t)K) : (int)(i / K);
     const int col = (int)(i - (int64_t)row * K);
     const uint32_t rk = seed ^ ((uint32_t)(row + 1) * 0x9e3779b9u);
     if (unit_open(rk) >= rate) continue;
@@ -158,11 +167,26 @@ __global__ void __launch_bounds__(128) genrand_kernel(
     xs_uniform(st);
     xs_uniform(st);
     uint8_t* row = pop + b * L;
+    // tokens are packed four to a word and stored a word at a time when rows are 4-byte
+    // aligned (byte stores from 32 rows per warp instruction would touch 32 sectors each)
+    const bool words = ((L & 3) == 0) && ((((uintptr_t)pop) & 3u) == 0);
+    uint32_t word = 0u;
+    auto put = [&](int j, uint8_t t) {
+      if (!words) {
+        row[j] = t;
+        return;
+      }
+      word |= (uint32_t)t << (8 * (j & 3));
+      if ((j & 3) == 3) {
+        *reinterpret_cast<uint32_t*>(row + (j & ~3)) = word;
+        word = 0u;
+      }
+    };
     int depth = 0;
     bool closed = false;
     for (int j = 0; j < L; ++j) {
       if (closed) {
-        row[j] = 0;
+        put(j, 0);
         continue;
       }
       const int rem = L - j - 1;
@@ -199,7 +223,7 @@ __global__ void __launch_bounds__(128) genrand_kernel(
         tok = bin[xs_int(st, nb)];
         dd = -1;
       }
-      row[j] = tok;
+      put(j, tok);
       depth += dd;
       if (depth == 1 && j > 0) closed = true;
     }
