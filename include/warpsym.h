@@ -266,6 +266,43 @@ ws_status ws_batch_update_best(const uint8_t* population, int64_t B, int64_t L,
                                int32_t* best_idx, float tolerance, void* stream);
 
 /*
+ * Structural hashing and deduplication (the reference's diversity exports, bindings.cpp:513-540
+ * -> diversity_kernels.cu).
+ * ws_population_hashes   replaces `compute_population_hashes` (:29-108): base-31 polynomial hash
+ *                        (mod 2^64) up to the first PAD, and the used-variable bitmask
+ *                        (var_presence may be NULL; hashes may be NULL for the mask alone, which
+ *                        replaces `compute_var_presence`, :465-515).
+ * ws_structural_dedup    replaces `structural_dedup` (:121-238): hash_table holds
+ *                        ws_dedup_table_slots() int64 entries set to -1 by the caller.  The
+ *                        reference lets thread timing pick which member of a group is the
+ *                        original; here it is the group's lowest index.
+ * ws_count_unique        replaces `count_unique` (:362-405): programs with duplicate flag 0,
+ *                        written to out_count[0] on the device.
+ * ws_replacement_positions replaces `get_replacement_positions` (:410-460): the duplicates'
+ *                        indices in ascending order (the reference's order is timing-dependent)
+ *                        and their number in n_replacements[0].
+ * ws_fitness_sharing_penalty replaces `fitness_sharing_penalty` (:224-355): keys
+ *                        [n_islands * ws_sharing_table_slots()] int64 set to -1 and counts of the
+ *                        same size set to 0 by the caller; out_penalty[B] = log2(count) of the
+ *                        program's island/prefix-hash group when the count exceeds threshold.
+ */
+ws_status ws_population_hashes(const uint8_t* population, int64_t B, int64_t L, int64_t* hashes,
+                               int32_t* var_presence, int32_t pad_id, int32_t id_x_start,
+                               int32_t num_vars, void* stream);
+ws_status ws_structural_dedup(const int64_t* hashes, int64_t B, int64_t* hash_table,
+                              int32_t* duplicate_mask, int64_t* original_index, void* stream);
+ws_status ws_count_unique(const int32_t* duplicate_mask, int64_t B, int64_t* out_count,
+                          void* stream);
+ws_status ws_replacement_positions(const int32_t* duplicate_mask, int64_t B, int64_t* positions,
+                                   int64_t* n_replacements, void* stream);
+ws_status ws_fitness_sharing_penalty(const uint8_t* population, int64_t B, int64_t L,
+                                     int32_t n_islands, int32_t island_size, int32_t threshold,
+                                     int32_t hash_len, int64_t* keys, int32_t* counts,
+                                     float* out_penalty, void* stream);
+int64_t ws_dedup_table_slots(void);
+int64_t ws_sharing_table_slots(void);
+
+/*
  * One genetic-programming generation, in place, for many problems at once.  Replaces the
  * breeding half of `evolve_generation` (rpn_kernels.cu:1810-2237: tournament K16, elitism
  * :1905-1907, subtree crossover K5/K6/K10, same-arity point mutation K7/K11, constant

@@ -133,6 +133,13 @@ _SIGS = {
                               C.c_float, _P]),
     "ws_check_improvement": (_I32, [_P, _I64, _P, _P, C.c_float, _P]),
     "ws_batch_update_best": (_I32, [_P, _I64, _I64, _P, _I64, _P, _P, _P, _P, _P, C.c_float, _P]),
+    "ws_population_hashes": (_I32, [_P, _I64, _I64, _P, _P, _I32, _I32, _I32, _P]),
+    "ws_structural_dedup": (_I32, [_P, _I64, _P, _P, _P, _P]),
+    "ws_count_unique": (_I32, [_P, _I64, _P, _P]),
+    "ws_replacement_positions": (_I32, [_P, _I64, _P, _P, _P]),
+    "ws_fitness_sharing_penalty": (_I32, [_P, _I64, _I64, _I32, _I32, _I32, _I32, _P, _P, _P, _P]),
+    "ws_dedup_table_slots": (_I64, []),
+    "ws_sharing_table_slots": (_I64, []),
     "ws_eval_rpn_backward": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
                                     C.POINTER(TokenMap), _P]),
     "ws_decode_rpn": (_I32, [_P, _I64, _I64, _P, _I32, _I64, C.POINTER(C.c_char_p), _I64, _P,

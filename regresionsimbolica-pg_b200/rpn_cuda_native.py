@@ -529,3 +529,91 @@ def batch_update_best(population, constants, fitness, best_rpn, best_consts, bes
     N.check(N.lib().ws_batch_update_best(ptr(population), B, L, ptr(constants), K, ptr(fitness),
                                          ptr(best_rpn), ptr(best_consts), ptr(best_rmse),
                                          ptr(best_idx), float(tolerance), stream_of(fitness)))
+
+
+# ---- structural hashing and deduplication (diversity exports of bindings.cpp) ----------------
+def compute_population_hashes(population, hashes, var_presence, PAD_ID, id_x_start, num_vars):
+    """Polynomial hashes [B] int64 and, when var_presence is non-empty, used-variable masks
+    [B] int32 (bindings.cpp:513 -> diversity_kernels.cu:29-108)."""
+    check_cuda(population, "population")
+    check_cuda(hashes, "hashes")
+    _expect(population, "population", torch.uint8)
+    _expect(hashes, "hashes", torch.int64)
+    vp = _optional(var_presence)
+    if vp is not None:
+        check_cuda(vp, "var_presence")
+        _expect(vp, "var_presence", torch.int32)
+    B, L = int(population.size(0)), int(population.size(1))
+    N.check(N.lib().ws_population_hashes(ptr(population), B, L, ptr(hashes), ptr(vp), int(PAD_ID),
+                                         int(id_x_start), int(num_vars), stream_of(population)))
+
+
+def compute_var_presence(population, var_presence, PAD_ID, id_x_start, num_vars):
+    """Used-variable bitmask per program (bindings.cpp:536 -> diversity_kernels.cu:465-515)."""
+    check_cuda(population, "population")
+    check_cuda(var_presence, "var_presence")
+    _expect(population, "population", torch.uint8)
+    _expect(var_presence, "var_presence", torch.int32)
+    B, L = int(population.size(0)), int(population.size(1))
+    N.check(N.lib().ws_population_hashes(ptr(population), B, L, None, ptr(var_presence),
+                                         int(PAD_ID), int(id_x_start), int(num_vars),
+                                         stream_of(population)))
+
+
+def structural_dedup(hashes, hash_table, duplicate_mask, original_index):
+    """Duplicate flags and originals by hash (bindings.cpp:518 -> diversity_kernels.cu:121-238);
+    hash_table [2^20] int64 filled with -1 by the caller.  A group's original is its lowest
+    index."""
+    for t, nm, dt in ((hashes, "hashes", torch.int64), (hash_table, "hash_table", torch.int64),
+                      (duplicate_mask, "duplicate_mask", torch.int32),
+                      (original_index, "original_index", torch.int64)):
+        check_cuda(t, nm)
+        _expect(t, nm, dt)
+    if hash_table.numel() < int(N.lib().ws_dedup_table_slots()):
+        raise RuntimeError("hash_table must hold %d entries" % N.lib().ws_dedup_table_slots())
+    N.check(N.lib().ws_structural_dedup(ptr(hashes), int(hashes.size(0)), ptr(hash_table),
+                                        ptr(duplicate_mask), ptr(original_index),
+                                        stream_of(hashes)))
+
+
+def count_unique(duplicate_mask):
+    """Number of programs whose duplicate flag is 0 (bindings.cpp:522 ->
+    diversity_kernels.cu:362-405); a host integer, as the reference returns."""
+    check_cuda(duplicate_mask, "duplicate_mask")
+    _expect(duplicate_mask, "duplicate_mask", torch.int32)
+    out = torch.zeros(1, dtype=torch.int64, device=duplicate_mask.device)
+    N.check(N.lib().ws_count_unique(ptr(duplicate_mask), int(duplicate_mask.size(0)), ptr(out),
+                                    stream_of(duplicate_mask)))
+    return int(out.item())
+
+
+def get_replacement_positions(duplicate_mask, replacement_positions, n_replacements):
+    """Indices of the duplicates, ascending, and their number (bindings.cpp:526 ->
+    diversity_kernels.cu:410-460); returns the number as a host integer."""
+    for t, nm, dt in ((duplicate_mask, "duplicate_mask", torch.int32),
+                      (replacement_positions, "replacement_positions", torch.int64),
+                      (n_replacements, "n_replacements", torch.int64)):
+        check_cuda(t, nm)
+        _expect(t, nm, dt)
+    n_replacements.zero_()
+    N.check(N.lib().ws_replacement_positions(ptr(duplicate_mask), int(duplicate_mask.size(0)),
+                                             ptr(replacement_positions), ptr(n_replacements),
+                                             stream_of(duplicate_mask)))
+    return int(n_replacements.item())
+
+
+def fitness_sharing_penalty(population, n_islands, island_size, threshold, hash_len=8):
+    """Per-island sharing penalty [B] float32 (bindings.cpp:530 -> diversity_kernels.cu:224-355)."""
+    check_cuda(population, "population")
+    _expect(population, "population", torch.uint8)
+    B, L = int(population.size(0)), int(population.size(1))
+    slots = int(N.lib().ws_sharing_table_slots())
+    dev = population.device
+    keys = torch.full((int(n_islands), slots), -1, dtype=torch.int64, device=dev)
+    counts = torch.zeros((int(n_islands), slots), dtype=torch.int32, device=dev)
+    out = torch.empty(B, dtype=torch.float32, device=dev)
+    N.check(N.lib().ws_fitness_sharing_penalty(ptr(population), B, L, int(n_islands),
+                                               int(island_size), int(threshold), int(hash_len),
+                                               ptr(keys), ptr(counts), ptr(out),
+                                               stream_of(population)))
+    return out
