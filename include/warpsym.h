@@ -363,6 +363,59 @@ ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* population, int64_t
                                int64_t K, const void* grad_output, void* grad_constants,
                                const ws_token_map* ids, void* stream);
 
+/*
+ * Loss and constant gradient in one launch, without per-row tensors.  Replaces the closure of the
+ * reference's torch L-BFGS (optimization.py:301-311: RPNBackwardFunction forward -> preds [B, D],
+ * mse = mean_d (preds - y)^2, loss.backward() -> eval_rpn_backward with
+ * grad_output = 2 (preds - y) / D).  Per program b:
+ *   out_loss[b]    = mean over rows of (pred[b, d] - y[d])^2                      (double)
+ *   out_grad[b, k] = d out_loss[b] / d C_k                                        (`dtype`)
+ * with the predictions and adjoints of ws_eval_rpn_backward's forward and adjoint rules.  A
+ * program whose final stack depth is not 1 gets an infinite loss and a zero gradient.  `active`
+ * (optional, int32 [B]) skips programs with 0; their outputs are left as they are.  Results are
+ * deterministic (partial sums per row range, reduced in a fixed order).  The workspace holds
+ * the partial sums; its size depends on (B, L, D, K) and the device.
+ */
+ws_status ws_loss_grad_workspace_bytes(int32_t dtype, int64_t B, int64_t L, int64_t D, int64_t K,
+                                       size_t* bytes);
+ws_status ws_loss_grad(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
+                       const void* x, int64_t num_vars, int64_t D, const void* constants,
+                       int64_t K, const void* y, const int32_t* active, double* out_loss,
+                       void* out_grad, const ws_token_map* ids, void* workspace,
+                       size_t workspace_bytes, void* stream);
+
+/*
+ * Per-program L-BFGS over ws_loss_grad, for populations of any size.  Replaces the reference's
+ * large-population constant fitting (`GPUOptimizer._lbfgs_pytorch_fallback`,
+ * optimization.py:281-343: torch.optim.LBFGS with a strong-Wolfe line search over the sum of all
+ * programs' losses) by one L-BFGS per program with the same algorithm (torch.optim.LBFGS.step,
+ * _strong_wolfe, _cubic_interpolate) and the same options, so that for a single program the two
+ * visit the same points.  `constants` [B, K] (`dtype`, K <= 32) are updated in place to the last
+ * accepted iterate; out_loss [B] (optional) receives its loss, out_evals [B] (optional) the
+ * loss evaluations used.  Each round is one loss-and-gradient launch over the programs still
+ * running plus one state launch; with sync_every > 0 the active count is read from the device
+ * every sync_every rounds (a stream synchronisation), and the call returns once no program runs.
+ */
+typedef struct ws_lbfgs_opts {
+  int32_t max_iter;         /* iterations per program (torch: max_iter) */
+  int32_t max_eval;         /* evaluations per program (torch: max_eval; the reference: 2 * max_iter) */
+  int32_t history;          /* curvature pairs kept, 1..32 (torch: history_size) */
+  int32_t max_ls;           /* evaluations per line search after the first (torch: 25) */
+  double lr;                /* initial step scale (torch: lr = 1) */
+  double tolerance_grad;    /* stop when max |g| <= this (the reference: 1e-7) */
+  double tolerance_change;  /* stop on smaller steps or loss changes (the reference: 1e-9) */
+  double grad_clip;         /* gradients clamped to [-clip, clip]; 0 = none (the reference: 1e4) */
+  int32_t sync_every;       /* rounds between reads of the active count; 0 = never (capturable) */
+  int32_t reserved;
+} ws_lbfgs_opts;
+ws_status ws_lbfgs_adjoint_workspace_bytes(int32_t dtype, int64_t B, int64_t L, int64_t D,
+                                           int64_t K, int32_t history, size_t* bytes);
+ws_status ws_lbfgs_adjoint(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
+                           const void* x, int64_t num_vars, int64_t D, void* constants, int64_t K,
+                           const void* y, const ws_lbfgs_opts* opts, double* out_loss,
+                           int32_t* out_evals, const ws_token_map* ids, void* workspace,
+                           size_t workspace_bytes, void* stream);
+
 /* ----------------------------------------------------------------------------------------------
  * Particle-swarm constant fitting.
  */

@@ -46,6 +46,9 @@ def lib():
             getattr(h, "ws_oracle_backward_" + suf).argtypes = [
                 _P, C.c_int64, C.c_int64, _P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P, _P,
                 _P]
+            getattr(h, "ws_oracle_loss_grad_" + suf).argtypes = [
+                _P, C.c_int64, C.c_int64, _P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P, _P,
+                _P, _P]
         for suf in ("f32", "f64"):
             getattr(h, "ws_oracle_pso_update_" + suf).argtypes = [
                 _P, _P, _P, _P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_int64, C.c_int64,
@@ -169,6 +172,25 @@ def backward(tmap, pop, X, consts, gout):
     getattr(lib(), "ws_oracle_backward_" + _suffix(X.dtype))(
         _p(pop), B, L, _p(X), V, D, _p(c), K, _p(g), C.byref(tmap), _p(grad), _p(absg))
     return grad, absg
+
+
+def loss_grad(tmap, pop, X, consts, y):
+    """Loss mode of the adjoint restatement: (loss [B] float64 = mean_d (pred - y)^2, infinite
+    without a result; grad [B, K] float64 = d loss / d C; sum of |terms| [B, K])."""
+    pop = np.ascontiguousarray(pop, dtype=np.uint8)
+    X = np.ascontiguousarray(X)
+    B, L = pop.shape
+    V, D = X.shape
+    c = np.ascontiguousarray(consts, dtype=X.dtype).reshape(B, -1)
+    K = c.shape[1]
+    yy = np.ascontiguousarray(y, dtype=X.dtype).reshape(D)
+    loss = np.empty(B, dtype=np.float64)
+    grad = np.empty((B, K), dtype=np.float64)
+    absg = np.empty((B, K), dtype=np.float64)
+    getattr(lib(), "ws_oracle_loss_grad_" + _suffix(X.dtype))(
+        _p(pop), B, L, _p(X), V, D, _p(c), K, _p(yy), C.byref(tmap), _p(loss), _p(grad),
+        _p(absg))
+    return loss, grad, absg
 
 
 # ---------------------------------------------------------------------------------------------

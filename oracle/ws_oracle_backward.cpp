@@ -20,15 +20,21 @@ namespace {
 
 constexpr int kStack = 32;
 
+// With y non-null (loss mode) the root adjoint of row d is (pred - y[d]) * (2 / D) and loss[b]
+// receives mean_d (pred - y[d])^2 (infinite for a program without a result): the loss and
+// gradient of the per-program L-BFGS (csrc/ws_lbfgs_batch.cu).
 template <typename T>
 void backward_rows(const uint8_t* pop, int64_t B, int64_t L, const T* x, int64_t num_vars,
                    int64_t D, const T* consts, int64_t K, const T* gout,
-                   const ws_token_map& m, double* grad, double* abssum) {
+                   const ws_token_map& m, double* grad, double* abssum, const T* y = nullptr,
+                   double* loss = nullptr) {
   const ws_token_map& v = m;
   std::vector<T> val_tape(L), adj_tape(L);
   std::vector<int> args_left(L), args_right(L), const_index(L);
+  const T scale = (T)(2.0 / (double)D);
   for (int64_t b = 0; b < B; ++b) {
     const uint8_t* prog = pop + b * L;
+    if (y) loss[b] = 0.0;
     for (int64_t d = 0; d < D; ++d) {
       int idx_stack[kStack];
       int sp = 0, root_pc = -1;
@@ -117,8 +123,17 @@ void backward_rows(const uint8_t* pop, int64_t B, int64_t L, const T* x, int64_t
         idx_stack[sp++] = pc;
         root_pc = pc;
       }
-      if (root_pc == -1 || sp != 1) continue;
-      adj_tape[root_pc] = gout[b * D + d];
+      if (root_pc == -1 || sp != 1) {
+        if (y) loss[b] = HUGE_VAL;
+        continue;
+      }
+      if (y) {
+        const T diff = val_tape[root_pc] - y[d];
+        loss[b] += (double)diff * (double)diff;
+        adj_tape[root_pc] = diff * scale;
+      } else {
+        adj_tape[root_pc] = gout[b * D + d];
+      }
       for (int pc = root_pc; pc >= 0; --pc) {
         const T adj = adj_tape[pc];
         if (adj == (T)0.0) continue;
@@ -170,6 +185,7 @@ void backward_rows(const uint8_t* pop, int64_t B, int64_t L, const T* x, int64_t
         }
       }
     }
+    if (y) loss[b] /= (double)D;
   }
 }
 
@@ -191,6 +207,22 @@ void ws_oracle_backward_f64(const uint8_t* pop, int64_t B, int64_t L, const doub
                             double* abssum) {
   for (int64_t i = 0; i < B * K; ++i) grad[i] = abssum[i] = 0.0;
   backward_rows<double>(pop, B, L, x, num_vars, D, consts, K, gout, *m, grad, abssum);
+}
+
+// loss [B], grad / abssum [B, K]: double, written here.
+void ws_oracle_loss_grad_f32(const uint8_t* pop, int64_t B, int64_t L, const float* x,
+                             int64_t num_vars, int64_t D, const float* consts, int64_t K,
+                             const float* y, const ws_token_map* m, double* loss, double* grad,
+                             double* abssum) {
+  for (int64_t i = 0; i < B * K; ++i) grad[i] = abssum[i] = 0.0;
+  backward_rows<float>(pop, B, L, x, num_vars, D, consts, K, nullptr, *m, grad, abssum, y, loss);
+}
+void ws_oracle_loss_grad_f64(const uint8_t* pop, int64_t B, int64_t L, const double* x,
+                             int64_t num_vars, int64_t D, const double* consts, int64_t K,
+                             const double* y, const ws_token_map* m, double* loss, double* grad,
+                             double* abssum) {
+  for (int64_t i = 0; i < B * K; ++i) grad[i] = abssum[i] = 0.0;
+  backward_rows<double>(pop, B, L, x, num_vars, D, consts, K, nullptr, *m, grad, abssum, y, loss);
 }
 
 }  // extern "C"

@@ -92,6 +92,14 @@ class GpOpts(C.Structure):
                 ("parsimony_eps", C.c_float), ("reserved", C.c_int32)]
 
 
+class LbfgsOpts(C.Structure):
+    """ws_lbfgs_opts: options of the per-program L-BFGS (torch.optim.LBFGS names)."""
+    _fields_ = [("max_iter", C.c_int32), ("max_eval", C.c_int32), ("history", C.c_int32),
+                ("max_ls", C.c_int32), ("lr", C.c_double), ("tolerance_grad", C.c_double),
+                ("tolerance_change", C.c_double), ("grad_clip", C.c_double),
+                ("sync_every", C.c_int32), ("reserved", C.c_int32)]
+
+
 _P = C.c_void_p
 _I64 = C.c_int64
 _I32 = C.c_int32
@@ -142,6 +150,15 @@ _SIGS = {
     "ws_sharing_table_slots": (_I64, []),
     "ws_eval_rpn_backward": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
                                     C.POINTER(TokenMap), _P]),
+    "ws_loss_grad_workspace_bytes": (_I32, [_I32, _I64, _I64, _I64, _I64,
+                                            C.POINTER(C.c_size_t)]),
+    "ws_loss_grad": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P, _P, _P,
+                            C.POINTER(TokenMap), _P, C.c_size_t, _P]),
+    "ws_lbfgs_adjoint_workspace_bytes": (_I32, [_I32, _I64, _I64, _I64, _I64, _I32,
+                                                C.POINTER(C.c_size_t)]),
+    "ws_lbfgs_adjoint": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P,
+                                C.POINTER(LbfgsOpts), _P, _P, C.POINTER(TokenMap), _P,
+                                C.c_size_t, _P]),
     "ws_decode_rpn": (_I32, [_P, _I64, _I64, _P, _I32, _I64, C.POINTER(C.c_char_p), _I64, _P,
                              _I64, _I32, _I32, _P, C.c_size_t, _P, C.POINTER(C.c_size_t)]),
     "ws_pso_update": (_I32, [_I32, _P, _P, _P, _P, _P, _P, C.c_float, C.c_float, C.c_float,

@@ -78,6 +78,12 @@ struct BwdParams {
   T* grad;
   int64_t n_splits, rows_per_split, n_items;
   int tape_stride;  // threads per block (row dimension of the tapes)
+  // loss mode: the root adjoint of row d is dL/dpred = 2 (pred - y[d]) / D, L = mean (pred - y)^2;
+  // each (program, row range) item writes its partial sums (no atomics, fixed order)
+  const T* y;
+  const int32_t* active;  // optional: programs with 0 are skipped
+  double* part_loss;      // [n_items]   sum over the item's rows of (pred - y)^2
+  double* part_grad;      // [n_items, K] sum over the item's rows of the constant adjoints
 };
 
 // Walks program b as the reference's forward loop does (backward_kernels.cu:84-195): PAD ends
@@ -244,16 +250,22 @@ __device__ __forceinline__ void deliver(uint8_t k, uint16_t i, T c, T* adj, int 
   }
 }
 
-template <typename T>
+// One tape slot per operator and thread holds the operator's value after the forward sweep and
+// its adjoint during the reverse sweep: the program is a tree, so the only reader of a value is
+// the operator's parent, which reads it before it writes the adjoint into the same slot.  The
+// two operators whose adjoint rule uses their own output (exp, pow) recompute it from their
+// operands, bit for bit.  One slot per operator halves the shared memory of separate value and
+// adjoint tapes, which is what limits how many blocks an SM holds.
+template <typename T, bool LOSS>
 __global__ void __launch_bounds__(128) backward_kernel(BwdParams<T> p, BwdLut lut) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int TS = p.tape_stride;
   BOp* ops = reinterpret_cast<BOp*>(smem);
   double* cacc = reinterpret_cast<double*>(smem + al16((size_t)kMaxL * sizeof(BOp)));
-  int* touched = reinterpret_cast<int*>(cacc + (size_t)p.K * TS);
-  T* val = reinterpret_cast<T*>(
+  double* lacc_s = cacc + (size_t)p.K * TS;  // loss mode: per-thread loss partials
+  int* touched = reinterpret_cast<int*>(lacc_s + (LOSS ? TS : 0));
+  T* tape = reinterpret_cast<T*>(
       reinterpret_cast<unsigned char*>(touched) + al16((size_t)p.K * sizeof(int)));
-  T* adj = val + (size_t)p.L * TS;
   __shared__ BRoot s_root;
   __shared__ int64_t s_prog;
   __shared__ T s_lit[10];
@@ -267,10 +279,12 @@ __global__ void __launch_bounds__(128) backward_kernel(BwdParams<T> p, BwdLut lu
   if (threadIdx.x < 10) s_lit[threadIdx.x] = (T)lut.lit[threadIdx.x];
   if (threadIdx.x == 0) s_prog = -1;
   const int tid = threadIdx.x;
+  const T loss_scale = LOSS ? (T)(2.0 / (double)p.D) : (T)0;
 
   for (int64_t item = blockIdx.x; item < p.n_items; item += gridDim.x) {
     const int64_t b = item / p.n_splits;
     const int64_t split = item - b * p.n_splits;
+    if (LOSS && p.active && p.active[b] == 0) continue;  // uniform over the block
     __syncthreads();
     if (tid == 0 && s_prog != b) {
       s_root = parse_program(p.pop + b * p.L, p.L, p.K, s_tab, ops);
@@ -280,7 +294,13 @@ __global__ void __launch_bounds__(128) backward_kernel(BwdParams<T> p, BwdLut lu
     for (int64_t k = 0; k < p.K; ++k) cacc[k * TS + tid] = 0.0;
     __syncthreads();
     const BRoot rt = s_root;
-    if (!rt.valid) continue;
+    if (!rt.valid) {
+      if (LOSS) {  // no prediction: infinite loss, no gradient
+        if (tid == 0) p.part_loss[item] = __longlong_as_double(0x7ff0000000000000ll);
+        for (int64_t k = tid; k < p.K; k += blockDim.x) p.part_grad[item * p.K + k] = 0.0;
+      }
+      continue;
+    }
 
     const int64_t d_begin = split * p.rows_per_split;
     int64_t d_end = d_begin + p.rows_per_split;
@@ -288,36 +308,45 @@ __global__ void __launch_bounds__(128) backward_kernel(BwdParams<T> p, BwdLut lu
     const T* xcol = p.x;
     const T* cst = p.consts + b * p.K;
     const int n = rt.n_ops;
+    double lacc = 0.0;
     for (int64_t d = d_begin + tid; d < d_end; d += blockDim.x) {
-      const T g_root = p.gout[b * p.D + d];
-      if (rt.kind != OPD_OP) {  // a one-terminal program
-        deliver<T>(rt.kind, rt.idx, g_root, adj, TS, tid, cacc, touched);
-        continue;
-      }
       // forward: operator values
       for (int o = 0; o < n; ++o) {
         const BOp op = ops[o];
-        const T v1 = operand<T>(op.ka, op.a, val, TS, tid, xcol, p.D, d, s_lit, cst);
+        const T v1 = operand<T>(op.ka, op.a, tape, TS, tid, xcol, p.D, d, s_lit, cst);
         T v;
         if (op.binary) {
-          const T v2 = operand<T>(op.kb, op.b, val, TS, tid, xcol, p.D, d, s_lit, cst);
+          const T v2 = operand<T>(op.kb, op.b, tape, TS, tid, xcol, p.D, d, s_lit, cst);
           v = fwd_binary<T>(op.fop, v1, v2);
         } else {
           v = fwd_unary<T>(op.fop, v1);
         }
-        val[(size_t)o * TS + tid] = v;
+        tape[(size_t)o * TS + tid] = v;
+      }
+      T g_root;
+      if (LOSS) {
+        const T pred = operand<T>(rt.kind, rt.idx, tape, TS, tid, xcol, p.D, d, s_lit, cst);
+        const T diff = pred - p.y[d];
+        lacc += (double)diff * (double)diff;
+        g_root = diff * loss_scale;
+      } else {
+        g_root = p.gout[b * p.D + d];
+      }
+      if (rt.kind != OPD_OP) {  // a one-terminal program
+        deliver<T>(rt.kind, rt.idx, g_root, tape, TS, tid, cacc, touched);
+        continue;
       }
       // reverse: each operator hands its adjoint to its operands
-      adj[(size_t)rt.idx * TS + tid] = g_root;
+      tape[(size_t)rt.idx * TS + tid] = g_root;
       for (int o = n - 1; o >= 0; --o) {
         const BOp op = ops[o];
         if (!op.reach) continue;
-        const T g = adj[(size_t)o * TS + tid];
+        const T g = tape[(size_t)o * TS + tid];
         T ca = (T)0, cb = (T)0;  // the operands' slots, as the reference leaves them
         if (g != (T)0) {
-          const T l_val = operand<T>(op.ka, op.a, val, TS, tid, xcol, p.D, d, s_lit, cst);
+          const T l_val = operand<T>(op.ka, op.a, tape, TS, tid, xcol, p.D, d, s_lit, cst);
           if (op.binary) {
-            const T r_val = operand<T>(op.kb, op.b, val, TS, tid, xcol, p.D, d, s_lit, cst);
+            const T r_val = operand<T>(op.kb, op.b, tape, TS, tid, xcol, p.D, d, s_lit, cst);
             switch (op.bop) {
               case BO_ADD: ca += g; cb += g; break;
               case BO_SUB: ca += g; cb -= g; break;
@@ -330,7 +359,7 @@ __global__ void __launch_bounds__(128) backward_kernel(BwdParams<T> p, BwdLut lu
                 break;
               case BO_POW:
                 if (l_val > 0) {
-                  const T out_val = val[(size_t)o * TS + tid];
+                  const T out_val = fwd_binary<T>(op.fop, l_val, r_val);
                   acc_d(ca, (double)r_val * pow((double)l_val, (double)r_val - 1.0), g);
                   acc_t(cb, out_val * log(l_val), g);
                 }
@@ -344,7 +373,7 @@ __global__ void __launch_bounds__(128) backward_kernel(BwdParams<T> p, BwdLut lu
               case BO_LOG:
                 if (fabs(l_val) > (T)1e-9) acc_d(ca, 1.0 / l_val, g);
                 break;
-              case BO_EXP: acc_t(ca, val[(size_t)o * TS + tid], g); break;
+              case BO_EXP: acc_t(ca, fwd_unary<T>(op.fop, l_val), g); break;
               case BO_SQRT:
                 if (l_val > (T)1e-9) acc_d(ca, 0.5 / sqrt(l_val), g);
                 break;
@@ -355,19 +384,55 @@ __global__ void __launch_bounds__(128) backward_kernel(BwdParams<T> p, BwdLut lu
         }
         // the right operand sits later in the program: its constants first, as the reference's
         // reverse walk meets them
-        if (op.binary) deliver<T>(op.kb, op.b, cb, adj, TS, tid, cacc, touched);
-        deliver<T>(op.ka, op.a, ca, adj, TS, tid, cacc, touched);
+        if (op.binary) deliver<T>(op.kb, op.b, cb, tape, TS, tid, cacc, touched);
+        deliver<T>(op.ka, op.a, ca, tape, TS, tid, cacc, touched);
       }
     }
+    if (LOSS) lacc_s[tid] = lacc;
     __syncthreads();
     // fixed-order reduction over the block's threads, one thread per slot
     for (int64_t k = tid; k < p.K; k += blockDim.x) {
+      if (LOSS) {
+        double s = 0.0;
+        if (touched[k])
+          for (int t = 0; t < (int)blockDim.x; ++t) s += cacc[k * TS + t];
+        p.part_grad[item * p.K + k] = s;
+        continue;
+      }
       if (!touched[k]) continue;
       double s = 0.0;
       for (int t = 0; t < (int)blockDim.x; ++t) s += cacc[k * TS + t];
       T* dst = p.grad + b * p.K + k;
       if (p.n_splits == 1) *dst = *dst + (T)s;
       else atomicAdd(dst, (T)s);
+    }
+    if (LOSS && tid == 0) {
+      double s = 0.0;
+      for (int t = 0; t < (int)blockDim.x; ++t) s += lacc_s[t];
+      p.part_loss[item] = s;
+    }
+  }
+}
+
+// Loss mode, second launch: a program's partials summed in row-range order; loss = sum / D.
+template <typename T>
+__global__ void __launch_bounds__(256) loss_grad_reduce_kernel(const double* __restrict__ part_loss,
+                                                               const double* __restrict__ part_grad,
+                                                               const int32_t* __restrict__ active,
+                                                               int64_t B, int64_t K,
+                                                               int64_t n_splits, int64_t D,
+                                                               double* __restrict__ loss,
+                                                               T* __restrict__ grad) {
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < B;
+       b += (int64_t)gridDim.x * blockDim.x) {
+    if (active && active[b] == 0) continue;
+    double l = 0.0;
+    for (int64_t s = 0; s < n_splits; ++s) l += part_loss[b * n_splits + s];
+    loss[b] = l / (double)D;
+    for (int64_t k = 0; k < K; ++k) {
+      double g = 0.0;
+      for (int64_t s = 0; s < n_splits; ++s) g += part_grad[(b * n_splits + s) * K + k];
+      grad[b * K + k] = (T)g;
     }
   }
 }
@@ -429,25 +494,33 @@ BwdLut build_bwd_lut(const ws_token_map& m, int64_t num_vars) {
   return lut;
 }
 
-template <typename T>
+template <typename T, bool LOSS>
 size_t backward_smem(int64_t L, int64_t K, int threads) {
   return al16((size_t)kMaxL * sizeof(BOp)) + (size_t)K * threads * sizeof(double) +
-         al16((size_t)K * sizeof(int)) + 2 * (size_t)L * threads * sizeof(T);
+         (LOSS ? (size_t)threads * sizeof(double) : 0) + al16((size_t)K * sizeof(int)) +
+         (size_t)L * threads * sizeof(T);
 }
 
-template <typename T>
-ws_status launch_backward_typed(const uint8_t* pop, int64_t B, int64_t L, const void* x,
-                                int64_t D, const void* consts, int64_t K, const void* gout,
-                                void* grad, const BwdLut& lut, cudaStream_t stream) {
+// Block size, shared memory and the split of rows into ranges for one launch.  Rows are split
+// only when there are too few programs to fill the GPU; the split depends on (B, L, K, D) and the
+// device alone.
+struct BwdPlan {
+  int threads;
+  size_t smem;
+  int64_t n_splits, rows, grid;
+};
+
+template <typename T, bool LOSS>
+ws_status backward_plan(int64_t B, int64_t L, int64_t D, int64_t K, BwdPlan* out) {
   const DeviceInfo& dev = device_info();
   const size_t budget = dev.smem_optin < (size_t)200 * 1024 ? dev.smem_optin : 200 * 1024;
   int threads = 128;
-  while (threads > 32 && backward_smem<T>(L, K, threads) > budget / 2) threads /= 2;
-  const size_t smem = backward_smem<T>(L, K, threads);
+  while (threads > 32 && backward_smem<T, LOSS>(L, K, threads) > budget / 2) threads /= 2;
+  const size_t smem = backward_smem<T, LOSS>(L, K, threads);
   if (smem > budget)
     return fail("backward: " + std::to_string(K) + " constants and " + std::to_string(L) +
                 " tokens need more shared memory than a block has");
-  auto kern = backward_kernel<T>;
+  auto kern = backward_kernel<T, LOSS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
@@ -456,7 +529,6 @@ ws_status launch_backward_typed(const uint8_t* pop, int64_t B, int64_t L, const 
   if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
   if (per_sm < 1) return fail("backward kernel cannot be resident");
   const int64_t slots = (int64_t)dev.sm_count * per_sm;
-  // split rows only when there are too few programs to fill the GPU
   int64_t n_splits = (2 * slots + B - 1) / B;
   const int64_t max_splits = (D + threads - 1) / threads;
   if (n_splits > max_splits) n_splits = max_splits;
@@ -464,6 +536,18 @@ ws_status launch_backward_typed(const uint8_t* pop, int64_t B, int64_t L, const 
   int64_t rows = (D + n_splits - 1) / n_splits;
   rows = (rows + threads - 1) / threads * threads;
   n_splits = (D + rows - 1) / rows;
+  out->threads = threads;
+  out->smem = smem;
+  out->n_splits = n_splits;
+  out->rows = rows;
+  const int64_t n_items = B * n_splits;
+  out->grid = n_items < slots ? n_items : slots;
+  return WS_OK;
+}
+
+template <typename T, bool LOSS>
+BwdParams<T> backward_params(const uint8_t* pop, int64_t B, int64_t L, const void* x, int64_t D,
+                             const void* consts, int64_t K, const BwdPlan& plan) {
   BwdParams<T> prm;
   prm.pop = pop;
   prm.B = B;
@@ -472,19 +556,77 @@ ws_status launch_backward_typed(const uint8_t* pop, int64_t B, int64_t L, const 
   prm.D = D;
   prm.consts = static_cast<const T*>(consts);
   prm.K = K;
+  prm.gout = nullptr;
+  prm.grad = nullptr;
+  prm.n_splits = plan.n_splits;
+  prm.rows_per_split = plan.rows;
+  prm.n_items = B * plan.n_splits;
+  prm.tape_stride = plan.threads;
+  prm.y = nullptr;
+  prm.active = nullptr;
+  prm.part_loss = nullptr;
+  prm.part_grad = nullptr;
+  return prm;
+}
+
+template <typename T>
+ws_status launch_backward_typed(const uint8_t* pop, int64_t B, int64_t L, const void* x,
+                                int64_t D, const void* consts, int64_t K, const void* gout,
+                                void* grad, const BwdLut& lut, cudaStream_t stream) {
+  BwdPlan plan;
+  ws_status st = backward_plan<T, false>(B, L, D, K, &plan);
+  if (st != WS_OK) return st;
+  BwdParams<T> prm = backward_params<T, false>(pop, B, L, x, D, consts, K, plan);
   prm.gout = static_cast<const T*>(gout);
   prm.grad = static_cast<T*>(grad);
-  prm.n_splits = n_splits;
-  prm.rows_per_split = rows;
-  prm.n_items = B * n_splits;
-  prm.tape_stride = threads;
-  const int64_t grid = prm.n_items < slots ? prm.n_items : slots;
-  kern<<<(unsigned)grid, threads, smem, stream>>>(prm, lut);
-  e = cudaGetLastError();
+  backward_kernel<T, false><<<(unsigned)plan.grid, plan.threads, plan.smem, stream>>>(prm, lut);
+  const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? WS_OK : fail_cuda(e, "eval_rpn_backward");
 }
 
 }  // namespace
+
+// Loss-and-gradient launch shared by ws_loss_grad and the batched L-BFGS: partial sums into
+// part_loss [B * n_splits] and part_grad [B * n_splits, K] (double), then, when loss / grad
+// are given, the reduce launch.
+template <typename T>
+ws_status launch_loss_grad(const uint8_t* pop, int64_t B, int64_t L, const void* x, int64_t D,
+                           const void* consts, int64_t K, const void* y, const int32_t* active,
+                           const ws_token_map& ids, int64_t num_vars, double* part_loss,
+                           double* part_grad, double* loss, void* grad, int64_t* n_splits_out,
+                           cudaStream_t stream) {
+  BwdPlan plan;
+  ws_status st = backward_plan<T, true>(B, L, D, K, &plan);
+  if (st != WS_OK) return st;
+  if (n_splits_out) *n_splits_out = plan.n_splits;
+  if (!part_loss) return WS_OK;  // plan query only
+  const BwdLut lut = build_bwd_lut(ids, num_vars);
+  BwdParams<T> prm = backward_params<T, true>(pop, B, L, x, D, consts, K, plan);
+  prm.y = static_cast<const T*>(y);
+  prm.active = active;
+  prm.part_loss = part_loss;
+  prm.part_grad = part_grad;
+  backward_kernel<T, true><<<(unsigned)plan.grid, plan.threads, plan.smem, stream>>>(prm, lut);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail_cuda(e, "loss_grad");
+  if (loss) {
+    const int64_t blocks = (B + 255) / 256;
+    loss_grad_reduce_kernel<T><<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, stream>>>(
+        part_loss, part_grad, active, B, K, plan.n_splits, D, loss, static_cast<T*>(grad));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "loss_grad");
+  }
+  return WS_OK;
+}
+
+template ws_status launch_loss_grad<float>(const uint8_t*, int64_t, int64_t, const void*,
+                                           int64_t, const void*, int64_t, const void*,
+                                           const int32_t*, const ws_token_map&, int64_t, double*,
+                                           double*, double*, void*, int64_t*, cudaStream_t);
+template ws_status launch_loss_grad<double>(const uint8_t*, int64_t, int64_t, const void*,
+                                            int64_t, const void*, int64_t, const void*,
+                                            const int32_t*, const ws_token_map&, int64_t, double*,
+                                            double*, double*, void*, int64_t*, cudaStream_t);
 }  // namespace ws
 
 extern "C" ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* population, int64_t B,
@@ -510,4 +652,78 @@ extern "C" ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* populati
                                         grad_constants, lut, s);
   return launch_backward_typed<double>(population, B, L, x, D, constants, K, grad_output,
                                        grad_constants, lut, s);
+}
+
+namespace {
+ws_status loss_grad_check(int32_t dtype, int64_t B, int64_t L, int64_t D, int64_t K,
+                          int64_t num_vars) {
+  using namespace ws;
+  if (dtype != WS_F32 && dtype != WS_F64) return fail("x must be float32 or float64");
+  if (B < 0 || L < 0 || D < 0 || K < 0 || num_vars < 0) return fail("negative dimension");
+  if (L > kMaxL) return fail("loss_grad supports programs of at most 256 tokens");
+  if (K > 0xFFFF) return fail("loss_grad supports at most 65535 constants per program");
+  if (num_vars > 255) return fail("at most 255 variables are addressable by uint8 tokens");
+  return WS_OK;
+}
+}  // namespace
+
+extern "C" ws_status ws_loss_grad_workspace_bytes(int32_t dtype, int64_t B, int64_t L, int64_t D,
+                                                  int64_t K, size_t* bytes) {
+  using namespace ws;
+  clear_error();
+  ws_status st = loss_grad_check(dtype, B, L, D, K, 0);
+  if (st != WS_OK) return st;
+  if (!bytes) return fail("null output pointer");
+  *bytes = 0;
+  if (B == 0 || D == 0 || L == 0) return WS_OK;
+  int64_t n_splits = 1;
+  st = dtype == WS_F32
+           ? launch_loss_grad<float>(nullptr, B, L, nullptr, D, nullptr, K, nullptr, nullptr,
+                                     ws_token_map{}, 0, nullptr, nullptr, nullptr, nullptr,
+                                     &n_splits, nullptr)
+           : launch_loss_grad<double>(nullptr, B, L, nullptr, D, nullptr, K, nullptr, nullptr,
+                                      ws_token_map{}, 0, nullptr, nullptr, nullptr, nullptr,
+                                      &n_splits, nullptr);
+  if (st != WS_OK) return st;
+  *bytes = (size_t)(B * n_splits) * (size_t)(K + 1) * sizeof(double) + 256;
+  return WS_OK;
+}
+
+extern "C" ws_status ws_loss_grad(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
+                                  const void* x, int64_t num_vars, int64_t D,
+                                  const void* constants, int64_t K, const void* y,
+                                  const int32_t* active, double* out_loss, void* out_grad,
+                                  const ws_token_map* ids, void* workspace, size_t workspace_bytes,
+                                  void* stream) {
+  using namespace ws;
+  clear_error();
+  ws_status st = loss_grad_check(dtype, B, L, D, K, num_vars);
+  if (st != WS_OK) return st;
+  if (!ids) return fail("token map is required");
+  if (B == 0) return WS_OK;
+  if (D == 0 || L == 0) return fail("loss_grad needs at least one row and one token");
+  if (!population || !y || !out_loss || (K > 0 && (!constants || !out_grad)) ||
+      (num_vars > 0 && !x) || !workspace)
+    return fail("null tensor pointer");
+  size_t need = 0;
+  st = ws_loss_grad_workspace_bytes(dtype, B, L, D, K, &need);
+  if (st != WS_OK) return st;
+  if (workspace_bytes < need) return fail("loss_grad workspace too small");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* part_loss = static_cast<double*>(workspace);
+  int64_t n_splits = 1;
+  st = dtype == WS_F32
+           ? launch_loss_grad<float>(nullptr, B, L, nullptr, D, nullptr, K, nullptr, nullptr,
+                                     *ids, 0, nullptr, nullptr, nullptr, nullptr, &n_splits,
+                                     nullptr)
+           : launch_loss_grad<double>(nullptr, B, L, nullptr, D, nullptr, K, nullptr, nullptr,
+                                      *ids, 0, nullptr, nullptr, nullptr, nullptr, &n_splits,
+                                      nullptr);
+  if (st != WS_OK) return st;
+  double* part_grad = part_loss + B * n_splits;
+  if (dtype == WS_F32)
+    return launch_loss_grad<float>(population, B, L, x, D, constants, K, y, active, *ids,
+                                   num_vars, part_loss, part_grad, out_loss, out_grad, nullptr, s);
+  return launch_loss_grad<double>(population, B, L, x, D, constants, K, y, active, *ids,
+                                  num_vars, part_loss, part_grad, out_loss, out_grad, nullptr, s);
 }

@@ -94,4 +94,16 @@ ws_status launch_fitness(const FitnessRequest& rq);
 // Number of evaluator schedules (index 0 = automatic choice).
 int schedule_count();
 
+// Loss (mean squared error against y) and its adjoint gradient with respect to the constants,
+// under the adjoint kernel's forward rules (ws_backward.cu).  part_loss [B * n_splits] and
+// part_grad [B * n_splits, K] receive per-row-range partial sums; with `loss` non-null a second
+// launch reduces them into loss [B] (double) and grad [B, K] (T).  Programs with active[b] == 0
+// are skipped.  With part_loss null only *n_splits_out is computed.
+template <typename T>
+ws_status launch_loss_grad(const uint8_t* pop, int64_t B, int64_t L, const void* x, int64_t D,
+                           const void* consts, int64_t K, const void* y, const int32_t* active,
+                           const ws_token_map& ids, int64_t num_vars, double* part_loss,
+                           double* part_grad, double* loss, void* grad, int64_t* n_splits_out,
+                           cudaStream_t stream);
+
 }  // namespace ws

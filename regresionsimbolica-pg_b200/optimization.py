@@ -9,7 +9,9 @@ of libwarpsym.
                                  pso_update_bests / pso_update kernels;
   lbfgs_optimize_top_k           the L-BFGS kernel for <= 64 programs and <= 1024 rows, else the
                                  torch L-BFGS (strong Wolfe) over RPNBackwardFunction, accepting
-                                 only improvements (:193-343).
+                                 only improvements (:193-343); with per_program=True, one L-BFGS
+                                 per program over the one-launch loss and adjoint gradient
+                                 (constfit.lbfgs).
 
 The random draws of the multi-kernel path are torch's, in the reference's order; the fused path
 draws the kernel's curand streams from the same seed formula.  As in the reference, the native
@@ -120,7 +122,12 @@ class GPUOptimizer:
 
     # ---- L-BFGS ------------------------------------------------------------------------------
     def lbfgs_optimize_top_k(self, population, constants, x, y_target, top_k: int = 50,
-                             max_iter: int = 30):
+                             max_iter: int = 30, per_program: bool = False,
+                             history_size: int = 10):
+        """per_program=False (default): the reference's dispatch.  per_program=True: one L-BFGS
+        per program over the adjoint gradient (constfit.lbfgs) with the reference fallback's
+        options (strong Wolfe, max_eval = 2 * max_iter, gradients clamped to 1e4), then the same
+        clamp, re-evaluation and improvement-only acceptance."""
         B, K = constants.shape
         if K == 0 or top_k <= 0 or B == 0:
             return constants, torch.full((B,), float("inf"), device=self.device, dtype=self.dtype)
@@ -129,6 +136,9 @@ class GPUOptimizer:
         c = constants[:actual_k].clone().to(self.dtype)
         best_errs_k = self.evaluator.evaluate_batch(pop_k, x, y_target, c).to(self.dtype)
         best_c_k = c.clone()
+        if per_program:
+            return self._lbfgs_per_program(pop_k, c, x, y_target, best_errs_k, best_c_k,
+                                           constants, max_iter, history_size)
         if actual_k <= 64 and y_target.numel() <= 1024:
             c_final, final_errs_k = self._lbfgs_cuda(pop_k, c, x, y_target, max_iter)
             improved = torch.isfinite(final_errs_k) & (final_errs_k < best_errs_k)
@@ -151,6 +161,30 @@ class GPUOptimizer:
         _rcn.lbfgs_optimize(population.contiguous(), c, x_cuda, y, out_rmse, max_iter, 10, 1e-7,
                             self.const_min, self.const_max, *self._ids, math.pi, math.e)
         return c, out_rmse
+
+    def _lbfgs_per_program(self, pop_k, c, x, y_target, best_errs_k, best_c_k, constants,
+                           max_iter, history_size):
+        from .constfit import lbfgs
+        x_v = self._vars_major(x, y_target.numel()).to(c.dtype)
+        y = y_target.to(c.dtype).contiguous()
+        c_fit, _, _ = lbfgs(pop_k, x_v, c.contiguous(), y, self._ids, max_iter=max_iter,
+                            max_eval=max_iter * 2, history_size=history_size,
+                            tolerance_grad=1e-7, tolerance_change=1e-9, grad_clip=1e4)
+        return self._accept(pop_k, c_fit, x, y_target, best_errs_k, best_c_k, constants)
+
+    def _accept(self, pop_k, c_fit, x, y_target, best_errs_k, best_c_k, constants):
+        actual_k = pop_k.shape[0]
+        c_final = c_fit.detach().clamp(self.const_min, self.const_max)
+        final_errs_k = self.evaluator.evaluate_batch(pop_k, x, y_target, c_final).to(self.dtype)
+        improved = torch.isfinite(final_errs_k) & (final_errs_k < best_errs_k)
+        best_c_k[improved] = c_final[improved]
+        best_errs_k[improved] = final_errs_k[improved]
+        result = constants.clone()
+        result[:actual_k] = best_c_k.to(constants.dtype)
+        full = torch.full((constants.shape[0],), float("inf"), device=self.device,
+                          dtype=self.dtype)
+        full[:actual_k] = best_errs_k
+        return result, full
 
     def _lbfgs_pytorch_fallback(self, pop_k, c, x, y_target, best_errs_k, best_c_k, constants,
                                 max_iter):
@@ -176,14 +210,4 @@ class GPUOptimizer:
             optimizer.step(closure)
         except RuntimeError:
             pass
-        c_final = c.detach().clamp(self.const_min, self.const_max)
-        final_errs_k = self.evaluator.evaluate_batch(pop_k, x, y_target, c_final).to(self.dtype)
-        improved = torch.isfinite(final_errs_k) & (final_errs_k < best_errs_k)
-        best_c_k[improved] = c_final[improved]
-        best_errs_k[improved] = final_errs_k[improved]
-        result = constants.clone()
-        result[:actual_k] = best_c_k.to(constants.dtype)
-        full = torch.full((constants.shape[0],), float("inf"), device=self.device,
-                          dtype=self.dtype)
-        full[:actual_k] = best_errs_k
-        return result, full
+        return self._accept(pop_k, c, x, y_target, best_errs_k, best_c_k, constants)
