@@ -49,18 +49,22 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--config", default="eval-scale",
-                    choices=["eval-scale", "batched", "serving", "kernels"],
+                    choices=["eval-scale", "batched", "serving", "kernels", "constopt"],
                     help="eval-scale: the evaluation-only scale test (default); batched: 256 "
                          "uneven problems scored by one graph-replayed launch per generation; "
                          "serving: a Poisson stream of fit/evaluate requests, continuously "
                          "batched, against one request at a time; kernels: every other kernel "
-                         "of the library on its own workload, timed against its roofline")
+                         "of the library on its own workload, timed against its roofline; "
+                         "constopt: PSO then per-program L-BFGS on 65,536 programs x 16,384 "
+                         "rows")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="kernels: fraction of the default sizes (smaller cases for profiling)")
     ap.add_argument("--requests", type=int, default=8)
     ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
     ap.add_argument("--problems", type=int, default=256)
     ap.add_argument("--generations", type=int, default=50)
+    ap.add_argument("--constopt-programs", type=int, default=65_536)
+    ap.add_argument("--constopt-rows", type=int, default=16_384)
     return ap.parse_args()
 
 
@@ -627,6 +631,163 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def run_constopt(args):
+    """Constant optimisation: 65,536 programs (lengths U{5..40}, 2..8 constants each, K = 8),
+    X ~ N(0,1)^{3 x 16,384}, y from a depth-4 tree plus 1% noise.  One step = PSO (32 particles x
+    20 steps; the multi-kernel path, whose evaluation is one fitness launch per step over the
+    2,097,152 particle programs) followed by per-program L-BFGS (10 iterations, history 5, strong
+    Wolfe, at most 20 evaluations, each one launch of loss and adjoint gradient) and the
+    improvement-only acceptance, through GPUOptimizer.  Beside it: the plain path for the L-BFGS
+    phase -- the reference's structure at this size (one joint torch.optim.LBFGS over
+    RPNBackwardFunction: per-row evaluator writing [B, D] predictions, torch reductions, adjoint
+    kernel) -- and the end-to-end figure with host arrays in and fitted constants out."""
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    entry.load_package()
+    from warpsymbolic_b200 import synthetic
+    from warpsymbolic_b200.evaluation import GPUEvaluator
+    from warpsymbolic_b200.optimization import GPUOptimizer
+    B, D = args.constopt_programs, args.constopt_rows
+    wl = synthetic.constopt_workload(seed=args.seed, n_programs=B, n_rows=D)
+    n_tok = wl.n_tokens()
+    tok_sum = float(n_tok.sum())
+    P_, STEPS, ITERS, HIST = 32, 20, 10, 5
+    ev = GPUEvaluator(wl.grammar, dev, dtype=torch.float32)
+    opt = GPUOptimizer(ev, dev, dtype=torch.float32)
+    h_pop = torch.from_numpy(wl.population).pin_memory()
+    h_c = torch.from_numpy(wl.constants).pin_memory()
+    h_X = torch.from_numpy(np.ascontiguousarray(wl.X)).pin_memory()
+    h_y = torch.from_numpy(wl.y).pin_memory()
+    d_pop, d_c, d_X, d_y = (t.to(dev) for t in (h_pop, h_c, h_X, h_y))
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    ev_ = lambda: torch.cuda.Event(enable_timing=True)
+
+    def job(pop, c, X, y):
+        torch.manual_seed(args.seed)
+        e0, e1, e2 = ev_(), ev_(), ev_()
+        e0.record(stream)
+        gpos, gerr = opt.nano_pso(pop, c, X, y, steps=STEPS, num_particles=P_)
+        e1.record(stream)
+        new_c, errs = opt.lbfgs_optimize_top_k(pop, gpos.to(torch.float32).contiguous(), X, y,
+                                               top_k=pop.shape[0], max_iter=ITERS,
+                                               per_program=True, history_size=HIST)
+        e2.record(stream)
+        return new_c, errs, gerr, (e0, e1, e2)
+
+    for _ in range(max(args.warmup, 1)):
+        job(d_pop, d_c, d_X, d_y)
+    torch.cuda.synchronize()
+    before = ev.evaluate_batch(d_pop, d_X, d_y, d_c)
+    pso_ms, lb_ms, evals_tot = [], [], []
+    with ClockSampler(0) as clk:
+        for _ in range(max(args.steps, 1)):
+            flush.zero_()
+            new_c, errs, gerr, (e0, e1, e2) = job(d_pop, d_c, d_X, d_y)
+            e2.synchronize()
+            pso_ms.append(e0.elapsed_time(e1))
+            lb_ms.append(e1.elapsed_time(e2))
+            evals = opt.last_lbfgs_evals.to(torch.float64).cpu().numpy()
+            evals_tot.append(evals)
+    pso_evals = float(STEPS) * P_ * tok_sum * D
+    ev_b = evals_tot[-1]
+    lbfgs_evals = float((ev_b * n_tok).sum()) * D + 2.0 * tok_sum * D  # + initial/final scoring
+    step_ms = float(np.median(np.array(pso_ms) + np.array(lb_ms)))
+    value = (pso_evals + lbfgs_evals) / (step_ms / 1e3)
+    rounds = int(ev_b.max())
+    launches = STEPS * 8 + 2 * 6 + 2 * (rounds + 1)
+
+    # end to end: host arrays in, fitted constants and RMSE out
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a = ev_()
+    a.record(stream)
+    pop_h2d, c_h2d, X_h2d, y_h2d = (t.to(dev, non_blocking=True) for t in (h_pop, h_c, h_X, h_y))
+    out_c, out_e, _, _ = job(pop_h2d, c_h2d, X_h2d, y_h2d)
+    res_c, res_e = out_c.cpu(), out_e.cpu()
+    b = ev_()
+    b.record(stream)
+    b.synchronize()
+    e2e_ms = a.elapsed_time(b)
+    e2e_wall = time.perf_counter() - t0
+
+    # plain path for the L-BFGS phase (joint torch L-BFGS, history 10 as the reference's fallback)
+    torch.manual_seed(args.seed)
+    gpos, gerr_p = opt.nano_pso(d_pop, d_c, d_X, d_y, steps=STEPS, num_particles=P_)
+    gpos = gpos.to(torch.float32).contiguous()
+    opt.lbfgs_optimize_top_k(d_pop[:4096], gpos[:4096], d_X, d_y, top_k=4096, max_iter=2)
+    torch.cuda.synchronize()
+    flush.zero_()
+    pa, pb = ev_(), ev_()
+    pa.record(stream)
+    plain_c, plain_e = opt.lbfgs_optimize_top_k(d_pop, gpos, d_X, d_y, top_k=B, max_iter=ITERS)
+    pb.record(stream)
+    pb.synchronize()
+    plain_ms = pa.elapsed_time(pb)
+
+    fin = torch.isfinite(before)
+    med = lambda t: float(torch.median(t[torch.isfinite(t)]).item())
+    cpu = None
+    if not args.no_cpu_baseline:
+        oracle = load_oracle()
+        tm = entry.load_package()._native.TokenMap.from_args(*wl.grammar.scalar_ids(),
+                                                             pi_val=np.pi, e_val=np.e)
+        n = 4
+        while True:
+            t0 = time.perf_counter()
+            oracle.loss_grad(tm, wl.population[:n], wl.X, wl.constants[:n], wl.y)
+            t = time.perf_counter() - t0
+            if t > args.cpu_seconds / 4 or n >= 4096:
+                break
+            n *= 4
+        cpu = {"value": float(n_tok[:n].sum()) * D / t, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "loss and adjoint gradient (the L-BFGS evaluation) of the first %d "
+                         "programs x %d rows, scalar C++ restatement (%.1f s)" % (n, D, t)}
+    peak = 148 * 128 * 1.965e9
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
+            "steps": len(pso_ms), "warmup": max(args.warmup, 1), "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded; the constant-optimisation config's shapes/distributions)",
+            "config": {"workload": "constant optimisation: %d programs (len U{5..40}, 2..8 C), "
+                                   "K=8, 3 vars, D=%d, PSO 32x20 then L-BFGS 10 it (m=5)"
+                                   % (B, D),
+                       "pso": "multi-kernel path, one fitness launch per step over %d particle "
+                              "programs" % (B * P_),
+                       "lbfgs": "per-program strong-Wolfe L-BFGS, max_eval 20, one loss+adjoint "
+                                "launch per evaluation round",
+                       "l2": "L2 flushed (256 MB write) before every timed step"},
+            "phases_ms": {"pso": float(np.median(pso_ms)), "lbfgs": float(np.median(lb_ms))},
+            "node_evals": {"pso": pso_evals, "lbfgs_forward": lbfgs_evals,
+                           "note": "L-BFGS evaluations traverse each program forward and in "
+                                   "reverse; counted once"},
+            "pso_node_evals_per_s": pso_evals / (np.median(pso_ms) / 1e3),
+            "lbfgs_node_evals_per_s": lbfgs_evals / (np.median(lb_ms) / 1e3),
+            "lbfgs_evals_per_program": {"mean": float(ev_b.mean()), "max": int(ev_b.max())},
+            "roofline": {"bound": "fp32-issue", "achieved": value, "peak": peak,
+                         "unit": "node-evals/s", "frac": value / peak,
+                         "peak_note": "1 FP32 lane-op per node-eval: 148 SMs x 128 lanes x "
+                                      "1.965 GHz (fallback; no measured-peaks file)",
+                         "traffic": None},
+            "quality": {"median_rmse_initial": med(before), "median_rmse_after_pso": med(gerr),
+                        "median_rmse_final": med(errs),
+                        "lbfgs_improved_frac": float((errs < gerr.to(errs.dtype)).float().mean()),
+                        "plain_median_rmse_final": med(plain_e),
+                        "plain_lbfgs_improved_frac":
+                            float((plain_e < gerr_p.to(plain_e.dtype)).float().mean())},
+            "plain_lbfgs_ms": plain_ms, "lbfgs_speedup_vs_plain": plain_ms / float(np.median(lb_ms)),
+            "clocks": clk.summary(),
+            "e2e": {"value": (pso_evals + lbfgs_evals) / (e2e_ms / 1e3), "unit": UNIT,
+                    "ms": e2e_ms, "wall_s": e2e_wall,
+                    "h2d_bytes_per_step": int(h_pop.numel() + 4 * h_c.numel() + 4 * h_X.numel()
+                                              + 4 * h_y.numel()),
+                    "d2h_bytes_per_step": int(4 * res_c.numel() + 4 * res_e.numel())},
+            "gpu_launches": launches}
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
 def run_kernels(args):
     """Every kernel beside the fitness evaluator on a workload of the benchmark configs' shapes,
     timed with CUDA events (median of 5 after 3 warm-ups, L2 flushed before each), one JSON line
@@ -813,6 +974,15 @@ def main():
                                              "one-request-at-a-time path is timed beside ours"}))
             return
         run_serving(args)
+        return
+    if args.config == "constopt":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "config": "constopt",
+                              "unavailable": "the reference's multi-kernel PSO cannot run this "
+                                             "size (B*P*D > 2^31 in its evaluator); its L-BFGS "
+                                             "structure is timed as the plain path beside ours"}))
+            return
+        run_constopt(args)
         return
     if args.config == "batched":
         if args.impl == "reference":

@@ -167,9 +167,10 @@ class GPUOptimizer:
         from .constfit import lbfgs
         x_v = self._vars_major(x, y_target.numel()).to(c.dtype)
         y = y_target.to(c.dtype).contiguous()
-        c_fit, _, _ = lbfgs(pop_k, x_v, c.contiguous(), y, self._ids, max_iter=max_iter,
-                            max_eval=max_iter * 2, history_size=history_size,
-                            tolerance_grad=1e-7, tolerance_change=1e-9, grad_clip=1e4)
+        c_fit, _, evals = lbfgs(pop_k, x_v, c.contiguous(), y, self._ids, max_iter=max_iter,
+                                max_eval=max_iter * 2, history_size=history_size,
+                                tolerance_grad=1e-7, tolerance_change=1e-9, grad_clip=1e4)
+        self.last_lbfgs_evals = evals  # loss evaluations per program (device tensor)
         return self._accept(pop_k, c_fit, x, y_target, best_errs_k, best_c_k, constants)
 
     def _accept(self, pop_k, c_fit, x, y_target, best_errs_k, best_c_k, constants):

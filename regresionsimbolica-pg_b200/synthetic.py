@@ -180,6 +180,30 @@ def eval_scale_workload(seed: int = 0, n_programs: int = 1_048_576, n_rows: int 
     return EvalWorkload(g, pop, consts, X, y)
 
 
+def constopt_workload(seed: int = 0, n_programs: int = 65_536, n_rows: int = 16_384,
+                      n_vars: int = 3, L: int = 40, len_low: int = 5, len_high: int = 40,
+                      K: int = 8, min_consts: int = 2, const_range=(-3.0, 3.0),
+                      target_depth: int = 4, noise_rel: float = 0.01,
+                      operators: Optional[Sequence[str]] = None) -> EvalWorkload:
+    """Constant-optimisation workload: programs of lengths U{5..40} with 2..8 `C` tokens each,
+    K = 8 constant slots U[-3,3], X ~ N(0,1)^{3 x 16,384}, y from a depth-4 tree with constants
+    U[-3,3] plus Gaussian noise of sigma = 0.01 * std(y)."""
+    rng = np.random.default_rng(seed)
+    g = GPUGrammar(num_variables=n_vars, operators=BENCH_OPERATORS if operators is None else operators)
+    c_id = g.token_to_id['C']
+    pop = random_programs(g, n_programs, len_low, len_high, L, rng, const_prob=0.45, max_consts=K)
+    for _ in range(50):  # redraw programs with fewer than min_consts constants
+        short = np.nonzero((pop == c_id).sum(axis=1) < min_consts)[0]
+        if len(short) == 0:
+            break
+        pop[short] = random_programs(g, len(short), len_low, len_high, L, rng, const_prob=0.6,
+                                     max_consts=K)
+    consts = rng.uniform(*const_range, size=(n_programs, K)).astype(np.float32)
+    X = rng.standard_normal((n_vars, n_rows)).astype(np.float32)
+    y, _ = random_target(rng, X, target_depth, noise_rel=noise_rel, const_range=const_range)
+    return EvalWorkload(g, pop, consts, X, y)
+
+
 @dataclass
 class BatchWorkload:
     """Independent regression problems, each an EvalWorkload with its own grammar (variable
