@@ -920,6 +920,12 @@ def run_kernels(args):
                                                            E_VAL),
           nbytes=4 * B3 * D3, evals=tok3 * D3,
           note="%d programs x %d rows, K=%d (bytes: grad_output)" % (B3, D3, K3))
+    from warpsymbolic_b200 import constfit
+    del gout
+    timed("loss_grad", lambda: constfit.loss_grad(dp3, X3, c3, y3, ids3),
+          evals=tok3 * D3,
+          note="%d programs x %d rows, K=%d (loss and adjoint gradient, one launch + reduce)"
+               % (B3, D3, K3))
     Bp, Dp = sc(8192), 1024
     Xp, yp = X3[:, :Dp].contiguous(), y3[:Dp].contiguous()
     gpos = torch.empty((Bp, K3), dtype=torch.float32, device=dev)

@@ -370,14 +370,15 @@ ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* population, int64_t
  * grad_output = 2 (preds - y) / D).  Per program b:
  *   out_loss[b]    = mean over rows of (pred[b, d] - y[d])^2                      (double)
  *   out_grad[b, k] = d out_loss[b] / d C_k                                        (`dtype`)
- * with the predictions and adjoints of ws_eval_rpn_backward's forward and adjoint rules.  A
+ * with the forward and adjoint rules of ws_eval_rpn_backward, evaluated in `dtype` (without the
+ * reference's double promotions, which only bit-exactness against it needs).  A
  * program whose final stack depth is not 1 gets an infinite loss and a zero gradient.  `active`
  * (optional, int32 [B]) skips programs with 0; their outputs are left as they are.  Results are
  * deterministic (partial sums per row range, reduced in a fixed order).  The workspace holds
- * the partial sums; its size depends on (B, L, D, K) and the device.
+ * the partial sums; its size depends on (B, L, num_vars, D, K) and the device.
  */
-ws_status ws_loss_grad_workspace_bytes(int32_t dtype, int64_t B, int64_t L, int64_t D, int64_t K,
-                                       size_t* bytes);
+ws_status ws_loss_grad_workspace_bytes(int32_t dtype, int64_t B, int64_t L, int64_t num_vars,
+                                       int64_t D, int64_t K, size_t* bytes);
 ws_status ws_loss_grad(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
                        const void* x, int64_t num_vars, int64_t D, const void* constants,
                        int64_t K, const void* y, const int32_t* active, double* out_loss,
@@ -408,8 +409,9 @@ typedef struct ws_lbfgs_opts {
   int32_t sync_every;       /* rounds between reads of the active count; 0 = never (capturable) */
   int32_t reserved;
 } ws_lbfgs_opts;
-ws_status ws_lbfgs_adjoint_workspace_bytes(int32_t dtype, int64_t B, int64_t L, int64_t D,
-                                           int64_t K, int32_t history, size_t* bytes);
+ws_status ws_lbfgs_adjoint_workspace_bytes(int32_t dtype, int64_t B, int64_t L,
+                                           int64_t num_vars, int64_t D, int64_t K,
+                                           int32_t history, size_t* bytes);
 ws_status ws_lbfgs_adjoint(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
                            const void* x, int64_t num_vars, int64_t D, void* constants, int64_t K,
                            const void* y, const ws_lbfgs_opts* opts, double* out_loss,

@@ -150,11 +150,11 @@ _SIGS = {
     "ws_sharing_table_slots": (_I64, []),
     "ws_eval_rpn_backward": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
                                     C.POINTER(TokenMap), _P]),
-    "ws_loss_grad_workspace_bytes": (_I32, [_I32, _I64, _I64, _I64, _I64,
+    "ws_loss_grad_workspace_bytes": (_I32, [_I32, _I64, _I64, _I64, _I64, _I64,
                                             C.POINTER(C.c_size_t)]),
     "ws_loss_grad": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P, _P, _P,
                             C.POINTER(TokenMap), _P, C.c_size_t, _P]),
-    "ws_lbfgs_adjoint_workspace_bytes": (_I32, [_I32, _I64, _I64, _I64, _I64, _I32,
+    "ws_lbfgs_adjoint_workspace_bytes": (_I32, [_I32, _I64, _I64, _I64, _I64, _I64, _I32,
                                                 C.POINTER(C.c_size_t)]),
     "ws_lbfgs_adjoint": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P,
                                 C.POINTER(LbfgsOpts), _P, _P, C.POINTER(TokenMap), _P,

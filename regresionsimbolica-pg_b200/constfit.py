@@ -63,7 +63,7 @@ def loss_grad(population: torch.Tensor, x: torch.Tensor, constants: torch.Tensor
     dt = dtype_code(x.dtype)
     lib = N.lib()
     need = C.c_size_t(0)
-    N.check(lib.ws_loss_grad_workspace_bytes(dt, B, L, D, K, C.byref(need)))
+    N.check(lib.ws_loss_grad_workspace_bytes(dt, B, L, V, D, K, C.byref(need)))
     ws = workspace(need.value, dev)
     m = _ids_map(ids, pi_val, e_val)
     N.check(lib.ws_loss_grad(dt, ptr(population), B, L, ptr(x), V, D, ptr(constants), K, ptr(y),
@@ -96,7 +96,7 @@ def lbfgs(population: torch.Tensor, x: torch.Tensor, constants: torch.Tensor, y:
     dt = dtype_code(x.dtype)
     lib = N.lib()
     need = C.c_size_t(0)
-    N.check(lib.ws_lbfgs_adjoint_workspace_bytes(dt, B, L, D, K, int(history_size),
+    N.check(lib.ws_lbfgs_adjoint_workspace_bytes(dt, B, L, V, D, K, int(history_size),
                                                  C.byref(need)))
     ws = workspace(need.value, dev)
     opts = N.LbfgsOpts(int(max_iter), int(max_eval), int(history_size), int(max_ls), float(lr),

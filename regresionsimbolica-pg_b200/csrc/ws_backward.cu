@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
+#include <type_traits>
 
 #include "ws_internal.h"
 
@@ -82,6 +83,11 @@ struct BwdParams {
   // each (program, row range) item writes its partial sums (no atomics, fixed order)
   const T* y;
   const int32_t* active;  // optional: programs with 0 are skipped
+  int64_t V;              // variables; with stage_x each thread copies its rows of x to shared
+  int stage_x;            // memory once per row group
+  int tape_ops;           // operator slots of the tape (>= every program's operator count)
+  const int32_t* list;        // optional: the programs of this launch (a bucket) ...
+  const int32_t* list_count;  // ... and how many there are (read on the device)
   double* part_loss;      // [n_items]   sum over the item's rows of (pred - y)^2
   double* part_grad;      // [n_items, K] sum over the item's rows of the constant adjoints
 };
@@ -223,49 +229,179 @@ __device__ __forceinline__ void acc_t(T& dst, T coef, T adj) {
   dst = fma(coef, adj, dst);
 }
 
-// One operand of a tape operator for this thread's row.
-template <typename T>
-__device__ __forceinline__ T operand(uint8_t k, uint16_t i, const T* val, int TS, int tid,
-                                     const T* x, int64_t D, int64_t d, const T* s_lit,
-                                     const T* cst) {
+// ---- the adjoint kernel ---------------------------------------------------------------------
+// One block owns one program for a range of rows; every thread carries R consecutive rows
+// through each tape step, so one decode of an operator (a broadcast shared-memory load and a
+// block-uniform branch) serves R rows, and the R rows' arithmetic is independent work for the
+// pipelines.  One tape slot per operator and thread ([op][thread][R] values, vector loads and
+// stores) holds the operator's values after the forward sweep and its adjoints during the reverse
+// sweep: the program is a tree, so the only reader of a value is the operator's parent, which
+// reads it before it writes the adjoint into the same slot; exp and pow, whose adjoint rules use
+// their own output, recompute it from their operands bit for bit.  The previous operator's values
+// and the adjoint handed to it stay in registers (BOp::pad bit 0 / bit 1: the left / right operand
+// is operator o-1), and constant adjoints are summed in registers when K <= kRegSlots (the slot of
+// a delivery is the same for the whole block, so the register is chosen by a uniform switch).
+//
+// LOSS = false (ws_eval_rpn_backward): the root adjoint of row d is grad_output[b, d] and every
+// per-row expression is the reference's, double promotions included (acc_d / acc_t), so per-row
+// adjoints are bit-identical to the reference's; per-row constant adjoints are summed in FP64.
+// LOSS = true (ws_loss_grad): the root adjoint is 2 (pred - y[d]) / D and the arithmetic is in T;
+// the loss is summed per thread in FP64.  Both skip the contributions of zero adjoints.
+constexpr int kRegSlots = 8;
+
+template <typename T, int R>
+__device__ __forceinline__ void ld_vec(const T* p, T (&o)[R]) {
+  if constexpr (R * sizeof(T) == 16) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    const T* q = reinterpret_cast<const T*>(&v);
+#pragma unroll
+    for (int r = 0; r < R; ++r) o[r] = q[r];
+  } else if constexpr (R * sizeof(T) == 8) {
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    const T* q = reinterpret_cast<const T*>(&v);
+#pragma unroll
+    for (int r = 0; r < R; ++r) o[r] = q[r];
+  } else {
+#pragma unroll
+    for (int r = 0; r < R; ++r) o[r] = p[r];
+  }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void st_vec(T* p, const T (&v)[R]) {
+  if constexpr (R * sizeof(T) == 16) {
+    float4 w;
+    T* q = reinterpret_cast<T*>(&w);
+#pragma unroll
+    for (int r = 0; r < R; ++r) q[r] = v[r];
+    *reinterpret_cast<float4*>(p) = w;
+  } else if constexpr (R * sizeof(T) == 8) {
+    float2 w;
+    T* q = reinterpret_cast<T*>(&w);
+#pragma unroll
+    for (int r = 0; r < R; ++r) q[r] = v[r];
+    *reinterpret_cast<float2*>(p) = w;
+  } else {
+#pragma unroll
+    for (int r = 0; r < R; ++r) p[r] = v[r];
+  }
+}
+
+// The R values of one operand: an earlier operator's (tape), a variable's (rows past d_end read
+// as 0), a constant's or a literal's.
+template <typename T, int R>
+__device__ __forceinline__ void operand_vec(uint8_t k, uint16_t i, const T* tape, int TS, int tid,
+                                            const T* x, int64_t D, int64_t d0, int64_t d_end,
+                                            const T* s_lit, const T* cst, const T* xs,
+                                            T (&o)[R]) {
   switch (k) {
-    case OPD_OP: return val[(size_t)i * TS + tid];
-    case OPD_VAR: return x[(int64_t)i * D + d];
-    case OPD_CONST: return cst[i];
-    default: return i < 10 ? s_lit[i] : (T)1.0;
+    case OPD_OP: ld_vec<T, R>(tape + ((size_t)i * TS + tid) * R, o); break;
+    case OPD_VAR: {
+      if (xs) {  // this thread's rows, staged at the start of the row group
+        ld_vec<T, R>(xs + ((size_t)i * TS + tid) * R, o);
+        break;
+      }
+      const T* xr = x + (int64_t)i * D;
+#pragma unroll
+      for (int r = 0; r < R; ++r) o[r] = d0 + r < d_end ? xr[d0 + r] : (T)0;
+      break;
+    }
+    case OPD_CONST: {
+      const T c = cst[i];
+#pragma unroll
+      for (int r = 0; r < R; ++r) o[r] = c;
+      break;
+    }
+    default: {
+      const T c = i < 10 ? s_lit[i] : (T)1.0;
+#pragma unroll
+      for (int r = 0; r < R; ++r) o[r] = c;
+    }
   }
 }
 
-// Hands an adjoint contribution to an operand: an operator's slot is written (the value the
-// reference's `+=` leaves in a zero slot); a constant slot accumulates it when nonzero (the
-// reference skips zero adjoints); variables and literals take none.
+#define WS_FOR_R for (int r = 0; r < R; ++r)
+
+template <typename T, int R>
+__device__ __forceinline__ void fwd_binary_vec(uint8_t op, const T (&a)[R], const T (&b)[R],
+                                               T (&v)[R]) {
+  switch (op) {
+    case FO_ADD: WS_FOR_R v[r] = a[r] + b[r]; break;
+    case FO_SUB: WS_FOR_R v[r] = a[r] - b[r]; break;
+    case FO_MUL: WS_FOR_R v[r] = a[r] * b[r]; break;
+    default: WS_FOR_R v[r] = fwd_binary<T>(op, a[r], b[r]); break;
+  }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void fwd_unary_vec(uint8_t op, const T (&a)[R], T (&v)[R]) {
+  switch (op) {
+    case FO_SIN: WS_FOR_R v[r] = sin(a[r]); break;
+    case FO_COS: WS_FOR_R v[r] = cos(a[r]); break;
+    case FO_NEG: WS_FOR_R v[r] = -a[r]; break;
+    default: WS_FOR_R v[r] = fwd_unary<T>(op, a[r]); break;
+  }
+}
+
 template <typename T>
-__device__ __forceinline__ void deliver(uint8_t k, uint16_t i, T c, T* adj, int TS, int tid,
-                                        double* cacc, int* touched) {
-  if (k == OPD_OP) {
-    adj[(size_t)i * TS + tid] = c;
-  } else if (k == OPD_CONST && c != (T)0) {
-    cacc[(size_t)i * TS + tid] += (double)c;
-    touched[i] = 1;
+__device__ __forceinline__ void creg_add(T (&cr)[kRegSlots], int i, T c) {
+  switch (i) {
+    case 0: cr[0] += c; break;
+    case 1: cr[1] += c; break;
+    case 2: cr[2] += c; break;
+    case 3: cr[3] += c; break;
+    case 4: cr[4] += c; break;
+    case 5: cr[5] += c; break;
+    case 6: cr[6] += c; break;
+    default: cr[7] += c; break;
   }
 }
 
-// One tape slot per operator and thread holds the operator's value after the forward sweep and
-// its adjoint during the reverse sweep: the program is a tree, so the only reader of a value is
-// the operator's parent, which reads it before it writes the adjoint into the same slot.  The
-// two operators whose adjoint rule uses their own output (exp, pow) recompute it from their
-// operands, bit for bit.  One slot per operator halves the shared memory of separate value and
-// adjoint tapes, which is what limits how many blocks an SM holds.
+// Constant-slot accumulator: FP64 per row for the reference path, T for the loss path.
 template <typename T, bool LOSS>
-__global__ void __launch_bounds__(128) backward_kernel(BwdParams<T> p, BwdLut lut) {
+using CAcc = typename std::conditional<LOSS, T, double>::type;
+
+template <typename T, int R, bool LOSS, bool KREG>
+__device__ __forceinline__ void deliver_vec(uint8_t k, uint16_t i, const T (&c)[R], bool to_carry,
+                                            T (&carry)[R], bool& have, T* tape, int TS, int tid,
+                                            CAcc<T, LOSS> (&cr)[kRegSlots], double* cacc,
+                                            int* touched) {
+  if (k == OPD_OP) {
+    if (to_carry) {
+      WS_FOR_R carry[r] = c[r];
+      have = true;
+    } else {
+      st_vec<T, R>(tape + ((size_t)i * TS + tid) * R, c);
+    }
+  } else if (k == OPD_CONST) {
+    using A = CAcc<T, LOSS>;
+    A s = (A)0;
+    bool any = false;
+    WS_FOR_R {
+      if (c[r] != (T)0) {
+        s += (A)c[r];
+        any = true;
+      }
+    }
+    if (any) {
+      if (KREG) creg_add<A>(cr, i, s);
+      else cacc[(size_t)i * TS + tid] += (double)s;
+      if (!LOSS) touched[i] = 1;
+    }
+  }
+}
+
+template <typename T, int R, bool LOSS, bool KREG>
+__global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int TS = p.tape_stride;
   BOp* ops = reinterpret_cast<BOp*>(smem);
   double* cacc = reinterpret_cast<double*>(smem + al16((size_t)kMaxL * sizeof(BOp)));
-  double* lacc_s = cacc + (size_t)p.K * TS;  // loss mode: per-thread loss partials
-  int* touched = reinterpret_cast<int*>(lacc_s + (LOSS ? TS : 0));
+  double* lacc_s = cacc + (size_t)p.K * TS;
+  int* touched = reinterpret_cast<int*>(lacc_s + TS);
   T* tape = reinterpret_cast<T*>(
       reinterpret_cast<unsigned char*>(touched) + al16((size_t)p.K * sizeof(int)));
+  T* xs = p.stage_x ? tape + (size_t)p.tape_ops * TS * R : nullptr;  // [V][thread][R]
   __shared__ BRoot s_root;
   __shared__ int64_t s_prog;
   __shared__ T s_lit[10];
@@ -280,137 +416,278 @@ __global__ void __launch_bounds__(128) backward_kernel(BwdParams<T> p, BwdLut lu
   if (threadIdx.x == 0) s_prog = -1;
   const int tid = threadIdx.x;
   const T loss_scale = LOSS ? (T)(2.0 / (double)p.D) : (T)0;
+  using A = CAcc<T, LOSS>;
 
-  for (int64_t item = blockIdx.x; item < p.n_items; item += gridDim.x) {
-    const int64_t b = item / p.n_splits;
-    const int64_t split = item - b * p.n_splits;
+  const int64_t n_items = p.list ? (int64_t)(*p.list_count) * p.n_splits : p.n_items;
+  for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int64_t li = item / p.n_splits;
+    const int64_t split = item - li * p.n_splits;
+    const int64_t b = p.list ? (int64_t)p.list[li] : li;
+    const int64_t slot = b * p.n_splits + split;  // partial sums of (program, row range)
     if (LOSS && p.active && p.active[b] == 0) continue;  // uniform over the block
     __syncthreads();
     if (tid == 0 && s_prog != b) {
-      s_root = parse_program(p.pop + b * p.L, p.L, p.K, s_tab, ops);
+      BRoot rt0 = parse_program(p.pop + b * p.L, p.L, p.K, s_tab, ops);
+      for (int o = 0; o < rt0.n_ops; ++o) {
+        uint16_t f = 0;
+        if (ops[o].ka == OPD_OP && (int)ops[o].a == o - 1) f |= 1;
+        if (ops[o].binary && ops[o].kb == OPD_OP && (int)ops[o].b == o - 1) f |= 2;
+        ops[o].pad = f;
+      }
+      s_root = rt0;
       s_prog = b;
     }
     for (int64_t k = tid; k < p.K; k += blockDim.x) touched[k] = 0;
-    for (int64_t k = 0; k < p.K; ++k) cacc[k * TS + tid] = 0.0;
+    if (!KREG)
+      for (int64_t k = 0; k < p.K; ++k) cacc[k * TS + tid] = 0.0;
     __syncthreads();
     const BRoot rt = s_root;
     if (!rt.valid) {
       if (LOSS) {  // no prediction: infinite loss, no gradient
-        if (tid == 0) p.part_loss[item] = __longlong_as_double(0x7ff0000000000000ll);
-        for (int64_t k = tid; k < p.K; k += blockDim.x) p.part_grad[item * p.K + k] = 0.0;
+        if (tid == 0) p.part_loss[slot] = __longlong_as_double(0x7ff0000000000000ll);
+        for (int64_t k = tid; k < p.K; k += blockDim.x) p.part_grad[slot * p.K + k] = 0.0;
       }
       continue;
     }
-
     const int64_t d_begin = split * p.rows_per_split;
     int64_t d_end = d_begin + p.rows_per_split;
     if (d_end > p.D) d_end = p.D;
     const T* xcol = p.x;
     const T* cst = p.consts + b * p.K;
     const int n = rt.n_ops;
+    A cr[kRegSlots];
+#pragma unroll
+    for (int k = 0; k < kRegSlots; ++k) cr[k] = (A)0;
     double lacc = 0.0;
-    for (int64_t d = d_begin + tid; d < d_end; d += blockDim.x) {
+
+    for (int64_t d0 = d_begin + (int64_t)tid * R; d0 < d_end; d0 += (int64_t)TS * R) {
+      // this thread's rows: x staged (only this thread reads them: no barrier), the root
+      // adjoint's inputs loaded now so that their latency overlaps the forward sweep
+      if (xs) {
+        for (int64_t v = 0; v < p.V; ++v) {
+          const T* xr = xcol + v * p.D;
+          T xv[R];
+          WS_FOR_R xv[r] = d0 + r < d_end ? xr[d0 + r] : (T)0;
+          st_vec<T, R>(xs + ((size_t)v * TS + tid) * R, xv);
+        }
+      }
+      T ext[R];  // y (loss) or grad_output (reference path) of the R rows
+      WS_FOR_R ext[r] = d0 + r < d_end ? (LOSS ? p.y[d0 + r] : p.gout[b * p.D + d0 + r]) : (T)0;
       // forward: operator values
+      T last[R];
+      WS_FOR_R last[r] = (T)0;
       for (int o = 0; o < n; ++o) {
         const BOp op = ops[o];
-        const T v1 = operand<T>(op.ka, op.a, tape, TS, tid, xcol, p.D, d, s_lit, cst);
-        T v;
-        if (op.binary) {
-          const T v2 = operand<T>(op.kb, op.b, tape, TS, tid, xcol, p.D, d, s_lit, cst);
-          v = fwd_binary<T>(op.fop, v1, v2);
+        T va[R], v[R];
+        if (op.pad & 1) {
+          WS_FOR_R va[r] = last[r];
         } else {
-          v = fwd_unary<T>(op.fop, v1);
+          operand_vec<T, R>(op.ka, op.a, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs, va);
         }
-        tape[(size_t)o * TS + tid] = v;
+        if (op.binary) {
+          T vb[R];
+          if (op.pad & 2) {
+            WS_FOR_R vb[r] = last[r];
+          } else {
+            operand_vec<T, R>(op.kb, op.b, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs, vb);
+          }
+          fwd_binary_vec<T, R>(op.fop, va, vb, v);
+        } else {
+          fwd_unary_vec<T, R>(op.fop, va, v);
+        }
+        st_vec<T, R>(tape + ((size_t)o * TS + tid) * R, v);
+        WS_FOR_R last[r] = v[r];
       }
-      T g_root;
+      // root adjoints
+      T g_root[R];
       if (LOSS) {
-        const T pred = operand<T>(rt.kind, rt.idx, tape, TS, tid, xcol, p.D, d, s_lit, cst);
-        const T diff = pred - p.y[d];
-        lacc += (double)diff * (double)diff;
-        g_root = diff * loss_scale;
+        T pred[R];
+        if (rt.kind == OPD_OP && (int)rt.idx == n - 1) {
+          WS_FOR_R pred[r] = last[r];
+        } else {
+          operand_vec<T, R>(rt.kind, rt.idx, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs,
+                            pred);
+        }
+        WS_FOR_R {
+          const T diff = d0 + r < d_end ? pred[r] - ext[r] : (T)0;
+          lacc += (double)diff * (double)diff;
+          g_root[r] = diff * loss_scale;
+        }
       } else {
-        g_root = p.gout[b * p.D + d];
+        WS_FOR_R g_root[r] = ext[r];
       }
+      T carry[R];
+      bool have = false;
       if (rt.kind != OPD_OP) {  // a one-terminal program
-        deliver<T>(rt.kind, rt.idx, g_root, tape, TS, tid, cacc, touched);
+        deliver_vec<T, R, LOSS, KREG>(rt.kind, rt.idx, g_root, false, carry, have, tape, TS, tid,
+                                      cr, cacc, touched);
         continue;
       }
+      if ((int)rt.idx == n - 1) {
+        WS_FOR_R carry[r] = g_root[r];
+        have = true;
+      } else {
+        st_vec<T, R>(tape + ((size_t)rt.idx * TS + tid) * R, g_root);
+      }
       // reverse: each operator hands its adjoint to its operands
-      tape[(size_t)rt.idx * TS + tid] = g_root;
       for (int o = n - 1; o >= 0; --o) {
         const BOp op = ops[o];
-        if (!op.reach) continue;
-        const T g = tape[(size_t)o * TS + tid];
-        T ca = (T)0, cb = (T)0;  // the operands' slots, as the reference leaves them
-        if (g != (T)0) {
-          const T l_val = operand<T>(op.ka, op.a, tape, TS, tid, xcol, p.D, d, s_lit, cst);
-          if (op.binary) {
-            const T r_val = operand<T>(op.kb, op.b, tape, TS, tid, xcol, p.D, d, s_lit, cst);
-            switch (op.bop) {
-              case BO_ADD: ca += g; cb += g; break;
-              case BO_SUB: ca += g; cb -= g; break;
-              case BO_MUL: acc_t(ca, r_val, g); acc_t(cb, l_val, g); break;
-              case BO_DIV:
-                if (fabs(r_val) >= (T)1e-9) {
-                  acc_d(ca, 1.0 / r_val, g);
-                  acc_t(cb, -(l_val / (r_val * r_val)), g);
+        if (!op.reach) {
+          have = false;
+          continue;
+        }
+        T g[R];
+        if (have) {
+          WS_FOR_R g[r] = carry[r];
+        } else {
+          ld_vec<T, R>(tape + ((size_t)o * TS + tid) * R, g);
+        }
+        have = false;
+        T lv[R], ca[R], cb[R];
+        operand_vec<T, R>(op.ka, op.a, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs, lv);
+        WS_FOR_R { ca[r] = (T)0; cb[r] = (T)0; }
+        if (op.binary) {
+          T rv[R];
+          operand_vec<T, R>(op.kb, op.b, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs, rv);
+          switch (op.bop) {
+            case BO_ADD: WS_FOR_R { ca[r] += g[r]; cb[r] += g[r]; } break;
+            case BO_SUB: WS_FOR_R { ca[r] += g[r]; cb[r] -= g[r]; } break;
+            case BO_MUL:
+              if (LOSS) WS_FOR_R { ca[r] = rv[r] * g[r]; cb[r] = lv[r] * g[r]; }
+              else WS_FOR_R { acc_t(ca[r], rv[r], g[r]); acc_t(cb[r], lv[r], g[r]); }
+              break;
+            case BO_DIV:
+              WS_FOR_R {
+                if (fabs(rv[r]) >= (T)1e-9) {
+                  if (LOSS) {
+                    ca[r] = g[r] / rv[r];
+                    cb[r] = -(lv[r] / (rv[r] * rv[r])) * g[r];
+                  } else {
+                    acc_d(ca[r], 1.0 / rv[r], g[r]);
+                    acc_t(cb[r], -(lv[r] / (rv[r] * rv[r])), g[r]);
+                  }
                 }
-                break;
-              case BO_POW:
-                if (l_val > 0) {
-                  const T out_val = fwd_binary<T>(op.fop, l_val, r_val);
-                  acc_d(ca, (double)r_val * pow((double)l_val, (double)r_val - 1.0), g);
-                  acc_t(cb, out_val * log(l_val), g);
+              }
+              break;
+            case BO_POW:
+              WS_FOR_R {
+                if (lv[r] > 0) {
+                  const T out_val = fwd_binary<T>(op.fop, lv[r], rv[r]);
+                  if (LOSS) {
+                    ca[r] = rv[r] * pow(lv[r], rv[r] - (T)1) * g[r];
+                    cb[r] = out_val * log(lv[r]) * g[r];
+                  } else {
+                    acc_d(ca[r], (double)rv[r] * pow((double)lv[r], (double)rv[r] - 1.0), g[r]);
+                    acc_t(cb[r], out_val * log(lv[r]), g[r]);
+                  }
                 }
-                break;
-              default: break;
-            }
-          } else {
-            switch (op.bop) {
-              case BO_SIN: acc_t(ca, cos(l_val), g); break;
-              case BO_COS: acc_t(ca, -sin(l_val), g); break;
-              case BO_LOG:
-                if (fabs(l_val) > (T)1e-9) acc_d(ca, 1.0 / l_val, g);
-                break;
-              case BO_EXP: acc_t(ca, fwd_unary<T>(op.fop, l_val), g); break;
-              case BO_SQRT:
-                if (l_val > (T)1e-9) acc_d(ca, 0.5 / sqrt(l_val), g);
-                break;
-              case BO_NEG: ca += -g; break;
-              default: break;
-            }
+              }
+              break;
+            default: break;
+          }
+          WS_FOR_R if (g[r] == (T)0) cb[r] = (T)0;
+          // the right operand sits later in the program: its constants first, as the
+          // reference's reverse walk meets them
+          deliver_vec<T, R, LOSS, KREG>(op.kb, op.b, cb, (op.pad & 2) != 0, carry, have, tape, TS,
+                                        tid, cr, cacc, touched);
+        } else {
+          switch (op.bop) {
+            case BO_SIN:
+              if (LOSS) WS_FOR_R ca[r] = cos(lv[r]) * g[r];
+              else WS_FOR_R acc_t(ca[r], cos(lv[r]), g[r]);
+              break;
+            case BO_COS:
+              if (LOSS) WS_FOR_R ca[r] = -sin(lv[r]) * g[r];
+              else WS_FOR_R acc_t(ca[r], -sin(lv[r]), g[r]);
+              break;
+            case BO_LOG:
+              WS_FOR_R {
+                if (fabs(lv[r]) > (T)1e-9) {
+                  if (LOSS) ca[r] = g[r] / lv[r];
+                  else acc_d(ca[r], 1.0 / lv[r], g[r]);
+                }
+              }
+              break;
+            case BO_EXP:
+              if (LOSS) WS_FOR_R ca[r] = fwd_unary<T>(op.fop, lv[r]) * g[r];
+              else WS_FOR_R acc_t(ca[r], fwd_unary<T>(op.fop, lv[r]), g[r]);
+              break;
+            case BO_SQRT:
+              WS_FOR_R {
+                if (lv[r] > (T)1e-9) {
+                  if (LOSS) ca[r] = (T)0.5 / sqrt(lv[r]) * g[r];
+                  else acc_d(ca[r], 0.5 / sqrt(lv[r]), g[r]);
+                }
+              }
+              break;
+            case BO_NEG: WS_FOR_R ca[r] += -g[r]; break;
+            default: break;
           }
         }
-        // the right operand sits later in the program: its constants first, as the reference's
-        // reverse walk meets them
-        if (op.binary) deliver<T>(op.kb, op.b, cb, tape, TS, tid, cacc, touched);
-        deliver<T>(op.ka, op.a, ca, tape, TS, tid, cacc, touched);
+        WS_FOR_R if (g[r] == (T)0) ca[r] = (T)0;
+        deliver_vec<T, R, LOSS, KREG>(op.ka, op.a, ca, (op.pad & 1) != 0, carry, have, tape, TS,
+                                      tid, cr, cacc, touched);
       }
+    }
+    if (KREG) {
+#pragma unroll
+      for (int k = 0; k < kRegSlots; ++k)
+        if (k < p.K) cacc[(size_t)k * TS + tid] = (double)cr[k];
     }
     if (LOSS) lacc_s[tid] = lacc;
     __syncthreads();
     // fixed-order reduction over the block's threads, one thread per slot
     for (int64_t k = tid; k < p.K; k += blockDim.x) {
-      if (LOSS) {
-        double s = 0.0;
-        if (touched[k])
-          for (int t = 0; t < (int)blockDim.x; ++t) s += cacc[k * TS + t];
-        p.part_grad[item * p.K + k] = s;
-        continue;
-      }
-      if (!touched[k]) continue;
       double s = 0.0;
       for (int t = 0; t < (int)blockDim.x; ++t) s += cacc[k * TS + t];
-      T* dst = p.grad + b * p.K + k;
-      if (p.n_splits == 1) *dst = *dst + (T)s;
-      else atomicAdd(dst, (T)s);
+      if (LOSS) {
+        p.part_grad[slot * p.K + k] = s;
+      } else if (touched[k]) {
+        T* dst = p.grad + b * p.K + k;
+        if (p.n_splits == 1) *dst = *dst + (T)s;
+        else atomicAdd(dst, (T)s);
+      }
     }
     if (LOSS && tid == 0) {
       double s = 0.0;
       for (int t = 0; t < (int)blockDim.x; ++t) s += lacc_s[t];
-      p.part_loss[item] = s;
+      p.part_loss[slot] = s;
     }
+  }
+}
+
+#undef WS_FOR_R
+
+// Programs grouped by operator count, so that each group runs with a tape sized for it: a
+// program's count of operator tokens before its first PAD bounds its tape length.  Programs with
+// active[b] == 0 are left out.  lists: [n_buckets, B]; the order inside a bucket does not matter
+// (every (program, row range) writes its own partial sums).
+constexpr int kMaxBuckets = 9;
+constexpr int kBucketOps[kMaxBuckets] = {8, 16, 24, 32, 48, 64, 96, 128, 256};
+__constant__ int c_bucket_ops[kMaxBuckets] = {8, 16, 24, 32, 48, 64, 96, 128, 256};
+
+__global__ void __launch_bounds__(256) bucket_kernel(const uint8_t* __restrict__ pop, int64_t B,
+                                                     int64_t L, BwdLut lut,
+                                                     const int32_t* __restrict__ active,
+                                                     int n_buckets, int32_t* counts,
+                                                     int32_t* lists) {
+  __shared__ uint8_t s_kind[256];
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) s_kind[t] = lut.kind[t];
+  __syncthreads();
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < B;
+       b += (int64_t)gridDim.x * blockDim.x) {
+    if (active && active[b] == 0) continue;
+    const uint8_t* row = pop + b * L;
+    int n = 0;
+    for (int64_t t = 0; t < L; ++t) {
+      const uint8_t k = s_kind[row[t]];
+      if (k == BK_PAD) break;
+      n += (k == BK_BIN || k == BK_UN) ? 1 : 0;
+    }
+    int j = 0;
+    while (j < n_buckets - 1 && n > c_bucket_ops[j]) ++j;
+    const int pos = atomicAdd(counts + j, 1);
+    lists[(int64_t)j * B + pos] = (int32_t)b;
   }
 }
 
@@ -494,50 +771,94 @@ BwdLut build_bwd_lut(const ws_token_map& m, int64_t num_vars) {
   return lut;
 }
 
-template <typename T, bool LOSS>
-size_t backward_smem(int64_t L, int64_t K, int threads) {
+constexpr int64_t kStageMaxVars = 16;  // x is staged in shared memory up to this many variables
+
+template <typename T>
+size_t backward_smem(int64_t L, int64_t K, int64_t V, int threads, int R) {
+  const int64_t vs = V <= kStageMaxVars ? V : 0;
   return al16((size_t)kMaxL * sizeof(BOp)) + (size_t)K * threads * sizeof(double) +
-         (LOSS ? (size_t)threads * sizeof(double) : 0) + al16((size_t)K * sizeof(int)) +
-         (size_t)L * threads * sizeof(T);
+         (size_t)threads * sizeof(double) + al16((size_t)K * sizeof(int)) +
+         (size_t)(L + vs) * threads * R * sizeof(T);
 }
 
-// Block size, shared memory and the split of rows into ranges for one launch.  Rows are split
-// only when there are too few programs to fill the GPU; the split depends on (B, L, K, D) and the
-// device alone.
+// Block size, rows per thread, shared memory and the split of rows into ranges for one launch.
+// Rows are split only when there are too few programs to fill the GPU; the split depends on
+// (B, L, K, D) and the device alone.
 struct BwdPlan {
-  int threads;
+  int threads, R;
   size_t smem;
   int64_t n_splits, rows, grid;
 };
 
+template <typename T>
+constexpr int kRowsMax = sizeof(T) == 4 ? 4 : 2;
+
 template <typename T, bool LOSS>
-ws_status backward_plan(int64_t B, int64_t L, int64_t D, int64_t K, BwdPlan* out) {
+void (*adj_fn(int R, bool kreg))(BwdParams<T>, BwdLut) {
+  constexpr int RM = kRowsMax<T>;
+  if (R == RM) return kreg ? adj_kernel<T, RM, LOSS, true> : adj_kernel<T, RM, LOSS, false>;
+  return kreg ? adj_kernel<T, 1, LOSS, true> : adj_kernel<T, 1, LOSS, false>;
+}
+
+// Block size, rows per thread and shared memory for a tape of M operator slots: the shape
+// with the most resident threads per SM.
+template <typename T, bool LOSS>
+ws_status backward_shape(int64_t M, int64_t K, int64_t V, BwdPlan* out, int* per_sm_out) {
   const DeviceInfo& dev = device_info();
   const size_t budget = dev.smem_optin < (size_t)200 * 1024 ? dev.smem_optin : 200 * 1024;
-  int threads = 128;
-  while (threads > 32 && backward_smem<T, LOSS>(L, K, threads) > budget / 2) threads /= 2;
-  const size_t smem = backward_smem<T, LOSS>(L, K, threads);
-  if (smem > budget)
-    return fail("backward: " + std::to_string(K) + " constants and " + std::to_string(L) +
-                " tokens need more shared memory than a block has");
-  auto kern = backward_kernel<T, LOSS>;
+  // R rows per thread while a 64-thread block's tape stays within 96 KB
+  const int64_t vs = V <= kStageMaxVars ? V : 0;
+  const int R = (size_t)(M + vs) * 64 * kRowsMax<T> * sizeof(T) <= (size_t)96 * 1024
+                    ? kRowsMax<T> : 1;
+  const bool kreg = K <= kRegSlots;
+  auto kern = adj_fn<T, LOSS>(R, kreg);
+  int best_threads = 0, best_per_sm = 0;
+  for (int threads = 128; threads >= 32; threads /= 2) {
+    const size_t smem = backward_smem<T>(M, K, V, threads, R);
+    if (smem > budget) continue;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
+    if (per_sm * threads > best_per_sm * best_threads) {
+      best_threads = threads;
+      best_per_sm = per_sm;
+    }
+  }
+  if (best_threads == 0 || best_per_sm < 1)
+    return fail("backward: " + std::to_string(K) + " constants and " + std::to_string(M) +
+                " operators need more shared memory than a block has");
+  const size_t smem = backward_smem<T>(M, K, V, best_threads, R);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
+  out->threads = best_threads;
+  out->R = R;
+  out->smem = smem;
+  *per_sm_out = best_per_sm;
+  return WS_OK;
+}
+
+// Rows are split into ranges only when there are too few programs to fill the GPU; ranges are
+// multiples of 512 rows (a whole number of row groups of every block shape).  The split depends
+// on (B, L, K, V, D) and the device alone.
+template <typename T, bool LOSS>
+ws_status backward_plan(int64_t B, int64_t L, int64_t D, int64_t K, int64_t V,
+                        BwdPlan* out) {
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
-  if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
-  if (per_sm < 1) return fail("backward kernel cannot be resident");
-  const int64_t slots = (int64_t)dev.sm_count * per_sm;
+  ws_status st = backward_shape<T, LOSS>(L, K, V, out, &per_sm);
+  if (st != WS_OK) return st;
+  const int64_t slots = (int64_t)device_info().sm_count * per_sm;
+  const int64_t group = 512;
   int64_t n_splits = (2 * slots + B - 1) / B;
-  const int64_t max_splits = (D + threads - 1) / threads;
+  const int64_t max_splits = (D + group - 1) / group;
   if (n_splits > max_splits) n_splits = max_splits;
   if (n_splits < 1) n_splits = 1;
   int64_t rows = (D + n_splits - 1) / n_splits;
-  rows = (rows + threads - 1) / threads * threads;
+  rows = (rows + group - 1) / group * group;
   n_splits = (D + rows - 1) / rows;
-  out->threads = threads;
-  out->smem = smem;
   out->n_splits = n_splits;
   out->rows = rows;
   const int64_t n_items = B * n_splits;
@@ -546,7 +867,8 @@ ws_status backward_plan(int64_t B, int64_t L, int64_t D, int64_t K, BwdPlan* out
 }
 
 template <typename T, bool LOSS>
-BwdParams<T> backward_params(const uint8_t* pop, int64_t B, int64_t L, const void* x, int64_t D,
+BwdParams<T> backward_params(const uint8_t* pop, int64_t B, int64_t L, const void* x, int64_t V,
+                             int64_t D,
                              const void* consts, int64_t K, const BwdPlan& plan) {
   BwdParams<T> prm;
   prm.pop = pop;
@@ -562,6 +884,11 @@ BwdParams<T> backward_params(const uint8_t* pop, int64_t B, int64_t L, const voi
   prm.rows_per_split = plan.rows;
   prm.n_items = B * plan.n_splits;
   prm.tape_stride = plan.threads;
+  prm.V = V;
+  prm.stage_x = V <= kStageMaxVars ? 1 : 0;
+  prm.tape_ops = (int)L;
+  prm.list = nullptr;
+  prm.list_count = nullptr;
   prm.y = nullptr;
   prm.active = nullptr;
   prm.part_loss = nullptr;
@@ -571,15 +898,17 @@ BwdParams<T> backward_params(const uint8_t* pop, int64_t B, int64_t L, const voi
 
 template <typename T>
 ws_status launch_backward_typed(const uint8_t* pop, int64_t B, int64_t L, const void* x,
-                                int64_t D, const void* consts, int64_t K, const void* gout,
+                                int64_t V, int64_t D, const void* consts, int64_t K,
+                                const void* gout,
                                 void* grad, const BwdLut& lut, cudaStream_t stream) {
   BwdPlan plan;
-  ws_status st = backward_plan<T, false>(B, L, D, K, &plan);
+  ws_status st = backward_plan<T, false>(B, L, D, K, V, &plan);
   if (st != WS_OK) return st;
-  BwdParams<T> prm = backward_params<T, false>(pop, B, L, x, D, consts, K, plan);
+  BwdParams<T> prm = backward_params<T, false>(pop, B, L, x, V, D, consts, K, plan);
   prm.gout = static_cast<const T*>(gout);
   prm.grad = static_cast<T*>(grad);
-  backward_kernel<T, false><<<(unsigned)plan.grid, plan.threads, plan.smem, stream>>>(prm, lut);
+  adj_fn<T, false>(plan.R, K <= kRegSlots)<<<(unsigned)plan.grid, plan.threads, plan.smem,
+                                              stream>>>(prm, lut);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? WS_OK : fail_cuda(e, "eval_rpn_backward");
 }
@@ -593,21 +922,53 @@ template <typename T>
 ws_status launch_loss_grad(const uint8_t* pop, int64_t B, int64_t L, const void* x, int64_t D,
                            const void* consts, int64_t K, const void* y, const int32_t* active,
                            const ws_token_map& ids, int64_t num_vars, double* part_loss,
-                           double* part_grad, double* loss, void* grad, int64_t* n_splits_out,
-                           cudaStream_t stream) {
+                           double* part_grad, double* loss, void* grad, int32_t* buckets,
+                           int64_t* n_splits_out, cudaStream_t stream) {
   BwdPlan plan;
-  ws_status st = backward_plan<T, true>(B, L, D, K, &plan);
+  ws_status st = backward_plan<T, true>(B, L, D, K, num_vars, &plan);
   if (st != WS_OK) return st;
   if (n_splits_out) *n_splits_out = plan.n_splits;
   if (!part_loss) return WS_OK;  // plan query only
   const BwdLut lut = build_bwd_lut(ids, num_vars);
-  BwdParams<T> prm = backward_params<T, true>(pop, B, L, x, D, consts, K, plan);
+  BwdParams<T> prm = backward_params<T, true>(pop, B, L, x, num_vars, D, consts, K, plan);
   prm.y = static_cast<const T*>(y);
   prm.active = active;
   prm.part_loss = part_loss;
   prm.part_grad = part_grad;
-  backward_kernel<T, true><<<(unsigned)plan.grid, plan.threads, plan.smem, stream>>>(prm, lut);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e;
+  if (!buckets) {
+    adj_fn<T, true>(plan.R, K <= kRegSlots)<<<(unsigned)plan.grid, plan.threads, plan.smem,
+                                               stream>>>(prm, lut);
+  } else {
+    // buckets[0..15]: counts; buckets + 16: lists [n_buckets, B]
+    int nb = 0;
+    while (nb < kMaxBuckets && (nb == 0 || kBucketOps[nb - 1] < L - 1)) ++nb;
+    int32_t* counts = buckets;
+    int32_t* lists = buckets + 16;
+    e = cudaMemsetAsync(counts, 0, 16 * sizeof(int32_t), stream);
+    if (e != cudaSuccess) return fail_cuda(e, "loss_grad");
+    const int64_t cb = (B + 255) / 256;
+    bucket_kernel<<<(unsigned)(cb < 2048 ? cb : 2048), 256, 0, stream>>>(pop, B, L, lut, active,
+                                                                         nb, counts, lists);
+    for (int j = 0; j < nb; ++j) {
+      const int64_t M = kBucketOps[j] < L ? kBucketOps[j] : L;
+      BwdPlan pj;
+      int per_sm = 0;
+      st = backward_shape<T, true>(M, K, num_vars, &pj, &per_sm);
+      if (st != WS_OK) return st;
+      BwdParams<T> q = prm;
+      q.tape_stride = pj.threads;
+      q.tape_ops = (int)M;
+      q.list = lists + (int64_t)j * B;
+      q.list_count = counts + j;
+      const int64_t slots = (int64_t)device_info().sm_count * per_sm;
+      const int64_t items = B * plan.n_splits;
+      const int64_t grid = items < slots ? items : slots;
+      adj_fn<T, true>(pj.R, K <= kRegSlots)<<<(unsigned)grid, pj.threads, pj.smem, stream>>>(
+          q, lut);
+    }
+  }
+  e = cudaGetLastError();
   if (e != cudaSuccess) return fail_cuda(e, "loss_grad");
   if (loss) {
     const int64_t blocks = (B + 255) / 256;
@@ -619,14 +980,21 @@ ws_status launch_loss_grad(const uint8_t* pop, int64_t B, int64_t L, const void*
   return WS_OK;
 }
 
+// Device scratch of the operator-count buckets of launch_loss_grad (counts and program lists).
+size_t loss_grad_bucket_bytes(int64_t B) {
+  return (size_t)(16 + (int64_t)kMaxBuckets * B) * sizeof(int32_t);
+}
+
 template ws_status launch_loss_grad<float>(const uint8_t*, int64_t, int64_t, const void*,
                                            int64_t, const void*, int64_t, const void*,
                                            const int32_t*, const ws_token_map&, int64_t, double*,
-                                           double*, double*, void*, int64_t*, cudaStream_t);
+                                           double*, double*, void*, int32_t*, int64_t*,
+                                           cudaStream_t);
 template ws_status launch_loss_grad<double>(const uint8_t*, int64_t, int64_t, const void*,
                                             int64_t, const void*, int64_t, const void*,
                                             const int32_t*, const ws_token_map&, int64_t, double*,
-                                            double*, double*, void*, int64_t*, cudaStream_t);
+                                            double*, double*, void*, int32_t*, int64_t*,
+                                            cudaStream_t);
 }  // namespace ws
 
 extern "C" ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* population, int64_t B,
@@ -648,9 +1016,11 @@ extern "C" ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* populati
   const BwdLut lut = build_bwd_lut(*ids, num_vars);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (dtype == WS_F32)
-    return launch_backward_typed<float>(population, B, L, x, D, constants, K, grad_output,
+    return launch_backward_typed<float>(population, B, L, x, num_vars, D, constants, K,
+                                        grad_output,
                                         grad_constants, lut, s);
-  return launch_backward_typed<double>(population, B, L, x, D, constants, K, grad_output,
+  return launch_backward_typed<double>(population, B, L, x, num_vars, D, constants, K,
+                                       grad_output,
                                        grad_constants, lut, s);
 }
 
@@ -667,11 +1037,12 @@ ws_status loss_grad_check(int32_t dtype, int64_t B, int64_t L, int64_t D, int64_
 }
 }  // namespace
 
-extern "C" ws_status ws_loss_grad_workspace_bytes(int32_t dtype, int64_t B, int64_t L, int64_t D,
-                                                  int64_t K, size_t* bytes) {
+extern "C" ws_status ws_loss_grad_workspace_bytes(int32_t dtype, int64_t B, int64_t L,
+                                                  int64_t num_vars, int64_t D, int64_t K,
+                                                  size_t* bytes) {
   using namespace ws;
   clear_error();
-  ws_status st = loss_grad_check(dtype, B, L, D, K, 0);
+  ws_status st = loss_grad_check(dtype, B, L, D, K, num_vars);
   if (st != WS_OK) return st;
   if (!bytes) return fail("null output pointer");
   *bytes = 0;
@@ -679,13 +1050,14 @@ extern "C" ws_status ws_loss_grad_workspace_bytes(int32_t dtype, int64_t B, int6
   int64_t n_splits = 1;
   st = dtype == WS_F32
            ? launch_loss_grad<float>(nullptr, B, L, nullptr, D, nullptr, K, nullptr, nullptr,
-                                     ws_token_map{}, 0, nullptr, nullptr, nullptr, nullptr,
-                                     &n_splits, nullptr)
+                                     ws_token_map{}, num_vars, nullptr, nullptr, nullptr,
+                                     nullptr, nullptr, &n_splits, nullptr)
            : launch_loss_grad<double>(nullptr, B, L, nullptr, D, nullptr, K, nullptr, nullptr,
-                                      ws_token_map{}, 0, nullptr, nullptr, nullptr, nullptr,
-                                      &n_splits, nullptr);
+                                      ws_token_map{}, num_vars, nullptr, nullptr, nullptr,
+                                      nullptr, nullptr, &n_splits, nullptr);
   if (st != WS_OK) return st;
-  *bytes = (size_t)(B * n_splits) * (size_t)(K + 1) * sizeof(double) + 256;
+  *bytes = (size_t)(B * n_splits) * (size_t)(K + 1) * sizeof(double) + 256 +
+           loss_grad_bucket_bytes(B);
   return WS_OK;
 }
 
@@ -706,7 +1078,7 @@ extern "C" ws_status ws_loss_grad(int32_t dtype, const uint8_t* population, int6
       (num_vars > 0 && !x) || !workspace)
     return fail("null tensor pointer");
   size_t need = 0;
-  st = ws_loss_grad_workspace_bytes(dtype, B, L, D, K, &need);
+  st = ws_loss_grad_workspace_bytes(dtype, B, L, num_vars, D, K, &need);
   if (st != WS_OK) return st;
   if (workspace_bytes < need) return fail("loss_grad workspace too small");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -714,16 +1086,19 @@ extern "C" ws_status ws_loss_grad(int32_t dtype, const uint8_t* population, int6
   int64_t n_splits = 1;
   st = dtype == WS_F32
            ? launch_loss_grad<float>(nullptr, B, L, nullptr, D, nullptr, K, nullptr, nullptr,
-                                     *ids, 0, nullptr, nullptr, nullptr, nullptr, &n_splits,
-                                     nullptr)
+                                     *ids, num_vars, nullptr, nullptr, nullptr, nullptr,
+                                     nullptr, &n_splits, nullptr)
            : launch_loss_grad<double>(nullptr, B, L, nullptr, D, nullptr, K, nullptr, nullptr,
-                                      *ids, 0, nullptr, nullptr, nullptr, nullptr, &n_splits,
-                                      nullptr);
+                                      *ids, num_vars, nullptr, nullptr, nullptr, nullptr,
+                                      nullptr, &n_splits, nullptr);
   if (st != WS_OK) return st;
   double* part_grad = part_loss + B * n_splits;
+  int32_t* buckets = reinterpret_cast<int32_t*>(part_grad + B * n_splits * K);
   if (dtype == WS_F32)
     return launch_loss_grad<float>(population, B, L, x, D, constants, K, y, active, *ids,
-                                   num_vars, part_loss, part_grad, out_loss, out_grad, nullptr, s);
+                                   num_vars, part_loss, part_grad, out_loss, out_grad, buckets,
+                                   nullptr, s);
   return launch_loss_grad<double>(population, B, L, x, D, constants, K, y, active, *ids,
-                                  num_vars, part_loss, part_grad, out_loss, out_grad, nullptr, s);
+                                  num_vars, part_loss, part_grad, out_loss, out_grad, buckets,
+                                  nullptr, s);
 }

@@ -103,7 +103,10 @@ template <typename T>
 ws_status launch_loss_grad(const uint8_t* pop, int64_t B, int64_t L, const void* x, int64_t D,
                            const void* consts, int64_t K, const void* y, const int32_t* active,
                            const ws_token_map& ids, int64_t num_vars, double* part_loss,
-                           double* part_grad, double* loss, void* grad, int64_t* n_splits_out,
-                           cudaStream_t stream);
+                           double* part_grad, double* loss, void* grad, int32_t* buckets,
+                           int64_t* n_splits_out, cudaStream_t stream);
+// Bytes of the `buckets` scratch of launch_loss_grad (programs grouped by operator count, each
+// group launched with a tape sized for it); null buckets: one launch sized for L.
+size_t loss_grad_bucket_bytes(int64_t B);
 
 }  // namespace ws

@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(128) lbfgs_state_kernel(LbbArgs<T> a, int mode
 }
 
 struct LbbLayout {
-  size_t state, ro, vec, trial, active, count, part_loss, part_grad, total;
+  size_t state, ro, vec, trial, active, count, part_loss, part_grad, buckets, total;
 };
 
 size_t al256(size_t v) { return (v + 255) / 256 * 256; }
@@ -391,6 +391,7 @@ LbbLayout lbb_layout(int64_t B, int64_t K, int m, int64_t n_splits, size_t tsize
   l.count = o; o = al256(o + 16);
   l.part_loss = o; o = al256(o + (size_t)B * n_splits * sizeof(double));
   l.part_grad = o; o = al256(o + (size_t)B * n_splits * K * sizeof(double));
+  l.buckets = o; o = al256(o + loss_grad_bucket_bytes(B));
   l.total = o;
   return l;
 }
@@ -403,8 +404,8 @@ ws_status lbfgs_batch_typed(const uint8_t* pop, int64_t B, int64_t L, const void
                             cudaStream_t stream) {
   int64_t n_splits = 1;
   ws_status st = launch_loss_grad<T>(nullptr, B, L, nullptr, D, nullptr, K, nullptr, nullptr,
-                                     ids, num_vars, nullptr, nullptr, nullptr, nullptr, &n_splits,
-                                     nullptr);
+                                     ids, num_vars, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                     &n_splits, nullptr);
   if (st != WS_OK) return st;
   const LbbLayout lay = lbb_layout(B, K, o.history, n_splits, sizeof(T));
   if (workspace_bytes < lay.total) return fail("lbfgs workspace too small");
@@ -452,7 +453,8 @@ ws_status lbfgs_batch_typed(const uint8_t* pop, int64_t B, int64_t L, const void
   if ((st = state(0)) != WS_OK) return st;
   for (int64_t r = 0; r < rounds; ++r) {
     st = launch_loss_grad<T>(pop, B, L, x, D, a.trial, K, y, a.active, ids, num_vars, part_loss,
-                             part_grad, nullptr, nullptr, nullptr, stream);
+                             part_grad, nullptr, nullptr,
+                             reinterpret_cast<int32_t*>(w + lay.buckets), nullptr, stream);
     if (st != WS_OK) return st;
     if ((st = state(1)) != WS_OK) return st;
     if (o.sync_every > 0 && (r + 1) % o.sync_every == 0) {
@@ -471,13 +473,14 @@ ws_status lbfgs_batch_typed(const uint8_t* pop, int64_t B, int64_t L, const void
 }  // namespace ws
 
 extern "C" ws_status ws_lbfgs_adjoint_workspace_bytes(int32_t dtype, int64_t B, int64_t L,
-                                                      int64_t D, int64_t K, int32_t history,
-                                                      size_t* bytes) {
+                                                      int64_t num_vars, int64_t D, int64_t K,
+                                                      int32_t history, size_t* bytes) {
   using namespace ws;
   clear_error();
   if (dtype != WS_F32 && dtype != WS_F64) return fail("x must be float32 or float64");
   if (!bytes) return fail("null output pointer");
   if (B < 0 || L < 0 || D < 0 || K < 0) return fail("negative dimension");
+  if (num_vars < 0 || num_vars > 255) return fail("num_vars must be in [0, 255]");
   if (K > kLbbMaxK) return fail("lbfgs supports at most 32 constants per program");
   if (history < 1 || history > kLbbMaxHistory) return fail("history must be in [1, 32]");
   *bytes = 0;
@@ -487,11 +490,11 @@ extern "C" ws_status ws_lbfgs_adjoint_workspace_bytes(int32_t dtype, int64_t B, 
   ws_token_map none{};
   ws_status st = dtype == WS_F32
                      ? launch_loss_grad<float>(nullptr, B, L, nullptr, D, nullptr, K, nullptr,
-                                               nullptr, none, 0, nullptr, nullptr, nullptr,
-                                               nullptr, &n_splits, nullptr)
+                                               nullptr, none, num_vars, nullptr, nullptr,
+                                               nullptr, nullptr, nullptr, &n_splits, nullptr)
                      : launch_loss_grad<double>(nullptr, B, L, nullptr, D, nullptr, K, nullptr,
-                                                nullptr, none, 0, nullptr, nullptr, nullptr,
-                                                nullptr, &n_splits, nullptr);
+                                                nullptr, none, num_vars, nullptr, nullptr,
+                                                nullptr, nullptr, nullptr, &n_splits, nullptr);
   if (st != WS_OK) return st;
   *bytes = lbb_layout(B, K, history, n_splits, dtype == WS_F32 ? 4 : 8).total;
   return WS_OK;
@@ -510,10 +513,9 @@ extern "C" ws_status ws_lbfgs_adjoint(int32_t dtype, const uint8_t* population, 
   if (o.max_iter < 1 || o.max_eval < 1 || o.max_ls < 1) return fail("iteration limits must be positive");
   if (!(o.lr > 0.0)) return fail("lr must be positive");
   size_t need = 0;
-  ws_status st = ws_lbfgs_adjoint_workspace_bytes(dtype, B, L, D, K, o.history, &need);
+  ws_status st = ws_lbfgs_adjoint_workspace_bytes(dtype, B, L, num_vars, D, K, o.history, &need);
   if (st != WS_OK) return st;
   if (B == 0) return WS_OK;
-  if (num_vars < 0 || num_vars > 255) return fail("num_vars must be in [0, 255]");
   if (!population || !y || (K > 0 && !constants) || (num_vars > 0 && !x) || !workspace)
     return fail("null tensor pointer");
   if (workspace_bytes < need) return fail("lbfgs workspace too small");

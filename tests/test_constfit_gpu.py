@@ -61,7 +61,7 @@ def test_loss_grad_deterministic_active_and_invalid():
     loss = torch.full((64,), -7.0, dtype=torch.float64, device=DEV)
     grad = torch.full(consts.shape, -7.0, dtype=torch.float64, device=DEV)
     need = C.c_size_t(0)
-    N.check(N.lib().ws_loss_grad_workspace_bytes(N.WS_F64, 64, pop.shape[1], 4096,
+    N.check(N.lib().ws_loss_grad_workspace_bytes(N.WS_F64, 64, pop.shape[1], 3, 4096,
                                                  consts.shape[1], C.byref(need)))
     ws = workspace(need.value, DEV)
     m = tmap(g)
