@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
+#include <cmath>
 #include <type_traits>
 
 #include "ws_internal.h"
@@ -395,12 +396,14 @@ template <typename T, int R, bool LOSS, bool KREG>
 __global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int TS = p.tape_stride;
+  // shared memory: operators | touched flags | (K > kRegSlots) FP64 constant accumulators |
+  // work: the tape and staged x during the rows, the block reduction after them
   BOp* ops = reinterpret_cast<BOp*>(smem);
-  double* cacc = reinterpret_cast<double*>(smem + al16((size_t)kMaxL * sizeof(BOp)));
-  double* lacc_s = cacc + (size_t)p.K * TS;
-  int* touched = reinterpret_cast<int*>(lacc_s + TS);
-  T* tape = reinterpret_cast<T*>(
-      reinterpret_cast<unsigned char*>(touched) + al16((size_t)p.K * sizeof(int)));
+  int* touched = reinterpret_cast<int*>(smem + al16((size_t)p.tape_ops * sizeof(BOp)));
+  double* cacc = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(touched) +
+                                           al16((size_t)p.K * sizeof(int)));
+  unsigned char* work = reinterpret_cast<unsigned char*>(cacc + (KREG ? 0 : (size_t)p.K * TS));
+  T* tape = reinterpret_cast<T*>(work);
   T* xs = p.stage_x ? tape + (size_t)p.tape_ops * TS * R : nullptr;  // [V][thread][R]
   __shared__ BRoot s_root;
   __shared__ int64_t s_prog;
@@ -629,17 +632,20 @@ __global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
                                       tid, cr, cacc, touched);
       }
     }
+    __syncthreads();  // the tape is free: the reduction reuses its memory
+    double* cred = KREG ? reinterpret_cast<double*>(work) : cacc;
+    double* lacc_s = reinterpret_cast<double*>(work) + (KREG ? (size_t)p.K * TS : 0);
     if (KREG) {
 #pragma unroll
       for (int k = 0; k < kRegSlots; ++k)
-        if (k < p.K) cacc[(size_t)k * TS + tid] = (double)cr[k];
+        if (k < p.K) cred[(size_t)k * TS + tid] = (double)cr[k];
     }
     if (LOSS) lacc_s[tid] = lacc;
     __syncthreads();
     // fixed-order reduction over the block's threads, one thread per slot
     for (int64_t k = tid; k < p.K; k += blockDim.x) {
       double s = 0.0;
-      for (int t = 0; t < (int)blockDim.x; ++t) s += cacc[k * TS + t];
+      for (int t = 0; t < (int)blockDim.x; ++t) s += cred[k * TS + t];
       if (LOSS) {
         p.part_grad[slot * p.K + k] = s;
       } else if (touched[k]) {
@@ -774,11 +780,13 @@ BwdLut build_bwd_lut(const ws_token_map& m, int64_t num_vars) {
 constexpr int64_t kStageMaxVars = 16;  // x is staged in shared memory up to this many variables
 
 template <typename T>
-size_t backward_smem(int64_t L, int64_t K, int64_t V, int threads, int R) {
+size_t backward_smem(int64_t M, int64_t K, int64_t V, int threads, int R) {
   const int64_t vs = V <= kStageMaxVars ? V : 0;
-  return al16((size_t)kMaxL * sizeof(BOp)) + (size_t)K * threads * sizeof(double) +
-         (size_t)threads * sizeof(double) + al16((size_t)K * sizeof(int)) +
-         (size_t)(L + vs) * threads * R * sizeof(T);
+  const bool kreg = K <= kRegSlots;
+  const size_t tape = (size_t)(M + vs) * threads * R * sizeof(T);
+  const size_t red = (size_t)((kreg ? K : 0) + 1) * threads * sizeof(double);
+  return al16((size_t)M * sizeof(BOp)) + al16((size_t)K * sizeof(int)) +
+         (kreg ? 0 : (size_t)K * threads * sizeof(double)) + (tape > red ? tape : red);
 }
 
 // Block size, rows per thread, shared memory and the split of rows into ranges for one launch.
@@ -793,11 +801,18 @@ struct BwdPlan {
 template <typename T>
 constexpr int kRowsMax = sizeof(T) == 4 ? 4 : 2;
 
+template <typename T, bool LOSS, int RR>
+void (*adj_pick(bool kreg))(BwdParams<T>, BwdLut) {
+  return kreg ? adj_kernel<T, RR, LOSS, true> : adj_kernel<T, RR, LOSS, false>;
+}
+
 template <typename T, bool LOSS>
 void (*adj_fn(int R, bool kreg))(BwdParams<T>, BwdLut) {
-  constexpr int RM = kRowsMax<T>;
-  if (R == RM) return kreg ? adj_kernel<T, RM, LOSS, true> : adj_kernel<T, RM, LOSS, false>;
-  return kreg ? adj_kernel<T, 1, LOSS, true> : adj_kernel<T, 1, LOSS, false>;
+  if constexpr (kRowsMax<T> >= 4) {
+    if (R == 4) return adj_pick<T, LOSS, 4>(kreg);
+  }
+  if (R == 2) return adj_pick<T, LOSS, 2>(kreg);
+  return adj_pick<T, LOSS, 1>(kreg);
 }
 
 // Block size, rows per thread and shared memory for a tape of M operator slots: the shape
@@ -806,36 +821,44 @@ template <typename T, bool LOSS>
 ws_status backward_shape(int64_t M, int64_t K, int64_t V, BwdPlan* out, int* per_sm_out) {
   const DeviceInfo& dev = device_info();
   const size_t budget = dev.smem_optin < (size_t)200 * 1024 ? dev.smem_optin : 200 * 1024;
-  // R rows per thread while a 64-thread block's tape stays within 96 KB
-  const int64_t vs = V <= kStageMaxVars ? V : 0;
-  const int R = (size_t)(M + vs) * 64 * kRowsMax<T> * sizeof(T) <= (size_t)96 * 1024
-                    ? kRowsMax<T> : 1;
   const bool kreg = K <= kRegSlots;
-  auto kern = adj_fn<T, LOSS>(R, kreg);
-  int best_threads = 0, best_per_sm = 0;
-  for (int threads = 128; threads >= 32; threads /= 2) {
-    const size_t smem = backward_smem<T>(M, K, V, threads, R);
-    if (smem > budget) continue;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
-    if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
-    if (per_sm * threads > best_per_sm * best_threads) {
-      best_threads = threads;
-      best_per_sm = per_sm;
+  // every (rows per thread, block size) shape that fits, scored by the rows its resident warps
+  // carry, with warps counted up to 32 per SM (measured: 2 rows per thread at twice the warps
+  // is no faster than 4 rows per thread, so rows are weighted fully)
+  double best_score = -1.0;
+  int best_threads = 0, best_per_sm = 0, best_r = 1;
+  for (int R = kRowsMax<T>; R >= 1; R /= 2) {
+    auto kern = adj_fn<T, LOSS>(R, kreg);
+    for (int threads = 128; threads >= 32; threads /= 2) {
+      const size_t smem = backward_smem<T>(M, K, V, threads, R);
+      if (smem > budget) continue;
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+      if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
+      int per_sm = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+      if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
+      if (per_sm < 1) continue;
+      double warps = (double)per_sm * threads / 32.0;
+      if (warps > 32.0) warps = 32.0;
+      const double score = warps * (double)R;
+      if (score > best_score + 1e-9) {
+        best_score = score;
+        best_threads = threads;
+        best_per_sm = per_sm;
+        best_r = R;
+      }
     }
   }
-  if (best_threads == 0 || best_per_sm < 1)
+  if (best_threads == 0)
     return fail("backward: " + std::to_string(K) + " constants and " + std::to_string(M) +
                 " operators need more shared memory than a block has");
-  const size_t smem = backward_smem<T>(M, K, V, best_threads, R);
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  const size_t smem = backward_smem<T>(M, K, V, best_threads, best_r);
+  cudaError_t e = cudaFuncSetAttribute(adj_fn<T, LOSS>(best_r, kreg),
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
   out->threads = best_threads;
-  out->R = R;
+  out->R = best_r;
   out->smem = smem;
   *per_sm_out = best_per_sm;
   return WS_OK;
