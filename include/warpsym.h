@@ -419,6 +419,69 @@ ws_status ws_lbfgs_adjoint(int32_t dtype, const uint8_t* population, int64_t B, 
                            size_t workspace_bytes, void* stream);
 
 /* ----------------------------------------------------------------------------------------------
+ * Device steps of one `evolve_generation` call (bindings.cpp:474 -> rpn_kernels.cu:1810-2237).
+ * The host sequence -- the torch random draws in the reference's order and the torch glue between
+ * the steps -- is rpn_cuda_native.evolve_generation; every step below gives the reference
+ * kernel's bytes / floats for the same inputs.  Row-index arrays (int64, device) may be NULL for
+ * the identity; uint8 masks are torch bool tensors.
+ *
+ * ws_subtree_pick replaces select_subtree_range_indirect_kernel (rpn_kernels.cu:597-640): for row
+ *   rows[n], len = tokens before PAD (>= 1), end = (int)(u[n] * len) clamped to [0, len),
+ *   start = where the arity balance from `end` back closes (end itself for a terminal).
+ * ws_splice_valid replaces validate_crossover_lengths_kernel (:642-679) followed by the
+ *   reference's logical_and_ with the candidate mask (NULL = all candidates).
+ * ws_splice_rows replaces crossover_splicing_mutation_kernel (:1020-1105) when `mutation` is
+ *   given and crossover_splicing_kernel (:927-1016) when it is NULL: child rows c1_rows[n] /
+ *   c2_rows[n] get p1[0:s1] + p2[s2:e2+1] + p1[e1+1:] and its mirror image (PAD past a source
+ *   row), or their parents where cx_mask is 0; then, with a mutation, a child row r != 0 whose
+ *   individual_rand[r] < cut has each token point-mutated (Philox4x32-10, see ws_evolve.cu).
+ * ws_mutate_rows replaces mutation_philox_indirect_kernel (:747-770).
+ * ws_sbx_constants replaces sbx_constants_kernel (:1225-1261); float32 constants.
+ * ws_splice_constants replaces crossover_constants_kernel (:1107-1223); float32 constants.
+ * ws_hoist_rows replaces hoist_mutation_indirect_kernel (:1363-1411).
+ */
+typedef struct ws_point_mutation {
+  const int32_t* arities;  /* [vocab] token arities (device) */
+  int32_t vocab;
+  int32_t n0, n1, n2;      /* sizes of the same-arity replacement lists */
+  const uint8_t* ids0;     /* [n0] / [n1] / [n2] replacement tokens (device) */
+  const uint8_t* ids1;
+  const uint8_t* ids2;
+  float rate;              /* per-token mutation probability */
+  int32_t reserved;
+  uint64_t seed, generation;
+} ws_point_mutation;
+ws_status ws_subtree_pick(const uint8_t* population, const int64_t* rows, int64_t N, int64_t L,
+                          const int32_t* arities, int32_t vocab, const float* u, int64_t* out_len,
+                          int64_t* out_start, int64_t* out_end, int32_t pad_id, void* stream);
+ws_status ws_splice_valid(const int64_t* len1, const int64_t* len2, const int64_t* s1,
+                          const int64_t* e1, const int64_t* s2, const int64_t* e2,
+                          const uint8_t* candidate, uint8_t* valid, int64_t N, int64_t L,
+                          void* stream);
+ws_status ws_splice_rows(const uint8_t* parent1, const uint8_t* parent2, const int64_t* p1_rows,
+                         const int64_t* p2_rows, const int64_t* c1_rows, const int64_t* c2_rows,
+                         const int64_t* s1, const int64_t* e1, const int64_t* s2,
+                         const int64_t* e2, const uint8_t* cx_mask, uint8_t* child1,
+                         uint8_t* child2, int64_t N, int64_t L, int32_t pad_id,
+                         const float* individual_rand, float cut,
+                         const ws_point_mutation* mutation, void* stream);
+ws_status ws_mutate_rows(uint8_t* population, const int64_t* rows, int64_t N, int64_t L,
+                         const float* individual_rand, float cut,
+                         const ws_point_mutation* mutation, int32_t pad_id, void* stream);
+ws_status ws_sbx_constants(const float* constants, const int64_t* p1_rows, const int64_t* p2_rows,
+                           const float* u_sbx, const float* mask_rand, float* out1, float* out2,
+                           int64_t n_pairs, int64_t K, float eta, void* stream);
+ws_status ws_splice_constants(const uint8_t* population, const int64_t* p1_rows,
+                              const int64_t* p2_rows, const float* consts1, const float* consts2,
+                              const int64_t* s1, const int64_t* e1, const int64_t* s2,
+                              const int64_t* e2, const uint8_t* cx_mask, float* child_consts,
+                              const int64_t* c1_rows, const int64_t* c2_rows, int64_t N,
+                              int64_t L, int64_t K, int32_t id_C, void* stream);
+ws_status ws_hoist_rows(uint8_t* population, const int64_t* rows, int64_t N, int64_t L,
+                        const int32_t* arities, int32_t vocab, const int64_t* rand_ints,
+                        int32_t pad_id, void* stream);
+
+/* ----------------------------------------------------------------------------------------------
  * Particle-swarm constant fitting.
  */
 

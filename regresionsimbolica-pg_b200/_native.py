@@ -100,6 +100,14 @@ class LbfgsOpts(C.Structure):
                 ("sync_every", C.c_int32), ("reserved", C.c_int32)]
 
 
+class PointMutation(C.Structure):
+    """ws_point_mutation: the Philox point mutation of evolve_generation (device pointers)."""
+    _fields_ = [("arities", C.c_void_p), ("vocab", C.c_int32), ("n0", C.c_int32),
+                ("n1", C.c_int32), ("n2", C.c_int32), ("ids0", C.c_void_p), ("ids1", C.c_void_p),
+                ("ids2", C.c_void_p), ("rate", C.c_float), ("reserved", C.c_int32),
+                ("seed", C.c_uint64), ("generation", C.c_uint64)]
+
+
 _P = C.c_void_p
 _I64 = C.c_int64
 _I32 = C.c_int32
@@ -150,6 +158,16 @@ _SIGS = {
     "ws_sharing_table_slots": (_I64, []),
     "ws_eval_rpn_backward": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
                                     C.POINTER(TokenMap), _P]),
+    "ws_subtree_pick": (_I32, [_P, _P, _I64, _I64, _P, _I32, _P, _P, _P, _P, _I32, _P]),
+    "ws_splice_valid": (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _I64, _I64, _P]),
+    "ws_splice_rows": (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I64,
+                              _I32, _P, C.c_float, C.POINTER(PointMutation), _P]),
+    "ws_mutate_rows": (_I32, [_P, _P, _I64, _I64, _P, C.c_float, C.POINTER(PointMutation), _I32,
+                              _P]),
+    "ws_sbx_constants": (_I32, [_P, _P, _P, _P, _P, _P, _P, _I64, _I64, C.c_float, _P]),
+    "ws_splice_constants": (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64,
+                                   _I64, _I64, _I32, _P]),
+    "ws_hoist_rows": (_I32, [_P, _P, _I64, _I64, _P, _I32, _P, _I32, _P]),
     "ws_loss_grad_workspace_bytes": (_I32, [_I32, _I64, _I64, _I64, _I64, _I64,
                                             C.POINTER(C.c_size_t)]),
     "ws_loss_grad": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P, _P, _P,

@@ -617,3 +617,228 @@ def fitness_sharing_penalty(population, n_islands, island_size, threshold, hash_
                                                ptr(keys), ptr(counts), ptr(out),
                                                stream_of(population)))
     return out
+
+
+def _f32(v) -> float:
+    """A Python number as the float32 the reference's pybind `float` parameters receive."""
+    import numpy as np
+    return float(np.float32(v))
+
+
+def evolve_generation(population, constants, fitness, abs_errors, X, Y_target, lengths,
+                      token_arities, arity_0_ids, arity_1_ids, arity_2_ids, mutation_bank,
+                      mad_eps, mutation_rate, crossover_rate, tournament_size, pso_steps,
+                      pso_particles, pso_w, pso_c1, pso_c2, PAD_ID,
+                      id_x_start, id_C, id_pi, id_e,
+                      id_0, id_1, id_2, id_3, id_4, id_5, id_6, id_10,
+                      op_add, op_sub, op_mul, op_div, op_pow, op_mod,
+                      op_sin, op_cos, op_tan, op_log, op_exp,
+                      op_sqrt, op_abs, op_neg,
+                      op_fact, op_floor, op_ceil, op_sign,
+                      op_gamma, op_lgamma, op_asin, op_acos, op_atan,
+                      pi_val, e_val, n_islands=1, cached_p1_src=None, cached_p2_src=None,
+                      cached_copy_src=None, cached_island_base=None, rng_seed=0, generation=0):
+    """One generation (bindings.cpp:474 -> rpn_kernels.cu:1810-2237): island tournament with
+    elitism at index 0, subtree crossover of fixed parent pairs with fused point mutation, copies
+    for the unpaired, SBX of constants and their transfer along the spliced `C` tokens,
+    structural (bank) and hoist mutation, then `pso_steps` PSO steps over `pso_particles`
+    particles.  Returns [population, constants, fitness] (fitness empty without PSO).
+
+    The random draws are torch's, on the current CUDA generator, with the reference's shapes and
+    order, and every device step gives the reference kernel's bytes / floats, so the same seed
+    gives the same generation.  `cached_island_base` is accepted and unused, as in the
+    reference."""
+    from warpsymbolic_b200._native import PointMutation
+    for t, nm in ((population, "population"), (constants, "constants"), (fitness, "fitness"),
+                  (X, "X"), (Y_target, "Y_target"), (token_arities, "token_arities")):
+        check_cuda(t, nm)
+    _expect(population, "population", torch.uint8)
+    _expect(constants, "constants", torch.float32)
+    _expect(token_arities, "token_arities", torch.int32)
+    for t, nm in ((arity_0_ids, "arity_0_ids"), (arity_1_ids, "arity_1_ids"),
+                  (arity_2_ids, "arity_2_ids")):
+        if t.numel() > 0:
+            check_cuda(t, nm)
+            _expect(t, nm, torch.uint8)
+    dev = population.device
+    B, L = int(population.size(0)), int(population.size(1))
+    K = int(constants.size(1))
+    n_data = int(X.size(1))
+    T = int(tournament_size)
+    vocab = int(token_arities.numel())
+    lib = N.lib()
+    st = stream_of(population)
+    i32 = dict(dtype=torch.int32, device=dev)
+    i64 = dict(dtype=torch.int64, device=dev)
+    f32 = dict(dtype=torch.float32, device=dev)
+    mutation_rate, crossover_rate = _f32(mutation_rate), _f32(crossover_rate)
+
+    # 1. selection
+    sel_size = max(1, B // n_islands) if n_islands > 1 else B
+    rand_offsets = torch.randint(0, sel_size, (B, T), **i32)
+    winner = torch.empty(B, **i64)
+    has_err = abs_errors is not None and abs_errors.numel() > 0
+    rand_cases = torch.randint(0, n_data, (B,), **i32) if has_err else torch.empty(0, **i32)
+    fit32 = fitness if fitness.dtype == torch.float32 else fitness.to(torch.float32)
+    err32 = (abs_errors if abs_errors.dtype == torch.float32 else abs_errors.to(torch.float32)) \
+        if has_err else None
+    len32 = lengths if (lengths is None or lengths.numel() == 0
+                        or lengths.dtype == torch.float32) else lengths.to(torch.float32)
+    mad32 = mad_eps if (mad_eps is None or mad_eps.numel() == 0
+                        or mad_eps.dtype == torch.float32) else mad_eps.to(torch.float32)
+    fit32, rand_offsets = fit32.contiguous(), rand_offsets.contiguous()
+    err32 = err32.contiguous() if err32 is not None else None
+    len32 = _optional(len32.contiguous()) if len32 is not None else None
+    mad32 = _optional(mad32.contiguous()) if mad32 is not None else None
+    N.check(lib.ws_tournament_select_offsets(ptr(fit32), B, ptr(err32),
+                                             n_data if has_err else 0, ptr(rand_offsets), T,
+                                             ptr(rand_cases if has_err else None), ptr(len32),
+                                             ptr(mad32), sel_size, int(n_islands), ptr(winner),
+                                             st))
+    winner[0] = torch.argmin(fit32)
+
+    # 2. crossover pairs inside islands (slot 0 holds the elite)
+    island_size = B // n_islands
+    if (cached_p1_src is not None and cached_p2_src is not None and cached_copy_src is not None
+            and cached_p1_src.numel() == cached_p2_src.numel() and cached_copy_src.numel() > 0):
+        p1_src, p2_src, copy_src = cached_p1_src, cached_p2_src, cached_copy_src
+    else:
+        p1_parts, p2_parts, copy_parts = [], [], [torch.zeros(1, **i64)]
+        for k in range(n_islands):
+            start, end = k * island_size, (k + 1) * island_size
+            avail_start = start + 1 if k == 0 else start
+            avail_len = end - avail_start
+            pairs = int(avail_len / 2)  # C++ integer division
+            if pairs > 0:
+                p1 = torch.arange(avail_start, avail_start + 2 * pairs, 2, **i64)
+                p1_parts.append(p1)
+                p2_parts.append(p1 + 1)
+            if avail_len % 2 != 0:
+                copy_parts.append(torch.full((1,), end - 1, **i64))
+        p1_src = torch.cat(p1_parts).contiguous() if p1_parts else torch.empty(0, **i64)
+        p2_src = torch.cat(p2_parts).contiguous() if p2_parts else torch.empty(0, **i64)
+        copy_src = torch.cat(copy_parts).contiguous()
+    n_pairs = int(p1_src.size(0))
+    p1_w = winner.index_select(0, p1_src)
+    p2_w = winner.index_select(0, p2_src)
+    copy_w = winner.index_select(0, copy_src)
+    cx_prob = torch.rand(n_pairs, **f32)
+    cx_candidate = cx_prob < crossover_rate
+    len1, len2 = torch.empty(n_pairs, **i64), torch.empty(n_pairs, **i64)
+    rand_e1 = torch.rand(n_pairs, **f32)
+    rand_e2 = torch.rand(n_pairs, **f32)
+    s1, e1 = torch.empty(n_pairs, **i64), torch.empty(n_pairs, **i64)
+    s2, e2 = torch.empty(n_pairs, **i64), torch.empty(n_pairs, **i64)
+    N.check(lib.ws_subtree_pick(ptr(population), ptr(p1_w), n_pairs, L, ptr(token_arities),
+                                vocab, ptr(rand_e1), ptr(len1), ptr(s1), ptr(e1), int(PAD_ID), st))
+    N.check(lib.ws_subtree_pick(ptr(population), ptr(p2_w), n_pairs, L, ptr(token_arities),
+                                vocab, ptr(rand_e2), ptr(len2), ptr(s2), ptr(e2), int(PAD_ID), st))
+    cx_mask = torch.empty(n_pairs, dtype=torch.bool, device=dev)
+    N.check(lib.ws_splice_valid(ptr(len1), ptr(len2), ptr(s1), ptr(e1), ptr(s2), ptr(e2),
+                                ptr(cx_candidate), ptr(cx_mask), n_pairs, L, st))
+    u_sbx = torch.rand(n_pairs, K, **f32)
+    mask_sbx = torch.rand(n_pairs, K, **f32)
+    mut_rand = torch.rand(B, **f32)
+    has_bank = mutation_bank is not None and mutation_bank.numel() > 0
+    point_cut = _f32(0.5 if has_bank else 0.8)
+    mut = PointMutation(ptr(token_arities).value, vocab, int(arity_0_ids.numel()),
+                        int(arity_1_ids.numel()), int(arity_2_ids.numel()),
+                        ptr(arity_0_ids).value, ptr(arity_1_ids).value, ptr(arity_2_ids).value,
+                        mutation_rate, 0, int(rng_seed) & 0xFFFFFFFFFFFFFFFF,
+                        int(generation) & 0xFFFFFFFFFFFFFFFF)
+    offspring = torch.empty_like(population)
+    N.check(lib.ws_splice_rows(ptr(population), ptr(population), ptr(p1_w), ptr(p2_w),
+                               ptr(p1_src), ptr(p2_src), ptr(s1), ptr(e1), ptr(s2), ptr(e2),
+                               ptr(cx_mask), ptr(offspring), ptr(offspring), n_pairs, L,
+                               int(PAD_ID), ptr(mut_rand), point_cut, C.byref(mut), st))
+    offspring.index_copy_(0, copy_src, population.index_select(0, copy_w))
+    N.check(lib.ws_mutate_rows(ptr(offspring), ptr(copy_src), int(copy_src.numel()), L,
+                               ptr(mut_rand), point_cut, C.byref(mut), int(PAD_ID), st))
+    consts1 = torch.empty(n_pairs, K, **f32)
+    consts2 = torch.empty(n_pairs, K, **f32)
+    N.check(lib.ws_sbx_constants(ptr(constants), ptr(p1_w), ptr(p2_w), ptr(u_sbx), ptr(mask_sbx),
+                                 ptr(consts1), ptr(consts2), n_pairs, K, 2.0, st))
+    offspring_consts = torch.empty_like(constants)
+    N.check(lib.ws_splice_constants(ptr(population), ptr(p1_w), ptr(p2_w), ptr(consts1),
+                                    ptr(consts2), ptr(s1), ptr(e1), ptr(s2), ptr(e2),
+                                    ptr(cx_mask), ptr(offspring_consts), ptr(p1_src),
+                                    ptr(p2_src), n_pairs, L, K, int(id_C), st))
+    offspring_consts.index_copy_(0, copy_src, constants.index_select(0, copy_w))
+
+    # 3. structural and hoist mutation (never the elite)
+    import numpy as np
+    mr = np.float32(mutation_rate)
+    hoist_cut = float(np.float32(0.8) + np.float32(0.2) * mr)
+    hoist_mask = (mut_rand >= 0.8) & (mut_rand < hoist_cut)
+    if has_bank:
+        struct_cut = float(np.float32(0.5) + np.float32(0.3) * mr)
+        struct_mask = (mut_rand >= 0.5) & (mut_rand < struct_cut)
+        struct_mask[0] = False
+    hoist_mask[0] = False
+    if has_bank:
+        check_cuda(mutation_bank, "mutation_bank")
+        _expect(mutation_bank, "mutation_bank", torch.uint8)
+        struct_idx = torch.nonzero(struct_mask).squeeze(1)
+        n_struct = int(struct_idx.size(0))
+        if n_struct > 0:
+            bank_idx = torch.randint(0, int(mutation_bank.size(0)), (n_struct,), **i64)
+            len_p, len_b = torch.empty(n_struct, **i64), torch.empty(n_struct, **i64)
+            rand_p = torch.rand(n_struct, **f32)
+            rand_b = torch.rand(n_struct, **f32)
+            sp_, ep_ = torch.empty(n_struct, **i64), torch.empty(n_struct, **i64)
+            sb_, eb_ = torch.empty(n_struct, **i64), torch.empty(n_struct, **i64)
+            N.check(lib.ws_subtree_pick(ptr(offspring), ptr(struct_idx), n_struct, L,
+                                        ptr(token_arities), vocab, ptr(rand_p), ptr(len_p),
+                                        ptr(sp_), ptr(ep_), int(PAD_ID), st))
+            N.check(lib.ws_subtree_pick(ptr(mutation_bank), ptr(bank_idx), n_struct, L,
+                                        ptr(token_arities), vocab, ptr(rand_b), ptr(len_b),
+                                        ptr(sb_), ptr(eb_), int(PAD_ID), st))
+            child = torch.empty(n_struct, L, dtype=torch.uint8, device=dev)
+            dummy = torch.empty(n_struct, L, dtype=torch.uint8, device=dev)
+            N.check(lib.ws_splice_rows(ptr(offspring), ptr(mutation_bank), ptr(struct_idx),
+                                       ptr(bank_idx), None, None, ptr(sp_), ptr(ep_), ptr(sb_),
+                                       ptr(eb_), None, ptr(child), ptr(dummy), n_struct, L,
+                                       int(PAD_ID), None, 0.0, None, st))
+            offspring.index_copy_(0, struct_idx, child)
+    hoist_idx = torch.nonzero(hoist_mask).squeeze(1)
+    n_hoist = int(hoist_idx.size(0))
+    if n_hoist > 0:
+        r_ints = torch.randint(0, 1000000, (n_hoist,), **i64)
+        N.check(lib.ws_hoist_rows(ptr(offspring), ptr(hoist_idx), n_hoist, L, ptr(token_arities),
+                                  vocab, ptr(r_ints), int(PAD_ID), st))
+
+    # 4. PSO over the offspring's constants (per-row evaluator, torch RMSE, bests, update)
+    final_consts, final_fit = offspring_consts, torch.empty(0, **f32)
+    if pso_steps > 0:
+        P = int(pso_particles)
+        gbest_pos = offspring_consts.clone()
+        gbest_err = torch.full((B,), float("inf"), **f32)
+        pop_expanded = offspring.repeat_interleave(P, 0)
+        pos = offspring_consts.unsqueeze(1).repeat(1, P, 1)
+        jitter = torch.randn(B, P - 1, K, **f32) * 1.0
+        pos[:, 1:, :] = pos[:, 1:, :] + jitter
+        vel = torch.randn_like(pos) * 0.1
+        pbest_pos = pos.clone()
+        pbest_err = torch.full((B, P), float("inf"), **f32)
+        preds = torch.empty(B * P, n_data, **f32)
+        sp = torch.empty(B * P * n_data, **i32)
+        err_flags = torch.empty(B * P * n_data, dtype=torch.uint8, device=dev)
+        ids = (PAD_ID, id_x_start, id_C, id_pi, id_e, id_0, id_1, id_2, id_3, id_4, id_5, id_6,
+               id_10, op_add, op_sub, op_mul, op_div, op_pow, op_mod, op_sin, op_cos, op_tan,
+               op_log, op_exp, op_sqrt, op_abs, op_neg, op_fact, op_floor, op_ceil, op_sign,
+               op_gamma, op_lgamma, op_asin, op_acos, op_atan)
+        for _ in range(int(pso_steps)):
+            flat_pos = pos.view(-1, K)
+            eval_rpn(pop_expanded, X, flat_pos, preds, sp, err_flags, *ids, pi_val, e_val, 0)
+            diff = preds - Y_target.unsqueeze(0)
+            mse = torch.mean(diff * diff, 1)
+            rmse = torch.sqrt(mse)
+            rmse = torch.where(torch.isnan(rmse), torch.full_like(rmse, float("inf")), rmse)
+            curr = rmse.view(B, P)
+            pso_update_bests(curr, pbest_err, pbest_pos, pos, gbest_err, gbest_pos)
+            r1 = torch.rand(B, P, K, **f32)
+            r2 = torch.rand(B, P, K, **f32)
+            pso_update(pos, vel, pbest_pos, gbest_pos, r1, r2, _f32(pso_w), _f32(pso_c1),
+                       _f32(pso_c2))
+        final_consts, final_fit = gbest_pos, gbest_err
+    return [offspring, final_consts, final_fit]
