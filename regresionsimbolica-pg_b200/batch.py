@@ -21,7 +21,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass
-from typing import Dict, List, Optional, Sequence, Tuple
+from typing import Callable, Dict, List, Optional, Sequence, Tuple
 
 import torch
 
@@ -49,7 +49,12 @@ class BatchedFitness:
 
     def __init__(self, problems: Sequence[BatchProblem], *, loss: str = "mse",
                  policy: str = "classic", strict_mode: int = 0, schedule: int = 0,
-                 invalid_value: Optional[float] = None, count_invalid: bool = False):
+                 invalid_value: Optional[float] = None, count_invalid: bool = False,
+                 workspace: Optional[Callable[[int], torch.Tensor]] = None):
+        """`workspace`, when given, returns a uint8 device tensor of at least the requested
+        bytes (256-byte aligned); a caller that replans often passes one buffer it reuses
+        instead of an allocation per plan (work on one stream is ordered, so a new plan may take
+        over memory that queued work of an older plan still uses)."""
         if not problems:
             raise ValueError("no problems")
         self.problems = list(problems)
@@ -106,8 +111,9 @@ class BatchedFitness:
         need = C.c_size_t(0)
         N.check(lib.ws_batch_workspace_bytes(code, C.cast(arr, C.c_void_p), len(arr), L,
                                              C.byref(self._opts), C.byref(need)))
-        self.workspace = torch.empty(max(int(need.value), 256), dtype=torch.uint8,
-                                     device=self.device)
+        nbytes = max(int(need.value), 256)
+        self.workspace = (workspace(nbytes) if workspace is not None else
+                          torch.empty(nbytes, dtype=torch.uint8, device=self.device))
         h = C.c_void_p()
         N.check(lib.ws_batch_create(code, C.cast(arr, C.c_void_p), len(arr), L,
                                     C.byref(self._opts), ptr(self.workspace),

@@ -15,7 +15,7 @@ fitness -- never on the other problems of the launch.
 from __future__ import annotations
 
 import ctypes as C
-from typing import List, Optional, Sequence
+from typing import Callable, List, Optional, Sequence
 
 import torch
 
@@ -29,7 +29,8 @@ class GPStep:
                  *, generations: Optional[Sequence[int]] = None, tournament_size: int = 3,
                  elitism: bool = True, crossover_rate: float = 0.7,
                  mutation_rate: float = 0.05, const_mutation_rate: float = 0.1,
-                 const_sigma: float = 0.1, parsimony_eps: float = 1e-9):
+                 const_sigma: float = 0.1, parsimony_eps: float = 1e-9,
+                 workspace: Optional[Callable[[int], torch.Tensor]] = None):
         if not problems:
             raise ValueError("no problems")
         if len(fitness) != len(problems) or len(seeds) != len(problems):
@@ -71,7 +72,9 @@ class GPStep:
         need = C.c_size_t(0)
         N.check(lib.ws_gp_workspace_bytes(code, C.cast(arr, C.c_void_p), len(arr), L, C.byref(need)))
         self.device = problems[0].population.device
-        self.workspace = torch.empty(max(int(need.value), 256), dtype=torch.uint8, device=self.device)
+        nbytes = max(int(need.value), 256)
+        self.workspace = (workspace(nbytes) if workspace is not None else
+                          torch.empty(nbytes, dtype=torch.uint8, device=self.device))
         h = C.c_void_p()
         N.check(lib.ws_gp_create(code, C.cast(arr, C.c_void_p), len(arr), L, C.byref(self._opts),
                                  ptr(self.workspace), int(self.workspace.numel()),

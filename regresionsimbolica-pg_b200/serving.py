@@ -75,6 +75,26 @@ class _Slot:
     gen: int = 0
 
 
+class _Pool:
+    """One device buffer reused by every plan of a serving run (plans change with the batch
+    membership; work on one stream is ordered, so a new plan may take over the memory that
+    queued ticks of the previous plan still use).  It grows by at least half when a plan needs
+    more; a replaced buffer is kept until the ticks queued before the growth have finished."""
+
+    def __init__(self, device):
+        self.device = device
+        self.buf: Optional[torch.Tensor] = None
+        self.retired: List[torch.Tensor] = []
+
+    def __call__(self, nbytes: int) -> torch.Tensor:
+        if self.buf is None or self.buf.numel() < nbytes:
+            if self.buf is not None:
+                self.retired.append(self.buf)
+            grow = 0 if self.buf is None else self.buf.numel() * 3 // 2
+            self.buf = torch.empty(max(int(nbytes), grow), dtype=torch.uint8, device=self.device)
+        return self.buf
+
+
 def footprint(req: Request, L: Optional[int] = None) -> int:
     """Estimated device bytes of an admitted request: data set, population, constants and
     losses, the evaluator's per-program scratch (header, tape, order, partial sums) and the GP
@@ -134,6 +154,7 @@ class ContinuousBatchingServer:
         ev0 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         retired = []  # plans still referenced by queued work
+        eval_pool, gp_pool = _Pool(self.device), _Pool(self.device)
 
         def drain_one():
             nonlocal used
@@ -179,14 +200,14 @@ class ContinuousBatchingServer:
             if k != key:  # membership changed: plan the batch again (stream-ordered uploads)
                 retired += [x for x in (gp, bf) if x is not None]
                 bf = BatchedFitness([s.prob for s in active], loss=self.loss, policy="classic",
-                                    schedule=self.schedule)
+                                    schedule=self.schedule, workspace=eval_pool)
                 gp = None
                 breeders = breed
                 if breed:
                     idx = {s.req.rid: j for j, s in enumerate(active)}
                     gp = GPStep([s.prob for s in breed], [bf.outputs[idx[s.req.rid]] for s in breed],
                                 [s.req.seed for s in breed], generations=[s.gen for s in breed],
-                                **self.gp_options)
+                                workspace=gp_pool, **self.gp_options)
                 key = k
             bf.evaluate()
             finished = [s for s in active if s.req.kind == "evaluate" or s.gen >= s.req.generations]
@@ -216,8 +237,11 @@ class ContinuousBatchingServer:
                 active = [s for s in active if s.req.rid not in gone]
             while len(inflight) > max_inflight:
                 drain_one()
-            if len(retired) > 8 and not inflight:
-                retired.clear()
+            if not inflight:
+                if len(retired) > 8:
+                    retired.clear()
+                eval_pool.retired.clear()
+                gp_pool.retired.clear()
         while inflight:
             drain_one()
         torch.cuda.synchronize(self.device)

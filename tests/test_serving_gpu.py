@@ -5,6 +5,8 @@ import numpy as np
 import pytest
 import torch
 
+import ws_testlib  # noqa: F401  (registers the package as warpsymbolic_b200)
+
 pytestmark = pytest.mark.gpu
 
 
