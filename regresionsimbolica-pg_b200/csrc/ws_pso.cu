@@ -13,7 +13,9 @@
 // swarm has more than 32 particles), four programs per 128-thread block, instead of one
 // P-thread block per program (20-thread blocks leave 12 lanes of every warp idle and cap
 // residency at 32 blocks per SM).  The program and its constants live in shared memory; the
-// token dispatch is a table lookup instead of a ~40-way comparison chain.
+// token dispatch is a table lookup instead of a ~40-way comparison chain; each lane carries 16
+// rows through one pass over the program (one decode per token for 16 rows) and then adds the
+// rows' squared errors one at a time in row order, so every RMSE keeps the reference's bits.
 #include <cuda_runtime.h>
 #include <curand_kernel.h>
 #include <cstdint>
@@ -104,6 +106,7 @@ __global__ void __launch_bounds__(256)
 // Fused PSO (float only, as the reference).
 constexpr int kPsoMaxL = 256, kPsoMaxK = 16, kPsoMaxD = 1024, kPsoMaxP = 64, kPsoStack = 32;
 constexpr float kPsoInf = 1e30f;
+constexpr int kPsoRows = 16;  // rows a lane evaluates per program decode
 
 // Token classes of eval_rpn_single's precedence (fused_pso_kernels.cu:81-183): PAD, variables,
 // literals 0..6, 10, pi, e, then C, then the binary operators, then the unary operators in the
@@ -128,116 +131,198 @@ __device__ __forceinline__ float safe_pow_pso(float a, float b) {
   return res;
 }
 
-// One row of eval_rpn_single (fused_pso_kernels.cu:57-197); constants are this lane's column
-// of the shared [K][G] position table.
-__device__ __forceinline__ float pso_eval_row(const uint8_t* s_prog, int L, const uint8_t* s_cls,
+// R consecutive rows of eval_rpn_single (fused_pso_kernels.cu:57-197) at once; constants are this
+// lane's column of the shared [K][G] position table.  The control flow of eval_rpn_single depends
+// on the tokens only (pushes, pops, the push-drop at depth 32, stack underflow), so the R rows
+// share it; where one row would stop with an error (a domain check, a non-finite result) it is
+// flagged instead and its later values are ignored.  One decode of a token serves R rows and the
+// stack moves R values per access.  Each row's result is the reference's for that row.
+template <int R>
+struct __align__(16) PsoV {
+  float v[R];
+};
+
+template <int R>
+__device__ __forceinline__ void pso_eval_rows(const uint8_t* s_prog, int L, const uint8_t* s_cls,
                                               const uint8_t* s_arg, const float* s_lit,
-                                              const float* __restrict__ x, int64_t D, int d,
-                                              const float* pos, int G, int K) {
-  float stack[kPsoStack];
+                                              const float* __restrict__ x, int64_t D, int d0,
+                                              int nrows, const float* pos, int G, int K,
+                                              float (&out)[R]) {
+  using PsoV4 = PsoV<R>;
+  PsoV4 stack[kPsoStack];
   int sp = 0;
   int c_idx = 0;
+  bool bad[R];
+#define WS_R4 _Pragma("unroll") for (int r = 0; r < R; ++r)
+  WS_R4 bad[r] = false;
   for (int pc = 0; pc < L; ++pc) {
     const int tok = s_prog[pc];
     const int cls = s_cls[tok];
     if (cls == T_PAD) break;
     if (cls == T_VAR || cls == T_LIT || cls == T_CONST) {
-      float val;
-      if (cls == T_VAR) val = __ldg(x + (int64_t)s_arg[tok] * D + d);
-      else if (cls == T_LIT) val = s_lit[s_arg[tok]];
-      else {
-        const int r = c_idx < K ? c_idx : K - 1;
-        val = r >= 0 ? pos[r * G] : 1.0f;
-        c_idx++;
+      PsoV4 val;
+      if (cls == T_VAR) {
+        const float* xr = x + (int64_t)s_arg[tok] * D + d0;
+        WS_R4 val.v[r] = r < nrows ? __ldg(xr + r) : 0.0f;
+      } else {
+        float c;
+        if (cls == T_LIT) {
+          c = s_lit[s_arg[tok]];
+        } else {
+          const int rr = c_idx < K ? c_idx : K - 1;
+          c = rr >= 0 ? pos[rr * G] : 1.0f;
+          c_idx++;
+        }
+        WS_R4 val.v[r] = c;
       }
       if (sp < kPsoStack) stack[sp++] = val;
       continue;
     }
     if (cls >= T_ADD && cls <= T_MOD) {
-      if (sp < 2) return kPsoInf;
-      const float b = stack[--sp];
-      const float a = stack[--sp];
-      float res = 0.0f;
+      if (sp < 2) {
+        WS_R4 out[r] = kPsoInf;
+        return;
+      }
+      const PsoV4 b = stack[--sp];
+      const PsoV4 a = stack[--sp];
+      PsoV4 res;
       switch (cls) {
-        case T_ADD: res = a + b; break;
-        case T_SUB: res = a - b; break;
-        case T_MUL: res = a * b; break;
+        case T_ADD: WS_R4 res.v[r] = a.v[r] + b.v[r]; break;
+        case T_SUB: WS_R4 res.v[r] = a.v[r] - b.v[r]; break;
+        case T_MUL: WS_R4 res.v[r] = a.v[r] * b.v[r]; break;
         case T_DIV:
-          if (fabsf(b) < 1e-12f) return kPsoInf;
-          res = a / b;
+          WS_R4 {
+            if (fabsf(b.v[r]) < 1e-12f) {
+              bad[r] = true;
+              res.v[r] = 0.0f;
+            } else {
+              res.v[r] = a.v[r] / b.v[r];
+            }
+          }
           break;
         case T_POW:
-          res = safe_pow_pso(a, b);
-          if (res >= 1e29f) return kPsoInf;
+          WS_R4 {
+            res.v[r] = safe_pow_pso(a.v[r], b.v[r]);
+            if (res.v[r] >= 1e29f) bad[r] = true;
+          }
           break;
         default:
-          if (fabsf(b) < 1e-12f) return kPsoInf;
-          res = fmodf(a, b);
+          WS_R4 {
+            if (fabsf(b.v[r]) < 1e-12f) {
+              bad[r] = true;
+              res.v[r] = 0.0f;
+            } else {
+              res.v[r] = fmodf(a.v[r], b.v[r]);
+            }
+          }
           break;
       }
       stack[sp++] = res;
       continue;
     }
-    if (sp < 1) return kPsoInf;
-    const float a = stack[--sp];
-    float res = 0.0f;
+    if (sp < 1) {
+      WS_R4 out[r] = kPsoInf;
+      return;
+    }
+    const PsoV4 a = stack[--sp];
+    PsoV4 res;
     switch (cls) {
-      case T_SIN: res = sinf(a); break;
-      case T_COS: res = cosf(a); break;
-      case T_TAN: res = tanf(a); break;
-      case T_ABS: res = fabsf(a); break;
-      case T_NEG: res = -a; break;
+      case T_SIN: WS_R4 res.v[r] = sinf(a.v[r]); break;
+      case T_COS: WS_R4 res.v[r] = cosf(a.v[r]); break;
+      case T_TAN: WS_R4 res.v[r] = tanf(a.v[r]); break;
+      case T_ABS: WS_R4 res.v[r] = fabsf(a.v[r]); break;
+      case T_NEG: WS_R4 res.v[r] = -a.v[r]; break;
       case T_SQRT:
-        if (a < 0.0f) return kPsoInf;
-        res = sqrtf(a);
+        WS_R4 {
+          if (a.v[r] < 0.0f) bad[r] = true;
+          res.v[r] = a.v[r] < 0.0f ? 0.0f : sqrtf(a.v[r]);
+        }
         break;
       case T_LOG:
-        if (a <= 1e-12f) return kPsoInf;
-        res = logf(a);
+        WS_R4 {
+          if (a.v[r] <= 1e-12f) bad[r] = true;
+          res.v[r] = a.v[r] <= 1e-12f ? 0.0f : logf(a.v[r]);
+        }
         break;
       case T_EXP:
-        if (a > 80.0f) return kPsoInf;
-        if (a < -80.0f) res = 0.0f;
-        else res = expf(a);
+        WS_R4 {
+          if (a.v[r] > 80.0f) {
+            bad[r] = true;
+            res.v[r] = 0.0f;
+          } else if (a.v[r] < -80.0f) {
+            res.v[r] = 0.0f;
+          } else {
+            res.v[r] = expf(a.v[r]);
+          }
+        }
         break;
-      case T_FLOOR: res = floorf(a); break;
-      case T_CEIL: res = ceilf(a); break;
-      case T_SIGN: res = (a > 0.0f) ? 1.0f : ((a < 0.0f) ? -1.0f : 0.0f); break;
+      case T_FLOOR: WS_R4 res.v[r] = floorf(a.v[r]); break;
+      case T_CEIL: WS_R4 res.v[r] = ceilf(a.v[r]); break;
+      case T_SIGN:
+        WS_R4 res.v[r] = (a.v[r] > 0.0f) ? 1.0f : ((a.v[r] < 0.0f) ? -1.0f : 0.0f);
+        break;
       case T_ASIN:
-        if (a < -1.0f || a > 1.0f) return kPsoInf;
-        res = asinf(a);
+        WS_R4 {
+          const bool out_of = a.v[r] < -1.0f || a.v[r] > 1.0f;
+          if (out_of) bad[r] = true;
+          res.v[r] = out_of ? 0.0f : asinf(a.v[r]);
+        }
         break;
       case T_ACOS:
-        if (a < -1.0f || a > 1.0f) return kPsoInf;
-        res = acosf(a);
+        WS_R4 {
+          const bool out_of = a.v[r] < -1.0f || a.v[r] > 1.0f;
+          if (out_of) bad[r] = true;
+          res.v[r] = out_of ? 0.0f : acosf(a.v[r]);
+        }
         break;
-      case T_ATAN: res = atanf(a); break;
+      case T_ATAN: WS_R4 res.v[r] = atanf(a.v[r]); break;
       case T_FACT:
-        if (a <= -1.0f && floorf(a + 1.0f) == (a + 1.0f)) return kPsoInf;
-        if (a > 50.0f) return kPsoInf;
-        res = tgammaf(a + 1.0f);
-        if (res != res || isinf(res)) return kPsoInf;
+        WS_R4 {
+          const float v = a.v[r];
+          if ((v <= -1.0f && floorf(v + 1.0f) == (v + 1.0f)) || v > 50.0f) {
+            bad[r] = true;
+            res.v[r] = 0.0f;
+          } else {
+            res.v[r] = tgammaf(v + 1.0f);
+          }
+        }
         break;
       case T_GAMMA:
-        if (a <= 0.0f && floorf(a) == a) return kPsoInf;
-        if (a > 50.0f) return kPsoInf;
-        res = tgammaf(a);
-        if (res != res || isinf(res)) return kPsoInf;
+        WS_R4 {
+          const float v = a.v[r];
+          if ((v <= 0.0f && floorf(v) == v) || v > 50.0f) {
+            bad[r] = true;
+            res.v[r] = 0.0f;
+          } else {
+            res.v[r] = tgammaf(v);
+          }
+        }
         break;
       case T_LGAMMA:
-        if (a <= 0.0f && floorf(a) == a) return kPsoInf;
-        res = lgammaf(a);
-        if (res != res || isinf(res)) return kPsoInf;
+        WS_R4 {
+          const float v = a.v[r];
+          if (v <= 0.0f && floorf(v) == v) {
+            bad[r] = true;
+            res.v[r] = 0.0f;
+          } else {
+            res.v[r] = lgammaf(v);
+          }
+        }
         break;
-      default: res = 0.0f; break;  // tokens without a rule push 0
+      default: WS_R4 res.v[r] = 0.0f; break;  // tokens without a rule push 0
     }
-    if (res != res || isinf(res)) return kPsoInf;
+    WS_R4 if (res.v[r] != res.v[r] || isinf(res.v[r])) bad[r] = true;
     stack[sp++] = res;
   }
-  if (sp != 1) return kPsoInf;
-  const float result = stack[0];
-  if (result != result || isinf(result)) return kPsoInf;
-  return result;
+  if (sp != 1) {
+    WS_R4 out[r] = kPsoInf;
+    return;
+  }
+  WS_R4 {
+    const float v = stack[0].v[r];
+    out[r] = (bad[r] || v != v || isinf(v)) ? kPsoInf : v;
+  }
+#undef WS_R4
 }
 
 struct FusedPsoArgs {
@@ -340,17 +425,25 @@ __global__ void __launch_bounds__(128) fused_pso_kernel(FusedPsoArgs a, PsoLut l
     for (int step = 0; step < a.steps; ++step) {
       if (live && active) {
         // 1. evaluate this particle over every row
+        // (kPsoRows rows per decode; the squared errors are summed one row at a time, in row
+        // order, as the reference does)
         float mse_sum = 0.0f;
         bool any_error = false;
-        for (int d = 0; d < (int)a.D; ++d) {
-          const float pred = pso_eval_row(sw.prog, a.L, s_cls, s_arg, s_lit, a.x, a.D, d, my_pos,
-                                          a.G, K);
-          if (pred >= 1e29f) {
-            any_error = true;
-            break;
+        for (int d = 0; d < (int)a.D && !any_error; d += kPsoRows) {
+          const int nr = (int)a.D - d < kPsoRows ? (int)a.D - d : kPsoRows;
+          float pr[kPsoRows];
+          pso_eval_rows<kPsoRows>(sw.prog, a.L, s_cls, s_arg, s_lit, a.x, a.D, d, nr, my_pos,
+                                  a.G, K, pr);
+#pragma unroll
+          for (int r = 0; r < kPsoRows; ++r) {
+            if (r >= nr || any_error) break;
+            if (pr[r] >= 1e29f) {
+              any_error = true;
+              break;
+            }
+            const float diff = pr[r] - a.y[d + r];
+            mse_sum += diff * diff;
           }
-          const float diff = pred - a.y[d];
-          mse_sum += diff * diff;
         }
         const float rmse = any_error ? kPsoInf : sqrtf(mse_sum / (float)a.D);
         // 2. personal best
