@@ -15,7 +15,19 @@
 
 namespace ws {
 
-template <typename T, bool STRICT>
+// A warp owns a tile of 32 * R rows of one program; lane t carries rows base + t + 32 r
+// (r < R), so x reads and output writes stay coalesced.  The interpreter's control flow depends
+// on the tokens only (pushes, pops, the push-drop at depth 32, underflow and unknown tokens), so
+// the R rows share it and one decode of a token serves them all; a row that the reference would
+// stop at an operator's error (a domain error, or what the protected operators report) is frozen
+// instead: its depth and stack top at that point are recorded and its later values ignored.
+// Each row's outputs are the reference's.
+template <typename T, int R>
+struct __align__(16) RowVec {
+  T v[R];
+};
+
+template <typename T, bool STRICT, int R>
 __global__ void __launch_bounds__(256) eval_rows_kernel(
     const uint8_t* __restrict__ pop, int64_t B, int64_t L, const T* __restrict__ x, int64_t D,
     const T* __restrict__ consts, int64_t K, TokenLut lut, T* __restrict__ out_preds,
@@ -28,58 +40,117 @@ __global__ void __launch_bounds__(256) eval_rows_kernel(
   if (threadIdx.x < N_LITERALS) s_lit[threadIdx.x] = (T)lut.lit[threadIdx.x];
   __syncthreads();
 
-  const int64_t total = B * D;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t b = idx / D, d = idx - b * D;
+  const int lane = threadIdx.x & 31;
+  const int64_t tile_rows = 32 * (int64_t)R;
+  const int64_t tiles_per_prog = (D + tile_rows - 1) / tile_rows;
+  const int64_t n_tiles = B * tiles_per_prog;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+       tile < n_tiles; tile += warps) {
+    const int64_t b = tile / tiles_per_prog;
+    const int64_t base = (tile - b * tiles_per_prog) * tile_rows + lane;
     const uint8_t* prog = pop + b * L;
-    T stack[32];
+    RowVec<T, R> stack[32];
     int sp = 0;
-    bool error = false;
     int64_t c_idx = 0;
-    for (int64_t pc = 0; pc < L; ++pc) {
+    // per row: frozen at an error (depth and top recorded then)
+    bool stopped[R];
+    int stop_sp[R];
+    T stop_top[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) stopped[r] = false;
+    bool all_stop = false;  // a token-driven error stops every row at once
+    for (int64_t pc = 0; pc < L && !all_stop; ++pc) {
       const int tok = prog[pc];
       const int cls = s_cls[tok];
       if (cls == T_PAD) break;
       if (is_leaf(cls)) {
-        T val;
+        RowVec<T, R> val;
         if (cls == T_VAR) {
-          val = x[(int64_t)s_arg[tok] * D + d];
-        } else if (cls == T_CONST) {
-          if (K > 0) {
-            const int64_t r = c_idx < K ? c_idx : K - 1;
-            val = consts[b * K + r];
-            c_idx++;
-          } else {
-            val = (T)1.0;
+          const T* xr = x + (int64_t)s_arg[tok] * D;
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int64_t d = base + 32 * r;
+            val.v[r] = d < D ? xr[d] : (T)0;
           }
         } else {
-          val = s_lit[s_arg[tok]];
+          T c;
+          if (cls == T_CONST) {
+            if (K > 0) {
+              const int64_t ri = c_idx < K ? c_idx : K - 1;
+              c = consts[b * K + ri];
+              c_idx++;
+            } else {
+              c = (T)1.0;
+            }
+          } else {
+            c = s_lit[s_arg[tok]];
+          }
+#pragma unroll
+          for (int r = 0; r < R; ++r) val.v[r] = c;
         }
         if (sp < 32) stack[sp++] = val;
         continue;
       }
       if (is_binary(cls)) {
-        if (sp < 2) { error = true; break; }
-        const T op2 = stack[--sp];
-        const T op1 = stack[--sp];
-        bool e = false;
-        const T res = apply_binary<T, STRICT>(cls, op1, op2, e);
-        if (e) { error = true; break; }
+        if (sp < 2) {
+          all_stop = true;
+          break;
+        }
+        const RowVec<T, R> op2 = stack[--sp];
+        const RowVec<T, R> op1 = stack[--sp];
+        RowVec<T, R> res;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          bool e = false;
+          res.v[r] = apply_binary<T, STRICT>(cls, op1.v[r], op2.v[r], e);
+          if (e && !stopped[r]) {
+            stopped[r] = true;
+            stop_sp[r] = sp;
+            stop_top[r] = sp > 0 ? stack[sp - 1].v[r] : Limits<T>::no_value;
+          }
+        }
         stack[sp++] = res;
         continue;
       }
-      if (sp < 1) { error = true; break; }
-      const T a = stack[--sp];
-      if (!is_unary(cls)) { error = true; break; }
-      bool e = false;
-      const T res = apply_unary<T, STRICT>(cls, a, e);
-      if (e) { error = true; break; }
+      if (sp < 1) {
+        all_stop = true;
+        break;
+      }
+      const RowVec<T, R> a = stack[--sp];
+      if (!is_unary(cls)) {
+        all_stop = true;
+        break;
+      }
+      RowVec<T, R> res;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        bool e = false;
+        res.v[r] = apply_unary<T, STRICT>(cls, a.v[r], e);
+        if (e && !stopped[r]) {
+          stopped[r] = true;
+          stop_sp[r] = sp;
+          stop_top[r] = sp > 0 ? stack[sp - 1].v[r] : Limits<T>::no_value;
+        }
+      }
       stack[sp++] = res;
     }
-    out_sp[idx] = sp;
-    out_err[idx] = error ? 1 : 0;
-    out_preds[idx] = sp > 0 ? stack[sp - 1] : Limits<T>::no_value;
+    // rows still running at a token-driven error or at the end take the current depth and top
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t d = base + 32 * r;
+      if (d >= D) continue;
+      const int64_t idx = b * D + d;
+      if (stopped[r]) {
+        out_sp[idx] = stop_sp[r];
+        out_err[idx] = 1;
+        out_preds[idx] = stop_top[r];
+      } else {
+        out_sp[idx] = sp;
+        out_err[idx] = all_stop ? 1 : 0;
+        out_preds[idx] = sp > 0 ? stack[sp - 1].v[r] : Limits<T>::no_value;
+      }
+    }
   }
 }
 
@@ -87,25 +158,27 @@ ws_status launch_eval_rows(int dtype, const uint8_t* pop, int64_t B, int64_t L, 
                            int64_t D, const void* consts, int64_t K, const TokenLut& lut,
                            void* out_preds, int32_t* out_sp, uint8_t* out_err, int strict,
                            cudaStream_t stream) {
-  const int64_t total = B * D;
-  if (total == 0) return WS_OK;
+  if (B * D == 0) return WS_OK;
   const int threads = 256;
-  int64_t blocks = (total + threads - 1) / threads;
+  constexpr int RF = 4, RD = 2;  // rows per lane (16-byte stack entries): float, double
+  const int64_t rows_per_tile = 32 * (int64_t)(dtype == WS_F32 ? RF : RD);
+  const int64_t tiles = B * ((D + rows_per_tile - 1) / rows_per_tile);
+  int64_t blocks = (tiles + (threads / 32) - 1) / (threads / 32);
   const int64_t cap = (int64_t)device_info().sm_count * 32;
   if (blocks > cap) blocks = cap;
   if (dtype == WS_F32) {
     if (strict)
-      eval_rows_kernel<float, true><<<(unsigned)blocks, threads, 0, stream>>>(
+      eval_rows_kernel<float, true, RF><<<(unsigned)blocks, threads, 0, stream>>>(
           pop, B, L, (const float*)x, D, (const float*)consts, K, lut, (float*)out_preds, out_sp, out_err);
     else
-      eval_rows_kernel<float, false><<<(unsigned)blocks, threads, 0, stream>>>(
+      eval_rows_kernel<float, false, RF><<<(unsigned)blocks, threads, 0, stream>>>(
           pop, B, L, (const float*)x, D, (const float*)consts, K, lut, (float*)out_preds, out_sp, out_err);
   } else {
     if (strict)
-      eval_rows_kernel<double, true><<<(unsigned)blocks, threads, 0, stream>>>(
+      eval_rows_kernel<double, true, RD><<<(unsigned)blocks, threads, 0, stream>>>(
           pop, B, L, (const double*)x, D, (const double*)consts, K, lut, (double*)out_preds, out_sp, out_err);
     else
-      eval_rows_kernel<double, false><<<(unsigned)blocks, threads, 0, stream>>>(
+      eval_rows_kernel<double, false, RD><<<(unsigned)blocks, threads, 0, stream>>>(
           pop, B, L, (const double*)x, D, (const double*)consts, K, lut, (double*)out_preds, out_sp, out_err);
   }
   cudaError_t e = cudaGetLastError();
