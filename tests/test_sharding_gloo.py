@@ -93,3 +93,69 @@ def test_shard_bounds_partition():
             assert max(sizes) - min(sizes) <= 1
     with pytest.raises(ValueError):
         shard_bounds(10, 2, 2)
+
+
+# ---- row sharding -----------------------------------------------------------------------
+def _row_case(dtype):
+    rng = np.random.default_rng(12)
+    g = tl.GPUGrammar(num_variables=3, operators=tl.C1_OPERATORS)
+    pop, consts = tl.random_population(g, 300, 24, 4, rng, valid_only=False)
+    X = rng.uniform(-3, 3, size=(3, 1001)).astype(dtype)
+    y = (np.sin(X[0]) + X[1] * X[2]).astype(dtype)
+    return g, pop, consts.astype(dtype), X, y
+
+
+def _row_worker(rank, world, port, dtype_name, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from warpsymbolic_b200.sharding import RowShardedEvaluator, shard_bounds
+        dtype = np.dtype(dtype_name)
+        g, pop, consts, X, y = _row_case(dtype)
+        tm = tl.token_map(g)
+        s, e = shard_bounds(X.shape[1], world, rank)
+
+        def partial(p, xs, ys, c):  # the oracle stands in for the GPU evaluator
+            sse, ninv = tl.oracle.fitness(tm, p.numpy(), xs.numpy(), c.numpy(), ys.numpy(),
+                                          policy="classic", loss="sse", with_ninv=True)
+            return torch.from_numpy(sse), torch.from_numpy(ninv)
+
+        ev = RowShardedEvaluator(partial_fn=partial)
+        out = {}
+        for loss in ("mse", "rmse", "r2"):
+            out[loss] = ev.evaluate(torch.from_numpy(pop), torch.from_numpy(X[:, s:e].copy()),
+                                    torch.from_numpy(y[s:e].copy()), torch.from_numpy(consts),
+                                    loss=loss).numpy()
+        q.put((rank, out))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("dtype_name", ["float32", "float64"])
+def test_two_rank_row_sharding_matches_single_process(dtype_name):
+    dtype = np.dtype(dtype_name)
+    g, pop, consts, X, y = _row_case(dtype)
+    tm = tl.token_map(g)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_row_worker, args=(r, 2, port, dtype_name, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for loss in ("mse", "rmse", "r2"):
+        want = tl.oracle.fitness(tm, pop, X, consts, y, policy="classic", loss=loss)
+        a, b = res[0][loss], res[1][loss]
+        np.testing.assert_array_equal(a, b)  # every rank forms the same losses
+        inv = 1e15 if dtype == np.float32 else 1e100
+        bad = np.abs(want) >= inv * 0.5
+        assert (np.abs(a) >= inv * 0.5).tolist() == bad.tolist(), loss
+        rtol = 1e-6 if dtype == np.float32 else 1e-12
+        # R^2 = 1 - MSE / Var(y) cancels near 0: an absolute floor of a few ulps of 1
+        atol = 0.0 if loss != "r2" else (1e-6 if dtype == np.float32 else 1e-14)
+        np.testing.assert_allclose(a[~bad], want[~bad], rtol=rtol, atol=atol)
+        assert (~bad).sum() > 100
