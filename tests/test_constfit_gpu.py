@@ -159,3 +159,33 @@ def test_optimizer_per_program_accepts_improvements_only():
     after = ev.evaluate_batch(P, Xd, yd, new_c)
     assert torch.equal(after, errs)
     assert float((errs < before).float().mean()) > 0.3
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_loss_grad_long_programs_many_constants(dtype):
+    """More than 8 constant slots (shared-memory accumulators) and 120-token programs (a tape too
+    long for 4 rows per thread): the other shapes of the kernel."""
+    rng = np.random.default_rng(13)
+    g = tl.GPUGrammar(num_variables=3, operators=SMOOTH_OPS)
+    B, L, K, D = 48, 120, 12, 3000
+    pop = tl.synthetic.random_programs(g, B, 40, L, L, rng, const_prob=0.5, max_consts=K)
+    consts = rng.uniform(-1, 1, size=(B, K)).astype(dtype)
+    X = rng.uniform(-1.5, 1.5, size=(3, D)).astype(dtype)
+    y = (np.sin(X[0]) + 0.3 * X[1] * X[2]).astype(dtype)
+    loss, grad = cf().loss_grad(T(pop), T(X), T(consts), T(y), g.scalar_ids())
+    loss, grad = loss.cpu().numpy(), grad.cpu().numpy().astype(np.float64)
+    ol, og, absg = O.loss_grad(tmap(g), pop, X, consts, y)
+    fin = np.isfinite(ol) & (ol < 1e30)
+    assert fin.sum() > B // 2
+    if dtype == np.float64:
+        np.testing.assert_allclose(loss[fin], ol[fin], rtol=1e-10, atol=0)
+        gtol = 1e-8 * (absg + 1e-12)
+        assert (np.abs(grad[fin] - og[fin]) <= gtol[fin] + 1e-300).all()
+    else:
+        # float32: the GPU's fast single-precision transcendentals against libm, compounded
+        # through 120-token chains; nearly every program agrees to 5e-4, none is far off
+        rel = np.abs(loss[fin] - ol[fin]) / np.abs(ol[fin])
+        assert (rel < 5e-4).mean() > 0.9 and rel.max() < 2e-2, rel.max()
+        gerr = np.abs(grad[fin] - og[fin]) / (absg[fin] + 1e-12)
+        assert (gerr < 5e-3).mean() > 0.9, (gerr < 5e-3).mean()
+    assert (np.abs(og[fin]) > 0).any()
