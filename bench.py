@@ -571,10 +571,12 @@ def run_serving(args):
     default), half fits
     (population 4,096, 30 generations) and half evaluations (4,096 programs), rows log-uniform in
     [1,000, 200,000], 1..8 variables, X ~ U[-3,3], targets from depth 3-6 trees with noise
-    0.01 * std(y).  Served by the continuous-batching loop (one batched evaluation and one batched
-    GP generation per tick for all admitted requests), then by the plain path (one request at a
-    time, one launch sequence per evaluation and per generation) on the same stream; every
-    request's result is checked to be identical on both."""
+    0.01 * std(y).  Served by the continuous-batching loop (requests grouped by the work of one
+    generation; per step of a group one batched evaluation and one batched GP generation, cheaper
+    groups stepped more often), then by the plain path (one request at a time, one launch
+    sequence per evaluation and per generation) on the same stream; every request's result is
+    checked to be identical on both.  Both paths first serve the stream once untimed, so that
+    neither pays first-time device allocations of these sizes in its timed run."""
     import torch
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
@@ -582,11 +584,11 @@ def run_serving(args):
     from warpsymbolic_b200 import synthetic
     from warpsymbolic_b200.serving import (ContinuousBatchingServer, serve_plain,
                                            latency_summary)
-    warm = synthetic.serving_stream(seed=99, n_requests=4, rate=1e6, rows=(1000, 3000),
-                                    population=512, generations=2)
-    ContinuousBatchingServer(dev).serve(warm, realtime=False)
-    serve_plain(warm, dev, realtime=False)
     reqs = synthetic.serving_stream(seed=args.seed, n_requests=args.requests, rate=args.rate)
+    # warm-up: both paths serve the same stream once, untimed, so that neither pays first-time
+    # device allocations of these request sizes inside its timed run (a server that has been up)
+    ContinuousBatchingServer(dev).serve(reqs, realtime=False)
+    serve_plain(reqs, dev, realtime=False)
     evals = 0.0
     for r in reqs:
         n_tok = float((r.population != 0).sum())

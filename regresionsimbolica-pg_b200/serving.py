@@ -1,10 +1,13 @@
 """A serving loop for fit and evaluate requests with continuous batching.
 
 Requests of different sizes arrive over time.  Each admitted request keeps its state on the
-device (data set, population, constants, losses) until it completes.  One tick of the loop runs
-ONE batched evaluation of every active request (libwarpsym's ws_batch_*) and ONE batched GP
-generation for every fit request that still has generations to run (ws_gp_*).  Requests that
-arrive while a tick runs are admitted at the next tick, in arrival order, as long as their
+device (data set, population, constants, losses) until it completes.  Admitted requests are
+grouped by the work of one of their generations (programs x rows, in doublings); a step of a
+group is ONE batched evaluation of its requests (libwarpsym's ws_batch_*) and ONE batched GP
+generation for its fits that still have generations to run (ws_gp_*).  A tick steps every group,
+the cheaper groups several times (2^j times for j doublings below the most expensive, up to 8),
+so small fits are not held to the pace of the large ones they share the GPU with.  Requests
+that arrive while a tick runs are admitted at the next tick, in arrival order, as long as their
 estimated device footprint fits the memory budget and a slot is free.
 
     server = ContinuousBatchingServer(hbm_budget=8 << 30)
@@ -64,6 +67,16 @@ class Result:
     @property
     def latency(self) -> float:
         return self.done - self.arrival
+
+
+@dataclass
+class _Group:
+    """Admitted requests of one cost class with the plans that serve them together."""
+    slots: list = field(default_factory=list)
+    key: Optional[tuple] = None
+    bf: Optional[BatchedFitness] = None
+    gp: Optional[GPStep] = None
+    breeders: list = field(default_factory=list)
 
 
 @dataclass
@@ -130,31 +143,41 @@ class ContinuousBatchingServer:
                             req.grammar)
         return _Slot(req, prob, footprint(req), now)
 
+    @staticmethod
+    def cost_class(req: Request) -> int:
+        """Work class of one generation of a request: doublings of programs x rows."""
+        work = max(1, int(req.population.shape[0]) * int(req.X.shape[1]))
+        return max(0, int(np.log2(work)))
+
     def serve(self, requests: Sequence[Request], realtime: bool = True,
-              max_inflight: int = 8) -> List[Result]:
+              max_inflight: int = 8, max_steps_per_tick: int = 8) -> List[Result]:
         """Serves the stream; with realtime=False arrivals only order the queue (a request is
-        admitted as soon as it is first in line and fits).  Ticks are queued on the GPU without
-        waiting for each other; at most `max_inflight` ticks are in flight, so a request that
-        arrives joins within that many ticks.  Results are read back (pinned memory) when the
-        tick that finishes them completes; completion times come from CUDA events."""
+        admitted as soon as it is first in line and fits).
+
+        Admitted requests are grouped by the work of one of their generations (cost_class);
+        each group has its own batch plan and GP step, replanned only when its membership
+        changes.  A tick runs every group once, and a group that is 2^j times cheaper than the
+        most expensive one runs min(2^j, max_steps_per_tick) generations in that tick, so a small
+        fit does not wait for the large fits it shares the GPU with.  Steps are queued on the
+        GPU without waiting for each other; at most `max_inflight` steps are in flight.  Results
+        are read back (pinned memory) when the step that finishes them completes; completion
+        times come from CUDA events.  A request stays in its group for life: its losses and
+        offspring are the same whatever it is served with."""
         reqs = sorted(requests, key=lambda r: (r.arrival, r.rid))
         waiting: collections.deque = collections.deque()
-        active: List[_Slot] = []
+        groups: Dict[int, _Group] = {}
         results: List[Result] = []
         inflight: collections.deque = collections.deque()  # (event, [(slot, host losses, snap)])
         used = 0
         i = 0
-        key = None
-        bf = gp = None
-        breeders: List[_Slot] = []
-        ticks = max_active_seen = 0
+        steps = max_active_seen = 0
         stream = torch.cuda.current_stream(self.device)
         torch.cuda.synchronize(self.device)
         t0 = time.perf_counter()
         ev0 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         retired = []  # plans still referenced by queued work
-        eval_pool, gp_pool = _Pool(self.device), _Pool(self.device)
+        pools = {}
 
         def drain_one():
             nonlocal used
@@ -177,79 +200,106 @@ class ContinuousBatchingServer:
                 results.append(res)
                 used -= slot.nbytes
 
-        while i < len(reqs) or waiting or active or inflight:
-            now = time.perf_counter() - t0
-            while i < len(reqs) and (reqs[i].arrival <= now or not realtime):
-                waiting.append(reqs[i])
-                i += 1
-            while (waiting and len(active) < self.max_active
-                   and (not active or used + footprint(waiting[0]) <= self.hbm_budget)):
-                r = waiting.popleft()
-                s = self._admit(r, max(now, r.arrival) if realtime else now)
-                used += s.nbytes
-                active.append(s)
-            if not active:
-                if inflight:
-                    drain_one()
-                elif i < len(reqs) and realtime:
-                    time.sleep(max(0.0, reqs[i].arrival - (time.perf_counter() - t0)))
-                continue
-            max_active_seen = max(max_active_seen, len(active))
+        def step(cls: int, grp: "_Group") -> None:
+            """One generation of a group: evaluate everything, read back what finishes, breed
+            the rest."""
+            nonlocal steps
+            active = grp.slots
             breed = [s for s in active if s.req.kind == "fit" and s.gen < s.req.generations]
             k = (tuple(s.req.rid for s in active), tuple(s.req.rid for s in breed))
-            if k != key:  # membership changed: plan the batch again (stream-ordered uploads)
-                retired += [x for x in (gp, bf) if x is not None]
-                bf = BatchedFitness([s.prob for s in active], loss=self.loss, policy="classic",
-                                    schedule=self.schedule, workspace=eval_pool)
-                gp = None
-                breeders = breed
+            if k != grp.key:  # membership changed: plan the group again (stream-ordered)
+                retired.extend(x for x in (grp.gp, grp.bf) if x is not None)
+                if cls not in pools:
+                    pools[cls] = (_Pool(self.device), _Pool(self.device))
+                ep, gpp = pools[cls]
+                grp.bf = BatchedFitness([s.prob for s in active], loss=self.loss,
+                                        policy="classic", schedule=self.schedule, workspace=ep)
+                grp.gp = None
+                grp.breeders = breed
                 if breed:
                     idx = {s.req.rid: j for j, s in enumerate(active)}
-                    gp = GPStep([s.prob for s in breed], [bf.outputs[idx[s.req.rid]] for s in breed],
-                                [s.req.seed for s in breed], generations=[s.gen for s in breed],
-                                workspace=gp_pool, **self.gp_options)
-                key = k
+                    grp.gp = GPStep([s.prob for s in breed],
+                                    [grp.bf.outputs[idx[s.req.rid]] for s in breed],
+                                    [s.req.seed for s in breed],
+                                    generations=[s.gen for s in breed], workspace=gpp,
+                                    **self.gp_options)
+                grp.key = k
+            bf = grp.bf
             bf.evaluate()
             finished = [s for s in active if s.req.kind == "evaluate" or s.gen >= s.req.generations]
             items = []
             for j, s in enumerate(active):
                 if s in finished:
-                    hl = torch.empty(bf.outputs[j].numel(), dtype=bf.outputs[j].dtype, pin_memory=True)
+                    hl = torch.empty(bf.outputs[j].numel(), dtype=bf.outputs[j].dtype,
+                                     pin_memory=True)
                     hl.copy_(bf.outputs[j], non_blocking=True)
                     snap = None
                     if s.req.kind == "fit":
-                        snap = (torch.empty(s.prob.population.shape, dtype=torch.uint8, pin_memory=True),
+                        snap = (torch.empty(s.prob.population.shape, dtype=torch.uint8,
+                                            pin_memory=True),
                                 torch.empty(s.prob.constants.shape, dtype=s.prob.constants.dtype,
                                             pin_memory=True))
                         snap[0].copy_(s.prob.population, non_blocking=True)
                         snap[1].copy_(s.prob.constants, non_blocking=True)
                     items.append((s, hl, snap))
-            if gp is not None:
-                gp.step()
+            if grp.gp is not None:
+                grp.gp.step()
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(stream)
             inflight.append((ev, items))
-            ticks += 1
-            for s in breeders:
+            steps += 1
+            for s in grp.breeders:
                 s.gen += 1
             if finished:
                 gone = {s.req.rid for s in finished}
-                active = [s for s in active if s.req.rid not in gone]
+                grp.slots = [s for s in active if s.req.rid not in gone]
             while len(inflight) > max_inflight:
                 drain_one()
+
+        while i < len(reqs) or waiting or any(g.slots for g in groups.values()) or inflight:
+            now = time.perf_counter() - t0
+            while i < len(reqs) and (reqs[i].arrival <= now or not realtime):
+                waiting.append(reqs[i])
+                i += 1
+            n_active = sum(len(g.slots) for g in groups.values())
+            while (waiting and n_active < self.max_active
+                   and (n_active == 0 or used + footprint(waiting[0]) <= self.hbm_budget)):
+                r = waiting.popleft()
+                s = self._admit(r, max(now, r.arrival) if realtime else now)
+                used += s.nbytes
+                groups.setdefault(self.cost_class(r), _Group()).slots.append(s)
+                n_active += 1
+            if n_active == 0:
+                if inflight:
+                    drain_one()
+                elif i < len(reqs) and realtime:
+                    time.sleep(max(0.0, reqs[i].arrival - (time.perf_counter() - t0)))
+                continue
+            max_active_seen = max(max_active_seen, n_active)
+            live = sorted(c for c, g in groups.items() if g.slots)
+            top = live[-1]
+            for cls in live:  # cheapest first: the quickest requests finish soonest
+                grp = groups[cls]
+                reps = min(max_steps_per_tick, 1 << min(top - cls, 30))
+                for _ in range(reps):
+                    if not grp.slots:
+                        break
+                    step(cls, grp)
             if not inflight:
                 if len(retired) > 8:
                     retired.clear()
-                eval_pool.retired.clear()
-                gp_pool.retired.clear()
+                for ep, gpp in pools.values():
+                    ep.retired.clear()
+                    gpp.retired.clear()
         while inflight:
             drain_one()
         torch.cuda.synchronize(self.device)
-        for x in retired + [gp, bf]:
-            if x is not None:
-                x.close()
-        self.stats = {"ticks": ticks, "max_active": max_active_seen,
-                      "makespan_s": time.perf_counter() - t0}
+        for g in groups.values():
+            retired.extend(x for x in (g.gp, g.bf) if x is not None)
+        for x in retired:
+            x.close()
+        self.stats = {"ticks": steps, "max_active": max_active_seen,
+                      "groups": len(groups), "makespan_s": time.perf_counter() - t0}
         return sorted(results, key=lambda r: r.rid)
 
 
