@@ -18,10 +18,13 @@
 // Since the trial gradients are overwritten unused, they are not computed here: the results are
 // the same and a line-search trial costs one fitness evaluation instead of 2K + 1.
 //
-// B200 layout: one 256-thread block per program (the reference runs ONE thread per program):
-// rows are evaluated in parallel into shared memory, then reduced in the reference's row order
-// (sequential fused multiply-adds) so that every RMSE is the reference's bit for bit; the 2K
-// finite-difference sums run in parallel, one thread per (constant, sign).
+// B200 layout: one 1024-thread block per program (the reference runs ONE thread per program):
+// rows are evaluated in parallel into shared memory (one row per thread at D <= 1024), then
+// reduced in the reference's row order (sequential fused multiply-adds, y staged in shared
+// memory) so that every RMSE is the reference's bit for bit; the 2K finite-difference sums run
+// in parallel, one thread per (constant, sign).  1024 threads rather than 256: the block owns
+// its program for the whole optimisation, so the rows are the only parallelism (64 programs x
+// 1024 rows x 10 iterations: 3.6 ms with 256 threads, 1.7 ms with 1024).
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
@@ -33,7 +36,7 @@ namespace {
 
 constexpr int kLbMaxK = 32, kLbMaxD = 1024, kLbHistory = 10, kLbStack = 64, kLbMaxL = 256,
               kLbMaxLineSearch = 20;
-constexpr int kLbThreads = 256;
+constexpr int kLbThreads = 1024;
 
 struct LbIds {
   int pad, xs, nvars, id_C, id_pi, id_e;
@@ -116,6 +119,8 @@ __global__ void __launch_bounds__(kLbThreads) lbfgs_kernel(LbArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem[];
   T* rowbuf = reinterpret_cast<T*>(smem);  // [2 * kc][D] predictions (or skipped rows)
   uint8_t* rowok = reinterpret_cast<uint8_t*>(rowbuf + (size_t)2 * a.kc * a.D);  // [2 kc][D]
+  // y staged once: the row-order sums below read it from shared memory, eight rows ahead
+  T* s_y = reinterpret_cast<T*>(rowok + ((size_t)2 * a.kc * a.D + 15) / 16 * 16);
   __shared__ uint8_t s_prog[kLbMaxL];
   __shared__ T s_pos[kLbMaxK];     // point being evaluated
   __shared__ T s_pm[2 * kLbMaxK];  // clamped +eps / -eps coordinate per chunk pair
@@ -127,6 +132,7 @@ __global__ void __launch_bounds__(kLbThreads) lbfgs_kernel(LbArgs<T> a) {
   __shared__ T s_hist[kLbHistory][kLbMaxK], y_hist[kLbHistory][kLbMaxK], rho_hist[kLbHistory];
   const int tid = threadIdx.x;
   const int K = a.K, D = (int)a.D;
+  for (int d = tid; d < D; d += blockDim.x) s_y[d] = a.y[d];
 
   for (int64_t b = blockIdx.x; b < a.B; b += gridDim.x) {
     __syncthreads();
@@ -154,8 +160,9 @@ __global__ void __launch_bounds__(kLbThreads) lbfgs_kernel(LbArgs<T> a) {
           s_f = (T)1e30;
         } else {
           T mse_sum = (T)0.0;
+#pragma unroll 8
           for (int d = 0; d < D; ++d) {
-            const T diff = rowbuf[d] - a.y[d];
+            const T diff = rowbuf[d] - s_y[d];
             mse_sum += diff * diff;
           }
           s_f = sqrtf(mse_sum / (T)D);
@@ -193,9 +200,10 @@ __global__ void __launch_bounds__(kLbThreads) lbfgs_kernel(LbArgs<T> a) {
         __syncthreads();
         if (tid < 2 * nk) {
           T mse = (T)0.0;
+#pragma unroll 8
           for (int d = 0; d < D; ++d) {
             if (!rowok[(size_t)tid * D + d]) continue;
-            const T diff = rowbuf[(size_t)tid * D + d] - a.y[d];
+            const T diff = rowbuf[(size_t)tid * D + d] - s_y[d];
             mse += diff * diff;
           }
           s_sum[tid] = sqrtf(mse / (T)D);
@@ -311,7 +319,7 @@ ws_status launch_lbfgs_typed(LbArgs<T> a, cudaStream_t stream) {
   if (kc > a.K) kc = a.K;
   if (kc < 1) kc = 1;
   a.kc = kc;
-  const size_t smem = 2 * (size_t)kc * per_pair + 16;
+  const size_t smem = 2 * (size_t)kc * per_pair + 16 + (size_t)a.D * sizeof(T) + 16;
   auto kern = lbfgs_kernel<T>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
