@@ -31,9 +31,17 @@ def dtype_code(dt: torch.dtype) -> int:
     raise RuntimeError("expected float32 or float64, got %s" % dt)
 
 
+_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+
+
 def stream_of(t: torch.Tensor) -> C.c_void_p:
     """The current torch stream on the tensor's device (launches never use the legacy
-    default stream unless it is current)."""
+    default stream unless it is current).  Read as a raw handle when torch offers it (a
+    fraction of a microsecond; building a Stream object costs a few, which shows on
+    microsecond kernels)."""
+    if _raw_stream is not None and t.is_cuda:
+        return C.c_void_p(_raw_stream(t.device.index if t.device.index is not None
+                                      else torch.cuda.current_device()))
     return C.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
 
 

@@ -35,6 +35,8 @@ unsigned blocks_for(int64_t n, int t) {
 
 // compute_population_hashes_kernel / compute_var_presence_kernel (diversity_kernels.cu:29-72,
 // 465-488); variables beyond bit 31 do not fit the int32 mask and are left out of it.
+// VEC: rows are 16-byte aligned multiples of 16 bytes and are read 16 bytes at a time.
+template <bool VEC>
 __global__ void __launch_bounds__(256) hash_kernel(const uint8_t* __restrict__ pop, int64_t B,
                                                    int L, int pad, int x0, int nv,
                                                    int64_t* __restrict__ hashes,
@@ -44,13 +46,29 @@ __global__ void __launch_bounds__(256) hash_kernel(const uint8_t* __restrict__ p
     const uint8_t* row = pop + b * L;
     uint64_t h = 0ull, p = 1ull;
     int32_t mask = 0;
-    for (int i = 0; i < L; ++i) {
-      const int t = row[i];
-      if (t == pad) break;
+    bool open = true;
+    auto take = [&](int t) {
+      if (!open || t == pad) {
+        open = false;
+        return;
+      }
       h += (uint64_t)t * p;
       p *= 31ull;
       const int v = t - x0;
       if (t >= x0 && v < nv && v < 32) mask |= (int32_t)(1u << v);
+    };
+    if (VEC) {
+      const uint4* r4 = reinterpret_cast<const uint4*>(row);
+      for (int c = 0; c < (L >> 4) && open; ++c) {
+        const uint4 w = r4[c];
+        const uint32_t words[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) take((int)((words[q] >> (8 * j)) & 0xFFu));
+      }
+    } else {
+      for (int i = 0; i < L && open; ++i) take(row[i]);
     }
     if (hashes) hashes[b] = (int64_t)h;
     if (presence) presence[b] = mask;
@@ -144,7 +162,14 @@ __device__ __forceinline__ uint64_t share_hash(const uint8_t* row, int L, int ha
   uint64_t h = 0ull;
   int lim = hash_len < L ? hash_len : L;
   if (lim > 8) lim = 8;
-  for (int i = 0; i < lim; ++i) h += (uint64_t)row[i] * w[i];
+  if (L >= 8 && ((uintptr_t)row & 7u) == 0) {  // the 8-token prefix in one load
+    const uint64_t v = *reinterpret_cast<const uint64_t*>(row);
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      if (i < lim) h += ((v >> (8 * i)) & 0xFFull) * w[i];
+  } else {
+    for (int i = 0; i < lim; ++i) h += (uint64_t)row[i] * w[i];
+  }
   h ^= h >> 16;
   h *= 0x7feb352dull;
   h ^= h >> 15;
@@ -226,8 +251,12 @@ ws_status ws_population_hashes(const uint8_t* population, int64_t B, int64_t L, 
   if (B < 0 || L < 0) return fail("negative size");
   if (B == 0) return WS_OK;
   if ((L > 0 && !population) || (!hashes && !var_presence)) return fail("null tensor pointer");
-  hash_kernel<<<blocks_for(B, 256), 256, 0, (cudaStream_t)stream>>>(
-      population, B, (int)L, pad_id, id_x_start, num_vars, hashes, var_presence);
+  if (L % 16 == 0 && ((uintptr_t)population & 15u) == 0)
+    hash_kernel<true><<<blocks_for(B, 256), 256, 0, (cudaStream_t)stream>>>(
+        population, B, (int)L, pad_id, id_x_start, num_vars, hashes, var_presence);
+  else
+    hash_kernel<false><<<blocks_for(B, 256), 256, 0, (cudaStream_t)stream>>>(
+        population, B, (int)L, pad_id, id_x_start, num_vars, hashes, var_presence);
   return after("population hash launch");
 }
 

@@ -118,23 +118,24 @@ template <typename T>
 __global__ void __launch_bounds__(256) perturb_kernel(T* __restrict__ c, int64_t B, int64_t K,
                                                       float rate, float sigma, float cmin,
                                                       float cmax, uint32_t seed) {
-  const int64_t total = B * K;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int row = total < ((int64_t)1 << 31) ? (int)((uint32_t)i / (uint32_t)K) : (int)(i / K);
-    const int col = (int)(i - (int64_t)row * K);
+  // one thread per row: the row's draw decides once whether any of its constants move
+  for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < B;
+       row += (int64_t)gridDim.x * blockDim.x) {
     const uint32_t rk = seed ^ ((uint32_t)(row + 1) * 0x9e3779b9u);
     if (unit_open(rk) >= rate) continue;
-    const uint32_t k1 = rk ^ ((uint32_t)(col + 1) * 0x85ebca6bu);
-    const uint32_t k2 = rk ^ ((uint32_t)(col + 1) * 0xc2b2ae35u);
-    const float u1 = fmaxf(unit_open(k1), 1e-7f);
-    const float u2 = unit_open(k2);
-    const float z = sqrtf(-2.0f * logf(u1)) * cosf(6.283185307179586f * u2);
-    const float v = (float)c[i];
-    const float scale = fabsf(v) * sigma + 1e-4f;
-    float nv = v + z * scale;
-    nv = fminf(fmaxf(nv, cmin), cmax);
-    c[i] = (T)nv;
+    T* cr = c + row * K;
+    for (int64_t col = 0; col < K; ++col) {
+      const uint32_t k1 = rk ^ ((uint32_t)(col + 1) * 0x85ebca6bu);
+      const uint32_t k2 = rk ^ ((uint32_t)(col + 1) * 0xc2b2ae35u);
+      const float u1 = fmaxf(unit_open(k1), 1e-7f);
+      const float u2 = unit_open(k2);
+      const float z = sqrtf(-2.0f * logf(u1)) * cosf(6.283185307179586f * u2);
+      const float v = (float)cr[col];
+      const float scale = fabsf(v) * sigma + 1e-4f;
+      float nv = v + z * scale;
+      nv = fminf(fmaxf(nv, cmin), cmax);
+      cr[col] = (T)nv;
+    }
   }
 }
 
@@ -376,7 +377,7 @@ ws_status ws_constant_perturbation(int32_t dtype, void* constants, int64_t B, in
   if (B < 0 || K < 0) return fail("negative size");
   if (B * K == 0 || rate <= 0.0f || sigma <= 0.0f) return WS_OK;
   if (!constants) return fail("null tensor pointer");
-  const unsigned g = grid_for(B * K, 256);
+  const unsigned g = grid_for(B, 256);
   if (dtype == WS_F32)
     perturb_kernel<float><<<g, 256, 0, (cudaStream_t)stream>>>(
         static_cast<float*>(constants), B, K, rate, sigma, c_min, c_max, seed);

@@ -267,6 +267,8 @@ __global__ void __launch_bounds__(kThreads) subtree_kernel(SubtreeArgs a) {
 // ---------------------------------------------------------------------------------------------
 // Tournament selection (rpn_kernels.cu:1535-1668).  OFFSETS selects the island-offset variant:
 // candidates are base + (offset % span), clamped into [0, B-1].
+constexpr int kTourFast = 8;  // tournaments up to this size keep their candidates in registers
+
 template <bool OFFSETS>
 __global__ void __launch_bounds__(256)
     tournament_kernel(const float* __restrict__ fitness, const float* __restrict__ errors,
@@ -297,6 +299,38 @@ __global__ void __launch_bounds__(256)
     if (lengths != nullptr)
       eps = (case_idx >= 0 && mad_eps != nullptr) ? mad_eps[case_idx]
                                                   : (case_idx >= 0 ? 1e-3f : 1e-9f);
+    if (T <= kTourFast) {
+      // all candidates, then all their values, then the comparisons in candidate order: two
+      // rounds of memory latency per program instead of two per candidate
+      int64_t cs[kTourFast];
+      float vals[kTourFast], lens[kTourFast];
+#pragma unroll
+      for (int k = 0; k < kTourFast; ++k)
+        if (k < T) cs[k] = candidate(k);
+#pragma unroll
+      for (int k = 0; k < kTourFast; ++k) {
+        if (k < T) {
+          vals[k] = by_case ? errors[cs[k] * n_data + case_idx] : fitness[cs[k]];
+          lens[k] = lengths != nullptr ? lengths[cs[k]] : 1000000.0f;
+        }
+      }
+      int64_t best = cs[0];
+      float best_val = vals[0], best_len = lens[0];
+#pragma unroll
+      for (int k = 1; k < kTourFast; ++k) {
+        if (k >= T) break;
+        bool improve = vals[k] < best_val;
+        if (!improve && lengths != nullptr)
+          improve = fabsf(vals[k] - best_val) < eps && lens[k] < best_len;
+        if (improve) {
+          best_val = vals[k];
+          best = cs[k];
+          best_len = lens[k];
+        }
+      }
+      selected[idx] = best;
+      continue;
+    }
     int64_t best = candidate(0);
     float best_val = by_case ? errors[best * n_data + case_idx] : fitness[best];
     float best_len = lengths != nullptr ? lengths[best] : 1000000.0f;
@@ -379,7 +413,8 @@ ws_status launch_tournament(const float* fitness, int64_t B, const float* errors
                             int island_size, int n_islands, int64_t* selected,
                             cudaStream_t stream) {
   if (B == 0) return WS_OK;
-  const int grid = grid_for(B, 256, 8);
+  // one program per thread: every program's gathers are in flight at once
+  const int grid = grid_for(B, 256, 64);
   if (rand_off != nullptr)
     tournament_kernel<true><<<grid, 256, 0, stream>>>(fitness, errors, nullptr, rand_off,
                                                       rand_cases, selected, lengths, mad_eps, B, T,
