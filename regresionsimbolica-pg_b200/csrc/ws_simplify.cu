@@ -18,8 +18,16 @@
 //     then shorter);  a x * b x * + -> a b + x * (and x a * x b * +);  x (x y +) + and
 //     x (y x +) + -> 2 x * y + (single-token x);  two literal operands fold to a literal;
 //   compact;  stop when nothing changed.
-// One thread rewrites one program (the rules are sequential within a program); the program
-// lives in thread-local memory as in the reference, the literal table in shared memory.
+// One thread rewrites one program (the rules are sequential within a program).  The working
+// program lives in shared memory as 16-bit tokens, position-major across the block's threads
+// (position i of thread t at [i * blockDim + t]: a warp at one position reads one 64-byte line),
+// so the rule scans run at shared-memory latency; the reference keeps 2 x 256 int64 per thread in
+// local memory, which at a few hundred threads per SM spills out of L1 into L2.  A row holding a
+// token outside the 16-bit range (possible only for tokens outside the vocabulary) is rewritten
+// from a thread-local int64 copy instead, with the same code.  The operand swap of + and * and
+// the y move of the x (x y +) + rule are done in place (a rotation by three reversals; a
+// downward copy), which gives the same program as the reference's copy through a scratch row.
+// Literal table and arity table in shared memory.
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
@@ -55,9 +63,21 @@ struct SimplifyArgs {
   SimplifyIds id;
 };
 
+// Position i of a thread's working program: 16-bit tokens in shared memory ...
+struct SmemRow {
+  int16_t* base;
+  int stride;
+  __device__ int16_t& operator[](int i) const { return base[i * stride]; }
+};
+// ... or int64 tokens in thread-local memory (rows with tokens outside the 16-bit range).
+struct LocalRow {
+  int64_t* base;
+  __device__ int64_t& operator[](int i) const { return base[i]; }
+};
+
+template <class Row>
 struct Program {
-  int64_t f[kMaxFormula];
-  int64_t scratch[kMaxFormula];  // operand copy of the swap / the associative rewrite
+  Row f;
   int n;  // positions considered (min(L, 256))
   const int32_t* ar;
   int max_id;
@@ -81,8 +101,10 @@ struct Program {
 
   __device__ void compact() {
     int w = 0;
-    for (int r = 0; r < n; ++r)
-      if (f[r] != kPad) f[w++] = f[r];
+    for (int r = 0; r < n; ++r) {
+      const int64_t t = f[r];
+      if (t != kPad) f[w++] = t;
+    }
     for (int i = w; i < n; ++i) f[i] = kPad;
   }
 
@@ -94,6 +116,21 @@ struct Program {
     for (int k = 0; k < len; ++k)
       if (f[a + k] != f[b + k]) return false;
     return true;
+  }
+
+  __device__ void reverse(int lo, int hi) {  // f[lo..hi] reversed
+    for (; lo < hi; ++lo, --hi) {
+      const int64_t t = f[lo];
+      f[lo] = f[hi];
+      f[hi] = t;
+    }
+  }
+
+  // f[s1..s2-1] f[s2..e-1]  ->  f[s2..e-1] f[s1..s2-1]
+  __device__ void swap_segments(int s1, int s2, int e) {
+    reverse(s1, s2 - 1);
+    reverse(s2, e - 1);
+    reverse(s1, e - 1);
   }
 };
 
@@ -144,10 +181,11 @@ __device__ float fold_binary(int64_t op, float v1, float v2, const SimplifyIds& 
 }
 
 // Phase 1 at position j (simplify_kernels.cu:144-251).  True when a rule rewrote.
-__device__ bool phase1_at(Program& p, int j, const SimplifyArgs& a, const int64_t* lit_ids,
+template <class Row>
+__device__ bool phase1_at(Program<Row>& p, int j, const SimplifyArgs& a, const int64_t* lit_ids,
                           const float* lit_vals, int n_lits) {
   const SimplifyIds& o = a.id;
-  int64_t* f = p.f;
+  const Row f = p.f;
   const int64_t tok = f[j];
   const int64_t prev = f[j - 1];
   if (tok == o.op_neg && prev == o.op_neg) {
@@ -159,7 +197,7 @@ __device__ bool phase1_at(Program& p, int j, const SimplifyArgs& a, const int64_
     f[j - 1] = f[j - 2] = kPad;
     return true;
   }
-  if (tok > 0 && tok < a.max_id && a.ar[tok] == 1 && prev != kPad) {
+  if (tok > 0 && tok < a.max_id && p.ar[tok] == 1 && prev != kPad) {
     const bool z = prev == o.id_0, one = prev == o.id_1, two = prev == o.id_2;
     const bool to_zero = (z && (tok == o.op_sin || tok == o.op_tan || tok == o.op_abs)) ||
                          (one && (tok == o.op_log || tok == o.op_lgamma)) ||
@@ -207,10 +245,11 @@ __device__ bool phase1_at(Program& p, int j, const SimplifyArgs& a, const int64_
 }
 
 // Phase 2 at binary position j (simplify_kernels.cu:257-591).
-__device__ bool phase2_at(Program& p, int j, const SimplifyArgs& a, const int64_t* lit_ids,
+template <class Row>
+__device__ bool phase2_at(Program<Row>& p, int j, const SimplifyArgs& a, const int64_t* lit_ids,
                           const float* lit_vals, int n_lits) {
   const SimplifyIds& o = a.id;
-  int64_t* f = p.f;
+  const Row f = p.f;
   const int64_t op = f[j];
   const int s2 = p.subtree_start(j - 1);
   const int s1 = p.subtree_start(s2 - 1);
@@ -263,10 +302,7 @@ __device__ bool phase2_at(Program& p, int j, const SimplifyArgs& a, const int64_
         f[s2 - 1] = arg2;
         f[j - 1] = arg1;
       } else {
-        int64_t* tmp = p.scratch;
-        for (int k = 0; k < len1; ++k) tmp[k] = f[s1 + k];
-        for (int k = 0; k < len2; ++k) f[s1 + k] = f[s2 + k];
-        for (int k = 0; k < len1; ++k) f[s1 + len2 + k] = tmp[k];
+        p.swap_segments(s1, s2, j);
       }
     }
   }
@@ -274,7 +310,7 @@ __device__ bool phase2_at(Program& p, int j, const SimplifyArgs& a, const int64_
   if (op == o.op_plus && j >= 6) {
     const int64_t v1 = f[j - 1], v2 = f[j - 2], v3 = f[j - 3], v4 = f[j - 4], v5 = f[j - 5],
                   v6 = f[j - 6];
-    auto term = [&](int64_t t) { return t >= 0 && t < a.max_id && a.ar[t] == 0; };
+    auto term = [&](int64_t t) { return t >= 0 && t < a.max_id && p.ar[t] == 0; };
     if (f[j] == o.op_plus && v1 == o.op_mult && v4 == o.op_mult) {
       int64_t ka = 0, kb = 0, kx = 0;
       bool hit = false;
@@ -319,14 +355,14 @@ __device__ bool phase2_at(Program& p, int j, const SimplifyArgs& a, const int64_
             }
           }
           if (y_from >= 0 && 4 + y_len <= j - s_o1 + 1) {
+            // y starts at s_o1 + 1 or s_o1 + 2 and moves up to s_o1 + 3: copied downwards, every
+            // source token is read before its position is written
             const int64_t x_tok = f[s_o1];
-            int64_t* ybuf = p.scratch;
-            for (int k = 0; k < y_len; ++k) ybuf[k] = f[y_from + k];
-            int w = s_o1;
-            f[w++] = o.id_2;
-            f[w++] = x_tok;
-            f[w++] = o.op_mult;
-            for (int k = 0; k < y_len; ++k) f[w++] = ybuf[k];
+            for (int k = y_len - 1; k >= 0; --k) f[s_o1 + 3 + k] = f[y_from + k];
+            f[s_o1] = o.id_2;
+            f[s_o1 + 1] = x_tok;
+            f[s_o1 + 2] = o.op_mult;
+            int w = s_o1 + 3 + y_len;
             f[w++] = o.op_plus;
             p.blank(w, j);
             return true;
@@ -351,39 +387,73 @@ __device__ bool phase2_at(Program& p, int j, const SimplifyArgs& a, const int64_
   return false;
 }
 
-__global__ void __launch_bounds__(128) simplify_kernel(SimplifyArgs a) {
+template <class Row>
+__device__ void simplify_program(Program<Row>& p, const SimplifyArgs& a, const int64_t* lit_ids,
+                                 const float* lit_vals, int n_lits) {
+  for (int pass = 0; pass < a.max_passes; ++pass) {
+    bool changed = false;
+    for (int j = 1; j < p.n; ++j) {
+      if (p.f[j] == kPad) continue;
+      if (phase1_at(p, j, a, lit_ids, lit_vals, n_lits)) changed = true;
+    }
+    p.compact();
+    for (int j = 2; j < p.n; ++j) {
+      const int64_t op = p.f[j];
+      if (op == kPad || op < 0 || op >= a.max_id || p.ar[op] != 2) continue;
+      if (phase2_at(p, j, a, lit_ids, lit_vals, n_lits)) changed = true;
+    }
+    p.compact();
+    if (!changed) break;
+  }
+}
+
+constexpr int kSimpThreads = 128;
+constexpr int kStagedArities = 1024;  // arity tables up to this length are read from shared memory
+
+// narrow != 0: every id fits a 16-bit token and dynamic shared memory holds n x blockDim of them.
+__global__ void __launch_bounds__(kSimpThreads) simplify_kernel(SimplifyArgs a, int narrow) {
+  extern __shared__ int16_t s_rows[];
   __shared__ int64_t s_lit_ids[kMaxLits];
   __shared__ float s_lit_vals[kMaxLits];
+  __shared__ int32_t s_ar[kStagedArities];
   const int n_lits = a.n_lits < kMaxLits ? a.n_lits : kMaxLits;
+  bool lits_fit = true;
   for (int i = threadIdx.x; i < n_lits; i += blockDim.x) {
-    s_lit_ids[i] = a.lit_ids[i];
+    const int64_t id = a.lit_ids[i];
+    s_lit_ids[i] = id;
     s_lit_vals[i] = a.lit_vals[i];
+    lits_fit = lits_fit && id == (int64_t)(int16_t)id;
   }
-  __syncthreads();
+  const bool staged_ar = a.max_id <= kStagedArities;
+  if (staged_ar)
+    for (int i = threadIdx.x; i < a.max_id; i += blockDim.x) s_ar[i] = a.ar[i];
+  const bool use_smem = __syncthreads_and(lits_fit) && narrow != 0;
+  const int32_t* ar = staged_ar ? s_ar : a.ar;
+  const int n = a.L < kMaxFormula ? a.L : kMaxFormula;
   for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < a.B;
        b += (int64_t)gridDim.x * blockDim.x) {
-    Program p;
-    p.ar = a.ar;
-    p.max_id = a.max_id;
-    p.n = a.L < kMaxFormula ? a.L : kMaxFormula;
     int64_t* row = a.pop + b * a.L;
-    for (int i = 0; i < p.n; ++i) p.f[i] = row[i];
-    for (int pass = 0; pass < a.max_passes; ++pass) {
-      bool changed = false;
-      for (int j = 1; j < p.n; ++j) {
-        if (p.f[j] == kPad) continue;
-        if (phase1_at(p, j, a, s_lit_ids, s_lit_vals, n_lits)) changed = true;
+    bool fits = use_smem;
+    if (fits) {
+      const SmemRow sr{s_rows + threadIdx.x, (int)blockDim.x};
+      for (int i = 0; i < n; ++i) {
+        const int64_t t = row[i];
+        sr[i] = (int16_t)t;
+        fits = fits && t == (int64_t)(int16_t)t;
       }
-      p.compact();
-      for (int j = 2; j < p.n; ++j) {
-        const int64_t op = p.f[j];
-        if (op == kPad || op < 0 || op >= a.max_id || a.ar[op] != 2) continue;
-        if (phase2_at(p, j, a, s_lit_ids, s_lit_vals, n_lits)) changed = true;
+      if (fits) {
+        Program<SmemRow> p{sr, n, ar, a.max_id};
+        simplify_program(p, a, s_lit_ids, s_lit_vals, n_lits);
+        for (int i = 0; i < n; ++i) row[i] = sr[i];
       }
-      p.compact();
-      if (!changed) break;
     }
-    for (int i = 0; i < p.n; ++i) row[i] = p.f[i];
+    if (!fits) {
+      int64_t loc[kMaxFormula];
+      for (int i = 0; i < n; ++i) loc[i] = row[i];
+      Program<LocalRow> p{LocalRow{loc}, n, ar, a.max_id};
+      simplify_program(p, a, s_lit_ids, s_lit_vals, n_lits);
+      for (int i = 0; i < n; ++i) row[i] = loc[i];
+    }
   }
 }
 
@@ -421,10 +491,24 @@ extern "C" ws_status ws_simplify_batch(int64_t* population, int64_t B, int64_t L
                      ids->op_sqrt,  ids->op_abs,   ids->op_gamma, ids->op_lgamma, ids->op_floor,
                      ids->op_ceil,  ids->op_sign,  ids->id_0,     ids->id_1,     ids->id_2,
                      ids->id_3,     ids->id_4,     ids->id_5,     ids->id_6};
-  const int64_t want = (B + 127) / 128;
+  // 16-bit working rows when every id the rules write fits one (the row's own tokens are checked
+  // per row in the kernel, the literal ids per block)
+  const int32_t* idv = &ids->op_plus;
+  bool narrow = max_id <= INT16_MAX;
+  for (size_t i = 0; i < sizeof(ws_simplify_ids) / sizeof(int32_t); ++i)
+    narrow = narrow && idv[i] >= INT16_MIN && idv[i] <= INT16_MAX;
+  const int n = (int)(L < kMaxFormula ? L : kMaxFormula);
+  const size_t smem = narrow ? (size_t)n * kSimpThreads * sizeof(int16_t) : 0;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(simplify_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return fail_cuda(e, "simplify_batch");
+  }
+  const int64_t want = (B + kSimpThreads - 1) / kSimpThreads;
   const int64_t cap = (int64_t)device_info().sm_count * 16;
   const int grid = (int)(want < cap ? want : cap);
-  simplify_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(a);
+  simplify_kernel<<<grid, kSimpThreads, smem, static_cast<cudaStream_t>(stream)>>>(
+      a, narrow ? 1 : 0);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? WS_OK : fail_cuda(e, "simplify_batch");
 }

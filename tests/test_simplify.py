@@ -138,3 +138,36 @@ def test_wrapper_rules():
     v_in = validate_population(P, ar, 0, "stack")
     v_out = validate_population(out, ar, 0, "stack")
     assert bool((v_out | ~v_in).all())
+
+
+@gpu
+def test_wide_tokens_take_the_same_rules():
+    """A row holding a token outside the 16-bit range is rewritten from an int64 copy: the same
+    rows with an out-of-vocabulary token of 200 (16-bit path) or 40000 (int64 path) at the same
+    positions simplify identically, and both agree with the oracle."""
+    from warpsymbolic_b200 import rpn_cuda_native as ours
+    g = tl.GPUGrammar(num_variables=3, operators=tl.ALL_OPERATORS)
+    B, L = 3000, 48
+    pop = literal_rich(g, B, L, 5)
+    rng = np.random.default_rng(6)
+    rows = rng.random(B) < 0.5
+    cols = rng.integers(0, L, size=B)
+    narrow, wide = pop.copy(), pop.copy()
+    narrow[rows, cols[rows]] = 200
+    wide[rows, cols[rows]] = 40000
+    wide[3, 0] = -(1 << 40)   # and one far outside
+    narrow[3, 0] = -7
+    ar, vt, li, lv, ids = _tables(g)
+    args = [torch.from_numpy(a).to(DEV) for a in (ar, vt, li, lv)]
+    outs = []
+    for p in (narrow, wide):
+        t = torch.from_numpy(p.copy()).to(DEV)
+        ours.simplify_batch(t, *args, 3, *[int(v) for v in ids])
+        outs.append(t.cpu().numpy())
+    back = outs[1].copy()
+    back[back == 40000] = 200
+    back[back == -(1 << 40)] = -7
+    assert np.array_equal(outs[0], back)
+    assert (outs[1] != wide).any(axis=1).mean() > 0.3
+    want = _simplify_oracle(g, wide, 3)
+    assert (want == outs[1]).all(axis=1).mean() > 0.999
