@@ -4,7 +4,6 @@ rounding over rows), at the torch.autograd.Function boundary with gradcheck, and
 constant-fitting shape (65,536 programs x 16,384 rows) with timing against the reference."""
 import json
 import math
-import os
 
 import numpy as np
 import pytest
@@ -283,8 +282,5 @@ def test_constant_fitting_shape_speed_vs_reference():
            "reference_ms": times["reference"], "speedup": times["reference"] / times["ours"],
            "ours_node_evals_per_s": n_tok * D / (times["ours"] / 1e3)}
     print(json.dumps(res))
-    out_dir = os.path.join(tl.REPO, "gpurun_out")
-    if os.path.isdir(out_dir):
-        with open(os.path.join(out_dir, "backward_speed.json"), "w") as f:
-            json.dump(res, f)
+    tl.write_report("backward_speed.json", res)
     assert times["ours"] < times["reference"]

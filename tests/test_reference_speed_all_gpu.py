@@ -2,9 +2,7 @@
 inputs (B200, CUDA events, median of 5 after 2 warm-up calls).  Records the table in
 the output folder's reference_speed_all.json (when that folder exists) and asserts that no
 export is slower than the reference's by more than timing noise."""
-import json
 import math
-import os
 import statistics
 
 import numpy as np
@@ -184,9 +182,7 @@ def test_every_export_matches_or_beats_the_reference():
         r = _time(make(ref))
         o = _time(make(ours))
         table.append({"kernel": name, "reference_ms": r, "ours_ms": o, "speedup": r / o})
-    if os.path.isdir("gpurun_out"):
-        with open(os.path.join("gpurun_out", "reference_speed_all.json"), "w") as f:
-            json.dump(table, f, indent=1)
+    tl.write_report("reference_speed_all.json", table)
     # microsecond kernels carry a few microseconds of host wrapper time between the events on
     # both sides: flag only what is clearly slower
     slow = [t for t in table if t["speedup"] < 0.8]

@@ -5,10 +5,9 @@ classic path: rpn_eval_kernel writes [B, D] predictions / stack depths / error b
 reductions (evaluation.py:128-198), chunked so that B*D < 2^31.  The test times that path and
 ours (one eval_fitness launch) on the same 4,096-program subset, checks the results agree, and
 requires ours to be faster.  The measured numbers are printed (pytest -s) and written to
-gpurun_out/reference_speed.json when that directory exists.
+$WS_REPORT_DIR/reference_speed.json when that variable names a directory.
 """
 import json
-import os
 
 import numpy as np
 import pytest
@@ -63,8 +62,5 @@ def test_scale_workload_speed_vs_reference_classic_path():
            "ours_node_evals_per_s": evals / (t_ours / 1e3),
            "reference_node_evals_per_s": evals / (t_ref / 1e3), "speedup": t_ref / t_ours}
     print(json.dumps(res))
-    out_dir = os.path.join(tl.REPO, "gpurun_out")
-    if os.path.isdir(out_dir):
-        with open(os.path.join(out_dir, "reference_speed.json"), "w") as f:
-            json.dump(res, f)
+    tl.write_report("reference_speed.json", res)
     assert t_ours < t_ref

@@ -30,6 +30,16 @@ ALL_OPERATORS = ('+', '-', '*', '/', 'pow', '%', 'sin', 'cos', 'tan', 'log', 'ex
                  'gamma', 'lgamma', 'asin', 'acos', 'atan', 'floor', 'ceil', 'sign', 'sqrt', 'abs')
 
 
+def write_report(name: str, obj) -> None:
+    """Writes a measurement table as JSON to $WS_REPORT_DIR/<name> when that variable names a
+    directory (nothing otherwise)."""
+    import json
+    out_dir = os.environ.get("WS_REPORT_DIR", "")
+    if out_dir and os.path.isdir(out_dir):
+        with open(os.path.join(out_dir, name), "w") as f:
+            json.dump(obj, f, indent=1)
+
+
 def token_map(g: GPUGrammar) -> N.TokenMap:
     return N.TokenMap.from_args(*g.scalar_ids(), pi_val=PI_VAL, e_val=E_VAL)
 
