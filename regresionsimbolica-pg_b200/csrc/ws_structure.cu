@@ -299,55 +299,76 @@ __global__ void __launch_bounds__(256)
     if (lengths != nullptr)
       eps = (case_idx >= 0 && mad_eps != nullptr) ? mad_eps[case_idx]
                                                   : (case_idx >= 0 ? 1e-3f : 1e-9f);
+    // A candidate's length only matters on a tie (|val - best_val| < eps), so lengths are read
+    // there alone: the incumbent's once, then the challenger's.  The comparisons are the
+    // reference's, in candidate order, so the winner is the same.
+    float best_len = 0.0f;
+    bool best_len_known = false;
+    int64_t best = -1;
+    float best_val = 0.0f;
+#define WS_CHALLENGE(C_, VAL_)                                                     \
+  {                                                                                \
+    const int64_t c_ = (C_);                                                       \
+    const float val_ = (VAL_);                                                     \
+    bool improve = val_ < best_val;                                                \
+    float len = 0.0f;                                                              \
+    const bool tie = !improve && lengths != nullptr && fabsf(val_ - best_val) < eps; \
+    if (tie) {                                                                     \
+      if (!best_len_known) best_len = lengths[best];                               \
+      best_len_known = true;                                                       \
+      len = lengths[c_];                                                           \
+      improve = len < best_len;                                                    \
+    }                                                                              \
+    if (improve) {                                                                 \
+      best_val = val_;                                                             \
+      best = c_;                                                                   \
+      best_len = len;                                                              \
+      best_len_known = tie;                                                        \
+    }                                                                              \
+  }
     if (T <= kTourFast) {
       // all candidates, then all their values, then the comparisons in candidate order: two
       // rounds of memory latency per program instead of two per candidate
       int64_t cs[kTourFast];
-      float vals[kTourFast], lens[kTourFast];
+      float vals[kTourFast];
+      if (!OFFSETS && (T % 2) == 0 && (reinterpret_cast<uintptr_t>(rand_idx) & 15) == 0) {
+        // even T on a 16-byte aligned base: every row of rand_idx starts on a 16-byte boundary
+        const longlong2* row = reinterpret_cast<const longlong2*>(rand_idx + idx * T);
+#pragma unroll
+        for (int k = 0; k < kTourFast; k += 2) {
+          if (k < T) {
+            const longlong2 v = row[k / 2];
+            cs[k] = v.x;
+            cs[k + 1] = v.y;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < kTourFast; ++k)
+          if (k < T) cs[k] = candidate(k);
+      }
 #pragma unroll
       for (int k = 0; k < kTourFast; ++k)
-        if (k < T) cs[k] = candidate(k);
-#pragma unroll
-      for (int k = 0; k < kTourFast; ++k) {
-        if (k < T) {
-          vals[k] = by_case ? errors[cs[k] * n_data + case_idx] : fitness[cs[k]];
-          lens[k] = lengths != nullptr ? lengths[cs[k]] : 1000000.0f;
-        }
-      }
-      int64_t best = cs[0];
-      float best_val = vals[0], best_len = lens[0];
+        if (k < T) vals[k] = by_case ? errors[cs[k] * n_data + case_idx] : fitness[cs[k]];
+      best = cs[0];
+      best_val = vals[0];
 #pragma unroll
       for (int k = 1; k < kTourFast; ++k) {
         if (k >= T) break;
-        bool improve = vals[k] < best_val;
-        if (!improve && lengths != nullptr)
-          improve = fabsf(vals[k] - best_val) < eps && lens[k] < best_len;
-        if (improve) {
-          best_val = vals[k];
-          best = cs[k];
-          best_len = lens[k];
-        }
+        WS_CHALLENGE(cs[k], vals[k]);
       }
       selected[idx] = best;
       continue;
     }
-    int64_t best = candidate(0);
-    float best_val = by_case ? errors[best * n_data + case_idx] : fitness[best];
-    float best_len = lengths != nullptr ? lengths[best] : 1000000.0f;
+    best = candidate(0);
+    best_val = by_case ? errors[best * n_data + case_idx] : fitness[best];
     for (int64_t k = 1; k < T; ++k) {
       const int64_t c = candidate(k);
-      const float val = by_case ? errors[c * n_data + case_idx] : fitness[c];
-      const float len = lengths != nullptr ? lengths[c] : 1000000.0f;
-      bool improve = val < best_val;
-      if (!improve && lengths != nullptr) improve = fabsf(val - best_val) < eps && len < best_len;
-      if (improve) {
-        best_val = val;
-        best = c;
-        best_len = len;
-      }
+      WS_CHALLENGE(c, by_case ? errors[c * n_data + case_idx] : fitness[c]);
     }
     selected[idx] = best;
   }
+#undef WS_CHALLENGE
 }
 
 int grid_for(int64_t units, int threads, int per_sm) {
