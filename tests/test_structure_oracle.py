@@ -106,3 +106,23 @@ def test_rules_on_hand_written_rows():
     pre = O.subtree_starts(rows.astype(np.int64), ar)
     assert pre[0].tolist() == [0, 1, 0, 0, -1, -1]
     assert pre[1].tolist() == [0, 1, -1, 3, -1, -1]  # binary at 3: both child lengths are 0
+
+
+def test_tournament_tie_rules_on_hand_written_cases():
+    """Known answers for the winner rule of rpn_kernels.cu:1535-1668: a strictly lower value
+    wins; within the tie epsilon (1e-9 without a case, 1e-3 with one, mad_eps[case] when given)
+    the shorter program wins, but only when lengths are given; a NaN never displaces the
+    incumbent, and a NaN incumbent is never displaced."""
+    fit = np.array([1.0, 1.0, 0.5, 0.5, np.nan, 2.0], dtype=np.float32)
+    lens = np.array([10, 5, 8, 3, 1, 1], dtype=np.float32)
+    cand = np.array([[0, 1, 2, 3], [3, 2, 0, 1], [4, 5, 0, 1], [0, 4, 5, 2]], dtype=np.int64)
+    assert O.tournament(fit, cand, lengths=lens).tolist() == [3, 3, 4, 2]
+    assert O.tournament(fit, cand).tolist() == [2, 3, 4, 2]
+    # by case: values from errors[:, case]; ties within 1e-3, or within mad_eps[case]
+    errs = np.array([[1.0], [1.0004], [0.9], [0.9002], [3.0], [3.0]], dtype=np.float32)
+    cases = np.zeros(2, dtype=np.int32)
+    cand2 = np.array([[0, 1, 2, 3], [1, 0, 3, 2]], dtype=np.int64)
+    fit2 = fit[:2]
+    assert O.tournament(fit2, cand2, errors=errs, cases=cases, lengths=lens).tolist() == [3, 2]
+    assert O.tournament(fit2, cand2, errors=errs, cases=cases, lengths=lens,
+                        mad_eps=np.array([1e-5], dtype=np.float32)).tolist() == [2, 2]
