@@ -167,6 +167,36 @@ def test_tournament_bit_exact(B, T_, opts):
     assert np.array_equal(out.cpu().numpy(), want)
 
 
+def test_tournament_tie_rules_on_hand_written_cases():
+    """The tie rules' known answers (strict win, shorter on a tie only with lengths, NaN
+    incumbent kept, case and MAD epsilons) through the drop-in, on the 16-byte candidate path
+    (T = 4) and the scalar one (T = 3)."""
+    from warpsymbolic_b200 import rpn_cuda_native as ours
+    fit = np.array([1.0, 1.0, 0.5, 0.5, np.nan, 2.0], dtype=np.float32)
+    lens = np.array([10, 5, 8, 3, 1, 1], dtype=np.float32)
+    errs = np.array([[1.0], [1.0004], [0.9], [0.9002], [3.0], [3.0]], dtype=np.float32)
+    e0 = torch.empty(0, dtype=torch.float32, device=DEV)
+    i0 = torch.empty(0, dtype=torch.int32, device=DEV)
+
+    def run(cand, errors=None, cases=None, lengths=None, mad=None):
+        out = torch.empty(len(cand), dtype=torch.int64, device=DEV)
+        ours.tournament_selection(T(fit[:len(cand)] if errors is not None else fit),
+                                  T(errors) if errors is not None else e0, T(cand),
+                                  T(cases) if cases is not None else i0, out,
+                                  T(lengths) if lengths is not None else e0,
+                                  T(mad) if mad is not None else e0)
+        return out.cpu().tolist()
+
+    cand = np.array([[0, 1, 2, 3], [3, 2, 0, 1], [4, 5, 0, 1], [0, 4, 5, 2]], dtype=np.int64)
+    assert run(cand, lengths=lens) == [3, 3, 4, 2]
+    assert run(cand) == [2, 3, 4, 2]
+    assert run(np.ascontiguousarray(cand[:, 1:]), lengths=lens) == [3, 2, 1, 4]
+    cand2 = np.array([[0, 1, 2, 3], [1, 0, 3, 2]], dtype=np.int64)
+    cases = np.zeros(2, dtype=np.int32)
+    assert run(cand2, errs, cases, lens) == [3, 2]
+    assert run(cand2, errs, cases, lens, np.array([1e-5], dtype=np.float32)) == [2, 2]
+
+
 @pytest.mark.parametrize("island_size,n_islands", [(512, 8), (100, 41), (1, 4096), (0, 3),
                                                    (4096, 1), (700, 6)])
 def test_island_offset_tournament_bit_exact(island_size, n_islands):
