@@ -49,14 +49,17 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--config", default="eval-scale",
-                    choices=["eval-scale", "batched", "serving", "kernels", "constopt"],
+                    choices=["eval-scale", "batched", "serving", "kernels", "constopt", "c1"],
                     help="eval-scale: the evaluation-only scale test (default); batched: 256 "
                          "uneven problems scored by one graph-replayed launch per generation; "
                          "serving: a Poisson stream of fit/evaluate requests, continuously "
                          "batched, against one request at a time; kernels: every other kernel "
                          "of the library on its own workload, timed against its roofline; "
                          "constopt: PSO then per-program L-BFGS on 65,536 programs x 16,384 "
-                         "rows")
+                         "rows; c1: the reference's own estimator and engine fitting the "
+                         "plain-method workload (1024x2 rows, population 1024, 20 "
+                         "generations), on this library's drop-in (--impl ours) or on the "
+                         "reference extension (--impl reference)")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="kernels: fraction of the default sizes (smaller cases for profiling)")
     ap.add_argument("--requests", type=int, default=8)
@@ -312,7 +315,7 @@ def run_ours(args):
             "unit": "T node-evals/s (1 FP32 lane-op per node-eval)", "frac": achieved / fp32_peak,
             "traffic": traffic_full,
             "traffic_note": "ncu dram read+write of one launch on 65,536 programs, scaled x16 "
-                            "to the full launch (per-program traffic); profiles/fitness_kernel_c2.md",
+                            "to the full launch (per-program traffic)",
             "kernel": "ws::fitness_kernel<float, 16, 0> (evaluate-only launches)",
             "kernel_ms": statistics.mean(kern_ms),
             "kernel_share_of_step": statistics.mean(kern_ms) / (1e3 * t_total / args.steps),
@@ -970,8 +973,116 @@ def run_kernels(args):
     print(json.dumps({"config": "kernels", "kernels": len(out)}), flush=True)
 
 
+def run_plain(args):
+    """The reference's WarpSymbolicRegressor.fit -> TensorGeneticEngine, unmodified, on the
+    plain-method workload, with `rpn_cuda_native` resolved to this library's drop-in (--impl
+    ours) or to the reference extension built from its sources (--impl reference).  A step is
+    one fit of 20 generations, timed by wall clock with the device synchronised on both sides
+    (the engine is host-driven: its generations interleave Python work and launches); the
+    population does not shard, so N > 1 runs N independent replicas."""
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    impl = args.impl
+    ref_pkg = os.path.join(REPO, "baseline", "_ref")
+    metric = "plain-method generations/s (reference engine, 1024x2 rows, population 1024)"
+    unit = "generations/s"
+    if not os.path.isdir(os.path.join(ref_pkg, "warpsymbolic")):
+        if rank == 0:
+            print(json.dumps({"impl": impl, "config": "c1", "unavailable":
+                              "the reference package is not installed in baseline/_ref"}))
+        return
+    if impl == "reference":
+        import glob
+        hits = glob.glob(os.path.join(REPO, "oracle", "_ref", "fastmath", "rpn_cuda_native*.so"))
+        if not hits:
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "config": "c1", "unavailable":
+                                  "the reference extension is not built (oracle/build_ref.sh)"}))
+            return
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    entry.load_package()
+    from warpsymbolic_b200 import reference_engine as RE
+    mod = RE.load_dropin() if impl == "ours" else RE.load_extension(hits[0])
+    runner = RE.PlainMethodRunner(mod, ref_pkg, keep_generations=False)
+    for _ in range(max(args.warmup, 3)):
+        res = runner.fit()
+        if res.engine_error is not None:
+            raise RuntimeError("engine failed: %s" % res.engine_error)
+    runner.reset_records()
+    fits = []
+    with ClockSampler(local) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            fits.append(runner.fit())
+        torch.cuda.synchronize(dev)
+        wall = time.perf_counter() - w0
+    if any(r.engine_error is not None or r.errors for r in fits):
+        raise RuntimeError("engine failed: %s" % [(r.engine_error, r.errors) for r in fits])
+    t_total = sum(r.seconds for r in fits)
+    if world > 1:
+        tt = torch.tensor([t_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_total = float(tt.item())
+    gens = sum(r.generations_run for r in fits)
+    value = gens * world / t_total
+    per_gen = [1e3 * g for r in fits for g in r.generation_seconds]
+    calls = dict(runner.rec.calls)
+    n_calls = sum(calls.values())
+    rows, nvars = runner.X.shape
+    h2d = runner.X.size * 4 + runner.y.size * 4
+    if rank == 0:
+        line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world,
+                "steps": args.steps, "warmup": max(args.warmup, 3),
+                "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded): X ~ U[-3,3]^(1024x2), y = x0^2 + 1.5 sin(x1) + "
+                        "N(0, 0.01^2)",
+                "config": {"workload": "plain method: WarpSymbolicRegressor.fit, population "
+                                       "1024, max 30 tokens, 20 generations, tournament 4, one "
+                                       "island, no holdout, protected evaluation",
+                           "step": "one fit (20 generations), wall clock, device synced",
+                           "native_module": "drop-in (libwarpsym.so)" if impl == "ours"
+                           else "reference extension built from its sources",
+                           "parallelism": "replicas x%d" % world,
+                           "l2": "inputs 12 KB (L2-resident by design of the workload)"},
+                "ms_per_generation": {"median": statistics.median(per_gen),
+                                      "mean": statistics.mean(per_gen),
+                                      "max": max(per_gen)},
+                "fit_seconds": [r.seconds for r in fits],
+                "final_formula": fits[-1].formula, "best_rmse": fits[-1].best_rmse,
+                "native_calls": calls,
+                "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": None,
+                        "note": "the step is already end to end: host arrays into the "
+                                "estimator, the formula string out"},
+                "clocks": clk.summary(), "wall_s_timed_region": wall}
+        if impl == "ours":
+            # every native call launches at least one of this library's kernels
+            line["gpu_launches"] = n_calls
+            line["gpu_launches_note"] = "drop-in calls in the timed region (a lower bound)"
+        else:
+            line["impl"] = "reference"
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
+    if args.config == "c1":
+        run_plain(args)
+        return
     if args.config == "kernels":
         run_kernels(args)
         return

@@ -8,9 +8,9 @@
 #   oracle/_ref/fastmath/  -- the reference's shipped nvcc flags (-O3 --use_fast_math)
 #   oracle/_ref/precise/   -- the same sources without --use_fast_math (IEEE sinf/expf/div ...)
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default: /root/reference)
+# Usage: oracle/build_ref.sh REFERENCE_ROOT      (the reference checkout)
 set -euo pipefail
-REF_ROOT="${1:-/root/reference}"
+REF_ROOT="${1:?usage: oracle/build_ref.sh REFERENCE_ROOT}"
 SRC="$REF_ROOT/src/warpsymbolic/gpu/cuda"
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"

@@ -75,13 +75,16 @@ def build_oracle() -> str:
     return ORACLE_LIB
 
 
-def build_reference_checker() -> None:
-    """Builds the reference extension from its sources into oracle/_ref when the reference
-    checkout is present (it is absent on GPU boxes, which use the prebuilt copy)."""
-    script = os.path.join(ORACLE_DIR, "build_ref.sh")
-    ref_root = os.environ.get("WS_REFERENCE_ROOT", "/root/reference")
-    if os.path.isdir(os.path.join(ref_root, "src")):
-        _run(["bash", script, ref_root])
+def build_reference_checker(ref_root: str) -> None:
+    """Builds the reference extension from its sources in the checkout `ref_root` into
+    oracle/_ref (test infrastructure), and installs the reference's Python package into
+    baseline/_ref when it is not there yet.  Nothing happens when the checkout is absent (GPU
+    boxes use the copies built here)."""
+    if not ref_root or not os.path.isdir(os.path.join(ref_root, "src")):
+        return
+    _run(["bash", os.path.join(ORACLE_DIR, "build_ref.sh"), ref_root])
+    if not os.path.isdir(os.path.join(REPO_DIR, "baseline", "_ref", "warpsymbolic")):
+        _run(["bash", os.path.join(REPO_DIR, "baseline", "install_ref.sh"), ref_root])
 
 
 if __name__ == "__main__":

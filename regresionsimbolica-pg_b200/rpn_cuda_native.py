@@ -3,8 +3,9 @@
 Same function names, argument order, keyword defaults and in-place output semantics as the
 pybind11 exports (bindings.cpp:434-581); the work is done by libwarpsym.so (sm_100a kernels,
 C ABI in include/warpsym.h).  Make this module importable as `rpn_cuda_native` (put this
-package directory on sys.path, or see INTEGRATION.md) and the reference's
-`cuda_loader.load_rpn_cuda_native()` resolves it.
+package directory on sys.path, or register it in sys.modules under that name before the
+reference's gpu package is imported, as reference_engine.install_native does) and the
+reference's `cuda_loader.load_rpn_cuda_native()` resolves it.
 
 Differences by design: launches go to torch's current stream (the reference uses the legacy
 default stream), the GIL is released during the native call (ctypes), and indices are 64-bit.

@@ -3,13 +3,13 @@
 vocab_ids.json is produced by importing the REFERENCE's own Python modules (GPUGrammar from
 src/warpsymbolic/gpu/grammar.py and CudaRPNVM._cache_ids from src/warpsymbolic/gpu/cuda_vm.py)
 for several operator configurations; it pins the bytecode (token IDs) and the ~36 scalar ID
-arguments every evaluator entry point receives.  Needs the reference checkout (default
-/root/reference, or WS_REFERENCE_ROOT); the GPU is not needed.
+arguments every evaluator entry point receives.  Needs the reference checkout, named by
+WS_REFERENCE_ROOT; the GPU is not needed.
 
 kats.json transcribes the known-answer tests of the reference test-suite for this path, with
 the file:line each comes from.
 
-Usage: python tests/golden/make_golden.py
+Usage: WS_REFERENCE_ROOT=<checkout> python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -18,7 +18,7 @@ import os
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("WS_REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("WS_REFERENCE_ROOT") or sys.exit("set WS_REFERENCE_ROOT to the reference checkout")
 
 ALL_FLAGS = ["PLUS", "MINUS", "MULT", "DIV", "POW", "MOD", "SIN", "COS", "TAN", "LOG", "EXP",
              "FACT", "GAMMA", "LGAMMA", "ASIN", "ACOS", "ATAN", "FLOOR", "CEIL", "SIGN", "SQRT",

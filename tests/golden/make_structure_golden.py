@@ -12,8 +12,8 @@ underflows, extra operands, out-of-table tokens):
   tour*_           TensorGeneticEngine.tournament_selection_island, torch path
                    (engine.py:899-966; the candidate matrix is re-drawn from the same seed)
 
-Needs the reference checkout (default /root/reference, or WS_REFERENCE_ROOT); no GPU.
-Usage: python tests/golden/make_structure_golden.py
+Needs the reference checkout, named by WS_REFERENCE_ROOT; no GPU.
+Usage: WS_REFERENCE_ROOT=<checkout> python tests/golden/make_structure_golden.py
 """
 from __future__ import annotations
 
@@ -25,7 +25,7 @@ import numpy as np
 import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("WS_REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("WS_REFERENCE_ROOT") or sys.exit("set WS_REFERENCE_ROOT to the reference checkout")
 
 
 def random_rows(rng, arity, n, L, pad=0):
