@@ -457,31 +457,23 @@ __device__ __forceinline__ void run_tape(const Instr<T>* __restrict__ tp, int n,
 // The FP32 interpreter for programs whose spill slots are all in shared memory (every program
 // but the deepest 0.2%): operands, spill slots and tape words are addressed as 32-bit shared
 // addresses.  xa: X tile at this pass and lane; sa: this warp's spill slot 0 at this lane; ta:
-// the tape.  One pass is 32*R rows = PASS*4 bytes = 1 << PSH.
+// the tape.  One pass is 32*R rows = PASS*4 bytes = 1 << PSH.  Each iteration reads its tape
+// word (a broadcast load), takes lane 0's copy (warp-uniform by construction), and dispatches;
+// a software-pipelined decode (next word in flight while the current one executes) measured
+// 5% more instructions per tape word on this loop and no faster, so the loop stays plain.
 template <int R, bool STRICT>
 __device__ __forceinline__ void run_tape_shared(uint32_t ta, int n, uint32_t xa, uint32_t sa,
                                                 float (&acc)[R], uint32_t& err) {
   static_assert(R == 8 || R == 16 || R == 32, "pass size");
   constexpr int PSH = R == 8 ? 10 : (R == 16 ? 11 : 12);
   err = 0u;
-  // software-pipelined decode: the next word is broadcast and its operand address computed
-  // while the current case executes; the word after it is already in flight
-  uint32_t nc, ni, c1, n1;
-  lds_word(c1, n1, ta);
-  lds_word(nc, ni, ta + 8u);
-  uint32_t cn = __shfl_sync(0xFFFFFFFFu, c1, 0);  // warp-uniform by construction
-  float sn = __uint_as_float(n1);
-  uint32_t van = ((cn & P_FETCH_SLOT) ? sa : xa) + ((cn >> P_SH_V) << PSH);
 #pragma unroll 1
   for (int i = 0; i < n; ++i) {
-    const uint32_t c = cn;
-    const float s = sn;
-    const uint32_t va = van;
-    cn = __shfl_sync(0xFFFFFFFFu, nc, 0);
-    sn = __uint_as_float(ni);
-    van = ((cn & P_FETCH_SLOT) ? sa : xa) + ((cn >> P_SH_V) << PSH);
-    ta += 8u;
-    lds_word(nc, ni, ta + 8u);  // up to two words past the end: inside the block's smem
+    uint32_t c0, ni;
+    lds_word(c0, ni, ta + 8u * (uint32_t)i);
+    const uint32_t c = __shfl_sync(0xFFFFFFFFu, c0, 0);
+    const float s = __uint_as_float(ni);
+    const uint32_t va = ((c & P_FETCH_SLOT) ? sa : xa) + ((c >> P_SH_V) << PSH);
     if (c & P_SLOW) {  // spill, accumulator load: rare
       if (c & P_SPILL) {
         const uint32_t a = sa + (((c >> P_SH_SLOT) & 7u) << PSH);
@@ -864,6 +856,174 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2)
   }
 }
 
+// ---- small data sets: several programs per warp ---------------------------------------------
+// With D <= 128 rows, a warp of fitness_kernel would carry mostly padding rows (one pass is
+// 32*R >= 256 rows; at D = 20, 92% of the lanes idle).  Here a warp holds PW = 32 / S programs,
+// S lanes each, and lane t of a subgroup carries rows [4t, 4t + 4) of the data set zero-padded
+// to DP = 4S rows, which every CTA stages once.  The subgroups of a warp run different tapes, so
+// their dispatches diverge; the tape-word load and the operand-address arithmetic still run once
+// for the whole warp, which makes one warp step advance PW programs.  Programs arrive sorted by
+// tape length, so the subgroups of a warp finish together.  All spill slots live in shared memory
+// (`NS` per lane, 16 or 32 bytes each).
+//
+// Per-row values are those of fitness_kernel (same compiler, same operator code).  A program's
+// loss sums its rows in order within a lane (in T), then the S lanes of its subgroup in FP64 by a
+// fixed butterfly: the order depends on D only, never on the other programs of the launch.
+
+// Operand loader for 4 contiguous rows of a lane (16-byte groups).
+template <typename T>
+struct ContigOperand {
+  const T* vp;
+  __device__ __forceinline__ void load(T (&v)[Vec16<T>::N], int g) const {
+    Vec16<T>::load(v, vp + g * Vec16<T>::N);
+  }
+};
+
+// One program tape over this lane's 4 rows.  xb: the staged data set at this lane's rows (one
+// variable every DP elements); sb: this lane's spill slot 0 (one slot every 32*4 elements).
+template <typename T, int DP, bool STRICT>
+__device__ __forceinline__ void run_tape_small(const Instr<T>* __restrict__ tp, int n,
+                                               const T* __restrict__ xb, T* __restrict__ sb,
+                                               T (&acc)[4], uint32_t& err) {
+  constexpr int N = Vec16<T>::N;
+  constexpr int SLOT = 32 * 4;
+  err = 0u;
+#pragma unroll 1
+  for (int i = 0; i < n; ++i) {
+    const Instr<T> ins = tp[i];
+    const uint32_t c = ins.ctrl;
+    const uint32_t off = c >> P_SH_V;
+    const T* vp = (c & P_FETCH_SLOT) ? sb + off * SLOT : xb + off * DP;
+    if (c & P_SLOW) {  // spill, accumulator load
+      if (c & P_SPILL) {
+        T* dst = sb + ((c >> P_SH_SLOT) & 7u) * SLOT;
+#pragma unroll
+        for (int g = 0; g < 4 / N; ++g) Vec16<T>::store(dst + g * N, &acc[g * N]);
+      }
+      if (c & P_LOADA_X) {
+        const T* src = xb + ((c >> P_SH_LA) & P_OFF_MASK) * DP;
+#pragma unroll
+        for (int g = 0; g < 4 / N; ++g) Vec16<T>::load(&acc[g * N], src + g * N);
+      } else if (c & P_LOADA_S) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[k] = ins.imm;
+      }
+    }
+    exec_case<T, 4, STRICT>(c & P_CASE_MASK, ins.imm, ContigOperand<T>{vp}, acc, err);
+  }
+}
+
+// Squared errors of a lane's 4 contiguous rows (row index first_row + k), summed in T in row
+// order, with the invalid-row count and the per-row metric-overflow flag of pass_epilogue.
+template <typename T, bool FUSED>
+__device__ __forceinline__ T small_epilogue(const T (&a)[4], uint32_t err, const T* __restrict__ yb,
+                                            int first_row, int rows, int& ninv, bool& ovf) {
+  constexpr T tmax = sizeof(T) == 4 ? (T)3.4028234663852886e38 : (T)1.7976931348623157e308;
+  T part = (T)0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const bool act = first_row + k < rows;
+    const T pv = a[k];
+    const bool bad = ((err >> k) & 1u) || !(m_abs(pv) <= tmax);  // error, NaN or inf
+    const T diff = pv - yb[k];
+    T sq;
+    if (FUSED) {
+      const bool o = !(m_abs(diff) <= Limits<T>::max_diff);
+      const T q = mul_rn(diff, diff);
+      const bool o2 = o || !(m_abs(q) <= tmax);
+      ovf = ovf || (act && !bad && o2);
+      sq = (bad || o2) ? (T)0 : q;
+    } else {
+      sq = bad ? (T)0 : mul_rn(diff, diff);
+    }
+    ninv += (act && bad) ? 1 : 0;
+    part += act ? sq : (T)0;
+  }
+  return part;
+}
+
+// P.PB = W * PW programs per work item (one problem, P.desc[0]); P.S = spill slots per lane.
+template <typename T, int S, bool STRICT>
+__global__ void __launch_bounds__(256) fitness_small_kernel(const FitParams<T> P) {
+  constexpr int PW = 32 / S;
+  constexpr int DP = 4 * S;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int W = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sub = lane / S, t = lane % S;
+  __shared__ ProbDesc<T> s_desc;
+  __shared__ int64_t s_item;
+  if (threadIdx.x == 0) s_desc = P.desc[0];
+  __syncthreads();
+  const ProbDesc<T>& d = s_desc;
+  const int V = d.V;
+  const int rows = (int)d.D;
+  const int tstride = P.Lcap + 1;  // odd word stride: the subgroups' tape words hit distinct banks
+  // data set [V + 1][DP] (y last), spill slots [W][S][32][4], tapes [PB][Lcap + 1], meta [PB]
+  T* xs = reinterpret_cast<T*>(smem_raw);
+  T* spill = xs + (size_t)(V + 1) * DP;
+  Instr<T>* tapes = reinterpret_cast<Instr<T>*>(spill + (size_t)W * P.S * 32 * 4);
+  int* meta_s = reinterpret_cast<int*>(tapes + (size_t)P.PB * tstride);
+  for (int i = threadIdx.x; i < (V + 1) * DP; i += blockDim.x) {
+    const int v = i / DP, r = i - v * DP;
+    xs[i] = r < rows ? (v < V ? d.x[(size_t)v * rows + r] : d.y[r]) : (T)0;
+  }
+  const T* xb = xs + t * 4;
+  const T* yb = xs + (size_t)V * DP + t * 4;
+  T* sb = spill + ((size_t)warp * P.S * 32 + lane) * 4;
+  const bool fused_policy = P.policy == WS_POLICY_FUSED;
+  const double yvar = P.yvar ? P.yvar[0] : 0.0;
+
+  for (;;) {
+    if (threadIdx.x == 0) s_item = (int64_t)atomicAdd(P.work, 1u);
+    __syncthreads();  // also: the data set is staged, the previous item's tapes are consumed
+    const int64_t item = s_item;
+    if (item >= P.n_items) break;
+    const int64_t p0 = item * P.PB;
+    const int np = (int)min((int64_t)P.PB, d.B - p0);
+    for (int q = warp; q < np; q += W) {  // warp-cooperative tape copies
+      const int64_t g = P.perm[p0 + q];
+      const ProgHdr h = P.hdr[g];
+      const Instr<T>* tg = P.tape + g * (int64_t)P.Lcap;
+      for (int i = lane; i < h.n_instr; i += 32) tapes[(size_t)q * tstride + i] = tg[i];
+      if (lane == 0) meta_s[q] = h.status == PROG_OK ? h.n_instr : -1;
+    }
+    __syncthreads();
+    const int q = warp * PW + sub;  // consecutive (similar-length) programs share a warp
+    const bool active = q < np;
+    const int meta = active ? meta_s[q] : -1;
+    T a[4];
+    uint32_t err = 0u;
+    if (meta >= 0) {
+      run_tape_small<T, DP, STRICT>(tapes + (size_t)q * tstride, meta, xb, sb, a, err);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a[k] = (T)0;
+      err = active ? 0xFu : 0u;  // a statically invalid program: every row is invalid
+    }
+    int ninv = 0;
+    bool ovf = false;
+    T part = (T)0;
+    if (active) {
+      part = fused_policy ? small_epilogue<T, true>(a, err, yb, t * 4, rows, ninv, ovf)
+                          : small_epilogue<T, false>(a, err, yb, t * 4, rows, ninv, ovf);
+    }
+    // the subgroup's sums, by a fixed butterfly over its S lanes (every lane takes part)
+    double sse = (double)part;
+    int ovf_i = ovf ? 1 : 0;
+#pragma unroll
+    for (int o = S / 2; o >= 1; o >>= 1) {
+      sse += __shfl_xor_sync(0xFFFFFFFFu, sse, o);
+      ninv += __shfl_xor_sync(0xFFFFFFFFu, ninv, o);
+      ovf_i |= __shfl_xor_sync(0xFFFFFFFFu, ovf_i, o);
+    }
+    if (active && t == 0) {
+      const int64_t pl = P.perm[p0 + q] - d.prog0;
+      write_final<T>(P, d, yvar, pl, PartRec{sse, ninv, ovf_i});
+    }
+  }
+}
+
 // ---- length-sorted schedule: counting sort of programs by (problem, tape length) -----------
 // Bins are problem-major; within a problem tape lengths descend and invalid programs come last,
 // so problem p's programs occupy perm[prog0, prog0 + B) longest first.
@@ -979,6 +1139,8 @@ constexpr Sched kSched[] = {
     {16, 8, 16, 100 * 1024},  // 11
 };
 constexpr int kNumSched = (int)(sizeof(kSched) / sizeof(kSched[0]));
+// schedules of the small-data-set evaluator, numbered after kSched (single-problem calls only)
+constexpr int kNumSmall = 5;
 
 Sched pick_schedule(int idx, int64_t D) {
   if (idx > 0 && idx < kNumSched) return kSched[idx];
@@ -1199,6 +1361,54 @@ struct RunArgs {
   cudaStream_t stream;
 };
 
+// Compile + length sort of the programs of the descriptors in the workspace (unless
+// evaluate-only), and the work-queue reset of an evaluate-only launch.  Kernels and memsets only.
+template <typename T, bool STRICT>
+ws_status compile_and_sort(int64_t total_B, int Lcap, int S, const FitnessWorkspace& lay,
+                           unsigned char* wsb, const RunArgs& a) {
+  ProgHdr* hdr = reinterpret_cast<ProgHdr*>(wsb + lay.hdr_off);
+  Instr<T>* tape = reinterpret_cast<Instr<T>*>(wsb + lay.tape_off);
+  unsigned* cnt = reinterpret_cast<unsigned*>(wsb + lay.cnt_off);
+  unsigned* misc = reinterpret_cast<unsigned*>(wsb + lay.misc_off);
+  int64_t* perm = reinterpret_cast<int64_t*>(wsb + lay.perm_off);
+  unsigned* bins = reinterpret_cast<unsigned*>(wsb + lay.bins_off);
+  const ProbDesc<T>* desc = reinterpret_cast<const ProbDesc<T>*>(wsb + lay.desc_off);
+  const TokenLut* luts = reinterpret_cast<const TokenLut*>(wsb + lay.lut_off);
+  int32_t* prob_of = reinterpret_cast<int32_t*>(wsb + lay.probof_off);
+  if (a.phase != WS_PHASE_EVALUATE) {
+    cudaError_t e0 = cudaMemsetAsync(bins, 0, (size_t)a.n_desc * kSortBins * sizeof(unsigned),
+                                     a.stream);
+    if (e0 != cudaSuccess) return fail_cuda(e0, "sort-bin reset");
+    const int ct = 128;
+    const unsigned grid = (unsigned)((total_B + ct - 1) / ct);
+    if (a.L <= 64)
+      compile_kernel<T, STRICT, 64><<<grid, ct, 0, a.stream>>>(
+          desc, a.n_desc, luts, total_B, (int)a.L, tape, Lcap, hdr, prob_of, cnt, misc, S);
+    else
+      compile_kernel<T, STRICT, 256><<<grid, ct, 0, a.stream>>>(
+          desc, a.n_desc, luts, total_B, (int)a.L, tape, Lcap, hdr, prob_of, cnt, misc, S);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "compile_kernel launch");
+    int64_t hgrid = (total_B + 4095) / 4096;
+    if (hgrid < 1) hgrid = 1;
+    if (hgrid > (int64_t)device_info().sm_count * 8) hgrid = (int64_t)device_info().sm_count * 8;
+    const int64_t per_block = (total_B + hgrid - 1) / hgrid;
+    sort_hist_kernel<<<(unsigned)hgrid, 256, 0, a.stream>>>(hdr, prob_of, total_B, per_block,
+                                                            bins);
+    sort_scan_kernel<<<1, 1024, 0, a.stream>>>(bins, a.n_desc);
+    int sgrid = (int)((total_B + 255) / 256);
+    if (sgrid > device_info().sm_count * 8) sgrid = device_info().sm_count * 8;
+    sort_scatter_kernel<<<sgrid, 256, 0, a.stream>>>(hdr, prob_of, total_B, bins, perm);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "sort kernels launch");
+  }
+  if (a.phase == WS_PHASE_EVALUATE) {  // the compile kernel is what resets the queue head
+    cudaError_t e = cudaMemsetAsync(misc, 0, 16, a.stream);
+    if (e != cudaSuccess) return fail_cuda(e, "work-queue reset");
+  }
+  return WS_OK;
+}
+
 // The launch sequence of a plan whose descriptors and token tables are in the workspace:
 // compile + length sort (unless evaluate-only), then the evaluator.  Kernels and memsets only,
 // so a CUDA graph can capture it.
@@ -1211,47 +1421,14 @@ ws_status run_plan(const Plan& pl, const FitnessWorkspace& lay, unsigned char* w
   unsigned* cnt = reinterpret_cast<unsigned*>(wsb + lay.cnt_off);
   unsigned* misc = reinterpret_cast<unsigned*>(wsb + lay.misc_off);
   int64_t* perm = reinterpret_cast<int64_t*>(wsb + lay.perm_off);
-  unsigned* bins = reinterpret_cast<unsigned*>(wsb + lay.bins_off);
   T* gspill = reinterpret_cast<T*>(wsb + lay.gspill_off);
   const ProbDesc<T>* desc = reinterpret_cast<const ProbDesc<T>*>(wsb + lay.desc_off);
-  const TokenLut* luts = reinterpret_cast<const TokenLut*>(wsb + lay.lut_off);
   double* yvar = reinterpret_cast<double*>(wsb + lay.yvar_off);
-  int32_t* prob_of = reinterpret_cast<int32_t*>(wsb + lay.probof_off);
   if (pl.total_B == 0) return WS_OK;
 
   // 1. compile, then order the programs by (problem, tape length)
-  if (a.phase != WS_PHASE_EVALUATE) {
-    cudaError_t e0 = cudaMemsetAsync(bins, 0, (size_t)a.n_desc * kSortBins * sizeof(unsigned),
-                                     a.stream);
-    if (e0 != cudaSuccess) return fail_cuda(e0, "sort-bin reset");
-    const int ct = 128;
-    const unsigned grid = (unsigned)((pl.total_B + ct - 1) / ct);
-    if (a.L <= 64)
-      compile_kernel<T, STRICT, 64><<<grid, ct, 0, a.stream>>>(
-          desc, a.n_desc, luts, pl.total_B, (int)a.L, tape, pl.Lcap, hdr, prob_of, cnt, misc, pl.S);
-    else
-      compile_kernel<T, STRICT, 256><<<grid, ct, 0, a.stream>>>(
-          desc, a.n_desc, luts, pl.total_B, (int)a.L, tape, pl.Lcap, hdr, prob_of, cnt, misc, pl.S);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return fail_cuda(e, "compile_kernel launch");
-    int64_t hgrid = (pl.total_B + 4095) / 4096;
-    if (hgrid < 1) hgrid = 1;
-    if (hgrid > (int64_t)device_info().sm_count * 8) hgrid = (int64_t)device_info().sm_count * 8;
-    const int64_t per_block = (pl.total_B + hgrid - 1) / hgrid;
-    sort_hist_kernel<<<(unsigned)hgrid, 256, 0, a.stream>>>(hdr, prob_of, pl.total_B, per_block,
-                                                            bins);
-    sort_scan_kernel<<<1, 1024, 0, a.stream>>>(bins, a.n_desc);
-    int sgrid = (int)((pl.total_B + 255) / 256);
-    if (sgrid > device_info().sm_count * 8) sgrid = device_info().sm_count * 8;
-    sort_scatter_kernel<<<sgrid, 256, 0, a.stream>>>(hdr, prob_of, pl.total_B, bins, perm);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return fail_cuda(e, "sort kernels launch");
-  }
-  if (a.phase == WS_PHASE_COMPILE) return WS_OK;
-  if (a.phase == WS_PHASE_EVALUATE) {  // the compile kernel is what resets the queue head
-    cudaError_t e = cudaMemsetAsync(misc, 0, 16, a.stream);
-    if (e != cudaSuccess) return fail_cuda(e, "work-queue reset");
-  }
+  ws_status st = compile_and_sort<T, STRICT>(pl.total_B, pl.Lcap, pl.S, lay, wsb, a);
+  if (st != WS_OK || a.phase == WS_PHASE_COMPILE) return st;
   if (a.loss == WS_LOSS_R2) {
     yvar_kernel<T><<<a.n_desc, 256, 0, a.stream>>>(desc, yvar);
     cudaError_t e = cudaGetLastError();
@@ -1325,7 +1502,7 @@ struct BatchState {
 
 }  // namespace
 
-int schedule_count() { return kNumSched; }
+int schedule_count() { return kNumSched + kNumSmall; }
 
 FitnessWorkspace fitness_workspace_layout(int64_t total_B, int64_t L, int dtype, int64_t n_prob,
                                           int64_t n_part) {
@@ -1373,6 +1550,126 @@ FitnessWorkspace fitness_workspace_layout(int64_t B, int64_t L, int dtype) {
   return fitness_workspace_layout(B, L, dtype, 1, B > 65536 ? B : 65536);
 }
 
+// ---- small data sets (fitness_small_kernel) --------------------------------------------------
+// Schedule index kNumSched + j runs the small-data-set evaluator with S = 2 << j lanes per program
+// (rows per program 4S = 8, 16, 32, 64, 128); the automatic choice (index 0) takes it for
+// 1 <= D <= 128 with the smallest S that covers D.
+int small_lanes(int schedule, int64_t D) {
+  if (schedule >= kNumSched && schedule < kNumSched + kNumSmall) return 2 << (schedule - kNumSched);
+  if (schedule == 0 && D >= 1 && D <= 128) {
+    int s = 2;
+    while (4 * s < D) s <<= 1;
+    return s;
+  }
+  return 0;
+}
+
+template <typename T, int S, bool STRICT>
+size_t small_max_dynamic_smem() {
+  static std::mutex mu;
+  static size_t cache[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  std::lock_guard<std::mutex> g(mu);
+  if (cache[dev] == 0) {
+    cudaFuncAttributes fa;
+    size_t stat = 0;
+    if (cudaFuncGetAttributes(&fa, fitness_small_kernel<T, S, STRICT>) == cudaSuccess)
+      stat = fa.sharedSizeBytes;
+    size_t lim = device_info().smem_optin > stat ? device_info().smem_optin - stat : 0;
+    if (cudaFuncSetAttribute(fitness_small_kernel<T, S, STRICT>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) != cudaSuccess) {
+      (void)cudaGetLastError();
+      lim = 48 * 1024 - stat;
+    }
+    cache[dev] = lim;
+  }
+  return cache[dev];
+}
+
+template <typename T, int S, bool STRICT>
+ws_status launch_small(const FitnessRequest& rq, const ProblemRequest& pr,
+                       const FitnessWorkspace& lay) {
+  constexpr int PW = 32 / S;
+  if (4 * (int64_t)S < rq.D) return fail("this schedule covers fewer rows than the data set");
+  unsigned char* wsb = static_cast<unsigned char*>(rq.workspace);
+  const int W = S <= 4 ? 4 : 8;
+  const int Lcap = tape_capacity(rq.L < 256 ? (int)rq.L : 256);
+  int NS = spill_slots_bound((int)rq.L);
+  if (NS < 1) NS = 1;
+  const int PB = W * PW;
+  const int64_t n_items = (rq.B + PB - 1) / PB;
+  const size_t smem = (size_t)(rq.V + 1) * 4 * S * sizeof(T) + (size_t)W * NS * 32 * 4 * sizeof(T) +
+                      (size_t)PB * (Lcap + 1) * sizeof(Instr<T>) + (size_t)PB * sizeof(int);
+  if (smem > small_max_dynamic_smem<T, S, STRICT>())
+    return fail("too many variables for the small-data-set evaluator");
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fitness_small_kernel<T, S, STRICT>,
+                                                    W * 32, smem) != cudaSuccess) {
+    (void)cudaGetLastError();
+    occ = 0;
+  }
+  if (occ <= 0) return fail("small-data-set evaluator cannot be resident");
+  ProbPlan pp;
+  pp.RC = 4 * S;
+  pp.xmul = 1;  // tape operand offsets count variables (rows of 4S elements)
+  pp.n_chunks = 1;
+  pp.cps = 1;
+  pp.n_splits = 1;
+  pp.n_blocks = n_items;
+  const ProbDesc<T> d = make_desc<T>(pr, pp);
+  write_desc_kernel<T><<<1, 128, 0, rq.stream>>>(
+      d, pr.lut, reinterpret_cast<ProbDesc<T>*>(wsb + lay.desc_off),
+      reinterpret_cast<TokenLut*>(wsb + lay.lut_off));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail_cuda(e, "descriptor write");
+  if (rq.B == 0) return WS_OK;
+  RunArgs a{rq.L, 1, rq.phase, rq.policy, rq.loss, rq.invalid_value, rq.stream};
+  ws_status st = compile_and_sort<T, STRICT>(rq.B, Lcap, NS, lay, wsb, a);
+  if (st != WS_OK || rq.phase == WS_PHASE_COMPILE) return st;
+  const ProbDesc<T>* desc = reinterpret_cast<const ProbDesc<T>*>(wsb + lay.desc_off);
+  double* yvar = reinterpret_cast<double*>(wsb + lay.yvar_off);
+  if (rq.loss == WS_LOSS_R2) {
+    yvar_kernel<T><<<1, 256, 0, rq.stream>>>(desc, yvar);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "yvar_kernel launch");
+  }
+  FitParams<T> P{};
+  P.desc = desc;
+  P.n_prob = 1;
+  P.tape = reinterpret_cast<const Instr<T>*>(wsb + lay.tape_off);
+  P.hdr = reinterpret_cast<const ProgHdr*>(wsb + lay.hdr_off);
+  P.Lcap = Lcap;
+  P.PB = PB;
+  P.n_items = n_items;
+  P.S = NS;
+  P.policy = rq.policy;
+  P.loss = rq.loss;
+  P.invalid_value = rq.invalid_value;
+  P.work = reinterpret_cast<unsigned*>(wsb + lay.misc_off);
+  P.yvar = rq.loss == WS_LOSS_R2 ? yvar : nullptr;
+  P.perm = reinterpret_cast<const int64_t*>(wsb + lay.perm_off);
+  const int64_t cap = (int64_t)occ * device_info().sm_count;
+  const int64_t grid = n_items < cap ? n_items : cap;
+  fitness_small_kernel<T, S, STRICT><<<(unsigned)grid, W * 32, smem, rq.stream>>>(P);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail_cuda(e, "fitness_small_kernel launch");
+  return WS_OK;
+}
+
+template <typename T, bool STRICT>
+ws_status launch_small_s(int S, const FitnessRequest& rq, const ProblemRequest& pr,
+                         const FitnessWorkspace& lay) {
+  switch (S) {
+    case 2: return launch_small<T, 2, STRICT>(rq, pr, lay);
+    case 4: return launch_small<T, 4, STRICT>(rq, pr, lay);
+    case 8: return launch_small<T, 8, STRICT>(rq, pr, lay);
+    case 16: return launch_small<T, 16, STRICT>(rq, pr, lay);
+    default: return launch_small<T, 32, STRICT>(rq, pr, lay);
+  }
+}
+
 ws_status launch_fitness(const FitnessRequest& rq) {
   const FitnessWorkspace lay = fitness_workspace_layout(rq.B, rq.L, rq.dtype);
   ProblemRequest pr;
@@ -1387,6 +1684,14 @@ ws_status launch_fitness(const FitnessRequest& rq) {
   pr.out_loss = rq.out_loss;
   pr.out_ninv = rq.out_ninv;
   pr.lut = rq.lut;
+  const int small = small_lanes(rq.schedule, rq.D);
+  if (small > 0) {
+    if (rq.dtype == WS_F64)
+      return rq.strict ? launch_small_s<double, true>(small, rq, pr, lay)
+                       : launch_small_s<double, false>(small, rq, pr, lay);
+    return rq.strict ? launch_small_s<float, true>(small, rq, pr, lay)
+                     : launch_small_s<float, false>(small, rq, pr, lay);
+  }
   const Sched sc = pick_schedule(rq.schedule, rq.D);
   unsigned char* wsb = static_cast<unsigned char*>(rq.workspace);
   return dispatch(rq.dtype, rq.strict != 0, sc, [&](auto tt_, auto rr_, auto ss_) -> ws_status {
@@ -1414,6 +1719,7 @@ static Sched batch_schedule(const ProblemRequest* probs, int n, int schedule) {
 
 ws_status batch_workspace_bytes(int dtype, const ProblemRequest* probs, int n, int64_t L,
                                 int strict, int schedule, size_t* out) {
+  if (schedule >= kNumSched) return fail("the small-data-set schedules take one problem per call");
   const Sched sc = batch_schedule(probs, n, schedule);
   return dispatch(dtype, strict != 0, sc, [&](auto tt_, auto rr_, auto ss_) -> ws_status {
     WS_DISPATCH_TYPES
@@ -1432,6 +1738,7 @@ ws_status batch_workspace_bytes(int dtype, const ProblemRequest* probs, int n, i
 ws_status batch_create(int dtype, const ProblemRequest* probs, int n, int64_t L, int strict,
                        int policy, int loss, int schedule, double invalid_value, void* workspace,
                        size_t workspace_bytes, cudaStream_t stream, void** out) {
+  if (schedule >= kNumSched) return fail("the small-data-set schedules take one problem per call");
   const Sched sc = batch_schedule(probs, n, schedule);
   BatchState* bs = new BatchState();
   bs->dtype = dtype;
