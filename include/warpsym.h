@@ -153,8 +153,9 @@ int32_t ws_schedule_count(void);
  * static 64 MiB device array inside the library (held by every GPU that loads it until exit);
  * requests whose ws_fitness_workspace_bytes(B, L, dtype) exceed ws_static_scratch_bytes() are
  * rejected with an error.  All calls share the array: calls that overlap on the GPU race and must
- * be serialised.  The first call on a device looks the array's address up; make it before any
- * stream capture.  Arguments and results are those of ws_eval_fitness.
+ * be serialised.  Each call looks the array's address up on the current device (a context
+ * re-created after a device reset is followed); make the first call on each device before any
+ * stream capture begins.  Arguments and results are those of ws_eval_fitness.
  */
 ws_status ws_eval_fitness_static(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
                                  const void* x, int64_t num_vars, int64_t D,

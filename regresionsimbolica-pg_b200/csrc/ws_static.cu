@@ -9,16 +9,20 @@
 // that loads libwarpsym holds these 64 MiB until the process exits.
 //
 // Rules of use:
-//   * the request's workspace must fit: ws_fitness_workspace_bytes(B, L, dtype) <= 64 MiB
-//     (about 46,000 programs of 64 tokens in FP32, or 1,024-program populations of any length up
-//     to 256); larger requests are rejected with a clear error and nothing is launched;
+//   * the request's workspace must fit: ws_fitness_workspace_bytes(B, L, dtype) <= 64 MiB; the
+//     largest B for a given L and dtype follows from that function (it includes a deep-spill
+//     area proportional to the GPU's SM count, ~19 MB for 64-token FP32 programs on 148 SMs,
+//     plus ~560 bytes per 64-token FP32 program); larger requests are rejected with a clear error
+//     and nothing is launched;
 //   * all calls share the one array and it keeps the last call's contents; the pipeline clears
 //     what must start at zero (queue head, sort bins, split counters) itself, but two calls whose
 //     work overlaps on the GPU (different streams, or different host threads) race on it --
 //     serialise them;
-//   * the first call on each device looks up the array's device address (cudaGetSymbolAddress,
-//     once per device, with that device current); make that first call before any stream
-//     capture begins.
+//   * each call looks up the array's device address on the current device (cudaGetSymbolAddress,
+//     with that device current), so that a context re-created after a device reset (the array
+//     then lives in a new context) is followed; the lookup can load the module, so make the first
+//     call on each device before any stream capture begins.  While the stream is being captured
+//     the lookup is skipped and the address remembered from the last lookup is used.
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <mutex>
@@ -34,20 +38,30 @@ constexpr size_t kStaticScratchBytes = 64ull << 20;
 // symbol, not a device address: a kernel must be given the address obtained below.
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
-// Device address of g_static_scratch on the current device (looked up once per device).
-static ws_status static_scratch_address(void** out) {
+// Device address of g_static_scratch on the current device: looked up afresh when `stream` is not
+// being captured (so a context re-created after a device reset is followed), the address
+// remembered from the last such lookup when it is.
+static ws_status static_scratch_address(cudaStream_t stream, void** out) {
   static std::mutex mu;
   static void* addr[64] = {nullptr};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail_cuda(e, "cudaGetDevice");
   if (dev < 0 || dev >= 64) return fail("device index out of range for the static scratch");
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
+    (void)cudaGetLastError();  // e.g. the legacy stream while another stream captures globally
+    cs = cudaStreamCaptureStatusActive;
+  }
   std::lock_guard<std::mutex> g(mu);
-  if (addr[dev] == nullptr) {
+  if (cs == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_static_scratch);
     if (e != cudaSuccess) return fail_cuda(e, "cudaGetSymbolAddress(static scratch)");
     addr[dev] = p;
+  } else if (addr[dev] == nullptr) {
+    return fail("ws_eval_fitness_static: the first call on a device must come before stream "
+                "capture (it looks up the static scratch's address)");
   }
   *out = addr[dev];
   return WS_OK;
@@ -75,7 +89,7 @@ ws_status ws_eval_fitness_static(int32_t dtype, const uint8_t* population, int64
                 " bytes (evaluate fewer programs per call, or use ws_eval_fitness with a workspace)");
   }
   void* scratch = nullptr;
-  ws_status st = static_scratch_address(&scratch);
+  ws_status st = static_scratch_address(static_cast<cudaStream_t>(stream), &scratch);
   if (st != WS_OK) return st;
   return ws_eval_fitness(dtype, population, B, L, x, num_vars, D, constants, K, y, out_loss,
                          out_ninvalid, ids, opts, scratch, kStaticScratchBytes, stream);

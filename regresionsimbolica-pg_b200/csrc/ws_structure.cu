@@ -269,6 +269,39 @@ __global__ void __launch_bounds__(kThreads) subtree_kernel(SubtreeArgs a) {
 // candidates are base + (offset % span), clamped into [0, B-1].
 constexpr int kTourFast = 8;  // tournaments up to this size keep their candidates in registers
 
+// State of one tournament: the incumbent, its value and (once read) its length.
+struct TourState {
+  const float* lengths;  // null: no parsimony tie-break
+  float eps;             // tie epsilon, used only with lengths
+  int64_t best = -1;
+  float best_val = 0.0f;
+  float best_len = 0.0f;
+  bool best_len_known = false;
+};
+
+// Candidate `c` with value `val` challenges the incumbent with the reference's comparisons
+// (rpn_kernels.cu:1603-1668): a strictly smaller value wins; otherwise, with lengths, a value
+// within eps of the incumbent's is a tie, won by a strictly shorter program.  A candidate's
+// length is only read on a tie (the incumbent's once, then the challenger's); the winner of a
+// tie keeps its length known, a strict winner's length is read on a later tie.
+__device__ __forceinline__ void tour_challenge(TourState& st, int64_t c, float val) {
+  bool improve = val < st.best_val;
+  float len = 0.0f;
+  const bool tie = !improve && st.lengths != nullptr && fabsf(val - st.best_val) < st.eps;
+  if (tie) {
+    if (!st.best_len_known) st.best_len = st.lengths[st.best];
+    st.best_len_known = true;
+    len = st.lengths[c];
+    improve = len < st.best_len;
+  }
+  if (improve) {
+    st.best_val = val;
+    st.best = c;
+    st.best_len = len;
+    st.best_len_known = tie;
+  }
+}
+
 template <bool OFFSETS>
 __global__ void __launch_bounds__(256)
     tournament_kernel(const float* __restrict__ fitness, const float* __restrict__ errors,
@@ -302,30 +335,9 @@ __global__ void __launch_bounds__(256)
     // A candidate's length only matters on a tie (|val - best_val| < eps), so lengths are read
     // there alone: the incumbent's once, then the challenger's.  The comparisons are the
     // reference's, in candidate order, so the winner is the same.
-    float best_len = 0.0f;
-    bool best_len_known = false;
-    int64_t best = -1;
-    float best_val = 0.0f;
-#define WS_CHALLENGE(C_, VAL_)                                                     \
-  {                                                                                \
-    const int64_t c_ = (C_);                                                       \
-    const float val_ = (VAL_);                                                     \
-    bool improve = val_ < best_val;                                                \
-    float len = 0.0f;                                                              \
-    const bool tie = !improve && lengths != nullptr && fabsf(val_ - best_val) < eps; \
-    if (tie) {                                                                     \
-      if (!best_len_known) best_len = lengths[best];                               \
-      best_len_known = true;                                                       \
-      len = lengths[c_];                                                           \
-      improve = len < best_len;                                                    \
-    }                                                                              \
-    if (improve) {                                                                 \
-      best_val = val_;                                                             \
-      best = c_;                                                                   \
-      best_len = len;                                                              \
-      best_len_known = tie;                                                        \
-    }                                                                              \
-  }
+    TourState st;
+    st.lengths = lengths;
+    st.eps = eps;
     if (T <= kTourFast) {
       // all candidates, then all their values, then the comparisons in candidate order: two
       // rounds of memory latency per program instead of two per candidate
@@ -350,25 +362,24 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int k = 0; k < kTourFast; ++k)
         if (k < T) vals[k] = by_case ? errors[cs[k] * n_data + case_idx] : fitness[cs[k]];
-      best = cs[0];
-      best_val = vals[0];
+      st.best = cs[0];
+      st.best_val = vals[0];
 #pragma unroll
       for (int k = 1; k < kTourFast; ++k) {
         if (k >= T) break;
-        WS_CHALLENGE(cs[k], vals[k]);
+        tour_challenge(st, cs[k], vals[k]);
       }
-      selected[idx] = best;
+      selected[idx] = st.best;
       continue;
     }
-    best = candidate(0);
-    best_val = by_case ? errors[best * n_data + case_idx] : fitness[best];
+    st.best = candidate(0);
+    st.best_val = by_case ? errors[st.best * n_data + case_idx] : fitness[st.best];
     for (int64_t k = 1; k < T; ++k) {
       const int64_t c = candidate(k);
-      WS_CHALLENGE(c, by_case ? errors[c * n_data + case_idx] : fitness[c]);
+      tour_challenge(st, c, by_case ? errors[c * n_data + case_idx] : fitness[c]);
     }
-    selected[idx] = best;
+    selected[idx] = st.best;
   }
-#undef WS_CHALLENGE
 }
 
 int grid_for(int64_t units, int threads, int per_sm) {

@@ -195,6 +195,35 @@ def test_tournament_tie_rules_on_hand_written_cases():
     cases = np.zeros(2, dtype=np.int32)
     assert run(cand2, errs, cases, lens) == [3, 2]
     assert run(cand2, errs, cases, lens, np.array([1e-5], dtype=np.float32)) == [2, 2]
+    # even T on a candidate matrix whose base is not 16-byte aligned (a view one int64 into its
+    # storage): the kernel's alignment check must route it to the scalar path, same winners
+    buf = torch.empty(cand.size + 1, dtype=torch.int64, device=DEV)
+    mis = buf[1:].view(cand.shape)
+    mis.copy_(T(cand))
+    assert mis.data_ptr() % 16 != 0 and mis.is_contiguous()
+    out = torch.empty(len(cand), dtype=torch.int64, device=DEV)
+    ours.tournament_selection(T(fit), e0, mis, i0, out, T(lens), e0)
+    assert out.cpu().tolist() == [3, 3, 4, 2]
+
+
+@pytest.mark.parametrize("T_", [2, 4, 8])
+def test_tournament_unaligned_candidates_bit_exact(T_):
+    """Random inputs with even T: the candidate matrix at a 16-byte aligned base and at a base
+    8 bytes past it give the oracle's winners."""
+    from warpsymbolic_b200 import rpn_cuda_native as ours
+    B = 5000
+    fit, errs, cand, cases, lens, mad = _tournament_inputs(B + T_, B, T_)
+    want = O.tournament(fit, cand, lengths=lens)
+    e0 = torch.empty(0, dtype=torch.float32, device=DEV)
+    i0 = torch.empty(0, dtype=torch.int32, device=DEV)
+    for shift in (0, 1):
+        buf = torch.empty(cand.size + 2, dtype=torch.int64, device=DEV)
+        c_t = buf[shift:shift + cand.size].view(cand.shape)
+        c_t.copy_(T(cand))
+        assert (c_t.data_ptr() % 16 == 0) == (shift == 0)
+        out = torch.empty(B, dtype=torch.int64, device=DEV)
+        ours.tournament_selection(T(fit), e0, c_t, i0, out, T(lens), e0)
+        assert np.array_equal(out.cpu().numpy(), want), shift
 
 
 @pytest.mark.parametrize("island_size,n_islands", [(512, 8), (100, 41), (1, 4096), (0, 3),

@@ -91,3 +91,59 @@ def test_static_scratch_rejects_requests_beyond_its_size():
                                     C.byref(m), C.byref(opts), None)
     assert st != 0
     assert "static scratch" in lib.ws_last_error().decode()
+
+
+def test_static_scratch_largest_request_and_no_device_allocation():
+    """The largest population of 64-token FP32 programs that fits the static scratch (found by
+    bisection on ws_fitness_workspace_bytes) evaluates like the workspace entry point, one more
+    program is rejected, and the calls take no device memory (free device memory is unchanged
+    across them once the library's module is loaded)."""
+    from warpsymbolic_b200.cuda_vm import CudaRPNVM
+    lib = tl.N.lib()
+    cap = lib.ws_static_scratch_bytes()
+    L = 64
+    lo, hi = 1, 1 << 22
+    assert lib.ws_fitness_workspace_bytes(lo, L, tl.N.WS_F32) <= cap
+    assert lib.ws_fitness_workspace_bytes(hi, L, tl.N.WS_F32) > cap
+    while hi - lo > 1:
+        mid = (lo + hi) // 2
+        if lib.ws_fitness_workspace_bytes(mid, L, tl.N.WS_F32) <= cap:
+            lo = mid
+        else:
+            hi = mid
+    Bmax = lo
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(91)
+    g = tl.GPUGrammar(num_variables=3, operators=tl.C1_OPERATORS)
+    pop = tl.synthetic.random_programs(g, Bmax + 1, 3, L, L, rng, max_consts=6)
+    consts = rng.uniform(-2, 2, size=(Bmax + 1, 6)).astype(np.float32)
+    X = rng.uniform(-3, 3, size=(3, 300)).astype(np.float32)
+    y = rng.standard_normal(300).astype(np.float32)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    pop_t, c_t, X_t, y_t = T(pop), T(consts), T(X), T(y)
+    want = CudaRPNVM(g, dev).eval_fitness(pop_t[:Bmax], X_t, c_t[:Bmax], y_t, policy="classic",
+                                          loss="mse").cpu().numpy()
+    got, _ = _static_call(g, pop_t[:Bmax], X_t, c_t[:Bmax], y_t, "classic", "mse")
+    torch.cuda.synchronize()
+    tl.assert_fitness_close(got.cpu().numpy(), want, rtol=1e-5, atol=1e-7, min_frac=1.0)
+    with pytest.raises(RuntimeError, match="static scratch"):
+        _static_call(g, pop_t, X_t, c_t, y_t, "classic", "mse")
+    # no device allocation by the calls: outputs are allocated first, then free memory is read
+    # before and after each call (the first call above already loaded the module)
+    for _ in range(2):
+        out = torch.empty(Bmax, dtype=torch.float32, device=dev)
+        ninv = torch.empty(Bmax, dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info(dev)
+        lk = tl.N.WS_LOSS_MSE
+        opts = tl.N.FitnessOpts(0, tl.N.WS_POLICY_CLASSIC, lk, 0, 1e15, 0, 0)
+        m = tl.token_map(g)
+        tl.N.check(lib.ws_eval_fitness_static(
+            tl.N.WS_F32, C.c_void_p(pop_t.data_ptr()), Bmax, L, C.c_void_p(X_t.data_ptr()), 3,
+            300, C.c_void_p(c_t.data_ptr()), 6, C.c_void_p(y_t.data_ptr()),
+            C.c_void_p(out.data_ptr()), C.c_void_p(ninv.data_ptr()), C.byref(m), C.byref(opts),
+            C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info(dev)
+        assert free1 == free0, (free0, free1)
+        tl.assert_fitness_close(out.cpu().numpy(), want, rtol=1e-5, atol=1e-7, min_frac=1.0)
