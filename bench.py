@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--config", default="eval-scale",
-                    choices=["eval-scale", "batched", "serving", "kernels", "constopt", "c1"],
+                    choices=["eval-scale", "batched", "serving", "kernels", "constopt", "c1",
+                             "opcost"],
                     help="eval-scale: the evaluation-only scale test (default); batched: 256 "
                          "uneven problems scored by one graph-replayed launch per generation; "
                          "serving: a Poisson stream of fit/evaluate requests, continuously "
@@ -59,7 +60,8 @@ def parse():
                          "rows; c1: the reference's own estimator and engine fitting the "
                          "plain-method workload (1024x2 rows, population 1024, 20 "
                          "generations), on this library's drop-in (--impl ours) or on the "
-                         "reference extension (--impl reference)")
+                         "reference extension (--impl reference); opcost: costs inside the "
+                         "fitness evaluator (schedule sweep, per-operator rows per clock)")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="kernels: fraction of the default sizes (smaller cases for profiling)")
     ap.add_argument("--requests", type=int, default=8)
@@ -106,14 +108,75 @@ def cpu_baseline(args, wl, n_tok, oracle, tmap):
     while True:
         t0 = time.perf_counter()
         oracle.fitness(tmap, wl.population[:n], wl.X, wl.constants[:n], wl.y, policy="classic",
-                       loss="mse", nthreads=threads)
+                       loss="mse", nthreads=threads, timed=True)
         t = time.perf_counter() - t0
         if t > args.cpu_seconds / 4 or n >= wl.population.shape[0]:
             break
         n = min(wl.population.shape[0], n * 4)
     evals = float(n_tok[:n].sum()) * D
     return {"value": evals / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "build": "g++ " + " ".join(oracle.NATIVE_FLAGS) + " on this host (programs split "
+                     "across threads)",
             "sample": "first %d programs x %d rows of the same workload (%.1f s)" % (n, D, t)}
+
+
+# FP32-pipe, MUFU and shared-memory costs per row of each operator class, for the op-mix bound
+MUFU_OPS = ("sin", "cos", "exp", "log", "sqrt", "/")
+PIPE_RATE = {"fp32": 128, "mufu": 16, "smem": 32}  # operations per clock per SM
+
+
+def op_mix_bound(wl, sms, f_hz):
+    """The evaluator's bound on this workload's operation counts if each pipe ran at its peak
+    and the interpretation itself (tape decode, dispatch) were free: one FP32 lane-op per
+    operator token plus 3 per row (difference, square, sum); one MUFU op per sin, cos, exp, log,
+    sqrt and division (the fast-math intrinsics: one multi-function-unit instruction each); one
+    4-byte shared-memory load per variable token plus one for y.  The pipes run concurrently,
+    so the slowest one bounds the launch."""
+    g = wl.grammar
+    counts = np.bincount(wl.population.reshape(-1), minlength=256)
+    op_ids = {op: g.token_to_id[op] for op in g.operators}
+    var_ids = [g.token_to_id[v] for v in g.active_variables]
+    n_ops = float(sum(counts[i] for i in op_ids.values()))
+    n_mufu = float(sum(counts[op_ids[o]] for o in MUFU_OPS if o in op_ids))
+    n_var = float(sum(counts[i] for i in var_ids))
+    B = wl.population.shape[0]
+    D = wl.X.shape[1]
+    work = {"fp32": (n_ops + 3.0 * B) * D, "mufu": n_mufu * D, "smem": (n_var + B) * D}
+    t = {k: v / (PIPE_RATE[k] * sms * f_hz) for k, v in work.items()}
+    pipe = max(t, key=t.get)
+    node_evals = float(wl.n_tokens().sum()) * D
+    return {"pipe": pipe, "peak_node_evals_per_s": node_evals / t[pipe],
+            "per_pipe_T_node_evals_per_s": {k: node_evals / v / 1e12 for k, v in t.items()},
+            "per_node_eval": {k: v / node_evals for k, v in work.items()}}
+
+
+def fp64_error(wl, gpu_mse, oracle, tmap, n):
+    """Relative error of the FP32 GPU MSE against the FP64 oracle (correctly rounded C-library
+    operators) on the first n programs; programs invalid on either side are counted apart."""
+    ref = oracle.fitness(tmap, wl.population[:n], wl.X.astype(np.float64),
+                         wl.constants[:n].astype(np.float64), wl.y.astype(np.float64),
+                         policy="classic", loss="mse", invalid_value=1e15)
+    got = np.asarray(gpu_mse[:n], dtype=np.float64)
+    ok_ref, ok_got = ref < 1e14, got < 1e14
+    both = ok_ref & ok_got & (ref > 0)
+    rel = np.abs(got[both] - ref[both]) / ref[both]
+    # the same statistic for the FP32 oracle (IEEE C-library math): FP32's own conditioning
+    f32 = oracle.fitness(tmap, wl.population[:n], wl.X, wl.constants[:n], wl.y,
+                         policy="classic", loss="mse", invalid_value=1e15).astype(np.float64)
+    both32 = ok_ref & (f32 < 1e14) & (ref > 0)
+    rel32 = np.abs(f32[both32] - ref[both32]) / ref[both32]
+    ieee = {"median_rel": float(np.median(rel32)) if rel32.size else None,
+            "p99_rel": float(np.percentile(rel32, 99)) if rel32.size else None,
+            "max_rel": float(rel32.max()) if rel32.size else None,
+            "frac_within_1e-5": float((rel32 <= 1e-5).mean()) if rel32.size else None}
+    return {"programs": int(n), "valid_both": int(both.sum()), "fp32_ieee_oracle": ieee,
+            "class_mismatch": int((ok_ref != ok_got).sum()),
+            "median_rel": float(np.median(rel)) if rel.size else None,
+            "p99_rel": float(np.percentile(rel, 99)) if rel.size else None,
+            "max_rel": float(rel.max()) if rel.size else None,
+            "frac_within_1e-5": float((rel <= 1e-5).mean()) if rel.size else None,
+            "note": "the GPU runs the reference's fast-math FP32 intrinsics; the oracle runs "
+                    "FP64 C-library math, so ill-conditioned programs amplify the difference"}
 
 
 class ClockSampler:
@@ -328,10 +391,22 @@ def run_ours(args):
     if clocks.get("sm_mhz"):
         roof["frac_at_sampled_clock"] = achieved / (sms * 128 * clocks["sm_mhz"] * 1e6)
 
+    mix = op_mix_bound(wl, sms, f_max * 1e6)
+    roof["op_mix"] = {"bound": mix["pipe"], "achieved": achieved / 1e12,
+                      "peak": mix["peak_node_evals_per_s"] / 1e12,
+                      "unit": "T node-evals/s", "frac": achieved / mix["peak_node_evals_per_s"],
+                      "per_pipe_peak": mix["per_pipe_T_node_evals_per_s"],
+                      "ops_per_node_eval": mix["per_node_eval"],
+                      "assumes": "pipes at peak (FP32 128, MUFU 16, shared 32 four-byte loads per "
+                                 "clock per SM), one MUFU op per sin/cos/exp/log/sqrt/division, "
+                                 "tape decode and dispatch free"}
     cpu = None
+    err64 = None
     if not args.no_cpu_baseline and world == 1:
         oracle = load_oracle()
         cpu = cpu_baseline(args, wl, n_tok, oracle, vm.token_map())
+        err64 = fp64_error(wl, out.cpu().numpy(), oracle, vm.token_map(),
+                           min(512, wl.population.shape[0]))
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t_total / args.steps,
@@ -340,7 +415,8 @@ def run_ours(args):
             "config": config_dict(args, world),
             "node_evals_per_step_per_gpu": evals_per_step,
             "hbm_gbs": alg_bytes / (t_total / args.steps) / 1e9,
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "roofline": roof, "cpu_baseline": cpu, "fp64_error": err64, "e2e": e2e,
+            "clocks": clocks,
             # per step: descriptor write, compile, sort (hist, scan, scatter), evaluator
             "gpu_launches": 6 * args.steps * world,
             "wall_s_timed_region": wall}
@@ -371,19 +447,19 @@ def run_reference(args):
     while True:
         t0 = time.perf_counter()
         oracle.fitness(tmap, wl.population[:n], wl.X, wl.constants[:n], wl.y, policy="classic",
-                       loss="mse", nthreads=threads)
+                       loss="mse", nthreads=threads, timed=True)
         dt = time.perf_counter() - t0
         if dt > per_step / 3 or n >= wl.population.shape[0]:
             break
         n *= 2
     for _ in range(args.warmup):
         oracle.fitness(tmap, wl.population[:n], wl.X, wl.constants[:n], wl.y, policy="classic",
-                       loss="mse", nthreads=threads)
+                       loss="mse", nthreads=threads, timed=True)
     ts = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
         oracle.fitness(tmap, wl.population[:n], wl.X, wl.constants[:n], wl.y, policy="classic",
-                       loss="mse", nthreads=threads)
+                       loss="mse", nthreads=threads, timed=True)
         ts.append(time.perf_counter() - t0)
     evals = float(n_tok[:n].sum()) * D
     value = evals * len(ts) / sum(ts)
@@ -394,6 +470,7 @@ def run_reference(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
             "config": config_dict(args, world),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "build": "g++ " + " ".join(oracle.NATIVE_FLAGS) + " on this host",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference has no CPU evaluator (rpn_kernels.cu:10,382 rejects CPU "
@@ -1078,8 +1155,86 @@ def run_plain(args):
         dist.destroy_process_group()
 
 
+def run_opcost(args):
+    """Costs inside the fitness evaluator: (1) every compiled schedule on a quarter of the scale
+    workload (262,144 programs x 100,000 rows), evaluate-only launches; (2) per-operator costs
+    on single-operator programs (65,536 programs of 63 tokens, 100,000 rows): rows per SM clock
+    for one tape instruction, against the pipe's peak."""
+    import torch
+    entry.load_package()
+    from warpsymbolic_b200 import synthetic, _native as N
+    from warpsymbolic_b200.cuda_vm import CudaRPNVM
+    dev = torch.device("cuda", 0)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    peaks, _ = measured_peaks()
+    f_hz = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    def timed(vm, pop, X, c, y, sched, reps=5):
+        B, L = pop.shape
+        ws = torch.empty(N.lib().ws_fitness_workspace_bytes(B, L, N.WS_F32), dtype=torch.uint8,
+                         device=dev)
+        out = torch.empty(B, dtype=torch.float32, device=dev)
+        f = lambda ph: vm.eval_fitness(pop, X, c, y, policy="classic", loss="mse", out=out,
+                                       workspace_tensor=ws, phase=ph, schedule=sched)
+        f(N.WS_PHASE_COMPILE)
+        for _ in range(max(args.warmup, 3)):
+            f(N.WS_PHASE_EVALUATE)
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            f(N.WS_PHASE_EVALUATE)
+            b.record()
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return statistics.median(ms)
+
+    wl = synthetic.eval_scale_workload(seed=0, n_programs=262_144, n_rows=100_000)
+    vm = CudaRPNVM(wl.grammar, dev)
+    evals = float(wl.n_tokens().sum()) * wl.X.shape[1]
+    args_w = (T(wl.population), T(wl.X), T(wl.constants), T(wl.y))
+    sched = {}
+    n_row_pass = int(N.lib().ws_schedule_count()) - 5  # the last five are the small-D evaluator
+    for s_ in range(n_row_pass):
+        ms = timed(vm, *args_w, s_)
+        sched[s_] = {"ms": ms, "T_node_evals_per_s": evals / ms / 1e9}
+    g = wl.grammar
+    tid = g.token_to_id
+    B = 65_536
+    X, y = args_w[1], args_w[3]
+    cc = T(np.full((B, 8), 0.37, dtype=np.float32))
+
+    def prog(tokens):
+        p = np.zeros((B, 64), dtype=np.uint8)
+        p[:, :len(tokens)] = [tid[t] for t in tokens]
+        return T(p)
+
+    cases = {}
+    for u in ("sin", "cos", "exp", "log", "sqrt", "neg"):
+        cases["unary " + u] = (["x0"] + [u] * 62, 62)
+    for b in ("+", "-", "*", "/"):
+        vec, sca = ["x0"], ["x0"]
+        for i in range(31):
+            vec += ["x%d" % ((i + 1) % 5), b]
+            sca += ["C", b]
+        cases["binary %s variable" % b] = (vec, 31)
+        cases["binary %s constant" % b] = (sca, 31)
+    ops = {}
+    for name, (toks, n_instr) in cases.items():
+        ms = timed(vm, prog(toks), X, cc, y, 0)
+        ops[name] = {"ms": ms, "rows_per_sm_clock": B * 1e5 * n_instr / (ms * 1e-3 * sms * f_hz)}
+    print(json.dumps({"config": "opcost", "schedules": sched, "operators": ops,
+                      "pipe_peaks_rows_per_sm_clock": {"fp32 (paired f32x2: 256)": 128,
+                                                       "mufu": 16}}), flush=True)
+
+
 def main():
     args = parse()
+    if args.config == "opcost":
+        run_opcost(args)
+        return
     if args.config == "c1":
         run_plain(args)
         return

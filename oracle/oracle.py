@@ -138,9 +138,61 @@ POLICY = {"fused": 0, "classic": 1}
 LOSS = {"rmse": 0, "mse": 1, "r2": 2, "sse": 3}
 
 
+# ---- the timed CPU baseline -----------------------------------------------------------------
+# The same fitness restatement (ws_oracle.cpp) compiled for speed on the host that runs it:
+# -O3 -march=native -fopenmp, programs split across all host threads.  It is built where it
+# runs (a -march=native binary must not travel to another CPU), into _native/ under a key of the
+# host's CPU model and flags.  Timing only: with -O3 the compiler may contract a*b+c into FMAs, so
+# the IEEE build above (libws_oracle.so, -O2 -ffp-contract=off) stays the checker.
+NATIVE_FLAGS = ["-O3", "-march=native", "-fopenmp"]
+_timed = None
+
+
+def _host_key() -> str:
+    import hashlib
+    info = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith(("model name", "flags")):
+                    info += line
+                    if line.startswith("flags"):
+                        break
+    except OSError:
+        pass
+    return hashlib.sha1(info.encode()).hexdigest()[:12]
+
+
+def timed_lib_path() -> str:
+    return os.path.join(HERE, "_native", "libws_oracle_native_%s.so" % _host_key())
+
+
+def timed_lib():
+    """ctypes handle of the host-tuned fitness restatement (built on first use)."""
+    global _timed
+    if _timed is None:
+        path = timed_lib_path()
+        src = os.path.join(HERE, "ws_oracle.cpp")
+        if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+            os.makedirs(os.path.dirname(path), exist_ok=True)
+            tmp = path + ".tmp%d" % os.getpid()
+            subprocess.run(["g++", "-std=c++17", "-fPIC", "-shared"] + NATIVE_FLAGS +
+                           [src, "-o", tmp], check=True)
+            os.replace(tmp, path)
+        h = C.CDLL(path)
+        for suf in ("f32", "f64"):
+            getattr(h, "ws_oracle_fitness_" + suf).argtypes = [
+                _P, C.c_int64, C.c_int64, _P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P, C.c_int,
+                C.c_int, C.c_int, C.c_double, _P, _P, C.c_int]
+        h.ws_oracle_threads.restype = C.c_int
+        _timed = h
+    return _timed
+
+
 def fitness(tmap, pop, X, consts, y, strict=0, policy="fused", loss="rmse", invalid_value=None,
-            nthreads=0, with_ninv=False):
-    """ws_eval_fitness semantics (FP64 sum of T-rounded squares)."""
+            nthreads=0, with_ninv=False, timed=False):
+    """ws_eval_fitness semantics (FP64 sum of T-rounded squares).  timed=True runs the
+    host-tuned build (the timed CPU baseline) instead of the IEEE checker."""
     pop = np.ascontiguousarray(pop, dtype=np.uint8)
     X = np.ascontiguousarray(X)
     B, L = pop.shape
@@ -152,9 +204,10 @@ def fitness(tmap, pop, X, consts, y, strict=0, policy="fused", loss="rmse", inva
         invalid_value = 1e15 if X.dtype == np.float32 else 1e100
     out = np.empty(B, dtype=np.float64 if loss == "sse" else X.dtype)
     ninv = np.empty(B, dtype=np.int32)
-    getattr(lib(), "ws_oracle_fitness_" + _suffix(X.dtype))(
+    h = timed_lib() if timed else lib()
+    getattr(h, "ws_oracle_fitness_" + _suffix(X.dtype))(
         _p(pop), B, L, _p(X), V, D, _p(c), K, _p(y), C.byref(tmap), int(strict), POLICY[policy],
-        LOSS[loss], float(invalid_value), _p(out), _p(ninv), int(nthreads or threads()))
+        LOSS[loss], float(invalid_value), _p(out), _p(ninv), int(nthreads or h.ws_oracle_threads()))
     return (out, ninv) if with_ninv else out
 
 

@@ -66,8 +66,19 @@ def test_small_rows_faster_than_reference(population):
                                                   tl.E_VAL, 0, mode))
         tl.assert_fitness_close(o.cpu().numpy(), r.cpu().numpy(), rtol=1e-5, atol=1e-7,
                                 min_frac=1.0)
+        # where the drop-in's time goes: compile + length sort, and the evaluator alone
+        from warpsymbolic_b200 import _native as N
+        from warpsymbolic_b200.cuda_vm import CudaRPNVM
+        vm = CudaRPNVM(g, DEV)
+        ws = torch.empty(N.lib().ws_fitness_workspace_bytes(P.shape[0], P.shape[1], N.WS_F32),
+                         dtype=torch.uint8, device=DEV)
+        ph = lambda k: vm.eval_fitness(P, X, C, y, policy="fused", loss="rmse", out=o,
+                                       workspace_tensor=ws, phase=k)
+        t_compile = _time(lambda: ph(N.WS_PHASE_COMPILE))
+        t_eval = _time(lambda: ph(N.WS_PHASE_EVALUATE))
         table[D] = {"reference_ms": t_ref, "dropin_ms": t_our, "speedup": t_ref / t_our,
                     "reference_launch_mode": mode,
+                    "dropin_compile_and_sort_ms": t_compile, "dropin_evaluate_ms": t_eval,
                     "dropin_node_evals_per_s": n_tok * D / (t_our * 1e-3)}
     tl.write_report("reference_speed_small.json", table)
     slower = {D: v for D, v in table.items() if v["dropin_ms"] > v["reference_ms"]}
