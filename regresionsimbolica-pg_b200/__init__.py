@@ -9,6 +9,8 @@ Drop-in for the reference's native extension `rpn_cuda_native` and its Python ca
   cuda_vm      -- CudaRPNVM mirror (eval, eval_fused, eval_fitness)
   evaluation   -- GPUEvaluator mirror (evaluate_batch, validate_strict, ...)
   rpn_cuda_native -- the extension drop-in (same function names and signatures)
+  population   -- GPUOperators' random generation and repair of invalid individuals
+  reference_engine -- runs the reference's own estimator / engine on a chosen native module
   _native      -- ctypes binding of libwarpsym.so (include/warpsym.h)
 """
 __version__ = "0.1.0"
