@@ -49,8 +49,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--config", default="eval-scale",
-                    choices=["eval-scale", "batched", "serving", "kernels", "constopt", "c1",
-                             "opcost"],
+                    choices=["eval-scale", "batched", "serving", "serving-ramp", "kernels",
+                             "constopt", "c1", "opcost"],
                     help="eval-scale: the evaluation-only scale test (default); batched: 256 "
                          "uneven problems scored by one graph-replayed launch per generation; "
                          "serving: a Poisson stream of fit/evaluate requests, continuously "
@@ -60,12 +60,16 @@ def parse():
                          "rows; c1: the reference's own estimator and engine fitting the "
                          "plain-method workload (1024x2 rows, population 1024, 20 "
                          "generations), on this library's drop-in (--impl ours) or on the "
-                         "reference extension (--impl reference); opcost: costs inside the "
+                         "reference extension (--impl reference); serving-ramp: sustainable "
+                         "request rate of both serving paths under a p99 bound; opcost: costs "
+                         "inside the "
                          "fitness evaluator (schedule sweep, per-operator rows per clock)")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="kernels: fraction of the default sizes (smaller cases for profiling)")
     ap.add_argument("--requests", type=int, default=8)
     ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
+    ap.add_argument("--ramp", default="20,40,80,160,320,640,1280",
+                    help="serving-ramp: arrival rates (requests/s) to serve")
     ap.add_argument("--problems", type=int, default=256)
     ap.add_argument("--generations", type=int, default=50)
     ap.add_argument("--constopt-programs", type=int, default=65_536)
@@ -713,6 +717,100 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serving_ramp(args):
+    """Sustainable request rate under a latency bound, continuous batching against the plain
+    path.  The bound is the plain path's p99 latency at the configured rate (20 requests/s).
+    Then, for each arrival rate of the ramp (`--ramp`, requests/s), the same seeded stream of
+    `--requests` requests (serving-config distributions: fit:evaluate 1:1, population 4,096,
+    30 generations, rows log-U[1e3, 2e5], 1-8 variables) is served by both paths in real time;
+    every request's result must be identical on both.  A path sustains a rate when its p99
+    stays within the bound; its sustainable rate is the highest such rate of the ramp."""
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    entry.load_package()
+    from warpsymbolic_b200 import synthetic
+    from warpsymbolic_b200.serving import (ContinuousBatchingServer, serve_plain,
+                                           latency_summary)
+    n = max(args.requests, 16)
+    rates = [float(r) for r in args.ramp.split(",")]
+
+    def same(a_res, b_res):
+        ok = True
+        for a, b in zip(a_res, b_res):
+            if a.kind == "evaluate":
+                ok &= bool(np.array_equal(a.losses, b.losses, equal_nan=True))
+            else:
+                ok &= a.best_loss == b.best_loss and bool(np.array_equal(a.best_program,
+                                                                         b.best_program))
+        return ok
+
+    def work(reqs):  # node-evals of every evaluation the stream asks for
+        return sum(float((r.population != 0).sum()) * r.X.shape[1]
+                   * ((r.generations + 1) if r.kind == "fit" else 1) for r in reqs)
+
+    def serve_both(reqs):
+        srv = ContinuousBatchingServer(dev)
+        b = srv.serve(reqs, realtime=True)
+        mk_b = max(r.done for r in b) - min(r.arrival for r in b)
+        p = serve_plain(reqs, dev, realtime=True)
+        mk_p = max(r.done for r in p) - min(r.arrival for r in p)
+        sb, sp = latency_summary(b, mk_b), latency_summary(p, mk_p)
+        w = work(reqs)
+        sb["node_evals_per_s"] = w / mk_b
+        sp["node_evals_per_s"] = w / mk_p
+        return sb, sp, same(b, p)
+
+    warm = synthetic.serving_stream(seed=args.seed, n_requests=n, rate=args.rate)
+    ContinuousBatchingServer(dev).serve(warm, realtime=False)
+    serve_plain(warm, dev, realtime=False)
+    torch.cuda.synchronize()
+    # the heaviest request of the stream served alone: no schedule can finish it sooner
+    heavy = max(warm, key=lambda r: work([r]))
+    import dataclasses
+    solo = serve_plain([dataclasses.replace(heavy, arrival=0.0)], dev, realtime=False)[0]
+    solo_s = solo.latency
+    with ClockSampler(0) as clk:
+        b0, p0, ok0 = serve_both(warm)
+        bound = p0["p99_s"]
+        curve = []
+        identical = ok0
+        for rate in rates:
+            reqs = synthetic.serving_stream(seed=args.seed, n_requests=n, rate=rate)
+            sb, sp, ok = serve_both(reqs)
+            identical &= ok
+            curve.append({"rate_req_s": rate, "batched": sb, "plain": sp, "identical": ok})
+    sus = {}
+    for path in ("batched", "plain"):
+        good = [c["rate_req_s"] for c in curve if c[path]["p99_s"] <= bound]
+        sus[path] = max(good) if good else None
+    top = curve[-1]
+    line = {"metric": "sustainable served request rate under a p99 bound, continuous batching "
+                      "vs plain", "value": sus["batched"], "unit": "requests/s",
+            "n_gpus": 1, "steps": len(rates), "warmup": 1, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Poisson streams with the serving config's distributions)",
+            "config": {"workload": "serving ramp: %d requests per rate, rates %s req/s, "
+                                   "fit:evaluate 1:1, population 4096, 30 generations, rows "
+                                   "log-U[1e3,2e5], vars U{1..8}" % (n, args.ramp),
+                       "p99_bound_s": bound,
+                       "p99_bound": "plain path's p99 at %g requests/s" % args.rate},
+            "heaviest_request_alone_s": solo_s,
+            "heaviest_request": {"kind": heavy.kind, "rows": int(heavy.X.shape[1]),
+                                 "programs": int(heavy.population.shape[0]),
+                                 "generations": int(getattr(heavy, "generations", 0))},
+            "sustainable_req_s": sus,
+            "sustainable_ratio": (sus["batched"] / sus["plain"]
+                                  if sus["batched"] and sus["plain"] else None),
+            "at_configured_rate": {"batched": b0, "plain": p0},
+            "at_top_rate": {"rate_req_s": top["rate_req_s"],
+                            "throughput_ratio": top["batched"]["throughput_req_s"]
+                            / top["plain"]["throughput_req_s"],
+                            "p99_ratio": top["plain"]["p99_s"] / top["batched"]["p99_s"]},
+            "curve": curve, "identical_results": identical, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def run_constopt(args):
     """Constant optimisation: 65,536 programs (lengths U{5..40}, 2..8 constants each, K = 8),
     X ~ N(0,1)^{3 x 16,384}, y from a depth-4 tree plus 1% noise.  One step = PSO (32 particles x
@@ -1047,6 +1145,57 @@ def run_kernels(args):
     timed("gp_generation", gps.step, nbytes=nch * (L + 8 * 4) * 3,
           note="%d problems x 2048 children (3 launches)" % len(probs))
     gps.close()
+    # diversity: hashes and variable masks, structural dedup (insert + lookup), unique count,
+    # replacement positions, fitness sharing
+    x0id = g.token_to_id["x0"]
+    hsh = torch.empty(B1, dtype=torch.int64, device=dev)
+    vpr = torch.empty(B1, dtype=torch.int32, device=dev)
+    timed("compute_population_hashes", lambda: R.compute_population_hashes(dpop, hsh, vpr, 0,
+                                                                           x0id, 5),
+          nbytes=B1 * (L + 8 + 4), note="%d x %d" % (B1, L))
+    table = torch.empty(1 << 21, dtype=torch.int64, device=dev)
+    dup = torch.empty(B1, dtype=torch.int32, device=dev)
+    orig = torch.empty(B1, dtype=torch.int64, device=dev)
+
+    def dedup():
+        table.fill_(-1)
+        R.structural_dedup(hsh, table, dup, orig)
+    timed("structural_dedup", dedup, nbytes=B1 * (8 + 4 + 8) + (1 << 21) * 8,
+          note="%d hashes into a 2^21-slot table (the table reset included)" % B1)
+    pos = torch.empty(B1, dtype=torch.int64, device=dev)
+    nrep = torch.zeros(1, dtype=torch.int64, device=dev)
+    timed("get_replacement_positions", lambda: R.get_replacement_positions(dup, pos, nrep),
+          nbytes=B1 * 4, note="%d flags (one block)" % B1)
+    timed("fitness_sharing_penalty", lambda: R.fitness_sharing_penalty(dpop, 4, B1 // 4, 2, 8),
+          nbytes=B1 * (L + 4), note="%d programs, 4 islands" % B1)
+    # evolve_generation: selection, crossover, mutation, constant operators (no PSO steps)
+    Be, Le, De = sc(262_144), 40, 64
+    ge = GPUGrammar(num_variables=3, operators=synthetic.BENCH_OPERATORS)
+    pe = synthetic.random_programs(ge, Be, 2, Le, Le, rng, const_prob=0.4, max_consts=8)
+    are = np.array(ge.arities(), dtype=np.int32)
+    ide = np.arange(ge.vocab_size)
+    ev = dict(pop=T(pe), c=T(rng.uniform(-2, 2, size=(Be, 8)).astype(np.float32)),
+              fit=T(rng.uniform(0.1, 5.0, size=Be).astype(np.float32)),
+              X=T(rng.uniform(-2, 2, size=(3, De)).astype(np.float32)),
+              lens=T((pe != 0).sum(1).astype(np.float32)),
+              bank=T(synthetic.random_programs(ge, 1024, 2, Le, Le, rng, max_consts=8)))
+    ev["y"] = (torch.sin(ev["X"][0]) + ev["X"][1] * ev["X"][2]).contiguous()
+    e64 = torch.empty(0, dtype=torch.int64, device=dev)
+    ef = torch.empty(0, dtype=torch.float32, device=dev)
+    argse = (T(are), T(ide[(are == 0) & (ide != 0)].astype(np.uint8)),
+             T(ide[are == 1].astype(np.uint8)), T(ide[are == 2].astype(np.uint8)))
+    timed("evolve_generation", lambda: R.evolve_generation(
+        ev["pop"], ev["c"], ev["fit"], ef, ev["X"], ev["y"], ev["lens"], *argse, ev["bank"], ef,
+        0.2, 0.5, 4, 0, 0, 0.5, 1.5, 1.5, *ge.scalar_ids(), PI_VAL, E_VAL, 4, e64, e64, e64, e64,
+        12345, 3),
+          nbytes=Be * (Le + 32) * 3, note="%d x %d, bank 1024, 4 islands, tournament 4, no PSO "
+                                          "(selection, crossover, mutation, constants)" % (Be, Le))
+    # per-program L-BFGS with adjoint gradients (loss_grad buckets + state launches)
+    Bl = sc(8192)
+    timed("lbfgs_adjoint", lambda: constfit.lbfgs(dp3[:Bl], X3, c3[:Bl], y3, ids3, max_iter=5,
+                                                  history_size=5),
+          evals=float((p3[:Bl] != 0).sum()) * D3,
+          note="%d programs x %d rows, 5 iterations, history 5 (evals: one pass)" % (Bl, D3))
     print(json.dumps({"config": "kernels", "kernels": len(out)}), flush=True)
 
 
@@ -1240,6 +1389,14 @@ def main():
         return
     if args.config == "kernels":
         run_kernels(args)
+        return
+    if args.config == "serving-ramp":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "config": "serving-ramp",
+                              "unavailable": "the reference has no serving loop; the plain "
+                                             "one-request-at-a-time path is timed beside ours"}))
+            return
+        run_serving_ramp(args)
         return
     if args.config == "serving":
         if args.impl == "reference":

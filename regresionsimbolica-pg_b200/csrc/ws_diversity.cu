@@ -124,33 +124,67 @@ __global__ void __launch_bounds__(256) dedup_lookup_kernel(const int64_t* __rest
   }
 }
 
-// One block: programs split into 1024 contiguous chunks, per-chunk counts, a block scan, then
-// each chunk writes its duplicates in order (ascending positions).  count_only: the number of
-// non-duplicates instead.
+// One block walks the flags in tiles of 1024 threads x 16 flags: each thread loads its 16
+// consecutive flags (four 16-byte loads when aligned: a warp reads 2 KB contiguous), keeps the
+// selected ones as a bit mask, and a block scan of the per-thread counts (warp shuffles, then the
+// 32 warp totals) gives every thread its first output position; positions come out ascending, the
+// running total carries from tile to tile.  count_unique: count the non-duplicates instead.
+constexpr int kScanPer = 16;
 __global__ void __launch_bounds__(1024) dup_scan_kernel(const int32_t* __restrict__ dup,
                                                         int64_t B, int64_t* __restrict__ pos,
                                                         int64_t* __restrict__ count,
                                                         int count_unique) {
-  __shared__ int64_t s[1024];
-  const int t = threadIdx.x;
-  const int64_t per = (B + 1023) / 1024;
-  const int64_t a = (int64_t)t * per;
-  const int64_t e = a + per < B ? a + per : B;
-  int64_t c = 0;
-  for (int64_t i = a; i < e; ++i) c += count_unique ? (dup[i] == 0) : (dup[i] == 1);
-  s[t] = c;
-  __syncthreads();
-  for (int o = 1; o < 1024; o <<= 1) {  // inclusive scan
-    const int64_t v = t >= o ? s[t - o] : 0;
+  __shared__ int64_t wsum[32];
+  __shared__ int64_t s_total;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int want = count_unique ? 0 : 1;
+  const bool vec = ((uintptr_t)dup & 15u) == 0;
+  const bool write = !count_unique && pos != nullptr;
+  int64_t base = 0;  // selected flags before this tile (the same in every thread)
+  for (int64_t t0 = 0; t0 < B; t0 += 1024 * kScanPer) {
+    const int64_t i0 = t0 + (int64_t)t * kScanPer;
+    uint32_t bits = 0u;
+    if (vec && i0 + kScanPer <= B) {
+      const int4* src = reinterpret_cast<const int4*>(dup + i0);
+#pragma unroll
+      for (int q = 0; q < kScanPer / 4; ++q) {
+        const int4 v = src[q];
+        bits |= (uint32_t)(v.x == want) << (4 * q) | (uint32_t)(v.y == want) << (4 * q + 1) |
+                (uint32_t)(v.z == want) << (4 * q + 2) | (uint32_t)(v.w == want) << (4 * q + 3);
+      }
+    } else {
+      for (int k = 0; k < kScanPer; ++k)
+        if (i0 + k < B && dup[i0 + k] == want) bits |= 1u << k;
+    }
+    const int c = __popc(bits);
+    int incl = c;  // inclusive scan over the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) wsum[w] = incl;  // warp totals
     __syncthreads();
-    s[t] += v;
+    if (w == 0) {  // exclusive offsets of the warps (each lane rewrites its own slot only)
+      const int64_t v = wsum[lane];
+      int64_t iv = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int64_t u = __shfl_up_sync(0xFFFFFFFFu, iv, o);
+        if (lane >= o) iv += u;
+      }
+      wsum[lane] = iv - v;
+      if (lane == 31) s_total = iv;  // the tile's selected flags
+    }
     __syncthreads();
+    if (write && bits) {
+      int64_t o = base + wsum[w] + (incl - c);
+      for (uint32_t m = bits; m; m &= m - 1) pos[o++] = i0 + __ffs(m) - 1;
+    }
+    base += s_total;
+    __syncthreads();  // wsum and s_total are rewritten by the next tile
   }
-  if (t == 1023) count[0] = s[1023];
-  if (count_unique || !pos) return;
-  int64_t w = s[t] - c;
-  for (int64_t i = a; i < e; ++i)
-    if (dup[i] == 1) pos[w++] = i;
+  if (t == 0) count[0] = base;
 }
 
 // fitness_sharing_hash8 / count / penalty kernels (diversity_kernels.cu:224-319): the first

@@ -310,6 +310,82 @@ __global__ void __launch_bounds__(128) hoist_rows_kernel(uint8_t* pop,
   }
 }
 
+// The same hoist with one warp per row (rows of at most kHoistStagedL tokens): the row and the
+// arity table sit in shared memory, each lane runs the backward subtree scan for its own end
+// positions e = lane, lane + 32, ..., and the reservoir sampling then walks the valid positions
+// in ascending order from a ballot mask -- the same LCG steps and the same picks as one thread
+// walking e = 0, 1, 2, ... -- identically in every lane.
+constexpr int kHoistStagedL = 255;
+constexpr int kHoistWarps = 4;
+__global__ void __launch_bounds__(32 * kHoistWarps) hoist_rows_warp_kernel(
+    uint8_t* pop, const int64_t* __restrict__ rows, int64_t N, int L,
+    const int32_t* __restrict__ ar, int vocab, const int64_t* __restrict__ rand_ints, int pad) {
+  __shared__ int32_t s_ar[256];
+  __shared__ uint8_t s_row[kHoistWarps][256];
+  __shared__ uint8_t s_start[kHoistWarps][256];
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) s_ar[t] = t < vocab ? ar[t] : 0;
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t* srow = s_row[w];
+  uint8_t* sst = s_start[w];
+  for (int64_t n = (int64_t)blockIdx.x * kHoistWarps + w; n < N;
+       n += (int64_t)gridDim.x * kHoistWarps) {
+    uint8_t* row = pop + rows[n] * (int64_t)L;
+    int len = L;  // the first PAD
+    for (int c0 = 0; c0 < L; c0 += 32) {
+      const int i = c0 + lane;
+      const uint8_t b = i < L ? row[i] : (uint8_t)pad;
+      if (i < L) srow[i] = b;
+      const unsigned m = __ballot_sync(0xFFFFFFFFu, i < L && (int)b == pad);
+      if (m) {
+        len = c0 + __ffs(m) - 1;
+        break;
+      }
+    }
+    __syncwarp();
+    const uint64_t state0 = (uint64_t)rand_ints[n];
+    uint64_t state = state0;
+    int pick_s = -1, pick_e = -1, seen = 0;
+    for (int c0 = 0; c0 < len; c0 += 32) {
+      const int e = c0 + lane;
+      bool ok = false;
+      int s = e;
+      if (e < len) {
+        const int a = s_ar[srow[e]];
+        ok = a == 0;
+        if (a > 0) {
+          int need = a;
+          for (int j = e - 1; j >= 0; --j) {
+            need += s_ar[srow[j]] - 1;
+            if (need == 0) {
+              s = j;
+              ok = true;
+              break;
+            }
+          }
+        }
+        sst[e] = (uint8_t)s;
+      }
+      unsigned m = __ballot_sync(0xFFFFFFFFu, ok);
+      __syncwarp();
+      for (; m; m &= m - 1) {  // valid subtrees in ascending end position: reservoir sampling
+        const int e2 = c0 + __ffs(m) - 1;
+        ++seen;
+        state = state * 6364136223846793005ull + 1ull;
+        if (state % (uint64_t)seen == 0) {
+          pick_e = e2;
+          pick_s = sst[e2];
+        }
+      }
+    }
+    if (pick_e >= 0) {
+      const int cnt = pick_e - pick_s + 1;
+      for (int i = lane; i < L; i += 32) row[i] = i < cnt ? srow[pick_s + i] : (uint8_t)pad;
+    }
+    __syncwarp();  // the row buffers are rewritten for the next row
+  }
+}
+
 unsigned grid_for(int64_t n, int threads) {
   const int64_t g = (n + threads - 1) / threads;
   return (unsigned)(g < 65535 * 16 ? (g > 0 ? g : 1) : 65535 * 16);
@@ -427,7 +503,13 @@ extern "C" ws_status ws_hoist_rows(uint8_t* population, const int64_t* rows, int
   if (N < 0 || L < 1 || L > 65535) return fail("hoist_rows: bad shape");
   if (N == 0) return WS_OK;
   if (!population || !rows || !arities || !rand_ints) return fail("null tensor pointer");
-  hoist_rows_kernel<<<grid_for(N, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(
-      population, rows, N, (int)L, arities, vocab, rand_ints, pad_id);
+  if (L <= kHoistStagedL && vocab <= 256) {
+    hoist_rows_warp_kernel<<<grid_for(N, kHoistWarps), 32 * kHoistWarps, 0,
+                             static_cast<cudaStream_t>(stream)>>>(
+        population, rows, N, (int)L, arities, vocab, rand_ints, pad_id);
+  } else {
+    hoist_rows_kernel<<<grid_for(N, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        population, rows, N, (int)L, arities, vocab, rand_ints, pad_id);
+  }
   return launched("hoist_rows");
 }

@@ -96,3 +96,23 @@ def test_identical_to_reference():
     for d in (r, o):
         assert np.array_equal(d["pos"], np.nonzero(d["dup"])[0])
     assert (o["pen"] > 0).any()
+
+
+@pytest.mark.parametrize("B,shift", [(100_003, 0), (70_001, 1), (16_384, 0), (16_385, 1),
+                                     (1, 0), (0, 0)])
+def test_replacement_positions_and_count_across_tiles(B, shift):
+    """The flag scan walks tiles of 16,384 flags: several tiles, a partial last tile, and a
+    flag array whose base is not 16-byte aligned (scalar loads) against numpy."""
+    from warpsymbolic_b200 import rpn_cuda_native as ours
+    rng = np.random.default_rng(B + shift)
+    flags = (rng.random(B) < 0.3).astype(np.int32)
+    buf = torch.empty(B + 4, dtype=torch.int32, device=DEV)
+    dup = buf[shift:shift + B]
+    dup.copy_(torch.from_numpy(flags).to(DEV))
+    assert ours.count_unique(dup) == int((flags == 0).sum())
+    pos = torch.empty(max(B, 1), dtype=torch.int64, device=DEV)
+    nr = torch.zeros(1, dtype=torch.int64, device=DEV)
+    n = ours.get_replacement_positions(dup, pos, nr)
+    want = np.nonzero(flags == 1)[0]
+    assert n == len(want) == int(nr.item())
+    assert np.array_equal(pos.cpu().numpy()[:n], want)
