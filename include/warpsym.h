@@ -677,7 +677,10 @@ ws_status ws_tournament_select_offsets(const float* fitness, int64_t B, const fl
  *   ws_debug_compile    -- compiles ONE host program into the evaluator's tape (ctrl words and
  *                          immediates, capacity max(L,1)); hdr_out = {n_instr, status
  *                          (0 ok / 1 statically invalid), spill slots, tokens};
- *   ws_debug_run_tape   -- scalar host interpretation of such a tape over D rows of a host x.
+ *   ws_debug_run_tape   -- scalar host interpretation of such a tape over D rows of a host x;
+ *   ws_debug_compile_agree -- compiles B host programs with both of the compiler's emitters
+ *                          (depth-first and linear) and counts the programs whose tapes differ
+ *                          (the device compiles with the linear one).
  */
 ws_status ws_debug_token_lut(const ws_token_map* ids, int64_t num_vars, int32_t fused_order,
                              uint8_t* cls_out, uint8_t* arg_out);
@@ -688,6 +691,10 @@ ws_status ws_debug_compile(int32_t dtype, const uint8_t* prog, int64_t L, const 
 ws_status ws_debug_run_tape(int32_t dtype, const uint32_t* ctrl, const double* imm, int32_t n,
                             const void* x, int64_t D, int32_t strict_mode, void* out_pred,
                             uint8_t* out_err);
+ws_status ws_debug_compile_agree(int32_t dtype, const uint8_t* progs, int64_t B, int64_t L,
+                                 const void* consts, int64_t K, const ws_token_map* ids,
+                                 int64_t num_vars, int32_t strict_mode, int32_t fused_order,
+                                 int32_t xmul, int64_t* mismatches_out);
 
 #ifdef __cplusplus
 }

@@ -199,6 +199,8 @@ _SIGS = {
     "ws_debug_compile": (_I32, [_I32, _P, _I64, _P, _I64, C.POINTER(TokenMap), _I64, _I32, _I32,
                                 _P, _P, _P]),
     "ws_debug_run_tape": (_I32, [_I32, _P, _P, _I32, _P, _I64, _I32, _P, _P]),
+    "ws_debug_compile_agree": (_I32, [_I32, _P, _I64, _I64, _P, _I64, C.POINTER(TokenMap),
+                                      _I64, _I32, _I32, _I32, _P]),
 }
 
 _lib = None

@@ -144,7 +144,9 @@ struct Emitter {
   int xmul;        // RC / pass
   int cap;         // capacity of `out`
   bool ok = true;  // false if an operand is not representable in the tape word
-  WS_HD void put(uint32_t c, T imm) {
+  WS_HD void put(uint32_t c, T imm) { put_at(n++, c, imm); }
+  // Encodes logical word c at tape position pos (the same lowering as put).
+  WS_HD void put_at(int pos, uint32_t c, T imm) {
     uint32_t w = lower_case(c);
     if (c & F_SPILL) w |= P_SLOW | P_SPILL | (((c >> SH_SLOT) & 7u) << P_SH_SLOT);
     const uint32_t la = (c >> SH_LA) & 3u, lai = (c >> SH_LA_IDX) & 63u;
@@ -168,12 +170,12 @@ struct Emitter {
     } else if (opk == OK_SCALAR && (c & F_OP_PARAM)) {
       ok = false;
     }
-    if (n >= cap) { ok = false; return; }
+    if (pos >= cap) { ok = false; return; }
     Instr<T> ins;
     ins.ctrl = w;
     ins.imm = imm;
     if constexpr (sizeof(Instr<T>) == 16) reinterpret_cast<Instr<double>&>(ins).pad = 0;
-    out[n++] = ins;
+    out[pos] = ins;
   }
 };
 
@@ -440,6 +442,208 @@ __host__ __device__ ProgHdr compile_program(const uint8_t* __restrict__ prog, in
     }
   }
   h.n_instr = em.n;
+  h.n_slots = max_depth;
+  if (!em.ok) h.status = PROG_UNREPRESENTABLE;
+  return h;
+}
+
+
+// ---- the same compiler with a linear emission -------------------------------------------------
+// compile_program_v2 produces the tape of compile_program, word for word, with less divergent
+// control flow for a GPU thread per program: the parse keeps the operator-node counts of every
+// subtree, and the emission replaces the depth-first walk with two linear passes.  Pass 1 visits
+// the nodes from the root down (creation order reversed: a parent is created after its children)
+// and gives every operator its tape position, its spill depth and, for the first instruction of
+// a subtree that must spill ACC, that spill: for a binary node whose children are both
+// operators, the child with the larger Sethi-Ullman need (the left one on a tie) owns the first
+// cnt(first) positions of the parent's range, the other child the next cnt(second), the parent
+// the last; the second child's first instruction spills ACC into slot depth.  Pass 2 writes every
+// operator's word at its position.
+enum : uint8_t { ER_ASSIGNED = 1, ER_SPILL = 2, ER_FIRST_LEFT = 4 };
+struct EmitRec {
+  int16_t pos;    // tape position of the node's own instruction
+  uint8_t depth;  // pending spilled values when the node's subtree starts
+  uint8_t flags;  // ER_*; with ER_SPILL, slot = bits 3..5
+};
+
+template <typename T, bool STRICT, bool BAKE, int LMAX>
+__host__ __device__ ProgHdr compile_program_v2(const uint8_t* __restrict__ prog, int L,
+                                               const T* __restrict__ consts, int K,
+                                               const TokenLut& lut, Instr<T>* __restrict__ tape,
+                                               int xmul) {
+  Node<T> nodes[LMAX];
+  uint8_t cnt[LMAX];  // operator nodes in each node's subtree (< 256: at most L - 1 <= 255)
+  EmitRec er[LMAX];
+  int16_t stk[33];
+  ProgHdr h;
+  h.n_instr = 0;
+  h.status = PROG_OK;
+  h.n_slots = 0;
+  h.n_tok = 0;
+  int sp = 0, nn = 0, c_idx = 0;
+  const int Lr = L < LMAX ? L : LMAX;
+
+  for (int pc = 0; pc < Lr; ++pc) {
+    const int tok = prog[pc];
+    const int cls = lut.cls[tok];
+    if (cls == T_PAD) break;
+    h.n_tok++;
+    const bool leaf = is_leaf(cls), bin = is_binary(cls), un = is_unary(cls);
+    if (!leaf && !bin && !un) { h.status = PROG_INVALID; break; }
+    const int ar = bin ? 2 : (un ? 1 : 0);
+    if (sp < ar) { h.status = PROG_INVALID; break; }
+    Node<T> nd;
+    nd.cls = leaf ? 0 : (uint8_t)cls;
+    nd.idx = 0;
+    nd.need = 0;
+    nd.imm = (T)0;
+    nd.l = nd.r = -1;
+    uint8_t c_ops = 0;
+    if (leaf) {
+      if (cls == T_VAR) {
+        nd.kind = N_VAR;
+        nd.idx = lut.arg[tok];
+      } else if (cls == T_CONST) {
+        nd.kind = N_IMM;
+        if (K > 0) {
+          const int slot = c_idx < K ? c_idx : K - 1;
+          c_idx++;
+          if (BAKE) {
+            nd.imm = consts[slot];
+          } else {
+            nd.kind = N_PARAM;
+            nd.idx = (uint8_t)slot;
+          }
+        } else {
+          nd.imm = (T)1.0;
+        }
+      } else {
+        nd.kind = N_IMM;
+        nd.imm = (T)lut.lit[lut.arg[tok]];
+      }
+      if (sp >= 32) continue;  // a push at depth 32 is dropped (the C slot was still consumed)
+    } else {
+      const int r = stk[sp - 1];
+      const int l = bin ? stk[sp - 2] : r;  // a unary operator's child is its left
+      sp -= ar;
+      const Node<T>& L_ = nodes[l];
+      const Node<T>& R_ = nodes[r];
+      if (L_.kind == N_IMM && R_.kind == N_IMM) {  // fold (for a unary node L_ is R_)
+        bool e = false;
+        nd.imm = bin ? apply_binary<T, STRICT>(cls, L_.imm, R_.imm, e)
+                     : apply_unary<T, STRICT>(cls, L_.imm, e);
+        if (e) { h.status = PROG_INVALID; break; }
+        nd.kind = N_IMM;
+      } else {
+        nd.kind = N_OP;
+        nd.l = (int16_t)l;
+        nd.r = bin ? (int16_t)r : (int16_t)-1;
+        const int a = L_.need, b = bin ? R_.need : 0;
+        int need;
+        if (!bin) need = a > 1 ? a : 1;
+        else if (a == 0 && b == 0) need = 1;
+        else if (a == 0) need = b;
+        else if (b == 0) need = a;
+        else need = (a == b) ? a + 1 : (a > b ? a : b);
+        nd.need = (uint8_t)need;
+        c_ops = (uint8_t)(1 + cnt[l] + (bin ? cnt[r] : 0));
+      }
+    }
+    nodes[nn] = nd;
+    cnt[nn] = c_ops;
+    stk[sp++] = (int16_t)nn++;
+  }
+  if (h.status == PROG_OK && sp != 1) h.status = PROG_INVALID;
+  if (h.status != PROG_OK) return h;
+
+  Emitter<T> em{tape, 0, xmul, tape_capacity(Lr)};
+  const int root = stk[0];
+  if (nodes[root].kind != N_OP) {  // the whole program is one terminal (or folded constant)
+    T imm = (T)0;
+    uint32_t bits = loada_bits(nodes[root], imm);
+    em.put(CASE_NOP | bits, imm);
+    h.n_instr = em.n;
+    if (!em.ok) h.status = PROG_UNREPRESENTABLE;
+    return h;
+  }
+  // pass 1: positions, depths, spills (parents before children)
+  for (int i = 0; i <= root; ++i) er[i].flags = 0;
+  er[root].pos = (int16_t)(cnt[root] - 1);
+  er[root].depth = 0;
+  er[root].flags = ER_ASSIGNED;
+  int max_depth = 0;
+  for (int v = root; v >= 0; --v) {
+    const uint8_t f = er[v].flags;
+    if (!(f & ER_ASSIGNED) || nodes[v].kind != N_OP) continue;
+    const Node<T>& nd = nodes[v];
+    const int pe = er[v].pos, d = er[v].depth;
+    const uint8_t spill = f & (uint8_t)(ER_SPILL | (7u << 3));
+    const bool lop = nodes[nd.l].kind == N_OP;
+    const bool rop = is_binary(nd.cls) && nodes[nd.r].kind == N_OP;
+    if (lop && rop) {
+      const bool first_left = nodes[nd.l].need >= nodes[nd.r].need;
+      const int F = first_left ? nd.l : nd.r, S = first_left ? nd.r : nd.l;
+      er[S].pos = (int16_t)(pe - 1);
+      er[S].depth = (uint8_t)(d + 1);
+      er[S].flags = (uint8_t)(ER_ASSIGNED | ER_SPILL | ((d & 7) << 3));
+      er[F].pos = (int16_t)(pe - 1 - cnt[S]);
+      er[F].depth = (uint8_t)d;
+      er[F].flags = (uint8_t)(ER_ASSIGNED | spill);
+      er[v].flags = (uint8_t)(ER_ASSIGNED | (first_left ? ER_FIRST_LEFT : 0));
+      if (d + 1 > max_depth) max_depth = d + 1;
+    } else if (lop || rop) {  // the operator child's subtree starts this node's range
+      const int c = lop ? nd.l : nd.r;
+      er[c].pos = (int16_t)(pe - 1);
+      er[c].depth = (uint8_t)d;
+      er[c].flags = (uint8_t)(ER_ASSIGNED | spill);
+      er[v].flags = ER_ASSIGNED;
+    }
+    // no operator child: this node's instruction is its subtree's first and keeps the spill
+  }
+  // pass 2: every operator's word at its position
+  for (int v = 0; v <= root; ++v) {
+    const uint8_t f = er[v].flags;
+    if (!(f & ER_ASSIGNED) || nodes[v].kind != N_OP) continue;
+    const Node<T>& nd = nodes[v];
+    const uint32_t sb = spill_bits((f & ER_SPILL) != 0, (f >> 3) & 7);
+    const Node<T>& L_ = nodes[nd.l];
+    T imm = (T)0;
+    uint32_t bits;
+    if (is_unary(nd.cls)) {
+      bits = L_.kind != N_OP ? (sb | loada_bits(L_, imm) | nd.cls) : (uint32_t)nd.cls;
+    } else {
+      const Node<T>& R_ = nodes[nd.r];
+      const bool lop = L_.kind == N_OP, rop = R_.kind == N_OP;
+      bool is_vec;
+      if (!lop && !rop) {
+        bits = sb;
+        if (L_.kind == N_VAR) {
+          bits |= loada_bits(L_, imm);
+          bits |= opnd_bits(R_, imm, is_vec);
+          bits |= bin_case(nd.cls, canon_form(nd.cls, is_vec ? FORM_AV : FORM_AS));
+        } else if (R_.kind == N_VAR) {
+          bits |= loada_bits(R_, imm);
+          bits |= opnd_bits(L_, imm, is_vec);
+          bits |= bin_case(nd.cls, canon_form(nd.cls, FORM_SA));
+        } else {
+          bits |= loada_bits(L_, imm);
+          bits |= opnd_bits(R_, imm, is_vec);
+          bits |= bin_case(nd.cls, canon_form(nd.cls, FORM_AS));
+        }
+      } else if (lop && !rop) {
+        bits = opnd_bits(R_, imm, is_vec);
+        bits |= bin_case(nd.cls, canon_form(nd.cls, is_vec ? FORM_AV : FORM_AS));
+      } else if (!lop && rop) {
+        bits = opnd_bits(L_, imm, is_vec);
+        bits |= bin_case(nd.cls, canon_form(nd.cls, is_vec ? FORM_VA : FORM_SA));
+      } else {
+        bits = ((uint32_t)OK_SLOT << SH_OPK) | ((uint32_t)er[v].depth << SH_OP_IDX);
+        bits |= bin_case(nd.cls, canon_form(nd.cls, (f & ER_FIRST_LEFT) ? FORM_VA : FORM_AV));
+      }
+    }
+    em.put_at(er[v].pos, bits, imm);
+  }
+  h.n_instr = cnt[root];
   h.n_slots = max_depth;
   if (!em.ok) h.status = PROG_UNREPRESENTABLE;
   return h;

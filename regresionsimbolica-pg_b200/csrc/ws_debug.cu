@@ -20,8 +20,8 @@ int32_t compile_host(const uint8_t* prog, int64_t L, const T* consts, int64_t K,
   const int Lcap = tape_capacity((int)L);
   std::vector<Instr<T>> tape((size_t)Lcap);
   // xmul = 1: tape offsets are plain variable / slot indices
-  const ProgHdr h = compile_program<T, STRICT, true, 256>(prog, (int)L, consts, (int)K, lut,
-                                                          tape.data(), 1);
+  const ProgHdr h = compile_program_v2<T, STRICT, true, 256>(prog, (int)L, consts, (int)K, lut,
+                                                             tape.data(), 1);
   hdr_out[0] = h.n_instr;
   hdr_out[1] = h.status;
   hdr_out[2] = h.n_slots;
@@ -69,6 +69,33 @@ void run_host(const uint32_t* ctrl, const double* imm, int n, const T* x, int64_
   }
 }
 
+// Compiles each of B programs with the depth-first emitter (compile_program) and the linear one
+// (compile_program_v2) and counts the programs whose headers or tape words differ.
+template <typename T, bool STRICT>
+int64_t compile_agree_host(const uint8_t* progs, int64_t B, int64_t L, const T* consts,
+                           int64_t K, const TokenLut& lut, int xmul) {
+  const int Lcap = tape_capacity((int)L);
+  std::vector<Instr<T>> a((size_t)Lcap), b((size_t)Lcap);
+  int64_t bad = 0;
+  for (int64_t p = 0; p < B; ++p) {
+    const uint8_t* prog = progs + p * L;
+    const T* c = K > 0 ? consts + p * K : nullptr;
+    std::memset(a.data(), 0, a.size() * sizeof(Instr<T>));
+    std::memset(b.data(), 0, b.size() * sizeof(Instr<T>));
+    const ProgHdr ha = compile_program<T, STRICT, true, 256>(prog, (int)L, c, (int)K, lut,
+                                                             a.data(), xmul);
+    const ProgHdr hb = compile_program_v2<T, STRICT, true, 256>(prog, (int)L, c, (int)K, lut,
+                                                                b.data(), xmul);
+    bool same = ha.status == hb.status && ha.n_tok == hb.n_tok;
+    if (same && ha.status == PROG_OK) {
+      same = ha.n_instr == hb.n_instr && ha.n_slots == hb.n_slots &&
+             std::memcmp(a.data(), b.data(), (size_t)ha.n_instr * sizeof(Instr<T>)) == 0;
+    }
+    bad += same ? 0 : 1;
+  }
+  return bad;
+}
+
 }  // namespace
 }  // namespace ws
 
@@ -101,6 +128,27 @@ ws_status ws_debug_compile(int32_t dtype, const uint8_t* prog, int64_t L, const 
   } else {
     if (strict_mode) compile_host<double, true>(prog, L, (const double*)consts, K, lut, ctrl_out, imm_out, hdr_out);
     else compile_host<double, false>(prog, L, (const double*)consts, K, lut, ctrl_out, imm_out, hdr_out);
+  }
+  return WS_OK;
+}
+
+ws_status ws_debug_compile_agree(int32_t dtype, const uint8_t* progs, int64_t B, int64_t L,
+                                 const void* consts, int64_t K, const ws_token_map* ids,
+                                 int64_t num_vars, int32_t strict_mode, int32_t fused_order,
+                                 int32_t xmul, int64_t* mismatches_out) {
+  clear_error();
+  if (!ids || !progs || !mismatches_out) return fail("null pointer");
+  if (L < 1 || L > 256 || B < 0 || xmul < 1) return fail("bad shape");
+  if (K < 0 || (K > 0 && !consts)) return fail("bad constants");
+  const TokenLut lut = build_lut(*ids, num_vars, fused_order != 0);
+  if (dtype == WS_F32) {
+    *mismatches_out = strict_mode
+        ? compile_agree_host<float, true>(progs, B, L, (const float*)consts, K, lut, xmul)
+        : compile_agree_host<float, false>(progs, B, L, (const float*)consts, K, lut, xmul);
+  } else {
+    *mismatches_out = strict_mode
+        ? compile_agree_host<double, true>(progs, B, L, (const double*)consts, K, lut, xmul)
+        : compile_agree_host<double, false>(progs, B, L, (const double*)consts, K, lut, xmul);
   }
   return WS_OK;
 }

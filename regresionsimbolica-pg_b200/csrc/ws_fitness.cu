@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(128) compile_kernel(const ProbDesc<T>* __restr
   const int pi = find_problem(desc, n_prob, g, false);
   const ProbDesc<T>& d = desc[pi];
   const int64_t p = g - d.prog0;
-  ProgHdr h = compile_program<T, STRICT, true, LMAX>(
+  ProgHdr h = compile_program_v2<T, STRICT, true, LMAX>(
       d.pop + p * (int64_t)L, L, d.K > 0 ? d.consts + p * (int64_t)d.K : nullptr, d.K, luts[pi],
       tape + g * (int64_t)Lcap, d.xmul);
   // Neither can happen (Sethi-Ullman bound; chunk size chosen for the offsets): guard anyway.

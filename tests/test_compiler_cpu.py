@@ -137,3 +137,47 @@ def test_fold_error_makes_program_invalid_in_strict_mode():
     assert hdr[1] == 1
     ctrl, imm, hdr = compile_host(g, np.array(prog), np.zeros(0, np.float32), 0)
     assert hdr[1] == 0
+
+
+def _deep_trees(g, n, rng, L):
+    names = g.active_variables + ['C', '1', 'pi']
+    bins = [o for o in g.operators if g.token_arity[o] == 2]
+    uns = [o for o in g.operators if g.token_arity[o] == 1]
+    pop = np.zeros((n, L), dtype=np.uint8)
+    for i in range(n):
+        def build(depth):
+            if depth == 0:
+                return [names[int(rng.integers(len(names)))]]
+            t = build(depth - 1) + build(depth - 1) + [bins[int(rng.integers(len(bins)))]]
+            if uns and rng.random() < 0.3:
+                t.append(uns[int(rng.integers(len(uns)))])
+            return t
+        toks = build(int(rng.integers(1, 6)))[:L]
+        pop[i, :len(toks)] = [g.token_to_id[t] for t in toks]
+    return pop
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("strict", [0, 1])
+@pytest.mark.parametrize("L,xmul", [(30, 1), (64, 7), (64, 100), (200, 2)])
+def test_linear_emitter_matches_depth_first(dtype, strict, L, xmul):
+    """The device compiler's linear emitter writes the depth-first emitter's tape word for word:
+    headers (status, length, spill slots, tokens) and every (ctrl, immediate) pair, over random
+    valid programs, token soup with invalid rows, PAD gaps and push-drop runs, literal-rich
+    (constant-folded) programs, complete trees that use the deepest spill slots, every operator,
+    and offsets that do not fit the tape word."""
+    rng = np.random.default_rng(L * 10 + xmul + 3 * strict)
+    g = tl.GPUGrammar(num_variables=4, operators=tl.ALL_OPERATORS)
+    parts = [tl.random_population(g, 3000, L, 6, rng, valid_only=False)[0],
+             tl.random_population(g, 1000, L, 6, rng, valid_only=True, use_literals=True)[0],
+             _deep_trees(g, 500, rng, L)]
+    pop = np.ascontiguousarray(np.concatenate(parts))
+    for K in (0, 1, 6):
+        consts = np.ascontiguousarray(rng.uniform(-3, 3, size=(len(pop), max(K, 1)))
+                                      .astype(dtype)[:, :K])
+        bad = C.c_int64(-1)
+        code = tl.N.WS_F32 if dtype == np.float32 else tl.N.WS_F64
+        tl.N.check(tl.N.lib().ws_debug_compile_agree(
+            code, pop.ctypes.data, len(pop), L, consts.ctypes.data if K else None, K,
+            C.byref(tl.token_map(g)), len(g.active_variables), strict, 0, xmul, C.byref(bad)))
+        assert bad.value == 0, (K, bad.value)
