@@ -21,6 +21,10 @@
 // sum, written without atomics when one block covers all rows of a program; only programs
 // split across blocks use one atomic per (block, slot) -- the reference issues one atomic per
 // (row, constant node).
+//
+// The loss-and-gradient of constant fitting (ws_loss_grad, the batched L-BFGS) runs its own
+// kernel, loss_kernel below, on the same parse rules: derivatives stored by the forward sweep,
+// an operator-independent reverse sweep, programs grouped by tape size.
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
@@ -86,7 +90,8 @@ struct BwdParams {
   const int32_t* active;  // optional: programs with 0 are skipped
   int64_t V;              // variables; with stage_x each thread copies its rows of x to shared
   int stage_x;            // memory once per row group
-  int tape_ops;           // operator slots of the tape (>= every program's operator count)
+  int tape_ops;           // tape slots (>= every program's operators; loss_kernel: operators,
+                          // constant leaves and staged variables)
   const int32_t* list;        // optional: the programs of this launch (a bucket) ...
   const int32_t* list_count;  // ... and how many there are (read on the device)
   double* part_loss;      // [n_items]   sum over the item's rows of (pred - y)^2
@@ -243,11 +248,9 @@ __device__ __forceinline__ void acc_t(T& dst, T coef, T adj) {
 // is operator o-1), and constant adjoints are summed in registers when K <= kRegSlots (the slot of
 // a delivery is the same for the whole block, so the register is chosen by a uniform switch).
 //
-// LOSS = false (ws_eval_rpn_backward): the root adjoint of row d is grad_output[b, d] and every
-// per-row expression is the reference's, double promotions included (acc_d / acc_t), so per-row
-// adjoints are bit-identical to the reference's; per-row constant adjoints are summed in FP64.
-// LOSS = true (ws_loss_grad): the root adjoint is 2 (pred - y[d]) / D and the arithmetic is in T;
-// the loss is summed per thread in FP64.  Both skip the contributions of zero adjoints.
+// The root adjoint of row d is grad_output[b, d] and every per-row expression is the reference's,
+// double promotions included (acc_d / acc_t), so per-row adjoints are bit-identical to the
+// reference's; per-row constant adjoints are summed in FP64; zero adjoints hand on nothing.
 constexpr int kRegSlots = 8;
 
 template <typename T, int R>
@@ -358,15 +361,10 @@ __device__ __forceinline__ void creg_add(T (&cr)[kRegSlots], int i, T c) {
   }
 }
 
-// Constant-slot accumulator: FP64 per row for the reference path, T for the loss path.
-template <typename T, bool LOSS>
-using CAcc = typename std::conditional<LOSS, T, double>::type;
-
-template <typename T, int R, bool LOSS, bool KREG>
+template <typename T, int R, bool KREG>
 __device__ __forceinline__ void deliver_vec(uint8_t k, uint16_t i, const T (&c)[R], bool to_carry,
                                             T (&carry)[R], bool& have, T* tape, int TS, int tid,
-                                            CAcc<T, LOSS> (&cr)[kRegSlots], double* cacc,
-                                            int* touched) {
+                                            double (&cr)[kRegSlots], double* cacc, int* touched) {
   if (k == OPD_OP) {
     if (to_carry) {
       WS_FOR_R carry[r] = c[r];
@@ -375,24 +373,23 @@ __device__ __forceinline__ void deliver_vec(uint8_t k, uint16_t i, const T (&c)[
       st_vec<T, R>(tape + ((size_t)i * TS + tid) * R, c);
     }
   } else if (k == OPD_CONST) {
-    using A = CAcc<T, LOSS>;
-    A s = (A)0;
+    double s = 0.0;
     bool any = false;
     WS_FOR_R {
       if (c[r] != (T)0) {
-        s += (A)c[r];
+        s += (double)c[r];
         any = true;
       }
     }
     if (any) {
-      if (KREG) creg_add<A>(cr, i, s);
-      else cacc[(size_t)i * TS + tid] += (double)s;
-      if (!LOSS) touched[i] = 1;
+      if (KREG) creg_add<double>(cr, i, s);
+      else cacc[(size_t)i * TS + tid] += s;
+      touched[i] = 1;
     }
   }
 }
 
-template <typename T, int R, bool LOSS, bool KREG>
+template <typename T, int R, bool KREG>
 __global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int TS = p.tape_stride;
@@ -418,16 +415,12 @@ __global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
   if (threadIdx.x < 10) s_lit[threadIdx.x] = (T)lut.lit[threadIdx.x];
   if (threadIdx.x == 0) s_prog = -1;
   const int tid = threadIdx.x;
-  const T loss_scale = LOSS ? (T)(2.0 / (double)p.D) : (T)0;
-  using A = CAcc<T, LOSS>;
 
   const int64_t n_items = p.list ? (int64_t)(*p.list_count) * p.n_splits : p.n_items;
   for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int64_t li = item / p.n_splits;
     const int64_t split = item - li * p.n_splits;
     const int64_t b = p.list ? (int64_t)p.list[li] : li;
-    const int64_t slot = b * p.n_splits + split;  // partial sums of (program, row range)
-    if (LOSS && p.active && p.active[b] == 0) continue;  // uniform over the block
     __syncthreads();
     if (tid == 0 && s_prog != b) {
       BRoot rt0 = parse_program(p.pop + b * p.L, p.L, p.K, s_tab, ops);
@@ -445,27 +438,20 @@ __global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
       for (int64_t k = 0; k < p.K; ++k) cacc[k * TS + tid] = 0.0;
     __syncthreads();
     const BRoot rt = s_root;
-    if (!rt.valid) {
-      if (LOSS) {  // no prediction: infinite loss, no gradient
-        if (tid == 0) p.part_loss[slot] = __longlong_as_double(0x7ff0000000000000ll);
-        for (int64_t k = tid; k < p.K; k += blockDim.x) p.part_grad[slot * p.K + k] = 0.0;
-      }
-      continue;
-    }
+    if (!rt.valid) continue;
     const int64_t d_begin = split * p.rows_per_split;
     int64_t d_end = d_begin + p.rows_per_split;
     if (d_end > p.D) d_end = p.D;
     const T* xcol = p.x;
     const T* cst = p.consts + b * p.K;
     const int n = rt.n_ops;
-    A cr[kRegSlots];
+    double cr[kRegSlots];
 #pragma unroll
-    for (int k = 0; k < kRegSlots; ++k) cr[k] = (A)0;
-    double lacc = 0.0;
+    for (int k = 0; k < kRegSlots; ++k) cr[k] = 0.0;
 
     for (int64_t d0 = d_begin + (int64_t)tid * R; d0 < d_end; d0 += (int64_t)TS * R) {
       // this thread's rows: x staged (only this thread reads them: no barrier), the root
-      // adjoint's inputs loaded now so that their latency overlaps the forward sweep
+      // adjoints loaded now so that their latency overlaps the forward sweep
       if (xs) {
         for (int64_t v = 0; v < p.V; ++v) {
           const T* xr = xcol + v * p.D;
@@ -474,8 +460,8 @@ __global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
           st_vec<T, R>(xs + ((size_t)v * TS + tid) * R, xv);
         }
       }
-      T ext[R];  // y (loss) or grad_output (reference path) of the R rows
-      WS_FOR_R ext[r] = d0 + r < d_end ? (LOSS ? p.y[d0 + r] : p.gout[b * p.D + d0 + r]) : (T)0;
+      T g_root[R];  // grad_output of the R rows
+      WS_FOR_R g_root[r] = d0 + r < d_end ? p.gout[b * p.D + d0 + r] : (T)0;
       // forward: operator values
       T last[R];
       WS_FOR_R last[r] = (T)0;
@@ -501,28 +487,10 @@ __global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
         st_vec<T, R>(tape + ((size_t)o * TS + tid) * R, v);
         WS_FOR_R last[r] = v[r];
       }
-      // root adjoints
-      T g_root[R];
-      if (LOSS) {
-        T pred[R];
-        if (rt.kind == OPD_OP && (int)rt.idx == n - 1) {
-          WS_FOR_R pred[r] = last[r];
-        } else {
-          operand_vec<T, R>(rt.kind, rt.idx, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs,
-                            pred);
-        }
-        WS_FOR_R {
-          const T diff = d0 + r < d_end ? pred[r] - ext[r] : (T)0;
-          lacc += (double)diff * (double)diff;
-          g_root[r] = diff * loss_scale;
-        }
-      } else {
-        WS_FOR_R g_root[r] = ext[r];
-      }
       T carry[R];
       bool have = false;
       if (rt.kind != OPD_OP) {  // a one-terminal program
-        deliver_vec<T, R, LOSS, KREG>(rt.kind, rt.idx, g_root, false, carry, have, tape, TS, tid,
+        deliver_vec<T, R, KREG>(rt.kind, rt.idx, g_root, false, carry, have, tape, TS, tid,
                                       cr, cacc, touched);
         continue;
       }
@@ -546,29 +514,34 @@ __global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
           ld_vec<T, R>(tape + ((size_t)o * TS + tid) * R, g);
         }
         have = false;
+        // the rules of + - and neg use no operand value, those of the unary operators only the
+        // left one: the other loads are skipped
         T lv[R], ca[R], cb[R];
-        operand_vec<T, R>(op.ka, op.a, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs, lv);
+        const bool need_l = op.bop != BO_ADD && op.bop != BO_SUB && op.bop != BO_NEG;
+        const bool need_r = op.bop == BO_MUL || op.bop == BO_DIV || op.bop == BO_POW;
+        if (need_l) {
+          operand_vec<T, R>(op.ka, op.a, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs, lv);
+        } else {
+          WS_FOR_R lv[r] = (T)0;
+        }
         WS_FOR_R { ca[r] = (T)0; cb[r] = (T)0; }
         if (op.binary) {
           T rv[R];
-          operand_vec<T, R>(op.kb, op.b, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs, rv);
+          if (need_r) {
+            operand_vec<T, R>(op.kb, op.b, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs,
+                              rv);
+          } else {
+            WS_FOR_R rv[r] = (T)0;
+          }
           switch (op.bop) {
             case BO_ADD: WS_FOR_R { ca[r] += g[r]; cb[r] += g[r]; } break;
             case BO_SUB: WS_FOR_R { ca[r] += g[r]; cb[r] -= g[r]; } break;
-            case BO_MUL:
-              if (LOSS) WS_FOR_R { ca[r] = rv[r] * g[r]; cb[r] = lv[r] * g[r]; }
-              else WS_FOR_R { acc_t(ca[r], rv[r], g[r]); acc_t(cb[r], lv[r], g[r]); }
-              break;
+            case BO_MUL: WS_FOR_R { acc_t(ca[r], rv[r], g[r]); acc_t(cb[r], lv[r], g[r]); } break;
             case BO_DIV:
               WS_FOR_R {
                 if (fabs(rv[r]) >= (T)1e-9) {
-                  if (LOSS) {
-                    ca[r] = g[r] / rv[r];
-                    cb[r] = -(lv[r] / (rv[r] * rv[r])) * g[r];
-                  } else {
-                    acc_d(ca[r], 1.0 / rv[r], g[r]);
-                    acc_t(cb[r], -(lv[r] / (rv[r] * rv[r])), g[r]);
-                  }
+                  acc_d(ca[r], 1.0 / rv[r], g[r]);
+                  acc_t(cb[r], -(lv[r] / (rv[r] * rv[r])), g[r]);
                 }
               }
               break;
@@ -576,13 +549,8 @@ __global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
               WS_FOR_R {
                 if (lv[r] > 0) {
                   const T out_val = fwd_binary<T>(op.fop, lv[r], rv[r]);
-                  if (LOSS) {
-                    ca[r] = rv[r] * pow(lv[r], rv[r] - (T)1) * g[r];
-                    cb[r] = out_val * log(lv[r]) * g[r];
-                  } else {
-                    acc_d(ca[r], (double)rv[r] * pow((double)lv[r], (double)rv[r] - 1.0), g[r]);
-                    acc_t(cb[r], out_val * log(lv[r]), g[r]);
-                  }
+                  acc_d(ca[r], (double)rv[r] * pow((double)lv[r], (double)rv[r] - 1.0), g[r]);
+                  acc_t(cb[r], out_val * log(lv[r]), g[r]);
                 }
               }
               break;
@@ -591,47 +559,520 @@ __global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
           WS_FOR_R if (g[r] == (T)0) cb[r] = (T)0;
           // the right operand sits later in the program: its constants first, as the
           // reference's reverse walk meets them
-          deliver_vec<T, R, LOSS, KREG>(op.kb, op.b, cb, (op.pad & 2) != 0, carry, have, tape, TS,
+          deliver_vec<T, R, KREG>(op.kb, op.b, cb, (op.pad & 2) != 0, carry, have, tape, TS,
                                         tid, cr, cacc, touched);
         } else {
           switch (op.bop) {
-            case BO_SIN:
-              if (LOSS) WS_FOR_R ca[r] = cos(lv[r]) * g[r];
-              else WS_FOR_R acc_t(ca[r], cos(lv[r]), g[r]);
-              break;
-            case BO_COS:
-              if (LOSS) WS_FOR_R ca[r] = -sin(lv[r]) * g[r];
-              else WS_FOR_R acc_t(ca[r], -sin(lv[r]), g[r]);
-              break;
+            case BO_SIN: WS_FOR_R acc_t(ca[r], cos(lv[r]), g[r]); break;
+            case BO_COS: WS_FOR_R acc_t(ca[r], -sin(lv[r]), g[r]); break;
             case BO_LOG:
-              WS_FOR_R {
-                if (fabs(lv[r]) > (T)1e-9) {
-                  if (LOSS) ca[r] = g[r] / lv[r];
-                  else acc_d(ca[r], 1.0 / lv[r], g[r]);
-                }
-              }
+              WS_FOR_R if (fabs(lv[r]) > (T)1e-9) acc_d(ca[r], 1.0 / lv[r], g[r]);
               break;
-            case BO_EXP:
-              if (LOSS) WS_FOR_R ca[r] = fwd_unary<T>(op.fop, lv[r]) * g[r];
-              else WS_FOR_R acc_t(ca[r], fwd_unary<T>(op.fop, lv[r]), g[r]);
-              break;
+            case BO_EXP: WS_FOR_R acc_t(ca[r], fwd_unary<T>(op.fop, lv[r]), g[r]); break;
             case BO_SQRT:
-              WS_FOR_R {
-                if (lv[r] > (T)1e-9) {
-                  if (LOSS) ca[r] = (T)0.5 / sqrt(lv[r]) * g[r];
-                  else acc_d(ca[r], 0.5 / sqrt(lv[r]), g[r]);
-                }
-              }
+              WS_FOR_R if (lv[r] > (T)1e-9) acc_d(ca[r], 0.5 / sqrt(lv[r]), g[r]);
               break;
             case BO_NEG: WS_FOR_R ca[r] += -g[r]; break;
             default: break;
           }
         }
         WS_FOR_R if (g[r] == (T)0) ca[r] = (T)0;
-        deliver_vec<T, R, LOSS, KREG>(op.ka, op.a, ca, (op.pad & 1) != 0, carry, have, tape, TS,
+        deliver_vec<T, R, KREG>(op.ka, op.a, ca, (op.pad & 1) != 0, carry, have, tape, TS,
                                       tid, cr, cacc, touched);
       }
     }
+    __syncthreads();  // the tape is free: the reduction reuses its memory
+    double* cred = KREG ? reinterpret_cast<double*>(work) : cacc;
+    if (KREG) {
+#pragma unroll
+      for (int k = 0; k < kRegSlots; ++k)
+        if (k < p.K) cred[(size_t)k * TS + tid] = cr[k];
+    }
+    __syncthreads();
+    // fixed-order reduction over the block's threads, one thread per slot
+    for (int64_t k = tid; k < p.K; k += blockDim.x) {
+      if (!touched[k]) continue;
+      double s = 0.0;
+      for (int t = 0; t < (int)blockDim.x; ++t) s += cred[k * TS + t];
+      T* dst = p.grad + b * p.K + k;
+      if (p.n_splits == 1) *dst = *dst + (T)s;
+      else atomicAdd(dst, (T)s);
+    }
+  }
+}
+
+// ---- loss mode: the loss and its gradient with respect to the constants ---------------------
+// The root adjoint of row d is dL/dpred = 2 (pred - y[d]) / D and the arithmetic is in T.  Every
+// operand that carries a gradient -- an earlier operator or a constant leaf -- owns a tape slot.
+// The forward sweep evaluates operator o from its operands, stores the value in slot o and writes
+// the local derivative of o with respect to each operand into that operand's slot, whose value o
+// has just consumed (the program is a tree: o is its only reader), or into a sink slot for an
+// operand without a gradient.  The reverse sweep is then the same steps for every operator
+// whatever its rule: load its adjoint, multiply each operand's derivative by it and store the
+// product where the derivative was.  A constant leaf's slot thus ends the row group holding its
+// adjoint, summed into the constant's accumulator by a short epilogue.  No rule is evaluated
+// twice, neither sweep branches on an operand's kind, and operand kinds are resolved once per
+// program, at parse time, into shared-memory addresses: a tape slot read at the thread's own
+// offset, or an entry of the program's scalar table (R copies of a constant or literal) read by
+// every thread at the same address.  The derivatives are the reference's adjoint rules with the
+// adjoint factored out (backward_kernels.cu:222-278), in T: + and - hand on +-1, * the other
+// operand, / 1/b and -(a/b^2) when |b| >= 1e-9, pow b*a^(b-1) and a^b*log(a) when a > 0, sin
+// cos(a), cos -sin(a), log 1/a when |a| > 1e-9, exp its value, sqrt 0.5/sqrt(a) when a > 1e-9,
+// neg -1, the other operators 0; zero adjoints hand on nothing.  Against the reference's
+// adjoint / b (and adjoint / a for log) the reciprocal rounds once more, and flushes to zero for
+// |b| > 2^126, where the contribution is below 2^-126 times the adjoint.
+enum : uint8_t {
+  LF_BIN = 1,     // binary operator
+  LF_A_VEC = 2,   // the left operand is a tape slot (else a scalar-table entry)
+  LF_B_VEC = 4,
+  LF_A_GRAD = 8,  // the left operand carries a gradient (LOp::fa is its slot)
+  LF_B_GRAD = 16,
+  LF_REACH = 32,  // the value flows into the root
+};
+// LOp::code: the adjoint code when the token's forward and adjoint rules are the pair of one
+// operator (every token of a real grammar), else kCodeGeneric (value by fop, derivatives by bop)
+constexpr uint8_t kCodeGeneric = 0xFF;
+
+// One operator of a loss-mode tape.  Addresses are in 16-byte units from the start of the
+// block's dynamic shared memory.
+struct __align__(16) LOp {
+  uint16_t a, b;    // operands (a unary operator reads its operand twice)
+  uint16_t fa, fb;  // where each operand's derivative goes: its slot, or the sink slot
+  uint16_t self;    // this operator's slot
+  uint8_t code, fop, bop, flags;
+  uint16_t pad;
+};
+
+// Shared memory of a loss-mode block (bytes): operators | staged-variable list | constant-leaf
+// list | scalar table (one 16-byte entry per terminal token at most) | (K > kRegSlots) FP64
+// constant accumulators | work: the tape (M slots and the sink) during the rows, the block
+// reduction after them.
+struct LossLayout {
+  size_t ops, stage, leaf, scal, cacc, work, bytes;
+};
+
+__host__ __device__ inline LossLayout loss_layout(int64_t M, int64_t L, int64_t K, int threads,
+                                                  size_t vec_bytes, bool kreg) {
+  LossLayout l;
+  l.ops = 0;
+  l.stage = al16((size_t)M * sizeof(LOp));
+  l.leaf = l.stage + al16((size_t)M);
+  l.scal = l.leaf + al16((size_t)M * sizeof(uint32_t));
+  l.cacc = l.scal + (size_t)L * 16;
+  l.work = l.cacc + (kreg ? 0 : (size_t)K * threads * sizeof(double));
+  const size_t tape = (size_t)(M + 1) * threads * vec_bytes;
+  const size_t red = (size_t)((kreg ? K : 0) + 1) * threads * sizeof(double);
+  l.bytes = l.work + (tape > red ? tape : red);
+  return l;
+}
+
+template <typename T>
+struct LRoot {
+  int n_ops;      // operators in the tape
+  int valid;      // the reference's forward pass yields a root (final depth 1)
+  int n_stage;    // distinct variables staged per row group ...
+  int stage0;     // ... in the slots from this address on (16-byte units, one slot apart)
+  int n_leaf;     // entries of the constant-leaf list (leaves whose parent reaches the root)
+  uint16_t kind;  // OPD_OP, OPD_VAR, OPD_LIT or OPD_CONST
+  uint16_t at;    // address of the root's slot (OPD_OP, OPD_VAR)
+  uint16_t ck;    // constant slot (OPD_CONST)
+  T scalar;       // value of a literal or constant root
+};
+
+__device__ __forceinline__ uint8_t loss_code(uint8_t fop, uint8_t bop) {
+  const uint8_t pair_fop[12] = {FO_NONE, FO_ADD, FO_SUB, FO_MUL, FO_DIV, FO_POW,
+                                FO_SIN,  FO_COS, FO_LOG, FO_EXP, FO_SQRT, FO_NEG};
+  return (bop != BO_NONE && bop < 12 && pair_fop[bop] == fop) ? bop : kCodeGeneric;
+}
+
+// Addresses of one block's tape (16-byte units): slot s sits at tape + s * slot, the sink is
+// slot M, the scalar table starts at scal.
+struct LossAddr {
+  uint32_t tape, slot, scal, sink;
+};
+
+// Walks program b with parse_program's rules (the reference's forward loop) and resolves each
+// operand into an address: operators take slots 0..n_ops-1, constant leaves the next slots, each
+// distinct variable the slots after them (x staged there once per row group); constants and
+// literals take scalar-table entries, filled here.  Slots in use <= operators + constant tokens +
+// distinct variables <= tokens.  `leaf` receives (address | constant slot << 16) of the constant
+// leaves whose parent reaches the root.
+template <typename T, int R>
+__device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t L, int64_t K,
+                                       const uint8_t* s_tab, const T* s_lit,
+                                       const T* __restrict__ cst, const LossAddr& ad,
+                                       unsigned char* smem, LOp* ops, uint8_t* stage,
+                                       uint32_t* leaf) {
+  const uint8_t* t_kind = s_tab;
+  const uint8_t* t_fop = s_tab + 256;
+  const uint8_t* t_bop = s_tab + 512;
+  const uint8_t* t_arg = s_tab + 768;
+  constexpr int kPer = 16 / (int)sizeof(T);  // values per scalar-table entry
+  T* scal = reinterpret_cast<T*>(smem + ((size_t)ad.scal << 4));
+  uint8_t sk[kStack];   // operand kind
+  uint16_t si[kStack];  // operator index, variable ordinal or scalar-table entry
+  uint16_t sl[kStack];  // constant-leaf ordinal of a constant
+  int sp = 0, n_ops = 0, n_leaf = 0, n_stage = 0, n_scal = 0;
+  int64_t c_idx = 0;
+  for (int pc = 0; pc < (int)L; ++pc) {
+    const int tok = prog[pc];
+    const uint8_t kind = t_kind[tok];
+    if (kind == BK_PAD) break;
+    if (kind == BK_VAR || kind == BK_LIT || kind == BK_CONST) {
+      uint8_t k = kind == BK_VAR ? OPD_VAR : OPD_LIT;
+      uint16_t ix = t_arg[tok], c = 0;
+      if (kind == BK_CONST) {
+        if (K > 0) {
+          k = OPD_CONST;
+          c = (uint16_t)(c_idx < K ? c_idx : K - 1);
+          c_idx++;
+        } else {
+          ix = 10;  // C without constants pushes 1.0 and takes no gradient
+        }
+      }
+      if (sp < kStack) {
+        uint16_t lo = 0;
+        if (k == OPD_VAR) {
+          int j = 0;
+          while (j < n_stage && stage[j] != ix) ++j;
+          if (j == n_stage) stage[n_stage++] = (uint8_t)ix;
+          ix = (uint16_t)j;
+        } else {
+          const T v = k == OPD_CONST ? cst[c] : (ix < 10 ? s_lit[ix] : (T)1.0);
+          for (int r = 0; r < R; ++r) scal[(size_t)n_scal * kPer + r] = v;
+          if (k == OPD_CONST) {
+            lo = (uint16_t)n_leaf;
+            leaf[n_leaf++] = c;
+          }
+          ix = (uint16_t)n_scal++;
+        }
+        sk[sp] = k;
+        si[sp] = ix;
+        sl[sp] = lo;
+        ++sp;
+      }
+      continue;
+    }
+    LOp o;
+    o.fop = t_fop[tok];
+    o.bop = t_bop[tok];
+    o.code = loss_code(o.fop, o.bop);
+    o.flags = 0;
+    o.a = o.b = o.fa = o.fb = 0;
+    o.self = (uint16_t)n_ops;
+    o.pad = 0;
+    const int n_in = kind == BK_BIN ? 2 : 1;
+    if (sp < n_in) break;
+    if (n_in == 2) o.flags |= LF_BIN;
+    for (int side = n_in - 1; side >= 0; --side) {  // the right operand is on top
+      --sp;
+      const uint8_t k = sk[sp];
+      uint8_t fl = 0;
+      uint16_t f = 0;
+      if (k == OPD_OP) {
+        fl = LF_A_VEC | LF_A_GRAD;
+      } else if (k == OPD_VAR) {
+        fl = LF_A_VEC;
+      } else if (k == OPD_CONST) {
+        fl = LF_A_GRAD;
+        f = sl[sp];
+      }
+      if (side == 0) {
+        o.a = si[sp], o.fa = f;
+        o.flags |= fl;
+      } else {
+        o.b = si[sp], o.fb = f;
+        o.flags |= (uint8_t)(fl << 1);  // the B flags are the A flags shifted by one
+      }
+    }
+    ops[n_ops] = o;
+    sk[sp] = OPD_OP;  // an operator always finds room: it just freed one or two slots
+    si[sp] = (uint16_t)n_ops;
+    ++sp;
+    ++n_ops;
+  }
+  const uint32_t stage_first = (uint32_t)(n_ops + n_leaf);
+  const uint16_t sink = (uint16_t)(ad.tape + ad.sink * ad.slot);
+  LRoot<T> r;
+  r.n_ops = n_ops;
+  r.valid = sp == 1 ? 1 : 0;
+  r.n_stage = n_stage;
+  r.stage0 = (int)(ad.tape + stage_first * ad.slot);
+  r.kind = sp >= 1 ? sk[0] : OPD_LIT;
+  r.at = 0;
+  r.ck = 0;
+  r.scalar = (T)0;
+  if (sp >= 1) {
+    if (r.kind == OPD_OP) r.at = (uint16_t)(ad.tape + si[0] * ad.slot);
+    else if (r.kind == OPD_VAR) r.at = (uint16_t)(ad.tape + (stage_first + si[0]) * ad.slot);
+    else r.scalar = scal[(size_t)si[0] * kPer];
+    if (r.kind == OPD_CONST) r.ck = (uint16_t)leaf[sl[0]];
+  }
+  constexpr uint8_t kOpA = LF_A_VEC | LF_A_GRAD, kOpB = LF_B_VEC | LF_B_GRAD;
+  if (r.valid && r.kind == OPD_OP) {  // mark the operators whose value reaches the root
+    ops[si[0]].flags |= LF_REACH;
+    for (int o = si[0]; o >= 0; --o) {
+      const LOp& q = ops[o];
+      if (!(q.flags & LF_REACH)) continue;
+      if ((q.flags & kOpA) == kOpA) ops[q.a].flags |= LF_REACH;
+      if ((q.flags & kOpB) == kOpB) ops[q.b].flags |= LF_REACH;
+      if ((q.flags & kOpA) == LF_A_GRAD) leaf[q.fa] |= 0x80000000u;  // a live constant leaf
+      if ((q.flags & kOpB) == LF_B_GRAD) leaf[q.fb] |= 0x80000000u;
+    }
+  }
+  for (int o = 0; o < n_ops; ++o) {  // indices to addresses
+    LOp& q = ops[o];
+    for (int side = 0; side < 2; ++side) {
+      const uint8_t fl = side ? (uint8_t)(q.flags >> 1) : q.flags;
+      uint16_t& x = side ? q.b : q.a;
+      uint16_t& f = side ? q.fb : q.fa;
+      if (side == 1 && !(q.flags & LF_BIN)) {  // a unary operator reads its operand twice
+        x = q.a;
+        f = sink;
+        if (q.flags & LF_A_VEC) q.flags |= LF_B_VEC;
+        continue;
+      }
+      if ((fl & kOpA) == kOpA) {
+        x = (uint16_t)(ad.tape + x * ad.slot);
+        f = x;
+      } else if (fl & LF_A_VEC) {
+        x = (uint16_t)(ad.tape + (stage_first + x) * ad.slot);
+        f = sink;
+      } else {
+        x = (uint16_t)(ad.scal + x);
+        f = (fl & LF_A_GRAD) ? (uint16_t)(ad.tape + (n_ops + f) * ad.slot) : sink;
+      }
+    }
+    q.self = (uint16_t)(ad.tape + o * ad.slot);
+  }
+  int n_live = 0;
+  for (int i = 0; i < n_leaf; ++i)
+    if (leaf[i] & 0x80000000u)
+      leaf[n_live++] = (ad.tape + (uint32_t)(n_ops + i) * ad.slot) | ((leaf[i] & 0xFFFFu) << 16);
+  r.n_leaf = n_live;
+  return r;
+}
+
+// The derivatives of an adjoint rule (bop) at operands a, b and value v: the fallback of
+// op_with_derivs for tokens whose forward and adjoint rules are not one operator's pair.
+template <typename T>
+__device__ __forceinline__ void derivs_generic(uint8_t bop, T a, T b, T v, T& da, T& db) {
+  da = (T)0;
+  db = (T)0;
+  switch (bop) {
+    case BO_ADD: da = (T)1; db = (T)1; break;
+    case BO_SUB: da = (T)1; db = (T)-1; break;
+    case BO_MUL: da = b; db = a; break;
+    case BO_DIV:
+      if (fabs(b) >= (T)1e-9) { da = (T)1 / b; db = -(a / (b * b)); }
+      break;
+    case BO_POW:
+      if (a > 0) { da = b * pow(a, b - (T)1); db = v * log(a); }
+      break;
+    case BO_SIN: da = cos(a); break;
+    case BO_COS: da = -sin(a); break;
+    case BO_LOG: if (fabs(a) > (T)1e-9) da = (T)1 / a; break;
+    case BO_EXP: da = v; break;
+    case BO_SQRT: if (a > (T)1e-9) da = (T)0.5 / sqrt(a); break;
+    case BO_NEG: da = (T)-1; break;
+    default: break;
+  }
+}
+
+// Value and the local derivatives with respect to both operands of one operator, R rows.
+template <typename T, int R>
+__device__ __forceinline__ void op_with_derivs(const LOp& op, const T (&a)[R], const T (&b)[R],
+                                               T (&v)[R], T (&da)[R], T (&db)[R]) {
+  WS_FOR_R db[r] = (T)0;
+  switch (op.code) {
+    case BO_ADD: WS_FOR_R { v[r] = a[r] + b[r]; da[r] = (T)1; db[r] = (T)1; } break;
+    case BO_SUB: WS_FOR_R { v[r] = a[r] - b[r]; da[r] = (T)1; db[r] = (T)-1; } break;
+    case BO_MUL: WS_FOR_R { v[r] = a[r] * b[r]; da[r] = b[r]; db[r] = a[r]; } break;
+    case BO_DIV:
+      WS_FOR_R {
+        v[r] = fwd_binary<T>(FO_DIV, a[r], b[r]);
+        const bool ok = fabs(b[r]) >= (T)1e-9;
+        da[r] = ok ? (T)1 / b[r] : (T)0;
+        db[r] = ok ? -(a[r] / (b[r] * b[r])) : (T)0;
+      }
+      break;
+    case BO_POW:
+      WS_FOR_R {
+        v[r] = fwd_binary<T>(FO_POW, a[r], b[r]);
+        da[r] = (T)0;
+        if (a[r] > 0) {
+          da[r] = b[r] * pow(a[r], b[r] - (T)1);
+          db[r] = v[r] * log(a[r]);
+        }
+      }
+      break;
+    case BO_SIN: WS_FOR_R { v[r] = sin(a[r]); da[r] = cos(a[r]); } break;
+    case BO_COS: WS_FOR_R { v[r] = cos(a[r]); da[r] = -sin(a[r]); } break;
+    case BO_LOG:
+      WS_FOR_R {
+        v[r] = fwd_unary<T>(FO_LOG, a[r]);
+        da[r] = fabs(a[r]) > (T)1e-9 ? (T)1 / a[r] : (T)0;
+      }
+      break;
+    case BO_EXP: WS_FOR_R { v[r] = fwd_unary<T>(FO_EXP, a[r]); da[r] = v[r]; } break;
+    case BO_SQRT:
+      WS_FOR_R {
+        v[r] = fwd_unary<T>(FO_SQRT, a[r]);
+        da[r] = a[r] > (T)1e-9 ? (T)0.5 / sqrt(a[r]) : (T)0;
+      }
+      break;
+    case BO_NEG: WS_FOR_R { v[r] = -a[r]; da[r] = (T)-1; } break;
+    default:
+      WS_FOR_R {
+        v[r] = (op.flags & LF_BIN) ? fwd_binary<T>(op.fop, a[r], b[r]) : fwd_unary<T>(op.fop, a[r]);
+        derivs_generic<T>(op.bop, a[r], b[r], v[r], da[r], db[r]);
+      }
+      break;
+  }
+}
+
+template <typename T, int R, bool KREG>
+__global__ void __launch_bounds__(128) loss_kernel(BwdParams<T> p, BwdLut lut) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int TS = p.tape_stride;
+  const int M = p.tape_ops;  // tape slots, the sink not counted
+  const LossLayout lay = loss_layout(M, p.L, p.K, TS, R * sizeof(T), KREG);
+  LOp* ops = reinterpret_cast<LOp*>(smem + lay.ops);
+  uint8_t* stage = smem + lay.stage;
+  uint32_t* leaf = reinterpret_cast<uint32_t*>(smem + lay.leaf);
+  double* cacc = reinterpret_cast<double*>(smem + lay.cacc);
+  unsigned char* work = smem + lay.work;
+  LossAddr ad;
+  ad.tape = (uint32_t)(lay.work >> 4);
+  ad.slot = (uint32_t)((size_t)TS * R * sizeof(T) >> 4);
+  ad.scal = (uint32_t)(lay.scal >> 4);
+  ad.sink = (uint32_t)M;
+  __shared__ LRoot<T> s_root;
+  __shared__ int64_t s_prog;
+  __shared__ T s_lit[10];
+  __shared__ uint8_t s_tab[1024];  // kind, forward op, adjoint op, argument per token byte
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) {
+    s_tab[t] = lut.kind[t];
+    s_tab[256 + t] = lut.fop[t];
+    s_tab[512 + t] = lut.bop[t];
+    s_tab[768 + t] = lut.arg[t];
+  }
+  if (threadIdx.x < 10) s_lit[threadIdx.x] = (T)lut.lit[threadIdx.x];
+  if (threadIdx.x == 0) s_prog = -1;
+  const int tid = threadIdx.x;
+  const uint32_t my = (uint32_t)tid * (uint32_t)(R * sizeof(T));  // this thread's part of a slot
+  // a tape slot (this thread's R values) or a scalar-table entry, by its 16-byte address
+#define WS_AT(addr, mine) reinterpret_cast<T*>(smem + ((uint32_t)(addr) << 4) + ((mine) ? my : 0u))
+  const T loss_scale = (T)(2.0 / (double)p.D);
+
+  const int64_t n_items = p.list ? (int64_t)(*p.list_count) * p.n_splits : p.n_items;
+  for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int64_t li = item / p.n_splits;
+    const int64_t split = item - li * p.n_splits;
+    const int64_t b = p.list ? (int64_t)p.list[li] : li;
+    const int64_t slot = b * p.n_splits + split;  // partial sums of (program, row range)
+    if (p.active && p.active[b] == 0) continue;  // uniform over the block
+    __syncthreads();
+    if (tid == 0 && s_prog != b) {
+      s_root = parse_loss_program<T, R>(p.pop + b * p.L, p.L, p.K, s_tab, s_lit,
+                                        p.consts + b * p.K, ad, smem, ops, stage, leaf);
+      s_prog = b;
+    }
+    if (!KREG)
+      for (int64_t k = 0; k < p.K; ++k) cacc[k * TS + tid] = 0.0;
+    __syncthreads();
+    const LRoot<T> rt = s_root;
+    if (!rt.valid) {  // no prediction: infinite loss, no gradient
+      if (tid == 0) p.part_loss[slot] = __longlong_as_double(0x7ff0000000000000ll);
+      for (int64_t k = tid; k < p.K; k += blockDim.x) p.part_grad[slot * p.K + k] = 0.0;
+      continue;
+    }
+    const int64_t d_begin = split * p.rows_per_split;
+    int64_t d_end = d_begin + p.rows_per_split;
+    if (d_end > p.D) d_end = p.D;
+    const int n = rt.n_ops;
+    T cr[kRegSlots];
+#pragma unroll
+    for (int k = 0; k < kRegSlots; ++k) cr[k] = (T)0;
+    double lacc = 0.0;
+
+    for (int64_t d0 = d_begin + (int64_t)tid * R; d0 < d_end; d0 += (int64_t)TS * R) {
+      // this thread's rows of the program's variables (only this thread reads them: no barrier)
+      for (int j = 0; j < rt.n_stage; ++j) {
+        const T* xr = p.x + (int64_t)stage[j] * p.D;
+        T xv[R];
+        WS_FOR_R xv[r] = d0 + r < d_end ? xr[d0 + r] : (T)0;
+        st_vec<T, R>(WS_AT(rt.stage0 + j * ad.slot, true), xv);
+      }
+      T yv[R];
+      WS_FOR_R yv[r] = d0 + r < d_end ? p.y[d0 + r] : (T)0;
+      // forward: values, and each operand's derivative where the operand was
+      for (int o = 0; o < n; ++o) {
+        const LOp op = ops[o];
+        T a[R], bv[R], v[R], da[R], db[R];
+        ld_vec<T, R>(WS_AT(op.a, op.flags & LF_A_VEC), a);
+        ld_vec<T, R>(WS_AT(op.b, op.flags & LF_B_VEC), bv);
+        op_with_derivs<T, R>(op, a, bv, v, da, db);
+        st_vec<T, R>(WS_AT(op.self, true), v);
+        st_vec<T, R>(WS_AT(op.fa, true), da);
+        st_vec<T, R>(WS_AT(op.fb, true), db);
+      }
+      // the root: prediction, loss, root adjoint
+      T pred[R];
+      if (rt.kind == OPD_OP || rt.kind == OPD_VAR) {
+        ld_vec<T, R>(WS_AT(rt.at, true), pred);
+      } else {
+        WS_FOR_R pred[r] = rt.scalar;
+      }
+      T g[R];
+      WS_FOR_R {
+        const T diff = d0 + r < d_end ? pred[r] - yv[r] : (T)0;
+        lacc += (double)diff * (double)diff;
+        g[r] = diff * loss_scale;
+      }
+      if (rt.kind == OPD_CONST) {  // a one-constant program
+        T s = (T)0;
+        WS_FOR_R s += g[r];
+        if (KREG) creg_add<T>(cr, rt.ck, s);
+        else cacc[(size_t)rt.ck * TS + tid] += (double)s;
+        continue;
+      }
+      if (rt.kind != OPD_OP) continue;  // a variable or a literal: no constant to move
+      st_vec<T, R>(WS_AT(rt.at, true), g);
+      // reverse: each operator's adjoint times the derivative in each operand's slot, stored
+      // back there (the right operand first, as the reference's reverse walk meets it)
+      for (int o = n - 1; o >= 0; --o) {
+        const LOp op = ops[o];
+        if (!(op.flags & LF_REACH)) continue;
+        T ga[R];
+        ld_vec<T, R>(WS_AT(op.self, true), ga);
+        if (op.flags & LF_B_GRAD) {
+          T* q = WS_AT(op.fb, true);
+          T f[R];
+          ld_vec<T, R>(q, f);
+          WS_FOR_R f[r] = ga[r] == (T)0 ? (T)0 : f[r] * ga[r];
+          st_vec<T, R>(q, f);
+        }
+        if (op.flags & LF_A_GRAD) {
+          T* q = WS_AT(op.fa, true);
+          T f[R];
+          ld_vec<T, R>(q, f);
+          WS_FOR_R f[r] = ga[r] == (T)0 ? (T)0 : f[r] * ga[r];
+          st_vec<T, R>(q, f);
+        }
+      }
+      // the constant leaves' adjoints into their constants' accumulators
+      for (int j = 0; j < rt.n_leaf; ++j) {
+        const uint32_t e = leaf[j];
+        T c[R];
+        ld_vec<T, R>(WS_AT(e & 0xFFFFu, true), c);
+        T s = (T)0;
+        WS_FOR_R s += c[r];
+        if (KREG) creg_add<T>(cr, (int)(e >> 16), s);
+        else cacc[(size_t)(e >> 16) * TS + tid] += (double)s;
+      }
+    }
+#undef WS_AT
     __syncthreads();  // the tape is free: the reduction reuses its memory
     double* cred = KREG ? reinterpret_cast<double*>(work) : cacc;
     double* lacc_s = reinterpret_cast<double*>(work) + (KREG ? (size_t)p.K * TS : 0);
@@ -640,21 +1081,15 @@ __global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
       for (int k = 0; k < kRegSlots; ++k)
         if (k < p.K) cred[(size_t)k * TS + tid] = (double)cr[k];
     }
-    if (LOSS) lacc_s[tid] = lacc;
+    lacc_s[tid] = lacc;
     __syncthreads();
     // fixed-order reduction over the block's threads, one thread per slot
     for (int64_t k = tid; k < p.K; k += blockDim.x) {
       double s = 0.0;
       for (int t = 0; t < (int)blockDim.x; ++t) s += cred[k * TS + t];
-      if (LOSS) {
-        p.part_grad[slot * p.K + k] = s;
-      } else if (touched[k]) {
-        T* dst = p.grad + b * p.K + k;
-        if (p.n_splits == 1) *dst = *dst + (T)s;
-        else atomicAdd(dst, (T)s);
-      }
+      p.part_grad[slot * p.K + k] = s;
     }
-    if (LOSS && tid == 0) {
+    if (tid == 0) {
       double s = 0.0;
       for (int t = 0; t < (int)blockDim.x; ++t) s += lacc_s[t];
       p.part_loss[slot] = s;
@@ -664,34 +1099,51 @@ __global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
 
 #undef WS_FOR_R
 
-// Programs grouped by operator count, so that each group runs with a tape sized for it: a
-// program's count of operator tokens before its first PAD bounds its tape length.  Programs with
-// active[b] == 0 are left out.  lists: [n_buckets, B]; the order inside a bucket does not matter
-// (every (program, row range) writes its own partial sums).
-constexpr int kMaxBuckets = 9;
-constexpr int kBucketOps[kMaxBuckets] = {8, 16, 24, 32, 48, 64, 96, 128, 256};
-__constant__ int c_bucket_ops[kMaxBuckets] = {8, 16, 24, 32, 48, 64, 96, 128, 256};
+// Programs grouped by tape slots, so that each group runs with a tape sized for it: a program's
+// operator tokens, constant tokens (when there are constant slots) and distinct variables before
+// its first PAD bound the slots parse_loss_program gives it.  Programs with active[b] == 0 are
+// left out.  lists: [n_buckets, B]; the order inside a bucket does not matter (every (program,
+// row range) writes its own partial sums).
+constexpr int kMaxBuckets = 13;
+static_assert(kMaxBuckets <= 16, "the bucket counts take 16 entries of the scratch");
+constexpr int kBucketSlots[kMaxBuckets] = {8, 12, 16, 20, 24, 28, 32, 40, 48, 64, 96, 128, 256};
+__constant__ int c_bucket_slots[kMaxBuckets] = {8,  12, 16, 20, 24,  28, 32,
+                                                40, 48, 64, 96, 128, 256};
 
 __global__ void __launch_bounds__(256) bucket_kernel(const uint8_t* __restrict__ pop, int64_t B,
-                                                     int64_t L, BwdLut lut,
+                                                     int64_t L, int64_t K, BwdLut lut,
                                                      const int32_t* __restrict__ active,
                                                      int n_buckets, int32_t* counts,
                                                      int32_t* lists) {
-  __shared__ uint8_t s_kind[256];
-  for (int t = threadIdx.x; t < 256; t += blockDim.x) s_kind[t] = lut.kind[t];
+  __shared__ uint8_t s_kind[256], s_arg[256];
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) {
+    s_kind[t] = lut.kind[t];
+    s_arg[t] = lut.arg[t];
+  }
   __syncthreads();
   for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < B;
        b += (int64_t)gridDim.x * blockDim.x) {
     if (active && active[b] == 0) continue;
     const uint8_t* row = pop + b * L;
     int n = 0;
+    uint64_t seen = 0;  // variables 0..63; higher ones are counted at every use (a bound)
     for (int64_t t = 0; t < L; ++t) {
       const uint8_t k = s_kind[row[t]];
       if (k == BK_PAD) break;
-      n += (k == BK_BIN || k == BK_UN) ? 1 : 0;
+      if (k == BK_BIN || k == BK_UN || (k == BK_CONST && K > 0)) {
+        ++n;
+      } else if (k == BK_VAR) {
+        const int v = s_arg[row[t]];
+        if (v >= 64) {
+          ++n;
+        } else if (!((seen >> v) & 1)) {
+          seen |= 1ull << v;
+          ++n;
+        }
+      }
     }
     int j = 0;
-    while (j < n_buckets - 1 && n > c_bucket_ops[j]) ++j;
+    while (j < n_buckets - 1 && n > c_bucket_slots[j]) ++j;
     const int pos = atomicAdd(counts + j, 1);
     lists[(int64_t)j * B + pos] = (int32_t)b;
   }
@@ -801,23 +1253,23 @@ struct BwdPlan {
 template <typename T>
 constexpr int kRowsMax = sizeof(T) == 4 ? 4 : 2;
 
-template <typename T, bool LOSS, int RR>
+template <typename T, int RR>
 void (*adj_pick(bool kreg))(BwdParams<T>, BwdLut) {
-  return kreg ? adj_kernel<T, RR, LOSS, true> : adj_kernel<T, RR, LOSS, false>;
+  return kreg ? adj_kernel<T, RR, true> : adj_kernel<T, RR, false>;
 }
 
-template <typename T, bool LOSS>
+template <typename T>
 void (*adj_fn(int R, bool kreg))(BwdParams<T>, BwdLut) {
   if constexpr (kRowsMax<T> >= 4) {
-    if (R == 4) return adj_pick<T, LOSS, 4>(kreg);
+    if (R == 4) return adj_pick<T, 4>(kreg);
   }
-  if (R == 2) return adj_pick<T, LOSS, 2>(kreg);
-  return adj_pick<T, LOSS, 1>(kreg);
+  if (R == 2) return adj_pick<T, 2>(kreg);
+  return adj_pick<T, 1>(kreg);
 }
 
 // Block size, rows per thread and shared memory for a tape of M operator slots: the shape
 // with the most resident threads per SM.
-template <typename T, bool LOSS>
+template <typename T>
 ws_status backward_shape(int64_t M, int64_t K, int64_t V, BwdPlan* out, int* per_sm_out) {
   const DeviceInfo& dev = device_info();
   const size_t budget = dev.smem_optin < (size_t)200 * 1024 ? dev.smem_optin : 200 * 1024;
@@ -828,7 +1280,7 @@ ws_status backward_shape(int64_t M, int64_t K, int64_t V, BwdPlan* out, int* per
   double best_score = -1.0;
   int best_threads = 0, best_per_sm = 0, best_r = 1;
   for (int R = kRowsMax<T>; R >= 1; R /= 2) {
-    auto kern = adj_fn<T, LOSS>(R, kreg);
+    auto kern = adj_fn<T>(R, kreg);
     for (int threads = 128; threads >= 32; threads /= 2) {
       const size_t smem = backward_smem<T>(M, K, V, threads, R);
       if (smem > budget) continue;
@@ -854,7 +1306,7 @@ ws_status backward_shape(int64_t M, int64_t K, int64_t V, BwdPlan* out, int* per
     return fail("backward: " + std::to_string(K) + " constants and " + std::to_string(M) +
                 " operators need more shared memory than a block has");
   const size_t smem = backward_smem<T>(M, K, V, best_threads, best_r);
-  cudaError_t e = cudaFuncSetAttribute(adj_fn<T, LOSS>(best_r, kreg),
+  cudaError_t e = cudaFuncSetAttribute(adj_fn<T>(best_r, kreg),
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
   out->threads = best_threads;
@@ -866,13 +1318,8 @@ ws_status backward_shape(int64_t M, int64_t K, int64_t V, BwdPlan* out, int* per
 
 // Rows are split into ranges only when there are too few programs to fill the GPU; ranges are
 // multiples of 512 rows (a whole number of row groups of every block shape).  The split depends
-// on (B, L, K, V, D) and the device alone.
-template <typename T, bool LOSS>
-ws_status backward_plan(int64_t B, int64_t L, int64_t D, int64_t K, int64_t V,
-                        BwdPlan* out) {
-  int per_sm = 0;
-  ws_status st = backward_shape<T, LOSS>(L, K, V, out, &per_sm);
-  if (st != WS_OK) return st;
+// on (B, D), the resident blocks per SM of the launch's shape and the device alone.
+void split_rows(int64_t B, int64_t D, int per_sm, BwdPlan* out) {
   const int64_t slots = (int64_t)device_info().sm_count * per_sm;
   const int64_t group = 512;
   int64_t n_splits = (2 * slots + B - 1) / B;
@@ -886,10 +1333,84 @@ ws_status backward_plan(int64_t B, int64_t L, int64_t D, int64_t K, int64_t V,
   out->rows = rows;
   const int64_t n_items = B * n_splits;
   out->grid = n_items < slots ? n_items : slots;
+}
+
+template <typename T>
+ws_status backward_plan(int64_t B, int64_t L, int64_t D, int64_t K, int64_t V,
+                        BwdPlan* out) {
+  int per_sm = 0;
+  ws_status st = backward_shape<T>(L, K, V, out, &per_sm);
+  if (st != WS_OK) return st;
+  split_rows(B, D, per_sm, out);
   return WS_OK;
 }
 
-template <typename T, bool LOSS>
+// Loss mode: shared memory of a block whose tape has M slots, and the shape with the most
+// resident rows per SM (the same scoring as backward_shape).
+template <typename T>
+size_t loss_smem(int64_t M, int64_t L, int64_t K, int threads, int R) {
+  return loss_layout(M, L, K, threads, (size_t)R * sizeof(T), K <= kRegSlots).bytes;
+}
+
+template <typename T, int RR>
+void (*loss_pick(bool kreg))(BwdParams<T>, BwdLut) {
+  return kreg ? loss_kernel<T, RR, true> : loss_kernel<T, RR, false>;
+}
+
+template <typename T>
+void (*loss_fn(int R, bool kreg))(BwdParams<T>, BwdLut) {
+  if constexpr (kRowsMax<T> >= 4) {
+    if (R == 4) return loss_pick<T, 4>(kreg);
+  }
+  if (R == 2) return loss_pick<T, 2>(kreg);
+  return loss_pick<T, 1>(kreg);
+}
+
+template <typename T>
+ws_status loss_shape(int64_t M, int64_t L, int64_t K, BwdPlan* out, int* per_sm_out) {
+  const DeviceInfo& dev = device_info();
+  const size_t budget = dev.smem_optin < (size_t)200 * 1024 ? dev.smem_optin : 200 * 1024;
+  const bool kreg = K <= kRegSlots;
+  double best_score = -1.0;
+  int best_threads = 0, best_per_sm = 0, best_r = 1;
+  for (int R = kRowsMax<T>; R >= 1; R /= 2) {
+    auto kern = loss_fn<T>(R, kreg);
+    for (int threads = 128; threads >= 32; threads /= 2) {
+      const size_t smem = loss_smem<T>(M, L, K, threads, R);
+      if (smem > budget) continue;
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+      if (e != cudaSuccess) return fail_cuda(e, "loss_grad");
+      int per_sm = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+      if (e != cudaSuccess) return fail_cuda(e, "loss_grad");
+      if (per_sm < 1) continue;
+      double warps = (double)per_sm * threads / 32.0;
+      if (warps > 32.0) warps = 32.0;
+      const double score = warps * (double)R;
+      if (score > best_score + 1e-9) {
+        best_score = score;
+        best_threads = threads;
+        best_per_sm = per_sm;
+        best_r = R;
+      }
+    }
+  }
+  if (best_threads == 0)
+    return fail("loss_grad: " + std::to_string(K) + " constants and " + std::to_string(M) +
+                " tape slots need more shared memory than a block has");
+  const size_t smem = loss_smem<T>(M, L, K, best_threads, best_r);
+  cudaError_t e = cudaFuncSetAttribute(loss_fn<T>(best_r, kreg),
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return fail_cuda(e, "loss_grad");
+  out->threads = best_threads;
+  out->R = best_r;
+  out->smem = smem;
+  *per_sm_out = best_per_sm;
+  return WS_OK;
+}
+
+template <typename T>
 BwdParams<T> backward_params(const uint8_t* pop, int64_t B, int64_t L, const void* x, int64_t V,
                              int64_t D,
                              const void* consts, int64_t K, const BwdPlan& plan) {
@@ -925,12 +1446,12 @@ ws_status launch_backward_typed(const uint8_t* pop, int64_t B, int64_t L, const 
                                 const void* gout,
                                 void* grad, const BwdLut& lut, cudaStream_t stream) {
   BwdPlan plan;
-  ws_status st = backward_plan<T, false>(B, L, D, K, V, &plan);
+  ws_status st = backward_plan<T>(B, L, D, K, V, &plan);
   if (st != WS_OK) return st;
-  BwdParams<T> prm = backward_params<T, false>(pop, B, L, x, V, D, consts, K, plan);
+  BwdParams<T> prm = backward_params<T>(pop, B, L, x, V, D, consts, K, plan);
   prm.gout = static_cast<const T*>(gout);
   prm.grad = static_cast<T*>(grad);
-  adj_fn<T, false>(plan.R, K <= kRegSlots)<<<(unsigned)plan.grid, plan.threads, plan.smem,
+  adj_fn<T>(plan.R, K <= kRegSlots)<<<(unsigned)plan.grid, plan.threads, plan.smem,
                                               stream>>>(prm, lut);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? WS_OK : fail_cuda(e, "eval_rpn_backward");
@@ -948,47 +1469,48 @@ ws_status launch_loss_grad(const uint8_t* pop, int64_t B, int64_t L, const void*
                            double* part_grad, double* loss, void* grad, int32_t* buckets,
                            int64_t* n_splits_out, cudaStream_t stream) {
   BwdPlan plan;
-  ws_status st = backward_plan<T, true>(B, L, D, K, num_vars, &plan);
+  int per_sm = 0;
+  ws_status st = loss_shape<T>(L, L, K, &plan, &per_sm);
   if (st != WS_OK) return st;
+  split_rows(B, D, per_sm, &plan);
   if (n_splits_out) *n_splits_out = plan.n_splits;
   if (!part_loss) return WS_OK;  // plan query only
   const BwdLut lut = build_bwd_lut(ids, num_vars);
-  BwdParams<T> prm = backward_params<T, true>(pop, B, L, x, num_vars, D, consts, K, plan);
+  BwdParams<T> prm = backward_params<T>(pop, B, L, x, num_vars, D, consts, K, plan);
   prm.y = static_cast<const T*>(y);
   prm.active = active;
   prm.part_loss = part_loss;
   prm.part_grad = part_grad;
+  const bool kreg = K <= kRegSlots;
   cudaError_t e;
   if (!buckets) {
-    adj_fn<T, true>(plan.R, K <= kRegSlots)<<<(unsigned)plan.grid, plan.threads, plan.smem,
-                                               stream>>>(prm, lut);
+    loss_fn<T>(plan.R, kreg)<<<(unsigned)plan.grid, plan.threads, plan.smem, stream>>>(prm, lut);
   } else {
     // buckets[0..15]: counts; buckets + 16: lists [n_buckets, B]
     int nb = 0;
-    while (nb < kMaxBuckets && (nb == 0 || kBucketOps[nb - 1] < L - 1)) ++nb;
+    while (nb < kMaxBuckets && (nb == 0 || kBucketSlots[nb - 1] < L)) ++nb;
     int32_t* counts = buckets;
     int32_t* lists = buckets + 16;
     e = cudaMemsetAsync(counts, 0, 16 * sizeof(int32_t), stream);
     if (e != cudaSuccess) return fail_cuda(e, "loss_grad");
     const int64_t cb = (B + 255) / 256;
-    bucket_kernel<<<(unsigned)(cb < 2048 ? cb : 2048), 256, 0, stream>>>(pop, B, L, lut, active,
+    bucket_kernel<<<(unsigned)(cb < 2048 ? cb : 2048), 256, 0, stream>>>(pop, B, L, K, lut, active,
                                                                          nb, counts, lists);
     for (int j = 0; j < nb; ++j) {
-      const int64_t M = kBucketOps[j] < L ? kBucketOps[j] : L;
+      const int64_t M = kBucketSlots[j] < L ? kBucketSlots[j] : L;
       BwdPlan pj;
-      int per_sm = 0;
-      st = backward_shape<T, true>(M, K, num_vars, &pj, &per_sm);
+      int pj_per_sm = 0;
+      st = loss_shape<T>(M, L, K, &pj, &pj_per_sm);
       if (st != WS_OK) return st;
       BwdParams<T> q = prm;
       q.tape_stride = pj.threads;
       q.tape_ops = (int)M;
       q.list = lists + (int64_t)j * B;
       q.list_count = counts + j;
-      const int64_t slots = (int64_t)device_info().sm_count * per_sm;
+      const int64_t slots = (int64_t)device_info().sm_count * pj_per_sm;
       const int64_t items = B * plan.n_splits;
       const int64_t grid = items < slots ? items : slots;
-      adj_fn<T, true>(pj.R, K <= kRegSlots)<<<(unsigned)grid, pj.threads, pj.smem, stream>>>(
-          q, lut);
+      loss_fn<T>(pj.R, kreg)<<<(unsigned)grid, pj.threads, pj.smem, stream>>>(q, lut);
     }
   }
   e = cudaGetLastError();
