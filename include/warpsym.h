@@ -98,6 +98,24 @@ const char* ws_version(void);
 const char* ws_last_error(void);
 
 /*
+ * Bounds-checked build (no counterpart in the reference, whose kernels rely on TORCH_CHECK shape
+ * guards, rpn_kernels.cu:2536-2557).  libwarpsym_bc.so is this library compiled with
+ * -DWS_BOUNDS_CHECK: its kernels test their shared- and global-memory indices against the
+ * extents of the buffers they address; an index out of range is recorded (the first per device
+ * module: check site << 32 | index) and its access skipped, never faulting.  Load it in place of
+ * libwarpsym.so (the Python package reads WARPSYM_LIB) to run small shapes under the checks.
+ *   ws_bounds_status          -- enabled_out = 1 in the checked build (0 here, word_out then 0);
+ *                                word_out = the first recorded violation, host-side checks first,
+ *                                then the device modules' (read when a device is present);
+ *                                reset != 0 clears the records.
+ *   ws_debug_bounds_selftest  -- checked build only, host only: reads a 4-element host array at
+ *                                indices 0..5 under the check; word_out = the record
+ *                                ((99 << 32) | 4), and the two out-of-range reads are skipped.
+ */
+ws_status ws_bounds_status(int32_t* enabled_out, uint64_t* word_out, int32_t reset);
+ws_status ws_debug_bounds_selftest(uint64_t* word_out);
+
+/*
  * Classic per-(program,row) interpreter.  Replaces `eval_rpn` (bindings.cpp:434 ->
  * launch_rpn_kernel, rpn_kernels.cu:361-429; kernel rpn_kernels.cu:202-358).
  * Writes out_preds[B*D] (dtype), out_sp[B*D] (int32), out_error[B*D] (uint8) exactly as the
@@ -186,6 +204,14 @@ size_t ws_static_scratch_bytes(void);
  *                             in place (their pointers and shapes are fixed by the plan)
  *   ws_batch_info             plan facts: 0 work items, 1 rows per lane, 2 programs per block,
  *                             3 dynamic shared memory per CTA, 4 resident CTAs, 5 programs
+ *   ws_batch_set_cancel       attaches a device int32 flag (NULL detaches).  The evaluator's
+ *                             CTAs read it before taking each work item; once it reads nonzero
+ *                             the launch takes no further items and ends after those in flight
+ *                             (no wait, no trap), leaving its outputs incomplete: the caller who
+ *                             set the flag discards them.  With a flag attached every launch
+ *                             also resets the per-program split counters, so the next launch
+ *                             after a cancelled one is exact.  Works inside captured graphs (the
+ *                             flag is read at run time).  No counterpart in the reference.
  *
  * All problems share dtype, program width L (<= 256), strict_mode, policy, loss, schedule and
  * invalid_value (from opts); opts->phase is ignored here (ws_batch_eval takes the phase).
@@ -212,6 +238,7 @@ ws_status ws_batch_create(int32_t dtype, const ws_problem* problems, int32_t n_p
                           void* stream, ws_batch** out_batch);
 ws_status ws_batch_eval(ws_batch* batch, int32_t phase, void* stream);
 int64_t ws_batch_info(const ws_batch* batch, int32_t what);
+ws_status ws_batch_set_cancel(ws_batch* batch, const int32_t* device_flag);
 void ws_batch_destroy(ws_batch* batch);
 
 /*

@@ -1,7 +1,8 @@
 """ctypes binding of libwarpsym.so (the C ABI declared in include/warpsym.h).
 
-The library is loaded from this package directory.  There is no fallback: if the shared
-library is missing or fails to load, every entry point raises.
+The library is loaded from this package directory, or from the path in the environment
+variable WARPSYM_LIB (for example the bounds-checked build libwarpsym_bc.so).  There is no
+fallback: if the shared library is missing or fails to load, every entry point raises.
 """
 from __future__ import annotations
 
@@ -10,7 +11,8 @@ import os
 import threading
 
 _PKG_DIR = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG_DIR, "libwarpsym.so")
+LIB_PATH = os.environ.get("WARPSYM_LIB") or os.path.join(_PKG_DIR, "libwarpsym.so")
+BC_LIB_PATH = os.path.join(_PKG_DIR, "libwarpsym_bc.so")  # the bounds-checked build
 
 WS_OK = 0
 WS_F32, WS_F64 = 0, 1
@@ -114,6 +116,8 @@ _I32 = C.c_int32
 _SIGS = {
     "ws_version": (C.c_char_p, []),
     "ws_last_error": (C.c_char_p, []),
+    "ws_bounds_status": (_I32, [C.POINTER(C.c_int32), C.POINTER(C.c_uint64), _I32]),
+    "ws_debug_bounds_selftest": (_I32, [C.POINTER(C.c_uint64)]),
     "ws_fitness_workspace_bytes": (C.c_size_t, [_I64, _I64, _I32]),
     "ws_schedule_count": (_I32, []),
     "ws_eval_rpn": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P, _P,
@@ -131,6 +135,7 @@ _SIGS = {
                                _P, C.POINTER(_P)]),
     "ws_batch_eval": (_I32, [_P, _I32, _P]),
     "ws_batch_info": (_I64, [_P, _I32]),
+    "ws_batch_set_cancel": (_I32, [_P, _P]),
     "ws_batch_destroy": (None, [_P]),
     "ws_gp_workspace_bytes": (_I32, [_I32, _P, _I32, _I64, C.POINTER(C.c_size_t)]),
     "ws_gp_create": (_I32, [_I32, _P, _I32, _I64, C.POINTER(GpOpts), _P, C.c_size_t, _P,
@@ -225,6 +230,14 @@ def lib():
                 fn.argtypes = args
             _lib = handle
     return _lib
+
+
+def bounds_status(reset: bool = False):
+    """(enabled, word): whether the loaded library is the bounds-checked build, and its first
+    recorded out-of-range index ((site << 32) | index; 0 when none)."""
+    en, w = C.c_int32(0), C.c_uint64(0)
+    check(lib().ws_bounds_status(C.byref(en), C.byref(w), 1 if reset else 0))
+    return bool(en.value), int(w.value)
 
 
 def check(status: int) -> None:

@@ -146,6 +146,16 @@ class BatchedFitness:
             self.evaluate()
         return g
 
+    def set_cancel_flag(self, flag: Optional[torch.Tensor]) -> None:
+        """Attaches a one-element int32 device tensor (None detaches): while it holds a nonzero
+        value, a launch takes no further work items and its outputs are incomplete (the caller
+        discards them); see ws_batch_set_cancel."""
+        if flag is not None and (flag.dtype != torch.int32 or flag.device != self.device
+                                 or flag.numel() != 1):
+            raise ValueError("the cancel flag is a one-element int32 tensor on the batch's device")
+        self._cancel = flag  # kept alive while attached
+        N.check(N.lib().ws_batch_set_cancel(self._h, ptr(flag) if flag is not None else None))
+
     def info(self) -> Dict[str, int]:
         lib = N.lib()
         keys = ("work_items", "rows_per_lane", "programs_per_block", "smem_bytes", "resident_ctas",

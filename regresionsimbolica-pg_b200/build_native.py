@@ -17,6 +17,10 @@ REPO_DIR = os.path.dirname(PKG_DIR)
 CSRC = os.path.join(PKG_DIR, "csrc")
 BUILD_DIR = os.path.join(PKG_DIR, "_build")
 LIB_PATH = os.path.join(PKG_DIR, "libwarpsym.so")
+# the bounds-checked build (-DWS_BOUNDS_CHECK): same sources, kernels record out-of-range
+# indices instead of faulting (csrc/ws_bounds.cuh)
+BC_BUILD_DIR = os.path.join(PKG_DIR, "_build_bc")
+BC_LIB_PATH = os.path.join(PKG_DIR, "libwarpsym_bc.so")
 ORACLE_DIR = os.path.join(REPO_DIR, "oracle")
 ORACLE_LIB = os.path.join(ORACLE_DIR, "libws_oracle.so")
 
@@ -37,32 +41,36 @@ def _run(cmd):
     return res.stdout + res.stderr
 
 
-def build_native(verbose: bool = False, jobs: int = 8) -> str:
-    """Compiles csrc/*.cu into libwarpsym.so (sm_100a).  Returns the library path."""
-    os.makedirs(BUILD_DIR, exist_ok=True)
+def build_native(verbose: bool = False, jobs: int = 8, bounds_check: bool = False) -> str:
+    """Compiles csrc/*.cu into libwarpsym.so (sm_100a), or with bounds_check into
+    libwarpsym_bc.so.  Returns the library path."""
+    build_dir = BC_BUILD_DIR if bounds_check else BUILD_DIR
+    lib_path = BC_LIB_PATH if bounds_check else LIB_PATH
+    flags = NVCC_FLAGS + (["-DWS_BOUNDS_CHECK"] if bounds_check else [])
+    os.makedirs(build_dir, exist_ok=True)
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
         glob.glob(os.path.join(REPO_DIR, "include", "*.h")) + [os.path.abspath(__file__)]
     hdr_time = _newest(headers)
     objs, todo = [], []
     for src in sources:
-        obj = os.path.join(BUILD_DIR, os.path.basename(src)[:-3] + ".o")
+        obj = os.path.join(build_dir, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
         if not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src), hdr_time):
             todo.append((src, obj))
 
     def compile_one(pair):
         src, obj = pair
-        return _run([NVCC, "-c", src, "-o", obj] + ARCH + NVCC_FLAGS)
+        return _run([NVCC, "-c", src, "-o", obj] + ARCH + flags)
 
     if todo:
         with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
             for out in ex.map(compile_one, todo):
                 if verbose and out.strip():
                     print(out)
-    if todo or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < _newest(objs):
-        _run([NVCC, "-shared", "-o", LIB_PATH] + objs + ARCH + ["-lcudart"])
-    return LIB_PATH
+    if todo or not os.path.exists(lib_path) or os.path.getmtime(lib_path) < _newest(objs):
+        _run([NVCC, "-shared", "-o", lib_path] + objs + ARCH + ["-lcudart"])
+    return lib_path
 
 
 def build_oracle() -> str:

@@ -103,7 +103,7 @@ struct BwdParams {
 // depth 32 are dropped, C takes slot min(c_idx, K-1) (1.0 without constants).  Operands are kept
 // on the stack as (kind, index) pairs, so terminals never enter the tape.
 __device__ BRoot parse_program(const uint8_t* __restrict__ prog, int64_t L, int64_t K,
-                               const uint8_t* s_tab, BOp* ops) {
+                               const uint8_t* s_tab, BOp* ops, int cap, int64_t V) {
   const uint8_t* t_kind = s_tab;
   const uint8_t* t_fop = s_tab + 256;
   const uint8_t* t_bop = s_tab + 512;
@@ -112,6 +112,7 @@ __device__ BRoot parse_program(const uint8_t* __restrict__ prog, int64_t L, int6
   uint16_t si[kStack];
   int sp = 0, n_ops = 0;
   int64_t c_idx = 0;
+  bool bad = false;  // an array bound was hit (bounds-checked build only)
   for (int pc = 0; pc < (int)L; ++pc) {
     const int tok = prog[pc];
     const uint8_t kind = t_kind[tok];
@@ -119,6 +120,10 @@ __device__ BRoot parse_program(const uint8_t* __restrict__ prog, int64_t L, int6
     if (kind == BK_VAR || kind == BK_LIT || kind == BK_CONST) {
       uint8_t k = kind == BK_VAR ? OPD_VAR : OPD_LIT;
       uint16_t ix = t_arg[tok];
+      if (kind == BK_VAR && !WS_BC(ix < V, BC_ADJ_OPERAND, ix)) {
+        bad = true;
+        break;
+      }
       if (kind == BK_CONST) {
         if (K > 0) {
           k = OPD_CONST;
@@ -158,6 +163,10 @@ __device__ BRoot parse_program(const uint8_t* __restrict__ prog, int64_t L, int6
       o.a = si[sp];
       o.binary = 0;
     }
+    if (!WS_BC(n_ops < cap, BC_ADJ_PARSE, n_ops)) {
+      bad = true;
+      break;
+    }
     ops[n_ops] = o;
     sk[sp] = OPD_OP;  // an operator always finds room: it just freed one or two slots
     si[sp] = (uint16_t)n_ops;
@@ -166,7 +175,7 @@ __device__ BRoot parse_program(const uint8_t* __restrict__ prog, int64_t L, int6
   }
   BRoot r;
   r.n_ops = n_ops;
-  r.valid = sp == 1 ? 1 : 0;
+  r.valid = (sp == 1 && !bad) ? 1 : 0;
   r.kind = sp >= 1 ? sk[0] : OPD_LIT;
   r.idx = sp >= 1 ? si[0] : 0;
   if (r.valid && r.kind == OPD_OP) {  // mark the operators whose value reaches the root
@@ -423,7 +432,7 @@ __global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
     const int64_t b = p.list ? (int64_t)p.list[li] : li;
     __syncthreads();
     if (tid == 0 && s_prog != b) {
-      BRoot rt0 = parse_program(p.pop + b * p.L, p.L, p.K, s_tab, ops);
+      BRoot rt0 = parse_program(p.pop + b * p.L, p.L, p.K, s_tab, ops, p.tape_ops, p.V);
       for (int o = 0; o < rt0.n_ops; ++o) {
         uint16_t f = 0;
         if (ops[o].ka == OPD_OP && (int)ops[o].a == o - 1) f |= 1;
@@ -700,9 +709,9 @@ struct LossAddr {
 template <typename T, int R>
 __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t L, int64_t K,
                                        const uint8_t* s_tab, const T* s_lit,
-                                       const T* __restrict__ cst, const LossAddr& ad,
-                                       unsigned char* smem, LOp* ops, uint8_t* stage,
-                                       uint32_t* leaf) {
+                                       const T* __restrict__ cst, int64_t V,
+                                       const LossAddr& ad, unsigned char* smem, LOp* ops,
+                                       uint8_t* stage, uint32_t* leaf) {
   const uint8_t* t_kind = s_tab;
   const uint8_t* t_fop = s_tab + 256;
   const uint8_t* t_bop = s_tab + 512;
@@ -714,6 +723,8 @@ __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t
   uint16_t sl[kStack];  // constant-leaf ordinal of a constant
   int sp = 0, n_ops = 0, n_leaf = 0, n_stage = 0, n_scal = 0;
   int64_t c_idx = 0;
+  bool bad = false;  // an array bound was hit (bounds-checked build only)
+  const int M = (int)ad.sink;
   for (int pc = 0; pc < (int)L; ++pc) {
     const int tok = prog[pc];
     const uint8_t kind = t_kind[tok];
@@ -721,6 +732,10 @@ __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t
     if (kind == BK_VAR || kind == BK_LIT || kind == BK_CONST) {
       uint8_t k = kind == BK_VAR ? OPD_VAR : OPD_LIT;
       uint16_t ix = t_arg[tok], c = 0;
+      if (kind == BK_VAR && !WS_BC(ix < V, BC_LOSS_PARSE, ix)) {
+        bad = true;
+        break;
+      }
       if (kind == BK_CONST) {
         if (K > 0) {
           k = OPD_CONST;
@@ -735,9 +750,19 @@ __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t
         if (k == OPD_VAR) {
           int j = 0;
           while (j < n_stage && stage[j] != ix) ++j;
-          if (j == n_stage) stage[n_stage++] = (uint8_t)ix;
+          if (j == n_stage) {
+            if (!WS_BC(n_stage < M, BC_LOSS_PARSE, n_stage)) {
+              bad = true;
+              break;
+            }
+            stage[n_stage++] = (uint8_t)ix;
+          }
           ix = (uint16_t)j;
         } else {
+          if (!WS_BC(n_scal < (int)L && (k != OPD_CONST || n_leaf < M), BC_LOSS_PARSE, n_scal)) {
+            bad = true;
+            break;
+          }
           const T v = k == OPD_CONST ? cst[c] : (ix < 10 ? s_lit[ix] : (T)1.0);
           for (int r = 0; r < R; ++r) scal[(size_t)n_scal * kPer + r] = v;
           if (k == OPD_CONST) {
@@ -785,23 +810,30 @@ __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t
         o.flags |= (uint8_t)(fl << 1);  // the B flags are the A flags shifted by one
       }
     }
+    if (!WS_BC(n_ops < M, BC_LOSS_PARSE, n_ops)) {
+      bad = true;
+      break;
+    }
     ops[n_ops] = o;
     sk[sp] = OPD_OP;  // an operator always finds room: it just freed one or two slots
     si[sp] = (uint16_t)n_ops;
     ++sp;
     ++n_ops;
   }
+  if (!WS_BC(n_ops + n_leaf + n_stage <= M, BC_LOSS_PARSE, n_ops + n_leaf + n_stage)) bad = true;
   const uint32_t stage_first = (uint32_t)(n_ops + n_leaf);
   const uint16_t sink = (uint16_t)(ad.tape + ad.sink * ad.slot);
   LRoot<T> r;
   r.n_ops = n_ops;
-  r.valid = sp == 1 ? 1 : 0;
+  r.valid = (sp == 1 && !bad) ? 1 : 0;
   r.n_stage = n_stage;
   r.stage0 = (int)(ad.tape + stage_first * ad.slot);
   r.kind = sp >= 1 ? sk[0] : OPD_LIT;
   r.at = 0;
   r.ck = 0;
   r.scalar = (T)0;
+  r.n_leaf = 0;
+  if (bad) return r;
   if (sp >= 1) {
     if (r.kind == OPD_OP) r.at = (uint16_t)(ad.tape + si[0] * ad.slot);
     else if (r.kind == OPD_VAR) r.at = (uint16_t)(ad.tape + (stage_first + si[0]) * ad.slot);
@@ -975,7 +1007,7 @@ __global__ void __launch_bounds__(128) loss_kernel(BwdParams<T> p, BwdLut lut) {
     __syncthreads();
     if (tid == 0 && s_prog != b) {
       s_root = parse_loss_program<T, R>(p.pop + b * p.L, p.L, p.K, s_tab, s_lit,
-                                        p.consts + b * p.K, ad, smem, ops, stage, leaf);
+                                        p.consts + b * p.K, p.V, ad, smem, ops, stage, leaf);
       s_prog = b;
     }
     if (!KREG)
@@ -1549,6 +1581,7 @@ extern "C" ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* populati
                                           const ws_token_map* ids, void* stream) {
   using namespace ws;
   clear_error();
+  NvtxRange nvtx("ws_eval_rpn_backward");
   if (dtype != WS_F32 && dtype != WS_F64) return fail("x must be float32 or float64");
   if (!ids) return fail("token map is required");
   if (B < 0 || L < 0 || D < 0 || K < 0 || num_vars < 0) return fail("negative dimension");
@@ -1614,6 +1647,7 @@ extern "C" ws_status ws_loss_grad(int32_t dtype, const uint8_t* population, int6
                                   void* stream) {
   using namespace ws;
   clear_error();
+  NvtxRange nvtx("ws_loss_grad");
   ws_status st = loss_grad_check(dtype, B, L, D, K, num_vars);
   if (st != WS_OK) return st;
   if (!ids) return fail("token map is required");

@@ -1,6 +1,7 @@
 // ws_capi.cu -- extern "C" entry points of libwarpsym (declared in include/warpsym.h).
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -23,6 +24,30 @@ ws_status fail(const std::string& msg) {
 ws_status fail_cuda(cudaError_t e, const char* where) {
   set_error(std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e));
   return WS_ERR_CUDA;
+}
+
+// ---- bounds-checked build: the host word and the device modules' readers -----------------
+namespace {
+std::atomic<unsigned long long> g_bc_host{0ull};
+std::mutex& bc_mutex() {
+  static std::mutex mu;
+  return mu;
+}
+std::vector<BcReader>& bc_readers() {
+  static std::vector<BcReader> readers;
+  return readers;
+}
+}  // namespace
+
+void bc_host_fail(uint32_t site, uint32_t idx) {
+  unsigned long long none = 0ull;
+  g_bc_host.compare_exchange_strong(none, ((unsigned long long)site << 32) | idx);
+}
+
+int bc_register(BcReader reader) {
+  std::lock_guard<std::mutex> g(bc_mutex());
+  bc_readers().push_back(reader);
+  return (int)bc_readers().size();
 }
 
 const DeviceInfo& device_info() {
@@ -113,6 +138,52 @@ const char* ws_version(void) { return "warpsym 0.1.0 (sm_100a)"; }
 
 const char* ws_last_error(void) { return g_last_error.c_str(); }
 
+ws_status ws_bounds_status(int32_t* enabled_out, uint64_t* word_out, int32_t reset) {
+  clear_error();
+  if (!enabled_out || !word_out) return fail("null output pointer");
+#ifdef WS_BOUNDS_CHECK
+  *enabled_out = 1;
+  unsigned long long w = g_bc_host.load();
+  if (reset) g_bc_host.store(0ull);
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) == cudaSuccess && n_dev > 0) {
+    std::lock_guard<std::mutex> g(bc_mutex());
+    for (BcReader r : bc_readers()) {
+      const unsigned long long v = r(reset != 0);
+      if (w == 0ull) w = v;
+    }
+  } else {
+    (void)cudaGetLastError();
+  }
+  *word_out = w;
+#else
+  (void)reset;
+  *enabled_out = 0;
+  *word_out = 0;
+#endif
+  return WS_OK;
+}
+
+ws_status ws_debug_bounds_selftest(uint64_t* word_out) {
+  clear_error();
+  if (!word_out) return fail("null output pointer");
+#ifdef WS_BOUNDS_CHECK
+  // a host array read with indices 0..5 of which 4 and 5 are out of range: both are skipped,
+  // the first is recorded
+  const int arr[4] = {1, 2, 3, 4};
+  int sum = 0;
+  g_bc_host.store(0ull);
+  for (int i = 0; i < 6; ++i)
+    if (WS_BC(i < 4, BC_SELFTEST, i)) sum += arr[i];
+  *word_out = g_bc_host.exchange(0ull);
+  if (sum != 10) return fail("bounds self-test: an out-of-range access was not skipped");
+  return WS_OK;
+#else
+  *word_out = 0;
+  return fail("not a bounds-checked build (libwarpsym_bc.so is)");
+#endif
+}
+
 size_t ws_fitness_workspace_bytes(int64_t B, int64_t L, int32_t dtype) {
   if (B < 0) B = 0;
   if (L < 0) L = 0;
@@ -126,6 +197,7 @@ ws_status ws_eval_rpn(int32_t dtype, const uint8_t* population, int64_t B, int64
                       int64_t K, void* out_preds, int32_t* out_sp, uint8_t* out_error,
                       const ws_token_map* ids, int32_t strict_mode, void* stream) {
   clear_error();
+  NvtxRange nvtx("ws_eval_rpn");
   if (dtype != WS_F32 && dtype != WS_F64) return fail("x must be float32 or float64");
   if (!ids) return fail("token map is required");
   if (B < 0 || L < 0 || D < 0 || K < 0 || num_vars < 0) return fail("negative dimension");
@@ -163,6 +235,7 @@ ws_status ws_eval_rpn_fused(int32_t dtype, const uint8_t* population, int64_t B,
                             size_t workspace_bytes, void* stream) {
   (void)launch_mode;
   clear_error();
+  NvtxRange nvtx("ws_eval_rpn_fused");
   if (dtype != WS_F32 && dtype != WS_F64) return fail("x must be float32 or float64");
   if (!ids) return fail("token map is required");
   // argument checks of launch_rpn_eval_fused, in its order (rpn_kernels.cu:2539-2545)
@@ -328,6 +401,13 @@ ws_status ws_batch_eval(ws_batch* batch, int32_t phase, void* stream) {
 int64_t ws_batch_info(const ws_batch* batch, int32_t what) {
   if (!batch) return -1;
   return batch_info(const_cast<ws_batch*>(batch), what);
+}
+
+ws_status ws_batch_set_cancel(ws_batch* batch, const int32_t* device_flag) {
+  clear_error();
+  if (!batch) return fail("batch is null");
+  batch_set_cancel(batch, device_flag);
+  return WS_OK;
 }
 
 void ws_batch_destroy(ws_batch* batch) {

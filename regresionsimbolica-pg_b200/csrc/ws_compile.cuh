@@ -24,6 +24,7 @@
 // of them is invalid, so they are never evaluated.
 #pragma once
 
+#include "ws_bounds.cuh"
 #include "ws_ops.cuh"
 
 namespace ws {
@@ -548,6 +549,10 @@ __host__ __device__ ProgHdr compile_program_v2(const uint8_t* __restrict__ prog,
         nd.need = (uint8_t)need;
         c_ops = (uint8_t)(1 + cnt[l] + (bin ? cnt[r] : 0));
       }
+    }
+    if (!WS_BC(nn < LMAX, BC_COMPILE_NODES, nn)) {
+      h.status = PROG_INVALID;
+      break;
     }
     nodes[nn] = nd;
     cnt[nn] = c_ops;

@@ -205,7 +205,17 @@ struct FitParams {
   const double* yvar;       // [n_prob] (WS_LOSS_R2)
   const int64_t* perm;      // programs in evaluation order: by problem, then tape length
   T* gspill;                // per-warp scratch for spill slots beyond the shared ones
+  const int32_t* cancel;    // optional: nonzero -> take no further work items
 };
+
+// The next work item of a persistent evaluator, or n_items (no more work) once the launch's
+// cancel flag reads nonzero: the flag is polled once per item, so a cancelled launch ends after
+// the items in flight, without any wait.
+__device__ __forceinline__ int64_t next_item(unsigned* work, const int32_t* cancel,
+                                             int64_t n_items) {
+  if (cancel && *reinterpret_cast<const volatile int32_t*>(cancel) != 0) return n_items;
+  return (int64_t)atomicAdd(work, 1u);
+}
 
 template <typename T> struct Vec16;
 template <> struct Vec16<float> {
@@ -421,7 +431,8 @@ __device__ __forceinline__ void exec_case(uint32_t cs, T s, const LD& ld, T (&ac
 template <typename T, int R, bool STRICT>
 __device__ __forceinline__ void run_tape(const Instr<T>* __restrict__ tp, int n,
                                          const T* __restrict__ xb, T* __restrict__ sb,
-                                         T* __restrict__ gb, T (&acc)[R], uint32_t& err) {
+                                         T* __restrict__ gb, T (&acc)[R], uint32_t& err,
+                                         uint32_t x_lim, uint32_t n_deep) {
   constexpr int PASS = 32 * R;
   err = 0u;
   // The next tape word is loaded while the current one executes (reading one word past the end
@@ -435,20 +446,29 @@ __device__ __forceinline__ void run_tape(const Instr<T>* __restrict__ tp, int n,
     // vector operand: an X row of the tile or a shared spill slot (dereferenced only by the
     // cases that read it)
     const T* vp = ((c & P_FETCH_SLOT) ? sb : xb) + (c >> P_SH_V) * PASS;
+#ifdef WS_BOUNDS_CHECK
+    if (pcase_fetches(c & P_CASE_MASK) && !(c & P_FETCH_SLOT) &&
+        !WS_BC((c >> P_SH_V) < x_lim, BC_FIT_X, c >> P_SH_V))
+      vp = xb;
+#endif
     if (c & P_SLOW) {  // spill, accumulator load, deep spill slot: rare
       if (c & P_SPILL) {
         const uint32_t sl = (c >> P_SH_SLOT) & 7u;
         if (sl < (uint32_t)kSharedSlots) lane_store<T, R>(sb + sl * PASS, acc);
-        else lane_store<T, R>(gb + (sl - kSharedSlots) * PASS, acc);
+        else if (WS_BC(sl - kSharedSlots < n_deep, BC_FIT_SLOT, sl))
+          lane_store<T, R>(gb + (sl - kSharedSlots) * PASS, acc);
       }
       if (c & P_LOADA_X) {
-        lane_load<T, R>(acc, xb + ((c >> P_SH_LA) & P_OFF_MASK) * PASS);
+        const uint32_t la = (c >> P_SH_LA) & P_OFF_MASK;
+        if (WS_BC(la < x_lim, BC_FIT_X, la)) lane_load<T, R>(acc, xb + la * PASS);
       } else if (c & P_LOADA_S) {
 #pragma unroll
         for (int k = 0; k < R; ++k) acc[k] = ins.imm;
       }
       const uint32_t off = c >> P_SH_V;
-      if ((c & P_FETCH_SLOT) && off >= (uint32_t)kSharedSlots) vp = gb + (off - kSharedSlots) * PASS;
+      if ((c & P_FETCH_SLOT) && off >= (uint32_t)kSharedSlots)
+        vp = WS_BC(off - kSharedSlots < n_deep, BC_FIT_SLOT, off) ? gb + (off - kSharedSlots) * PASS
+                                                                   : sb;
     }
     exec_case<T, R, STRICT>(c & P_CASE_MASK, ins.imm, GenericOperand<T>{vp}, acc, err);
   }
@@ -463,7 +483,7 @@ __device__ __forceinline__ void run_tape(const Instr<T>* __restrict__ tp, int n,
 // 5% more instructions per tape word on this loop and no faster, so the loop stays plain.
 template <int R, bool STRICT>
 __device__ __forceinline__ void run_tape_shared(uint32_t ta, int n, uint32_t xa, uint32_t sa,
-                                                float (&acc)[R], uint32_t& err) {
+                                                float (&acc)[R], uint32_t& err, uint32_t x_lim) {
   static_assert(R == 8 || R == 16 || R == 32, "pass size");
   constexpr int PSH = R == 8 ? 10 : (R == 16 ? 11 : 12);
   err = 0u;
@@ -473,15 +493,23 @@ __device__ __forceinline__ void run_tape_shared(uint32_t ta, int n, uint32_t xa,
     lds_word(c0, ni, ta + 8u * (uint32_t)i);
     const uint32_t c = __shfl_sync(0xFFFFFFFFu, c0, 0);
     const float s = __uint_as_float(ni);
-    const uint32_t va = ((c & P_FETCH_SLOT) ? sa : xa) + ((c >> P_SH_V) << PSH);
+    uint32_t va = ((c & P_FETCH_SLOT) ? sa : xa) + ((c >> P_SH_V) << PSH);
+#ifdef WS_BOUNDS_CHECK
+    if (pcase_fetches(c & P_CASE_MASK) &&
+        !((c & P_FETCH_SLOT) ? WS_BC((c >> P_SH_V) < (uint32_t)kSharedSlots, BC_FIT_SLOT, c >> P_SH_V)
+                             : WS_BC((c >> P_SH_V) < x_lim, BC_FIT_X, c >> P_SH_V)))
+      va = xa;
+#endif
     if (c & P_SLOW) {  // spill, accumulator load: rare
-      if (c & P_SPILL) {
+      if ((c & P_SPILL) &&
+          WS_BC(((c >> P_SH_SLOT) & 7u) < (uint32_t)kSharedSlots, BC_FIT_SLOT, (c >> P_SH_SLOT) & 7u)) {
         const uint32_t a = sa + (((c >> P_SH_SLOT) & 7u) << PSH);
 #pragma unroll
         for (int g = 0; g < R / 4; ++g)
           sts4(a + g * 512, acc[4 * g], acc[4 * g + 1], acc[4 * g + 2], acc[4 * g + 3]);
       }
-      if (c & P_LOADA_X) {
+      if ((c & P_LOADA_X) &&
+          WS_BC(((c >> P_SH_LA) & P_OFF_MASK) < x_lim, BC_FIT_X, (c >> P_SH_LA) & P_OFF_MASK)) {
         const uint32_t a = xa + (((c >> P_SH_LA) & P_OFF_MASK) << PSH);
 #pragma unroll
         for (int g = 0; g < R / 4; ++g) {
@@ -695,7 +723,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2)
 
   for (;;) {
     if (threadIdx.x == 0) {
-      const int64_t it = (int64_t)atomicAdd(P.work, 1u);
+      const int64_t it = next_item(P.work, P.cancel, P.n_items);
       s_item = it;
       if (it < P.n_items) {
         const int pi = find_problem(P.desc, P.n_prob, it, true);
@@ -719,9 +747,11 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2)
     // so a static warp assignment is balanced)
     for (int q = warp; q < np; q += W) {
       const int64_t g = P.perm[p0 + q];
-      const ProgHdr h = P.hdr[g];
+      ProgHdr h = P.hdr[g];
+      if (!WS_BC(h.n_instr <= P.Lcap, BC_FIT_TAPE_LEN, h.n_instr)) h.status = PROG_INVALID;
       const Instr<T>* tg = P.tape + g * (int64_t)P.Lcap;
-      for (int i = lane; i < h.n_instr; i += 32) tapes[(size_t)q * P.Lcap + i] = tg[i];
+      for (int i = lane; i < h.n_instr && WS_BC(i < P.Lcap, BC_FIT_TAPE_LEN, i); i += 32)
+        tapes[(size_t)q * P.Lcap + i] = tg[i];
       lane_sse[q * kLaneStride + lane] = 0.0;
       if (lane == 0) {
         // n_instr, kMetaGlobalSpill if a spill slot lives in global memory; -1: invalid
@@ -771,17 +801,19 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && R <= 16) ? 3 : 2)
         for (int pass = 0; pass < npass; ++pass) {
           T a[R];
           uint32_t err;
+          // variable operands lie below this offset (in passes) from the pass's X row
+          const uint32_t x_lim = (uint32_t)(d.V * (d.RC / PASS) - pass);
           if constexpr (F32) {
             if (shared_only)
               run_tape_shared<R, STRICT>(smem_u32(tape_q), n_instr,
                                          smem_u32(xs + pass * PASS + lane * N), smem_u32(sp_w),
-                                         *reinterpret_cast<float(*)[R]>(&a), err);
+                                         *reinterpret_cast<float(*)[R]>(&a), err, x_lim);
             else
               run_tape<T, R, STRICT>(tape_q, n_instr, xs + pass * PASS + lane * N, sp_w, gsp_w,
-                                     a, err);
+                                     a, err, x_lim, (uint32_t)deep);
           } else {
             run_tape<T, R, STRICT>(tape_q, n_instr, xs + pass * PASS + lane * N, sp_w, gsp_w, a,
-                                   err);
+                                   err, x_lim, (uint32_t)deep);
           }
           const T* yb = ys + pass * PASS + lane * N;
           T part;
@@ -884,7 +916,8 @@ struct ContigOperand {
 template <typename T, int DP, bool STRICT>
 __device__ __forceinline__ void run_tape_small(const Instr<T>* __restrict__ tp, int n,
                                                const T* __restrict__ xb, T* __restrict__ sb,
-                                               T (&acc)[4], uint32_t& err) {
+                                               T (&acc)[4], uint32_t& err, uint32_t n_vars,
+                                               uint32_t n_slots) {
   constexpr int N = Vec16<T>::N;
   constexpr int SLOT = 32 * 4;
   err = 0u;
@@ -894,13 +927,21 @@ __device__ __forceinline__ void run_tape_small(const Instr<T>* __restrict__ tp, 
     const uint32_t c = ins.ctrl;
     const uint32_t off = c >> P_SH_V;
     const T* vp = (c & P_FETCH_SLOT) ? sb + off * SLOT : xb + off * DP;
+#ifdef WS_BOUNDS_CHECK
+    if (pcase_fetches(c & P_CASE_MASK) &&
+        !((c & P_FETCH_SLOT) ? WS_BC(off < n_slots, BC_SMALL_SLOT, off)
+                             : WS_BC(off < n_vars, BC_SMALL_X, off)))
+      vp = xb;
+#endif
     if (c & P_SLOW) {  // spill, accumulator load
-      if (c & P_SPILL) {
+      if ((c & P_SPILL) &&
+          WS_BC(((c >> P_SH_SLOT) & 7u) < n_slots, BC_SMALL_SLOT, (c >> P_SH_SLOT) & 7u)) {
         T* dst = sb + ((c >> P_SH_SLOT) & 7u) * SLOT;
 #pragma unroll
         for (int g = 0; g < 4 / N; ++g) Vec16<T>::store(dst + g * N, &acc[g * N]);
       }
-      if (c & P_LOADA_X) {
+      if ((c & P_LOADA_X) &&
+          WS_BC(((c >> P_SH_LA) & P_OFF_MASK) < n_vars, BC_SMALL_X, (c >> P_SH_LA) & P_OFF_MASK)) {
         const T* src = xb + ((c >> P_SH_LA) & P_OFF_MASK) * DP;
 #pragma unroll
         for (int g = 0; g < 4 / N; ++g) Vec16<T>::load(&acc[g * N], src + g * N);
@@ -975,7 +1016,7 @@ __global__ void __launch_bounds__(256) fitness_small_kernel(const FitParams<T> P
   const double yvar = P.yvar ? P.yvar[0] : 0.0;
 
   for (;;) {
-    if (threadIdx.x == 0) s_item = (int64_t)atomicAdd(P.work, 1u);
+    if (threadIdx.x == 0) s_item = next_item(P.work, P.cancel, P.n_items);
     __syncthreads();  // also: the data set is staged, the previous item's tapes are consumed
     const int64_t item = s_item;
     if (item >= P.n_items) break;
@@ -983,9 +1024,11 @@ __global__ void __launch_bounds__(256) fitness_small_kernel(const FitParams<T> P
     const int np = (int)min((int64_t)P.PB, d.B - p0);
     for (int q = warp; q < np; q += W) {  // warp-cooperative tape copies
       const int64_t g = P.perm[p0 + q];
-      const ProgHdr h = P.hdr[g];
+      ProgHdr h = P.hdr[g];
+      if (!WS_BC(h.n_instr <= P.Lcap, BC_SMALL_TAPE_LEN, h.n_instr)) h.status = PROG_INVALID;
       const Instr<T>* tg = P.tape + g * (int64_t)P.Lcap;
-      for (int i = lane; i < h.n_instr; i += 32) tapes[(size_t)q * tstride + i] = tg[i];
+      for (int i = lane; i < h.n_instr && WS_BC(i < P.Lcap, BC_SMALL_TAPE_LEN, i); i += 32)
+        tapes[(size_t)q * tstride + i] = tg[i];
       if (lane == 0) meta_s[q] = h.status == PROG_OK ? h.n_instr : -1;
     }
     __syncthreads();
@@ -995,7 +1038,8 @@ __global__ void __launch_bounds__(256) fitness_small_kernel(const FitParams<T> P
     T a[4];
     uint32_t err = 0u;
     if (meta >= 0) {
-      run_tape_small<T, DP, STRICT>(tapes + (size_t)q * tstride, meta, xb, sb, a, err);
+      run_tape_small<T, DP, STRICT>(tapes + (size_t)q * tstride, meta, xb, sb, a, err,
+                                    (uint32_t)V, (uint32_t)P.S);
     } else {
 #pragma unroll
       for (int k = 0; k < 4; ++k) a[k] = (T)0;
@@ -1359,6 +1403,7 @@ struct RunArgs {
   int phase, policy, loss;
   double invalid_value;
   cudaStream_t stream;
+  const int32_t* cancel = nullptr;  // see FitParams::cancel
 };
 
 // Compile + length sort of the programs of the descriptors in the workspace (unless
@@ -1366,6 +1411,7 @@ struct RunArgs {
 template <typename T, bool STRICT>
 ws_status compile_and_sort(int64_t total_B, int Lcap, int S, const FitnessWorkspace& lay,
                            unsigned char* wsb, const RunArgs& a) {
+  NvtxRange nvtx("compile_and_sort");
   ProgHdr* hdr = reinterpret_cast<ProgHdr*>(wsb + lay.hdr_off);
   Instr<T>* tape = reinterpret_cast<Instr<T>*>(wsb + lay.tape_off);
   unsigned* cnt = reinterpret_cast<unsigned*>(wsb + lay.cnt_off);
@@ -1405,6 +1451,12 @@ ws_status compile_and_sort(int64_t total_B, int Lcap, int S, const FitnessWorksp
   if (a.phase == WS_PHASE_EVALUATE) {  // the compile kernel is what resets the queue head
     cudaError_t e = cudaMemsetAsync(misc, 0, 16, a.stream);
     if (e != cudaSuccess) return fail_cuda(e, "work-queue reset");
+    // a cancelled launch can leave split counters mid-count (the last split of a program is
+    // what zeroes its counter): with a cancel flag attached they are reset every launch
+    if (a.cancel) {
+      e = cudaMemsetAsync(cnt, 0, (size_t)total_B * sizeof(unsigned), a.stream);
+      if (e != cudaSuccess) return fail_cuda(e, "split-counter reset");
+    }
   }
   return WS_OK;
 }
@@ -1436,6 +1488,7 @@ ws_status run_plan(const Plan& pl, const FitnessWorkspace& lay, unsigned char* w
   }
 
   // 2. evaluate
+  NvtxRange nvtx("evaluate");
   FitParams<T> P;
   P.desc = desc;
   P.n_prob = a.n_desc;
@@ -1455,6 +1508,7 @@ ws_status run_plan(const Plan& pl, const FitnessWorkspace& lay, unsigned char* w
   P.yvar = a.loss == WS_LOSS_R2 ? yvar : nullptr;
   P.perm = perm;
   P.gspill = gspill;
+  P.cancel = a.cancel;
   const int64_t grid = pl.n_items < pl.n_ctas ? pl.n_items : pl.n_ctas;
   if (grid <= 0) return WS_OK;
   fitness_kernel<T, R, STRICT><<<(unsigned)grid, pl.W * 32, pl.smem, a.stream>>>(P);
@@ -1498,6 +1552,7 @@ struct BatchState {
   Plan plan;
   FitnessWorkspace lay{};
   unsigned char* wsb = nullptr;
+  const int32_t* cancel = nullptr;  // ws_batch_set_cancel
 };
 
 }  // namespace
@@ -1635,6 +1690,7 @@ ws_status launch_small(const FitnessRequest& rq, const ProblemRequest& pr,
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "yvar_kernel launch");
   }
+  NvtxRange nvtx("evaluate");
   FitParams<T> P{};
   P.desc = desc;
   P.n_prob = 1;
@@ -1671,6 +1727,7 @@ ws_status launch_small_s(int S, const FitnessRequest& rq, const ProblemRequest& 
 }
 
 ws_status launch_fitness(const FitnessRequest& rq) {
+  NvtxRange nvtx("ws_eval_fitness");
   const FitnessWorkspace lay = fitness_workspace_layout(rq.B, rq.L, rq.dtype);
   ProblemRequest pr;
   pr.pop = rq.pop;
@@ -1799,12 +1856,18 @@ ws_status batch_create(int dtype, const ProblemRequest* probs, int n, int64_t L,
 }
 
 ws_status batch_eval(void* handle, int phase, cudaStream_t stream) {
+  NvtxRange nvtx("ws_batch_eval");
   BatchState* bs = static_cast<BatchState*>(handle);
   return dispatch(bs->dtype, bs->strict != 0, bs->sc, [&](auto tt_, auto rr_, auto ss_) -> ws_status {
     WS_DISPATCH_TYPES
-    RunArgs a{bs->L, bs->n_desc, phase, bs->policy, bs->loss, bs->invalid_value, stream};
+    RunArgs a{bs->L, bs->n_desc, phase, bs->policy, bs->loss, bs->invalid_value, stream,
+              bs->cancel};
     return run_plan<T, R, S>(bs->plan, bs->lay, bs->wsb, a);
   });
+}
+
+void batch_set_cancel(void* handle, const int32_t* flag) {
+  static_cast<BatchState*>(handle)->cancel = flag;
 }
 
 void batch_destroy(void* handle) { delete static_cast<BatchState*>(handle); }

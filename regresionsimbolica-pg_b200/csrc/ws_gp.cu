@@ -493,6 +493,7 @@ ws_status ws_gp_create(int32_t dtype, const ws_gp_problem* problems, int32_t n_p
 
 ws_status ws_gp_step(ws_gp* handle, void* stream) {
   clear_error();
+  NvtxRange nvtx("ws_gp_step");
   if (!handle) return fail("handle is null");
   GpState* gs = reinterpret_cast<GpState*>(handle);
   if (gs->total == 0) return WS_OK;

@@ -6,10 +6,24 @@
 #include <cstddef>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/warpsym.h"
+#include "ws_bounds.cuh"
 #include "ws_ops.cuh"
 
 namespace ws {
+
+// Scoped NVTX range around a pipeline stage: visible to Nsight tools (`ncu --nvtx
+// --nvtx-include "ws_eval_fitness/"` captures only that stage's kernels); a call without an
+// attached tool is a no-op (header-only NVTX v3, nothing to link).
+class NvtxRange {
+ public:
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Thread-local message of the last failed API call (read back by ws_last_error()).
 void set_error(const std::string& msg);
@@ -67,6 +81,7 @@ ws_status batch_create(int dtype, const ProblemRequest* probs, int n, int64_t L,
                        int policy, int loss, int schedule, double invalid_value, void* workspace,
                        size_t workspace_bytes, cudaStream_t stream, void** out);
 ws_status batch_eval(void* handle, int phase, cudaStream_t stream);
+void batch_set_cancel(void* handle, const int32_t* flag);
 void batch_destroy(void* handle);
 int64_t batch_info(void* handle, int what);
 

@@ -343,6 +343,7 @@ extern "C" ws_status ws_lbfgs_optimize(int32_t dtype, const uint8_t* population,
   using namespace ws;
   (void)history_size;  // the reference kernel's history is fixed at 10 entries
   clear_error();
+  NvtxRange nvtx("ws_lbfgs_optimize");
   if (!ids) return fail("token map is required");
   if (dtype != WS_F32 && dtype != WS_F64) return fail("x must be float32 or float64");
   // launch_lbfgs_optimize's checks, in its order (lbfgs_kernels.cu:661-663)

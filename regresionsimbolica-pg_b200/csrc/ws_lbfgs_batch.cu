@@ -508,6 +508,7 @@ extern "C" ws_status ws_lbfgs_adjoint(int32_t dtype, const uint8_t* population, 
                                       void* workspace, size_t workspace_bytes, void* stream) {
   using namespace ws;
   clear_error();
+  NvtxRange nvtx("ws_lbfgs_adjoint");
   if (!opts || !ids) return fail("options and token map are required");
   const ws_lbfgs_opts& o = *opts;
   if (o.max_iter < 1 || o.max_eval < 1 || o.max_ls < 1) return fail("iteration limits must be positive");

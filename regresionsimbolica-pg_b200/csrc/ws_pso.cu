@@ -620,6 +620,7 @@ extern "C" ws_status ws_fused_pso(int32_t dtype, const uint8_t* population, int6
                                   const ws_token_map* ids, uint64_t rng_seed, void* stream) {
   using namespace ws;
   clear_error();
+  NvtxRange nvtx("ws_fused_pso");
   if (!ids) return fail("token map is required");
   // launch_fused_pso's checks, in its order (fused_pso_kernels.cu:466-476)
   if (L > kPsoMaxL) return fail("Formula length exceeds PSO_MAX_L");

@@ -468,6 +468,7 @@ extern "C" ws_status ws_simplify_batch(int64_t* population, int64_t B, int64_t L
                                        void* stream) {
   using namespace ws;
   clear_error();
+  NvtxRange nvtx("ws_simplify_batch");
   if (!ids) return fail("simplify ids are required");
   if (B < 0 || L < 0 || max_id < 0 || n_literals < 0) return fail("negative dimension");
   if (B == 0 || L == 0 || max_passes <= 0) return WS_OK;

@@ -81,6 +81,7 @@ ws_status ws_eval_fitness_static(int32_t dtype, const uint8_t* population, int64
                                  int32_t* out_ninvalid, const ws_token_map* ids,
                                  const ws_fitness_opts* opts, void* stream) {
   clear_error();
+  NvtxRange nvtx("ws_eval_fitness_static");
   const int64_t Bn = B < 0 ? 0 : B, Ln = L < 0 ? 0 : L;
   const size_t need = ws_fitness_workspace_bytes(Bn, Ln, dtype);
   if (need > kStaticScratchBytes) {

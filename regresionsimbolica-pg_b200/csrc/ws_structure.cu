@@ -471,6 +471,7 @@ extern "C" ws_status ws_validate_rpn_batch(const void* population, int32_t token
                                            uint8_t* out_valid, void* stream) {
   using namespace ws;
   clear_error();
+  NvtxRange nvtx("ws_validate_rpn_batch");
   if (B < 0 || L < 0) return fail("population must have non-negative shape");
   if (token_bytes != 1 && token_bytes != 8) return fail("token_bytes must be 1 or 8");
   if (mode < WS_VALIDATE_KERNEL || mode > WS_VALIDATE_STACK)

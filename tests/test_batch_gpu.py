@@ -2,7 +2,8 @@
 single-problem ws_eval_fitness call on it with the same schedule, bit for bit, for uneven
 programs, rows, variable counts and vocabularies, and do not depend on the other problems; FP64 exact-operator
 batches agree with the CPU oracle; a captured CUDA graph replays the whole pipeline after the
-populations are rewritten in place; the autotuner picks a runnable schedule."""
+populations are rewritten in place; a cancel flag stops a launch without any wait and leaves the
+next launch exact; the autotuner picks a runnable schedule."""
 import numpy as np
 import pytest
 import torch
@@ -102,6 +103,49 @@ def test_batch_graph_replay_after_in_place_rewrite():
     assert any(not torch.equal(a, f) for a, f in zip(replayed, first))
     del g
     bf.close()
+
+
+def test_batch_cancel_flag_stops_a_launch_and_the_next_is_exact():
+    """A set cancel flag: the evaluator takes no work item and the outputs keep their previous
+    values, eagerly and in a graph replay; once the flag is cleared, the next launch (evaluate
+    only, on the tapes the cancelled one compiled) and the next replay equal a batch without a
+    flag bit for bit, also for problems whose rows are split across CTAs."""
+    from warpsymbolic_b200.batch import BatchedFitness
+    probs, _ = _problems(9, 5, valid_only=True, Ds=[50_000, 120, 30_000, 8_000, 90_000])
+    ref = BatchedFitness(probs, loss="mse", policy="classic")
+    ref.evaluate()
+    torch.cuda.synchronize()
+    want = [o.clone() for o in ref.outputs]
+    ref.close()
+    bf = BatchedFitness(probs, loss="mse", policy="classic")
+    flag = torch.ones(1, dtype=torch.int32, device=DEV)
+    bf.set_cancel_flag(flag)
+    for o in bf.outputs:
+        o.fill_(-7.0)
+    bf.evaluate()
+    torch.cuda.synchronize()
+    assert all(bool((o == -7.0).all()) for o in bf.outputs)
+    flag.zero_()
+    bf.evaluate(phase=2)
+    torch.cuda.synchronize()
+    assert all(torch.equal(a, b) for a, b in zip(bf.outputs, want))
+    g = bf.capture()
+    for o in bf.outputs:
+        o.fill_(-7.0)
+    flag.fill_(1)
+    g.replay()
+    torch.cuda.synchronize()
+    assert all(bool((o == -7.0).all()) for o in bf.outputs)
+    flag.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    assert all(torch.equal(a, b) for a, b in zip(bf.outputs, want))
+    del g
+    bf.set_cancel_flag(None)
+    bf.close()
+    with pytest.raises(ValueError):
+        BatchedFitness(probs, loss="mse").set_cancel_flag(torch.ones(2, dtype=torch.int32,
+                                                                     device=DEV))
 
 
 def test_batch_is_independent_of_its_neighbours():

@@ -159,3 +159,54 @@ def test_two_rank_row_sharding_matches_single_process(dtype_name):
         atol = 0.0 if loss != "r2" else (1e-6 if dtype == np.float32 else 1e-14)
         np.testing.assert_allclose(a[~bad], want[~bad], rtol=rtol, atol=atol)
         assert (~bad).sum() > 100
+
+
+# ---- failure detection: a rank whose evaluator fails ----------------------------------------
+def _failing_worker(rank, world, port, q):
+    import datetime
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    # a short process-group timeout bounds how long the healthy rank can wait for the failed one
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=10))
+    try:
+        from warpsymbolic_b200.sharding import ShardedEvaluator
+        g, pop, consts, X, y = _case()
+        tm = tl.token_map(g)
+
+        def score(p, c):
+            if rank == 1:
+                raise RuntimeError("injected evaluator failure")
+            return torch.from_numpy(tl.oracle.fitness(tm, p.numpy(), X, c.numpy(), y,
+                                                      policy="classic", loss="rmse"))
+
+        try:
+            ShardedEvaluator(score).evaluate(torch.from_numpy(pop), torch.from_numpy(consts))
+            q.put((rank, "completed"))
+        except Exception as e:  # the failure, as each rank sees it
+            q.put((rank, "%s: %s" % (type(e).__name__, str(e)[:200])))
+    finally:
+        try:
+            dist.destroy_process_group()
+        except Exception:
+            pass
+
+
+def test_a_failing_rank_ends_the_sharded_evaluation_with_an_error():
+    """Rank 1's evaluator raises before the gather (a host-made failure); rank 1 reports it and
+    leaves; rank 0's gather then ends with an error (peer closed, or the process group's 10 s
+    timeout) instead of waiting: both ranks report an error and exit."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        if p.is_alive():
+            p.kill()
+        assert not p.is_alive()
+    assert "injected evaluator failure" in res[1], res
+    assert res[0] != "completed", res
