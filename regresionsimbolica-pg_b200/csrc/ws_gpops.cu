@@ -45,6 +45,36 @@ __global__ void __launch_bounds__(256) mutate_kernel(
   }
 }
 
+// The same, four tokens per thread: one 4-byte token load, one 16-byte load of their uniforms,
+// the replacement ids read only for the tokens that mutate, one 4-byte store when any did
+// (total % 4 == 0, the population 4-byte and the uniforms 16-byte aligned).
+__global__ void __launch_bounds__(256) mutate4_kernel(
+    uint8_t* __restrict__ pop, int64_t total4, const float* __restrict__ rf,
+    const int64_t* __restrict__ ri, const int32_t* __restrict__ arities, int vocab,
+    const uint8_t* __restrict__ a0, int n0, const uint8_t* __restrict__ a1, int n1,
+    const uint8_t* __restrict__ a2, int n2, float rate, int pad) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total4;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t w = reinterpret_cast<const uint32_t*>(pop)[q];
+    const float4 f = __ldg(reinterpret_cast<const float4*>(rf) + q);
+    const float fr[4] = {f.x, f.y, f.z, f.w};
+    uint32_t nw = w;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int tok = (w >> (8 * k)) & 0xFFu;
+      if (tok == pad || !(fr[k] < rate)) continue;
+      const int ar = tok < vocab ? __ldg(arities + tok) : 0;
+      const uint64_t r = (uint64_t)__ldg(reinterpret_cast<const long long*>(ri) + 4 * q + k);
+      int nt = tok;
+      if (ar == 0 && n0 > 0) nt = a0[r % (uint64_t)n0];
+      else if (ar == 1 && n1 > 0) nt = a1[r % (uint64_t)n1];
+      else if (ar == 2 && n2 > 0) nt = a2[r % (uint64_t)n2];
+      nw = (nw & ~(0xFFu << (8 * k))) | ((uint32_t)nt << (8 * k));
+    }
+    if (nw != w) reinterpret_cast<uint32_t*>(pop)[q] = nw;
+  }
+}
+
 // crossover_splicing_kernel (rpn_kernels.cu:927-1016): child1 = p1[0:s1] + p2[s2:e2+1] +
 // p1[e1+1:], child2 symmetric; positions whose source index leaves [0, L) are PAD; pairs with a
 // false mask copy their parents.
@@ -95,6 +125,49 @@ __global__ void __launch_bounds__(256) splice_kernel(
     }
     c1[i] = splice_at(a, b, s1[n], e1[n], s2[n], e2[n], t, L, pad);
     c2[i] = splice_at(b, a, s2[n], e2[n], s1[n], e1[n], t, L, pad);
+  }
+}
+
+// The same with rows of L % 16 == 0 bytes (L <= 256, 16-byte aligned rows): a pair's two parent
+// rows are staged in shared memory by 16-byte loads (S = L / 16 threads per pair), each thread
+// builds one 16-byte segment of both children there and writes each with one 16-byte store.
+// 8 KB of shared memory per 256-thread block.
+__global__ void __launch_bounds__(256) splice16_kernel(
+    const uint8_t* __restrict__ p1, const uint8_t* __restrict__ p2, int64_t N, int64_t L,
+    const int64_t* __restrict__ s1, const int64_t* __restrict__ e1,
+    const int64_t* __restrict__ s2, const int64_t* __restrict__ e2,
+    const uint8_t* __restrict__ mask, uint8_t* __restrict__ c1, uint8_t* __restrict__ c2,
+    int pad) {
+  __shared__ __align__(16) uint8_t sm[256 * 2 * 16];  // [pairs][parent][L]
+  const int S = (int)(L >> 4);
+  const int P = (int)blockDim.x / S;  // pairs per block step
+  const int pr = (int)threadIdx.x / S, seg = (int)threadIdx.x - pr * S;
+  uint8_t* ra = sm + (size_t)pr * 2 * L;
+  uint8_t* rb = ra + L;
+  for (int64_t n0 = (int64_t)blockIdx.x * P; n0 < N; n0 += (int64_t)gridDim.x * P) {
+    const int64_t n = n0 + pr;
+    const bool act = pr < P && n < N;
+    if (act) {
+      reinterpret_cast<uint4*>(ra)[seg] = __ldg(reinterpret_cast<const uint4*>(p1 + n * L) + seg);
+      reinterpret_cast<uint4*>(rb)[seg] = __ldg(reinterpret_cast<const uint4*>(p2 + n * L) + seg);
+    }
+    __syncthreads();
+    if (act) {
+      const bool copy = mask && !mask[n];
+      const int64_t as = s1[n], ae = e1[n], bs = s2[n], be = e2[n];
+      uint32_t o1[4] = {0u, 0u, 0u, 0u}, o2[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const int64_t t = (int64_t)seg * 16 + k;
+        const uint32_t x1 = copy ? ra[t] : splice_at(ra, rb, as, ae, bs, be, t, L, pad);
+        const uint32_t x2 = copy ? rb[t] : splice_at(rb, ra, bs, be, as, ae, t, L, pad);
+        o1[k >> 2] |= x1 << (8 * (k & 3));
+        o2[k >> 2] |= x2 << (8 * (k & 3));
+      }
+      reinterpret_cast<uint4*>(c1 + n * L)[seg] = make_uint4(o1[0], o1[1], o1[2], o1[3]);
+      reinterpret_cast<uint4*>(c2 + n * L)[seg] = make_uint4(o2[0], o2[1], o2[2], o2[3]);
+    }
+    __syncthreads();
   }
 }
 
@@ -348,9 +421,15 @@ ws_status ws_mutate_population(uint8_t* population, int64_t B, int64_t L, const 
   if (!population || !rand_floats || !rand_ints || (vocab_size > 0 && !token_arities) ||
       (n0 > 0 && !arity0_ids) || (n1 > 0 && !arity1_ids) || (n2 > 0 && !arity2_ids))
     return fail("null tensor pointer");
-  mutate_kernel<<<grid_for(B * L, 256), 256, 0, (cudaStream_t)stream>>>(
-      population, B * L, rand_floats, rand_ints, token_arities, (int)vocab_size, arity0_ids,
-      (int)n0, arity1_ids, (int)n1, arity2_ids, (int)n2, mutation_rate, pad_id);
+  const int64_t total = B * L;
+  if (total % 4 == 0 && (uintptr_t)population % 4 == 0 && (uintptr_t)rand_floats % 16 == 0)
+    mutate4_kernel<<<grid_for(total / 4, 256), 256, 0, (cudaStream_t)stream>>>(
+        population, total / 4, rand_floats, rand_ints, token_arities, (int)vocab_size,
+        arity0_ids, (int)n0, arity1_ids, (int)n1, arity2_ids, (int)n2, mutation_rate, pad_id);
+  else
+    mutate_kernel<<<grid_for(total, 256), 256, 0, (cudaStream_t)stream>>>(
+        population, total, rand_floats, rand_ints, token_arities, (int)vocab_size, arity0_ids,
+        (int)n0, arity1_ids, (int)n1, arity2_ids, (int)n2, mutation_rate, pad_id);
   return launched("mutate_population launch");
 }
 
@@ -364,8 +443,18 @@ ws_status ws_crossover_splicing(const uint8_t* parent1, const uint8_t* parent2, 
   if (N * L == 0) return WS_OK;
   if (!parent1 || !parent2 || !starts1 || !ends1 || !starts2 || !ends2 || !child1 || !child2)
     return fail("null tensor pointer");
-  splice_kernel<<<grid_for(N * L, 256), 256, 0, (cudaStream_t)stream>>>(
-      parent1, parent2, N, L, starts1, ends1, starts2, ends2, cx_mask, child1, child2, pad_id);
+  const bool rows16 = L % 16 == 0 && L <= 256 &&
+                      (((uintptr_t)parent1 | (uintptr_t)parent2 | (uintptr_t)child1 |
+                        (uintptr_t)child2) % 16) == 0;
+  if (rows16) {
+    const int64_t per_block = 256 / (L / 16);
+    splice16_kernel<<<grid_for((N + per_block - 1) / per_block * 256, 256), 256, 0,
+                      (cudaStream_t)stream>>>(parent1, parent2, N, L, starts1, ends1, starts2,
+                                              ends2, cx_mask, child1, child2, pad_id);
+  } else {
+    splice_kernel<<<grid_for(N * L, 256), 256, 0, (cudaStream_t)stream>>>(
+        parent1, parent2, N, L, starts1, ends1, starts2, ends2, cx_mask, child1, child2, pad_id);
+  }
   return launched("crossover_splicing launch");
 }
 

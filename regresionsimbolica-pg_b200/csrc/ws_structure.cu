@@ -25,7 +25,7 @@ namespace {
 constexpr int kThreads = 128;  // one block = 128 programs
 constexpr int kStagedMaxBytes = 96 * 1024;
 
-// Reads one program row as a token stream: 4 bytes per load when the row allows it.
+// Reads one program row as a token stream: 16 or 4 bytes per load when the row allows it.
 template <typename Tok>
 struct RowReader;
 
@@ -34,9 +34,19 @@ struct RowReader<uint8_t> {
   const uint8_t* row;
   int64_t L;
   bool vec4;
+  bool vec16 = false;  // L % 16 == 0 and a 16-byte aligned row
   template <typename F>
   __device__ __forceinline__ void for_each(F&& f) const {
-    if (vec4) {
+    if (vec16) {
+      const uint4* w = reinterpret_cast<const uint4*>(row);
+      for (int64_t i0 = 0; i0 < L; i0 += 16) {
+        const uint4 v = __ldg(w + (i0 >> 4));
+        const uint32_t q[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+          if (!f(i0 + k, (int64_t)((q[k >> 2] >> (8 * (k & 3))) & 0xFFu))) return;
+      }
+    } else if (vec4) {
       const uint32_t* w = reinterpret_cast<const uint32_t*>(row);
       for (int64_t i0 = 0; i0 < L; i0 += 4) {
         uint32_t v = __ldg(w + (i0 >> 2));
@@ -76,30 +86,36 @@ __device__ __forceinline__ int32_t arity_clamped(const int32_t* ar, int64_t n_ar
 // Validation.  mode 0: validate_rpn_batch_kernel; 1: operators.py torch fallback (arity looked
 // up with the token clamped into the table); 2: gpu_simplifier._validate_batch_stack (no
 // contiguity rule, minimum over every position, at least one non-PAD token).
+// uint8 tokens: the arity of every byte value is staged in shared memory once per block (the
+// rule's lookup: mode 0 zero outside the table, modes 1-2 the clamped entry) and rows are read
+// 16 bytes per load when their length and address allow.
 template <typename Tok>
 __global__ void __launch_bounds__(kThreads)
     validate_kernel(const Tok* __restrict__ pop, int64_t B, int64_t L,
                     const int32_t* __restrict__ ar, int64_t n_ar, int64_t pad, int mode,
-                    bool vec4, uint8_t* __restrict__ out) {
+                    bool vec4, bool vec16, uint8_t* __restrict__ out) {
+  constexpr bool U8 = sizeof(Tok) == 1;
+  __shared__ int32_t s_ar[U8 ? 256 : 1];
+  if (U8) {
+    for (int t = threadIdx.x; t < 256; t += blockDim.x)
+      s_ar[t] = mode == 0 ? arity_of(ar, n_ar, t) : arity_clamped(ar, n_ar, t);
+    __syncthreads();
+  }
+  auto arity = [&](int64_t t) -> int64_t {
+    if (U8) return s_ar[t];
+    return mode == 0 ? arity_of(ar, n_ar, t) : arity_clamped(ar, n_ar, t);
+  };
   for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < B;
        b += (int64_t)gridDim.x * blockDim.x) {
     RowReader<Tok> rd{pop + b * L, L, vec4};
+    if constexpr (U8) rd.vec16 = vec16;
     int64_t stack = 0;
     bool ok = true, pad_seen = false, has_tok = false;
-    if (mode == 0) {
+    if (mode != 2) {
       rd.for_each([&](int64_t, int64_t t) {
         if (t == pad) { pad_seen = true; return true; }
         if (pad_seen) { ok = false; return false; }
-        stack += 1 - (int64_t)arity_of(ar, n_ar, t);
-        if (stack < 1) { ok = false; return false; }
-        return true;
-      });
-      ok = ok && stack == 1;
-    } else if (mode == 1) {
-      rd.for_each([&](int64_t, int64_t t) {
-        if (t == pad) { pad_seen = true; return true; }
-        if (pad_seen) { ok = false; return false; }
-        stack += 1 - (int64_t)arity_clamped(ar, n_ar, t);
+        stack += 1 - arity(t);
         if (stack < 1) { ok = false; return false; }
         return true;
       });
@@ -108,7 +124,7 @@ __global__ void __launch_bounds__(kThreads)
       rd.for_each([&](int64_t, int64_t t) {
         if (t != pad) {
           has_tok = true;
-          stack += 1 - (int64_t)arity_clamped(ar, n_ar, t);
+          stack += 1 - arity(t);
         }
         if (stack < 1) { ok = false; return false; }
         return true;
@@ -485,13 +501,14 @@ extern "C" ws_status ws_validate_rpn_batch(const void* population, int32_t token
   const int grid = grid_for(B, kThreads, 16);
   if (token_bytes == 1) {
     const bool vec4 = (L % 4 == 0) && ((uintptr_t)population % 4 == 0);
+    const bool vec16 = (L % 16 == 0) && ((uintptr_t)population % 16 == 0);
     validate_kernel<uint8_t><<<grid, kThreads, 0, s>>>(static_cast<const uint8_t*>(population),
                                                        B, L, token_arities, n_arities, pad_id,
-                                                       mode, vec4, out_valid);
+                                                       mode, vec4, vec16, out_valid);
   } else {
     validate_kernel<int64_t><<<grid, kThreads, 0, s>>>(static_cast<const int64_t*>(population),
                                                        B, L, token_arities, n_arities, pad_id,
-                                                       mode, false, out_valid);
+                                                       mode, false, false, out_valid);
   }
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? WS_OK : fail_cuda(e, "validate_rpn_batch");
