@@ -9,22 +9,21 @@
 // Per-row arithmetic follows the reference expression by expression, including its mixed
 // float/double promotions, so per-row adjoints are the reference's bit for bit.
 //
-// B200 layout: one block owns one program for a range of rows.  The program is parsed once per
-// block into a shared-memory tape of its OPERATORS only, each naming its operands (an earlier
-// operator, a variable, a literal or a constant slot) and whether its value reaches the root;
-// terminals are read where they are used.  Every thread evaluates rows: operator values and
-// adjoints live in shared memory as [operator][thread] (all lanes touch the same operator at the
-// same time: conflict-free).  The program is a tree, so each node receives exactly one adjoint
-// contribution: a child's slot is written with the value the reference's `+=` leaves in it
-// (`0 + contribution`, or 0 where the reference adds nothing), and constant adjoints go straight
-// into per-thread FP64 accumulators.  The reduction over rows is a fixed-order block
-// sum, written without atomics when one block covers all rows of a program; only programs
-// split across blocks use one atomic per (block, slot) -- the reference issues one atomic per
-// (row, constant node).
-//
-// The loss-and-gradient of constant fitting (ws_loss_grad, the batched L-BFGS) runs its own
-// kernel, loss_kernel below, on the same parse rules: derivatives stored by the forward sweep,
-// an operator-independent reverse sweep, programs grouped by tape size.
+// B200 layout: one block owns one program for a range of rows.  Thread 0 parses the program once
+// per block (parse_loss_program) into a shared-memory tape whose operands are resolved to
+// addresses: operators, constant leaves and the program's distinct variables own [thread][R]
+// slots, constants and literals sit in a broadcast scalar table, so neither sweep branches on an
+// operand's kind.  The program is a tree, so the only reader of a value is its parent, which
+// reads it before writing the adjoint into the same slot.  Two kernels share this tape:
+//   ref_kernel  (ws_eval_rpn_backward): values forward, the reference's adjoint expressions
+//               backward (the operator's rule, from the operand values), constant-leaf rows
+//               summed in FP64 in the order the reference's reverse walk meets them; a
+//               fixed-order block sum writes grad_constants without atomics when one block covers
+//               all rows of a program, one atomic per (block, slot) otherwise -- the reference
+//               issues one atomic per (row, constant node);
+//   loss_kernel (ws_loss_grad, the batched L-BFGS): the forward sweep also stores each operand's
+//               local derivative in the operand's slot, so the reverse sweep is the same multiply
+//               for every operator; programs are grouped by tape size, one launch per group.
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
@@ -52,21 +51,6 @@ struct BwdLut {
 // Operand kinds of a tape operator.
 enum : uint8_t { OPD_OP = 0, OPD_VAR, OPD_LIT, OPD_CONST };
 
-struct BOp {
-  uint8_t fop, bop;   // forward and adjoint operator codes
-  uint8_t ka, kb;     // operand kinds (kb unused for unary operators)
-  uint16_t a, b;      // operand: operator index, variable, literal index (10 = 1.0), constant slot
-  uint8_t binary, reach;  // reach: the value flows into the root
-  uint16_t pad;
-};
-
-struct BRoot {
-  int n_ops;          // operators in the tape (0: the program is one terminal)
-  uint8_t kind;       // root operand kind (OPD_OP: the last operator)
-  uint16_t idx;
-  int valid;          // the reference's forward pass yields a root (final depth 1)
-};
-
 constexpr int kMaxL = 256;
 
 __host__ __device__ constexpr size_t al16(size_t v) { return (v + 15) / 16 * 16; }
@@ -88,8 +72,7 @@ struct BwdParams {
   // each (program, row range) item writes its partial sums (no atomics, fixed order)
   const T* y;
   const int32_t* active;  // optional: programs with 0 are skipped
-  int64_t V;              // variables; with stage_x each thread copies its rows of x to shared
-  int stage_x;            // memory once per row group
+  int64_t V;              // variables
   int tape_ops;           // tape slots (>= every program's operators; loss_kernel: operators,
                           // constant leaves and staged variables)
   const int32_t* list;        // optional: the programs of this launch (a bucket) ...
@@ -97,97 +80,6 @@ struct BwdParams {
   double* part_loss;      // [n_items]   sum over the item's rows of (pred - y)^2
   double* part_grad;      // [n_items, K] sum over the item's rows of the constant adjoints
 };
-
-// Walks program b as the reference's forward loop does (backward_kernels.cu:84-195): PAD ends
-// it, an operator that finds too few operands ends it (the prefix is the program), pushes beyond
-// depth 32 are dropped, C takes slot min(c_idx, K-1) (1.0 without constants).  Operands are kept
-// on the stack as (kind, index) pairs, so terminals never enter the tape.
-__device__ BRoot parse_program(const uint8_t* __restrict__ prog, int64_t L, int64_t K,
-                               const uint8_t* s_tab, BOp* ops, int cap, int64_t V) {
-  const uint8_t* t_kind = s_tab;
-  const uint8_t* t_fop = s_tab + 256;
-  const uint8_t* t_bop = s_tab + 512;
-  const uint8_t* t_arg = s_tab + 768;
-  uint8_t sk[kStack];
-  uint16_t si[kStack];
-  int sp = 0, n_ops = 0;
-  int64_t c_idx = 0;
-  bool bad = false;  // an array bound was hit (bounds-checked build only)
-  for (int pc = 0; pc < (int)L; ++pc) {
-    const int tok = prog[pc];
-    const uint8_t kind = t_kind[tok];
-    if (kind == BK_PAD) break;
-    if (kind == BK_VAR || kind == BK_LIT || kind == BK_CONST) {
-      uint8_t k = kind == BK_VAR ? OPD_VAR : OPD_LIT;
-      uint16_t ix = t_arg[tok];
-      if (kind == BK_VAR && !WS_BC(ix < V, BC_ADJ_OPERAND, ix)) {
-        bad = true;
-        break;
-      }
-      if (kind == BK_CONST) {
-        if (K > 0) {
-          k = OPD_CONST;
-          ix = (uint16_t)(c_idx < K ? c_idx : K - 1);
-          c_idx++;
-        } else {
-          ix = 10;  // C without constants pushes 1.0 and takes no gradient
-        }
-      }
-      if (sp < kStack) {
-        sk[sp] = k;
-        si[sp] = ix;
-        ++sp;
-      }
-      continue;
-    }
-    BOp o;
-    o.fop = t_fop[tok];
-    o.bop = t_bop[tok];
-    o.reach = 0;
-    o.pad = 0;
-    o.kb = OPD_LIT;
-    o.b = 0;
-    if (kind == BK_BIN) {
-      if (sp < 2) break;
-      --sp;
-      o.kb = sk[sp];
-      o.b = si[sp];
-      --sp;
-      o.ka = sk[sp];
-      o.a = si[sp];
-      o.binary = 1;
-    } else {
-      if (sp < 1) break;
-      --sp;
-      o.ka = sk[sp];
-      o.a = si[sp];
-      o.binary = 0;
-    }
-    if (!WS_BC(n_ops < cap, BC_ADJ_PARSE, n_ops)) {
-      bad = true;
-      break;
-    }
-    ops[n_ops] = o;
-    sk[sp] = OPD_OP;  // an operator always finds room: it just freed one or two slots
-    si[sp] = (uint16_t)n_ops;
-    ++sp;
-    ++n_ops;
-  }
-  BRoot r;
-  r.n_ops = n_ops;
-  r.valid = (sp == 1 && !bad) ? 1 : 0;
-  r.kind = sp >= 1 ? sk[0] : OPD_LIT;
-  r.idx = sp >= 1 ? si[0] : 0;
-  if (r.valid && r.kind == OPD_OP) {  // mark the operators whose value reaches the root
-    ops[r.idx].reach = 1;
-    for (int o = r.idx; o >= 0; --o) {
-      if (!ops[o].reach) continue;
-      if (ops[o].ka == OPD_OP) ops[ops[o].a].reach = 1;
-      if (ops[o].binary && ops[o].kb == OPD_OP) ops[ops[o].b].reach = 1;
-    }
-  }
-  return r;
-}
 
 // ---- forward values (backward_kernels.cu:146-188) ------------------------------------------
 template <typename T>
@@ -244,22 +136,11 @@ __device__ __forceinline__ void acc_t(T& dst, T coef, T adj) {
   dst = fma(coef, adj, dst);
 }
 
-// ---- the adjoint kernel ---------------------------------------------------------------------
-// One block owns one program for a range of rows; every thread carries R consecutive rows
-// through each tape step, so one decode of an operator (a broadcast shared-memory load and a
-// block-uniform branch) serves R rows, and the R rows' arithmetic is independent work for the
-// pipelines.  One tape slot per operator and thread ([op][thread][R] values, vector loads and
-// stores) holds the operator's values after the forward sweep and its adjoints during the reverse
-// sweep: the program is a tree, so the only reader of a value is the operator's parent, which
-// reads it before it writes the adjoint into the same slot; exp and pow, whose adjoint rules use
-// their own output, recompute it from their operands bit for bit.  The previous operator's values
-// and the adjoint handed to it stay in registers (BOp::pad bit 0 / bit 1: the left / right operand
-// is operator o-1), and constant adjoints are summed in registers when K <= kRegSlots (the slot of
-// a delivery is the same for the whole block, so the register is chosen by a uniform switch).
-//
-// The root adjoint of row d is grad_output[b, d] and every per-row expression is the reference's,
-// double promotions included (acc_d / acc_t), so per-row adjoints are bit-identical to the
-// reference's; per-row constant adjoints are summed in FP64; zero adjoints hand on nothing.
+// ---- helpers of the adjoint kernels ---------------------------------------------------------
+// Every thread carries R consecutive rows through each tape step, so one decode of an operator
+// serves R rows; a tape slot holds [thread][R] values (16-byte vector accesses).  Constant
+// adjoints are summed in registers when K <= kRegSlots (the slot of a delivery is the same for
+// the whole block, so the register is chosen by a uniform switch).
 constexpr int kRegSlots = 8;
 
 template <typename T, int R>
@@ -300,39 +181,6 @@ __device__ __forceinline__ void st_vec(T* p, const T (&v)[R]) {
   }
 }
 
-// The R values of one operand: an earlier operator's (tape), a variable's (rows past d_end read
-// as 0), a constant's or a literal's.
-template <typename T, int R>
-__device__ __forceinline__ void operand_vec(uint8_t k, uint16_t i, const T* tape, int TS, int tid,
-                                            const T* x, int64_t D, int64_t d0, int64_t d_end,
-                                            const T* s_lit, const T* cst, const T* xs,
-                                            T (&o)[R]) {
-  switch (k) {
-    case OPD_OP: ld_vec<T, R>(tape + ((size_t)i * TS + tid) * R, o); break;
-    case OPD_VAR: {
-      if (xs) {  // this thread's rows, staged at the start of the row group
-        ld_vec<T, R>(xs + ((size_t)i * TS + tid) * R, o);
-        break;
-      }
-      const T* xr = x + (int64_t)i * D;
-#pragma unroll
-      for (int r = 0; r < R; ++r) o[r] = d0 + r < d_end ? xr[d0 + r] : (T)0;
-      break;
-    }
-    case OPD_CONST: {
-      const T c = cst[i];
-#pragma unroll
-      for (int r = 0; r < R; ++r) o[r] = c;
-      break;
-    }
-    default: {
-      const T c = i < 10 ? s_lit[i] : (T)1.0;
-#pragma unroll
-      for (int r = 0; r < R; ++r) o[r] = c;
-    }
-  }
-}
-
 #define WS_FOR_R for (int r = 0; r < R; ++r)
 
 template <typename T, int R>
@@ -367,246 +215,6 @@ __device__ __forceinline__ void creg_add(T (&cr)[kRegSlots], int i, T c) {
     case 5: cr[5] += c; break;
     case 6: cr[6] += c; break;
     default: cr[7] += c; break;
-  }
-}
-
-template <typename T, int R, bool KREG>
-__device__ __forceinline__ void deliver_vec(uint8_t k, uint16_t i, const T (&c)[R], bool to_carry,
-                                            T (&carry)[R], bool& have, T* tape, int TS, int tid,
-                                            double (&cr)[kRegSlots], double* cacc, int* touched) {
-  if (k == OPD_OP) {
-    if (to_carry) {
-      WS_FOR_R carry[r] = c[r];
-      have = true;
-    } else {
-      st_vec<T, R>(tape + ((size_t)i * TS + tid) * R, c);
-    }
-  } else if (k == OPD_CONST) {
-    double s = 0.0;
-    bool any = false;
-    WS_FOR_R {
-      if (c[r] != (T)0) {
-        s += (double)c[r];
-        any = true;
-      }
-    }
-    if (any) {
-      if (KREG) creg_add<double>(cr, i, s);
-      else cacc[(size_t)i * TS + tid] += s;
-      touched[i] = 1;
-    }
-  }
-}
-
-template <typename T, int R, bool KREG>
-__global__ void __launch_bounds__(128) adj_kernel(BwdParams<T> p, BwdLut lut) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int TS = p.tape_stride;
-  // shared memory: operators | touched flags | (K > kRegSlots) FP64 constant accumulators |
-  // work: the tape and staged x during the rows, the block reduction after them
-  BOp* ops = reinterpret_cast<BOp*>(smem);
-  int* touched = reinterpret_cast<int*>(smem + al16((size_t)p.tape_ops * sizeof(BOp)));
-  double* cacc = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(touched) +
-                                           al16((size_t)p.K * sizeof(int)));
-  unsigned char* work = reinterpret_cast<unsigned char*>(cacc + (KREG ? 0 : (size_t)p.K * TS));
-  T* tape = reinterpret_cast<T*>(work);
-  T* xs = p.stage_x ? tape + (size_t)p.tape_ops * TS * R : nullptr;  // [V][thread][R]
-  __shared__ BRoot s_root;
-  __shared__ int64_t s_prog;
-  __shared__ T s_lit[10];
-  __shared__ uint8_t s_tab[1024];  // kind, forward op, adjoint op, argument per token byte
-  for (int t = threadIdx.x; t < 256; t += blockDim.x) {
-    s_tab[t] = lut.kind[t];
-    s_tab[256 + t] = lut.fop[t];
-    s_tab[512 + t] = lut.bop[t];
-    s_tab[768 + t] = lut.arg[t];
-  }
-  if (threadIdx.x < 10) s_lit[threadIdx.x] = (T)lut.lit[threadIdx.x];
-  if (threadIdx.x == 0) s_prog = -1;
-  const int tid = threadIdx.x;
-
-  const int64_t n_items = p.list ? (int64_t)(*p.list_count) * p.n_splits : p.n_items;
-  for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
-    const int64_t li = item / p.n_splits;
-    const int64_t split = item - li * p.n_splits;
-    const int64_t b = p.list ? (int64_t)p.list[li] : li;
-    __syncthreads();
-    if (tid == 0 && s_prog != b) {
-      BRoot rt0 = parse_program(p.pop + b * p.L, p.L, p.K, s_tab, ops, p.tape_ops, p.V);
-      for (int o = 0; o < rt0.n_ops; ++o) {
-        uint16_t f = 0;
-        if (ops[o].ka == OPD_OP && (int)ops[o].a == o - 1) f |= 1;
-        if (ops[o].binary && ops[o].kb == OPD_OP && (int)ops[o].b == o - 1) f |= 2;
-        ops[o].pad = f;
-      }
-      s_root = rt0;
-      s_prog = b;
-    }
-    for (int64_t k = tid; k < p.K; k += blockDim.x) touched[k] = 0;
-    if (!KREG)
-      for (int64_t k = 0; k < p.K; ++k) cacc[k * TS + tid] = 0.0;
-    __syncthreads();
-    const BRoot rt = s_root;
-    if (!rt.valid) continue;
-    const int64_t d_begin = split * p.rows_per_split;
-    int64_t d_end = d_begin + p.rows_per_split;
-    if (d_end > p.D) d_end = p.D;
-    const T* xcol = p.x;
-    const T* cst = p.consts + b * p.K;
-    const int n = rt.n_ops;
-    double cr[kRegSlots];
-#pragma unroll
-    for (int k = 0; k < kRegSlots; ++k) cr[k] = 0.0;
-
-    for (int64_t d0 = d_begin + (int64_t)tid * R; d0 < d_end; d0 += (int64_t)TS * R) {
-      // this thread's rows: x staged (only this thread reads them: no barrier), the root
-      // adjoints loaded now so that their latency overlaps the forward sweep
-      if (xs) {
-        for (int64_t v = 0; v < p.V; ++v) {
-          const T* xr = xcol + v * p.D;
-          T xv[R];
-          WS_FOR_R xv[r] = d0 + r < d_end ? xr[d0 + r] : (T)0;
-          st_vec<T, R>(xs + ((size_t)v * TS + tid) * R, xv);
-        }
-      }
-      T g_root[R];  // grad_output of the R rows
-      WS_FOR_R g_root[r] = d0 + r < d_end ? p.gout[b * p.D + d0 + r] : (T)0;
-      // forward: operator values
-      T last[R];
-      WS_FOR_R last[r] = (T)0;
-      for (int o = 0; o < n; ++o) {
-        const BOp op = ops[o];
-        T va[R], v[R];
-        if (op.pad & 1) {
-          WS_FOR_R va[r] = last[r];
-        } else {
-          operand_vec<T, R>(op.ka, op.a, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs, va);
-        }
-        if (op.binary) {
-          T vb[R];
-          if (op.pad & 2) {
-            WS_FOR_R vb[r] = last[r];
-          } else {
-            operand_vec<T, R>(op.kb, op.b, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs, vb);
-          }
-          fwd_binary_vec<T, R>(op.fop, va, vb, v);
-        } else {
-          fwd_unary_vec<T, R>(op.fop, va, v);
-        }
-        st_vec<T, R>(tape + ((size_t)o * TS + tid) * R, v);
-        WS_FOR_R last[r] = v[r];
-      }
-      T carry[R];
-      bool have = false;
-      if (rt.kind != OPD_OP) {  // a one-terminal program
-        deliver_vec<T, R, KREG>(rt.kind, rt.idx, g_root, false, carry, have, tape, TS, tid,
-                                      cr, cacc, touched);
-        continue;
-      }
-      if ((int)rt.idx == n - 1) {
-        WS_FOR_R carry[r] = g_root[r];
-        have = true;
-      } else {
-        st_vec<T, R>(tape + ((size_t)rt.idx * TS + tid) * R, g_root);
-      }
-      // reverse: each operator hands its adjoint to its operands
-      for (int o = n - 1; o >= 0; --o) {
-        const BOp op = ops[o];
-        if (!op.reach) {
-          have = false;
-          continue;
-        }
-        T g[R];
-        if (have) {
-          WS_FOR_R g[r] = carry[r];
-        } else {
-          ld_vec<T, R>(tape + ((size_t)o * TS + tid) * R, g);
-        }
-        have = false;
-        // the rules of + - and neg use no operand value, those of the unary operators only the
-        // left one: the other loads are skipped
-        T lv[R], ca[R], cb[R];
-        const bool need_l = op.bop != BO_ADD && op.bop != BO_SUB && op.bop != BO_NEG;
-        const bool need_r = op.bop == BO_MUL || op.bop == BO_DIV || op.bop == BO_POW;
-        if (need_l) {
-          operand_vec<T, R>(op.ka, op.a, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs, lv);
-        } else {
-          WS_FOR_R lv[r] = (T)0;
-        }
-        WS_FOR_R { ca[r] = (T)0; cb[r] = (T)0; }
-        if (op.binary) {
-          T rv[R];
-          if (need_r) {
-            operand_vec<T, R>(op.kb, op.b, tape, TS, tid, xcol, p.D, d0, d_end, s_lit, cst, xs,
-                              rv);
-          } else {
-            WS_FOR_R rv[r] = (T)0;
-          }
-          switch (op.bop) {
-            case BO_ADD: WS_FOR_R { ca[r] += g[r]; cb[r] += g[r]; } break;
-            case BO_SUB: WS_FOR_R { ca[r] += g[r]; cb[r] -= g[r]; } break;
-            case BO_MUL: WS_FOR_R { acc_t(ca[r], rv[r], g[r]); acc_t(cb[r], lv[r], g[r]); } break;
-            case BO_DIV:
-              WS_FOR_R {
-                if (fabs(rv[r]) >= (T)1e-9) {
-                  acc_d(ca[r], 1.0 / rv[r], g[r]);
-                  acc_t(cb[r], -(lv[r] / (rv[r] * rv[r])), g[r]);
-                }
-              }
-              break;
-            case BO_POW:
-              WS_FOR_R {
-                if (lv[r] > 0) {
-                  const T out_val = fwd_binary<T>(op.fop, lv[r], rv[r]);
-                  acc_d(ca[r], (double)rv[r] * pow((double)lv[r], (double)rv[r] - 1.0), g[r]);
-                  acc_t(cb[r], out_val * log(lv[r]), g[r]);
-                }
-              }
-              break;
-            default: break;
-          }
-          WS_FOR_R if (g[r] == (T)0) cb[r] = (T)0;
-          // the right operand sits later in the program: its constants first, as the
-          // reference's reverse walk meets them
-          deliver_vec<T, R, KREG>(op.kb, op.b, cb, (op.pad & 2) != 0, carry, have, tape, TS,
-                                        tid, cr, cacc, touched);
-        } else {
-          switch (op.bop) {
-            case BO_SIN: WS_FOR_R acc_t(ca[r], cos(lv[r]), g[r]); break;
-            case BO_COS: WS_FOR_R acc_t(ca[r], -sin(lv[r]), g[r]); break;
-            case BO_LOG:
-              WS_FOR_R if (fabs(lv[r]) > (T)1e-9) acc_d(ca[r], 1.0 / lv[r], g[r]);
-              break;
-            case BO_EXP: WS_FOR_R acc_t(ca[r], fwd_unary<T>(op.fop, lv[r]), g[r]); break;
-            case BO_SQRT:
-              WS_FOR_R if (lv[r] > (T)1e-9) acc_d(ca[r], 0.5 / sqrt(lv[r]), g[r]);
-              break;
-            case BO_NEG: WS_FOR_R ca[r] += -g[r]; break;
-            default: break;
-          }
-        }
-        WS_FOR_R if (g[r] == (T)0) ca[r] = (T)0;
-        deliver_vec<T, R, KREG>(op.ka, op.a, ca, (op.pad & 1) != 0, carry, have, tape, TS,
-                                      tid, cr, cacc, touched);
-      }
-    }
-    __syncthreads();  // the tape is free: the reduction reuses its memory
-    double* cred = KREG ? reinterpret_cast<double*>(work) : cacc;
-    if (KREG) {
-#pragma unroll
-      for (int k = 0; k < kRegSlots; ++k)
-        if (k < p.K) cred[(size_t)k * TS + tid] = cr[k];
-    }
-    __syncthreads();
-    // fixed-order reduction over the block's threads, one thread per slot
-    for (int64_t k = tid; k < p.K; k += blockDim.x) {
-      if (!touched[k]) continue;
-      double s = 0.0;
-      for (int t = 0; t < (int)blockDim.x; ++t) s += cred[k * TS + t];
-      T* dst = p.grad + b * p.K + k;
-      if (p.n_splits == 1) *dst = *dst + (T)s;
-      else atomicAdd(dst, (T)s);
-    }
   }
 }
 
@@ -653,21 +261,25 @@ struct __align__(16) LOp {
 };
 
 // Shared memory of a loss-mode block (bytes): operators | staged-variable list | constant-leaf
-// list | scalar table (one 16-byte entry per terminal token at most) | (K > kRegSlots) FP64
+// slots and list | scalar table (one 16-byte entry per terminal token at most) | (K > kRegSlots) FP64
 // constant accumulators | work: the tape (M slots and the sink) during the rows, the block
 // reduction after them.
 struct LossLayout {
-  size_t ops, stage, leaf, scal, cacc, work, bytes;
+  size_t ops, stage, leaf, scal, touched, cacc, work, bytes;
 };
 
+// `touched`: room for the per-constant "received a contribution" flags (the reference-mode
+// kernel writes only those slots).
 __host__ __device__ inline LossLayout loss_layout(int64_t M, int64_t L, int64_t K, int threads,
-                                                  size_t vec_bytes, bool kreg) {
+                                                  size_t vec_bytes, bool kreg,
+                                                  bool touched = false) {
   LossLayout l;
   l.ops = 0;
   l.stage = al16((size_t)M * sizeof(LOp));
   l.leaf = l.stage + al16((size_t)M);
-  l.scal = l.leaf + al16((size_t)M * sizeof(uint32_t));
-  l.cacc = l.scal + (size_t)L * 16;
+  l.scal = l.leaf + al16((size_t)2 * M * sizeof(uint32_t));
+  l.touched = l.scal + (size_t)L * 16;
+  l.cacc = l.touched + (touched ? al16((size_t)K * sizeof(int)) : 0);
   l.work = l.cacc + (kreg ? 0 : (size_t)K * threads * sizeof(double));
   const size_t tape = (size_t)(M + 1) * threads * vec_bytes;
   const size_t red = (size_t)((kreg ? K : 0) + 1) * threads * sizeof(double);
@@ -704,8 +316,9 @@ struct LossAddr {
 // operand into an address: operators take slots 0..n_ops-1, constant leaves the next slots, each
 // distinct variable the slots after them (x staged there once per row group); constants and
 // literals take scalar-table entries, filled here.  Slots in use <= operators + constant tokens +
-// distinct variables <= tokens.  `leaf` receives (address | constant slot << 16) of the constant
-// leaves whose parent reaches the root.
+// distinct variables <= tokens.  leaf[0, M) holds each constant leaf's constant slot, leaf[M, 2M)
+// receives (address | constant slot << 16) of the leaves whose parent reaches the root, in the
+// order a reverse walk meets them.
 template <typename T, int R>
 __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t L, int64_t K,
                                        const uint8_t* s_tab, const T* s_lit,
@@ -732,7 +345,7 @@ __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t
     if (kind == BK_VAR || kind == BK_LIT || kind == BK_CONST) {
       uint8_t k = kind == BK_VAR ? OPD_VAR : OPD_LIT;
       uint16_t ix = t_arg[tok], c = 0;
-      if (kind == BK_VAR && !WS_BC(ix < V, BC_LOSS_PARSE, ix)) {
+      if (kind == BK_VAR && !WS_BC(ix < V, BC_ADJ_PARSE, ix)) {
         bad = true;
         break;
       }
@@ -751,7 +364,7 @@ __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t
           int j = 0;
           while (j < n_stage && stage[j] != ix) ++j;
           if (j == n_stage) {
-            if (!WS_BC(n_stage < M, BC_LOSS_PARSE, n_stage)) {
+            if (!WS_BC(n_stage < M, BC_ADJ_PARSE, n_stage)) {
               bad = true;
               break;
             }
@@ -759,7 +372,7 @@ __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t
           }
           ix = (uint16_t)j;
         } else {
-          if (!WS_BC(n_scal < (int)L && (k != OPD_CONST || n_leaf < M), BC_LOSS_PARSE, n_scal)) {
+          if (!WS_BC(n_scal < (int)L && (k != OPD_CONST || n_leaf < M), BC_ADJ_PARSE, n_scal)) {
             bad = true;
             break;
           }
@@ -810,7 +423,7 @@ __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t
         o.flags |= (uint8_t)(fl << 1);  // the B flags are the A flags shifted by one
       }
     }
-    if (!WS_BC(n_ops < M, BC_LOSS_PARSE, n_ops)) {
+    if (!WS_BC(n_ops < M, BC_ADJ_PARSE, n_ops)) {
       bad = true;
       break;
     }
@@ -820,7 +433,7 @@ __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t
     ++sp;
     ++n_ops;
   }
-  if (!WS_BC(n_ops + n_leaf + n_stage <= M, BC_LOSS_PARSE, n_ops + n_leaf + n_stage)) bad = true;
+  if (!WS_BC(n_ops + n_leaf + n_stage <= M, BC_ADJ_PARSE, n_ops + n_leaf + n_stage)) bad = true;
   const uint32_t stage_first = (uint32_t)(n_ops + n_leaf);
   const uint16_t sink = (uint16_t)(ad.tape + ad.sink * ad.slot);
   LRoot<T> r;
@@ -841,6 +454,8 @@ __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t
     if (r.kind == OPD_CONST) r.ck = (uint16_t)leaf[sl[0]];
   }
   constexpr uint8_t kOpA = LF_A_VEC | LF_A_GRAD, kOpB = LF_B_VEC | LF_B_GRAD;
+  uint32_t* live = leaf + M;
+  int n_live = 0;
   if (r.valid && r.kind == OPD_OP) {  // mark the operators whose value reaches the root
     ops[si[0]].flags |= LF_REACH;
     for (int o = si[0]; o >= 0; --o) {
@@ -848,8 +463,12 @@ __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t
       if (!(q.flags & LF_REACH)) continue;
       if ((q.flags & kOpA) == kOpA) ops[q.a].flags |= LF_REACH;
       if ((q.flags & kOpB) == kOpB) ops[q.b].flags |= LF_REACH;
-      if ((q.flags & kOpA) == LF_A_GRAD) leaf[q.fa] |= 0x80000000u;  // a live constant leaf
-      if ((q.flags & kOpB) == LF_B_GRAD) leaf[q.fb] |= 0x80000000u;
+      // the constant leaves of the operators that reach, in the order a reverse walk meets
+      // them (operators from the last, the right operand first): (slot | constant slot << 16)
+      if ((q.flags & kOpB) == LF_B_GRAD)
+        live[n_live++] = (ad.tape + (uint32_t)(n_ops + q.fb) * ad.slot) | (leaf[q.fb] << 16);
+      if ((q.flags & kOpA) == LF_A_GRAD)
+        live[n_live++] = (ad.tape + (uint32_t)(n_ops + q.fa) * ad.slot) | (leaf[q.fa] << 16);
     }
   }
   for (int o = 0; o < n_ops; ++o) {  // indices to addresses
@@ -877,10 +496,6 @@ __device__ LRoot<T> parse_loss_program(const uint8_t* __restrict__ prog, int64_t
     }
     q.self = (uint16_t)(ad.tape + o * ad.slot);
   }
-  int n_live = 0;
-  for (int i = 0; i < n_leaf; ++i)
-    if (leaf[i] & 0x80000000u)
-      leaf[n_live++] = (ad.tape + (uint32_t)(n_ops + i) * ad.slot) | ((leaf[i] & 0xFFFFu) << 16);
   r.n_leaf = n_live;
   return r;
 }
@@ -1095,7 +710,7 @@ __global__ void __launch_bounds__(128) loss_kernel(BwdParams<T> p, BwdLut lut) {
       }
       // the constant leaves' adjoints into their constants' accumulators
       for (int j = 0; j < rt.n_leaf; ++j) {
-        const uint32_t e = leaf[j];
+        const uint32_t e = leaf[M + j];
         T c[R];
         ld_vec<T, R>(WS_AT(e & 0xFFFFu, true), c);
         T s = (T)0;
@@ -1125,6 +740,197 @@ __global__ void __launch_bounds__(128) loss_kernel(BwdParams<T> p, BwdLut lut) {
       double s = 0.0;
       for (int t = 0; t < (int)blockDim.x; ++t) s += lacc_s[t];
       p.part_loss[slot] = s;
+    }
+  }
+}
+
+// ---- reference mode on the resolved tape (ws_eval_rpn_backward) ------------------------------
+// The program parsed as for the loss mode (operands as shared-memory addresses, constant leaves
+// with their own slots), but the forward sweep stores values only: the reverse sweep evaluates
+// the reference's own adjoint expressions (backward_kernels.cu:222-278, double promotions
+// included: acc_d / acc_t) from the operand values, which sit in the operands' slots until the
+// operator writes their adjoints there.  A constant leaf's contribution goes to its slot and an
+// epilogue adds the leaves' rows to their constants' FP64 accumulators in the order the reverse
+// walk met them, so every per-row term and every sum is the one of the direct formulation.
+template <typename T, int R, bool KREG>
+__global__ void __launch_bounds__(128) ref_kernel(BwdParams<T> p, BwdLut lut) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int TS = p.tape_stride;
+  const int M = p.tape_ops;
+  const LossLayout lay = loss_layout(M, p.L, p.K, TS, R * sizeof(T), KREG, true);
+  LOp* ops = reinterpret_cast<LOp*>(smem + lay.ops);
+  uint8_t* stage = smem + lay.stage;
+  uint32_t* leaf = reinterpret_cast<uint32_t*>(smem + lay.leaf);
+  int* touched = reinterpret_cast<int*>(smem + lay.touched);
+  double* cacc = reinterpret_cast<double*>(smem + lay.cacc);
+  unsigned char* work = smem + lay.work;
+  LossAddr ad;
+  ad.tape = (uint32_t)(lay.work >> 4);
+  ad.slot = (uint32_t)((size_t)TS * R * sizeof(T) >> 4);
+  ad.scal = (uint32_t)(lay.scal >> 4);
+  ad.sink = (uint32_t)M;
+  __shared__ LRoot<T> s_root;
+  __shared__ int64_t s_prog;
+  __shared__ T s_lit[10];
+  __shared__ uint8_t s_tab[1024];
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) {
+    s_tab[t] = lut.kind[t];
+    s_tab[256 + t] = lut.fop[t];
+    s_tab[512 + t] = lut.bop[t];
+    s_tab[768 + t] = lut.arg[t];
+  }
+  if (threadIdx.x < 10) s_lit[threadIdx.x] = (T)lut.lit[threadIdx.x];
+  if (threadIdx.x == 0) s_prog = -1;
+  const int tid = threadIdx.x;
+  const uint32_t my = (uint32_t)tid * (uint32_t)(R * sizeof(T));
+#define WS_AT(addr, mine) reinterpret_cast<T*>(smem + ((uint32_t)(addr) << 4) + ((mine) ? my : 0u))
+
+  for (int64_t item = blockIdx.x; item < p.n_items; item += gridDim.x) {
+    const int64_t b = item / p.n_splits;
+    const int64_t split = item - b * p.n_splits;
+    __syncthreads();
+    if (tid == 0 && s_prog != b) {
+      s_root = parse_loss_program<T, R>(p.pop + b * p.L, p.L, p.K, s_tab, s_lit,
+                                        p.consts + b * p.K, p.V, ad, smem, ops, stage, leaf);
+      s_prog = b;
+    }
+    for (int64_t k = tid; k < p.K; k += blockDim.x) touched[k] = 0;
+    if (!KREG)
+      for (int64_t k = 0; k < p.K; ++k) cacc[k * TS + tid] = 0.0;
+    __syncthreads();
+    const LRoot<T> rt = s_root;
+    if (!rt.valid) continue;
+    const int64_t d_begin = split * p.rows_per_split;
+    int64_t d_end = d_begin + p.rows_per_split;
+    if (d_end > p.D) d_end = p.D;
+    const int n = rt.n_ops;
+    double cr[kRegSlots];
+#pragma unroll
+    for (int k = 0; k < kRegSlots; ++k) cr[k] = 0.0;
+    auto add_const = [&](int ck, const T (&c)[R]) {
+      double s = 0.0;
+      bool any = false;
+      WS_FOR_R {
+        if (c[r] != (T)0) {
+          s += (double)c[r];
+          any = true;
+        }
+      }
+      if (any) {
+        if (KREG) creg_add<double>(cr, ck, s);
+        else cacc[(size_t)ck * TS + tid] += s;
+        touched[ck] = 1;
+      }
+    };
+
+    for (int64_t d0 = d_begin + (int64_t)tid * R; d0 < d_end; d0 += (int64_t)TS * R) {
+      for (int j = 0; j < rt.n_stage; ++j) {
+        const T* xr = p.x + (int64_t)stage[j] * p.D;
+        T xv[R];
+        WS_FOR_R xv[r] = d0 + r < d_end ? xr[d0 + r] : (T)0;
+        st_vec<T, R>(WS_AT(rt.stage0 + j * ad.slot, true), xv);
+      }
+      T g[R];  // grad_output of the R rows
+      WS_FOR_R g[r] = d0 + r < d_end ? p.gout[b * p.D + d0 + r] : (T)0;
+      // forward: values
+      for (int o = 0; o < n; ++o) {
+        const LOp op = ops[o];
+        T a[R], v[R];
+        ld_vec<T, R>(WS_AT(op.a, op.flags & LF_A_VEC), a);
+        if (op.flags & LF_BIN) {
+          T bv[R];
+          ld_vec<T, R>(WS_AT(op.b, op.flags & LF_B_VEC), bv);
+          fwd_binary_vec<T, R>(op.fop, a, bv, v);
+        } else {
+          fwd_unary_vec<T, R>(op.fop, a, v);
+        }
+        st_vec<T, R>(WS_AT(op.self, true), v);
+      }
+      if (rt.kind == OPD_CONST) {  // a one-constant program
+        add_const(rt.ck, g);
+        continue;
+      }
+      if (rt.kind != OPD_OP) continue;  // a variable or a literal: no constant to move
+      st_vec<T, R>(WS_AT(rt.at, true), g);
+      // reverse: the reference's rules from the operand values, adjoints into the operands'
+      // slots (the right operand first)
+      for (int o = n - 1; o >= 0; --o) {
+        const LOp op = ops[o];
+        if (!(op.flags & LF_REACH)) continue;
+        T ga[R], lv[R], ca[R], cb[R];
+        ld_vec<T, R>(WS_AT(op.self, true), ga);
+        ld_vec<T, R>(WS_AT(op.a, op.flags & LF_A_VEC), lv);
+        WS_FOR_R { ca[r] = (T)0; cb[r] = (T)0; }
+        if (op.flags & LF_BIN) {
+          T rv[R];
+          ld_vec<T, R>(WS_AT(op.b, op.flags & LF_B_VEC), rv);
+          switch (op.bop) {
+            case BO_ADD: WS_FOR_R { ca[r] += ga[r]; cb[r] += ga[r]; } break;
+            case BO_SUB: WS_FOR_R { ca[r] += ga[r]; cb[r] -= ga[r]; } break;
+            case BO_MUL: WS_FOR_R { acc_t(ca[r], rv[r], ga[r]); acc_t(cb[r], lv[r], ga[r]); } break;
+            case BO_DIV:
+              WS_FOR_R {
+                if (fabs(rv[r]) >= (T)1e-9) {
+                  acc_d(ca[r], 1.0 / rv[r], ga[r]);
+                  acc_t(cb[r], -(lv[r] / (rv[r] * rv[r])), ga[r]);
+                }
+              }
+              break;
+            case BO_POW:
+              WS_FOR_R {
+                if (lv[r] > 0) {
+                  const T out_val = fwd_binary<T>(op.fop, lv[r], rv[r]);
+                  acc_d(ca[r], (double)rv[r] * pow((double)lv[r], (double)rv[r] - 1.0), ga[r]);
+                  acc_t(cb[r], out_val * log(lv[r]), ga[r]);
+                }
+              }
+              break;
+            default: break;
+          }
+          WS_FOR_R if (ga[r] == (T)0) cb[r] = (T)0;
+          if (op.flags & LF_B_GRAD) st_vec<T, R>(WS_AT(op.fb, true), cb);
+        } else {
+          switch (op.bop) {
+            case BO_SIN: WS_FOR_R acc_t(ca[r], cos(lv[r]), ga[r]); break;
+            case BO_COS: WS_FOR_R acc_t(ca[r], -sin(lv[r]), ga[r]); break;
+            case BO_LOG:
+              WS_FOR_R if (fabs(lv[r]) > (T)1e-9) acc_d(ca[r], 1.0 / lv[r], ga[r]);
+              break;
+            case BO_EXP: WS_FOR_R acc_t(ca[r], fwd_unary<T>(op.fop, lv[r]), ga[r]); break;
+            case BO_SQRT:
+              WS_FOR_R if (lv[r] > (T)1e-9) acc_d(ca[r], 0.5 / sqrt(lv[r]), ga[r]);
+              break;
+            case BO_NEG: WS_FOR_R ca[r] += -ga[r]; break;
+            default: break;
+          }
+        }
+        WS_FOR_R if (ga[r] == (T)0) ca[r] = (T)0;
+        if (op.flags & LF_A_GRAD) st_vec<T, R>(WS_AT(op.fa, true), ca);
+      }
+      for (int j = 0; j < rt.n_leaf; ++j) {
+        const uint32_t e = leaf[M + j];
+        T c[R];
+        ld_vec<T, R>(WS_AT(e & 0xFFFFu, true), c);
+        add_const((int)(e >> 16), c);
+      }
+    }
+#undef WS_AT
+    __syncthreads();  // the tape is free: the reduction reuses its memory
+    double* cred = KREG ? reinterpret_cast<double*>(work) : cacc;
+    if (KREG) {
+#pragma unroll
+      for (int k = 0; k < kRegSlots; ++k)
+        if (k < p.K) cred[(size_t)k * TS + tid] = cr[k];
+    }
+    __syncthreads();
+    // fixed-order reduction over the block's threads, one thread per slot
+    for (int64_t k = tid; k < p.K; k += blockDim.x) {
+      if (!touched[k]) continue;
+      double s = 0.0;
+      for (int t = 0; t < (int)blockDim.x; ++t) s += cred[k * TS + t];
+      T* dst = p.grad + b * p.K + k;
+      if (p.n_splits == 1) *dst = *dst + (T)s;
+      else atomicAdd(dst, (T)s);
     }
   }
 }
@@ -1261,18 +1067,6 @@ BwdLut build_bwd_lut(const ws_token_map& m, int64_t num_vars) {
   return lut;
 }
 
-constexpr int64_t kStageMaxVars = 16;  // x is staged in shared memory up to this many variables
-
-template <typename T>
-size_t backward_smem(int64_t M, int64_t K, int64_t V, int threads, int R) {
-  const int64_t vs = V <= kStageMaxVars ? V : 0;
-  const bool kreg = K <= kRegSlots;
-  const size_t tape = (size_t)(M + vs) * threads * R * sizeof(T);
-  const size_t red = (size_t)((kreg ? K : 0) + 1) * threads * sizeof(double);
-  return al16((size_t)M * sizeof(BOp)) + al16((size_t)K * sizeof(int)) +
-         (kreg ? 0 : (size_t)K * threads * sizeof(double)) + (tape > red ? tape : red);
-}
-
 // Block size, rows per thread, shared memory and the split of rows into ranges for one launch.
 // Rows are split only when there are too few programs to fill the GPU; the split depends on
 // (B, L, K, D) and the device alone.
@@ -1284,69 +1078,6 @@ struct BwdPlan {
 
 template <typename T>
 constexpr int kRowsMax = sizeof(T) == 4 ? 4 : 2;
-
-template <typename T, int RR>
-void (*adj_pick(bool kreg))(BwdParams<T>, BwdLut) {
-  return kreg ? adj_kernel<T, RR, true> : adj_kernel<T, RR, false>;
-}
-
-template <typename T>
-void (*adj_fn(int R, bool kreg))(BwdParams<T>, BwdLut) {
-  if constexpr (kRowsMax<T> >= 4) {
-    if (R == 4) return adj_pick<T, 4>(kreg);
-  }
-  if (R == 2) return adj_pick<T, 2>(kreg);
-  return adj_pick<T, 1>(kreg);
-}
-
-// Block size, rows per thread and shared memory for a tape of M operator slots: the shape
-// with the most resident threads per SM.
-template <typename T>
-ws_status backward_shape(int64_t M, int64_t K, int64_t V, BwdPlan* out, int* per_sm_out) {
-  const DeviceInfo& dev = device_info();
-  const size_t budget = dev.smem_optin < (size_t)200 * 1024 ? dev.smem_optin : 200 * 1024;
-  const bool kreg = K <= kRegSlots;
-  // every (rows per thread, block size) shape that fits, scored by the rows its resident warps
-  // carry, with warps counted up to 32 per SM (measured: 2 rows per thread at twice the warps
-  // is no faster than 4 rows per thread, so rows are weighted fully)
-  double best_score = -1.0;
-  int best_threads = 0, best_per_sm = 0, best_r = 1;
-  for (int R = kRowsMax<T>; R >= 1; R /= 2) {
-    auto kern = adj_fn<T>(R, kreg);
-    for (int threads = 128; threads >= 32; threads /= 2) {
-      const size_t smem = backward_smem<T>(M, K, V, threads, R);
-      if (smem > budget) continue;
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem);
-      if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
-      int per_sm = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
-      if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
-      if (per_sm < 1) continue;
-      double warps = (double)per_sm * threads / 32.0;
-      if (warps > 32.0) warps = 32.0;
-      const double score = warps * (double)R;
-      if (score > best_score + 1e-9) {
-        best_score = score;
-        best_threads = threads;
-        best_per_sm = per_sm;
-        best_r = R;
-      }
-    }
-  }
-  if (best_threads == 0)
-    return fail("backward: " + std::to_string(K) + " constants and " + std::to_string(M) +
-                " operators need more shared memory than a block has");
-  const size_t smem = backward_smem<T>(M, K, V, best_threads, best_r);
-  cudaError_t e = cudaFuncSetAttribute(adj_fn<T>(best_r, kreg),
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
-  out->threads = best_threads;
-  out->R = best_r;
-  out->smem = smem;
-  *per_sm_out = best_per_sm;
-  return WS_OK;
-}
 
 // Rows are split into ranges only when there are too few programs to fill the GPU; ranges are
 // multiples of 512 rows (a whole number of row groups of every block shape).  The split depends
@@ -1367,38 +1098,31 @@ void split_rows(int64_t B, int64_t D, int per_sm, BwdPlan* out) {
   out->grid = n_items < slots ? n_items : slots;
 }
 
-template <typename T>
-ws_status backward_plan(int64_t B, int64_t L, int64_t D, int64_t K, int64_t V,
-                        BwdPlan* out) {
-  int per_sm = 0;
-  ws_status st = backward_shape<T>(L, K, V, out, &per_sm);
-  if (st != WS_OK) return st;
-  split_rows(B, D, per_sm, out);
-  return WS_OK;
-}
-
-// Loss mode: shared memory of a block whose tape has M slots, and the shape with the most
-// resident rows per SM (the same scoring as backward_shape).
-template <typename T>
+// Resolved-tape kernels (REF: the reference-mode ref_kernel, else loss_kernel): shared memory of
+// a block whose tape has M slots, and the shape with the most resident rows per SM: every
+// (rows per thread, block size) that fits, scored by the rows its resident warps carry, warps
+// counted up to 32 per SM.
+template <typename T, bool REF>
 size_t loss_smem(int64_t M, int64_t L, int64_t K, int threads, int R) {
-  return loss_layout(M, L, K, threads, (size_t)R * sizeof(T), K <= kRegSlots).bytes;
+  return loss_layout(M, L, K, threads, (size_t)R * sizeof(T), K <= kRegSlots, REF).bytes;
 }
 
-template <typename T, int RR>
+template <typename T, bool REF, int RR>
 void (*loss_pick(bool kreg))(BwdParams<T>, BwdLut) {
+  if constexpr (REF) return kreg ? ref_kernel<T, RR, true> : ref_kernel<T, RR, false>;
   return kreg ? loss_kernel<T, RR, true> : loss_kernel<T, RR, false>;
 }
 
-template <typename T>
+template <typename T, bool REF = false>
 void (*loss_fn(int R, bool kreg))(BwdParams<T>, BwdLut) {
   if constexpr (kRowsMax<T> >= 4) {
-    if (R == 4) return loss_pick<T, 4>(kreg);
+    if (R == 4) return loss_pick<T, REF, 4>(kreg);
   }
-  if (R == 2) return loss_pick<T, 2>(kreg);
-  return loss_pick<T, 1>(kreg);
+  if (R == 2) return loss_pick<T, REF, 2>(kreg);
+  return loss_pick<T, REF, 1>(kreg);
 }
 
-template <typename T>
+template <typename T, bool REF = false>
 ws_status loss_shape(int64_t M, int64_t L, int64_t K, BwdPlan* out, int* per_sm_out) {
   const DeviceInfo& dev = device_info();
   const size_t budget = dev.smem_optin < (size_t)200 * 1024 ? dev.smem_optin : 200 * 1024;
@@ -1406,9 +1130,9 @@ ws_status loss_shape(int64_t M, int64_t L, int64_t K, BwdPlan* out, int* per_sm_
   double best_score = -1.0;
   int best_threads = 0, best_per_sm = 0, best_r = 1;
   for (int R = kRowsMax<T>; R >= 1; R /= 2) {
-    auto kern = loss_fn<T>(R, kreg);
+    auto kern = loss_fn<T, REF>(R, kreg);
     for (int threads = 128; threads >= 32; threads /= 2) {
-      const size_t smem = loss_smem<T>(M, L, K, threads, R);
+      const size_t smem = loss_smem<T, REF>(M, L, K, threads, R);
       if (smem > budget) continue;
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem);
@@ -1431,8 +1155,8 @@ ws_status loss_shape(int64_t M, int64_t L, int64_t K, BwdPlan* out, int* per_sm_
   if (best_threads == 0)
     return fail("loss_grad: " + std::to_string(K) + " constants and " + std::to_string(M) +
                 " tape slots need more shared memory than a block has");
-  const size_t smem = loss_smem<T>(M, L, K, best_threads, best_r);
-  cudaError_t e = cudaFuncSetAttribute(loss_fn<T>(best_r, kreg),
+  const size_t smem = loss_smem<T, REF>(M, L, K, best_threads, best_r);
+  cudaError_t e = cudaFuncSetAttribute(loss_fn<T, REF>(best_r, kreg),
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return fail_cuda(e, "loss_grad");
   out->threads = best_threads;
@@ -1461,7 +1185,6 @@ BwdParams<T> backward_params(const uint8_t* pop, int64_t B, int64_t L, const voi
   prm.n_items = B * plan.n_splits;
   prm.tape_stride = plan.threads;
   prm.V = V;
-  prm.stage_x = V <= kStageMaxVars ? 1 : 0;
   prm.tape_ops = (int)L;
   prm.list = nullptr;
   prm.list_count = nullptr;
@@ -1478,13 +1201,15 @@ ws_status launch_backward_typed(const uint8_t* pop, int64_t B, int64_t L, const 
                                 const void* gout,
                                 void* grad, const BwdLut& lut, cudaStream_t stream) {
   BwdPlan plan;
-  ws_status st = backward_plan<T>(B, L, D, K, V, &plan);
+  int per_sm = 0;
+  ws_status st = loss_shape<T, true>(L, L, K, &plan, &per_sm);
   if (st != WS_OK) return st;
+  split_rows(B, D, per_sm, &plan);
   BwdParams<T> prm = backward_params<T>(pop, B, L, x, V, D, consts, K, plan);
   prm.gout = static_cast<const T*>(gout);
   prm.grad = static_cast<T*>(grad);
-  adj_fn<T>(plan.R, K <= kRegSlots)<<<(unsigned)plan.grid, plan.threads, plan.smem,
-                                              stream>>>(prm, lut);
+  loss_fn<T, true>(plan.R, K <= kRegSlots)<<<(unsigned)plan.grid, plan.threads, plan.smem,
+                                             stream>>>(prm, lut);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? WS_OK : fail_cuda(e, "eval_rpn_backward");
 }

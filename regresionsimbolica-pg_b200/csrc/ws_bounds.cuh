@@ -28,10 +28,8 @@ enum BcSite : uint32_t {
   BC_SMALL_SLOT = 6,     // small-data-set fitness: spill slot outside the lane's slots
   BC_SMALL_TAPE_LEN = 7,
   BC_COMPILE_NODES = 8,  // compiler: node count beyond its node array
-  BC_LOSS_PARSE = 9,     // loss-gradient parse: operators, leaves, variables or scalars
-                         // beyond the block's arrays
-  BC_ADJ_PARSE = 11,     // reference-mode adjoint parse: operators beyond the tape
-  BC_ADJ_OPERAND = 12,   // reference-mode adjoint: an operand index outside its array
+  BC_ADJ_PARSE = 9,      // adjoint parse (both modes): operators, constant leaves, variables or
+                         // scalars beyond the block's arrays, a variable index beyond V
   BC_SELFTEST = 99,      // ws_debug_bounds_selftest
 };
 
