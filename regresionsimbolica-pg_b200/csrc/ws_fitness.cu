@@ -6,7 +6,9 @@
 // path's [B, D] materialisation:
 //
 //   1. compile_kernel  -- one thread per program: tokens -> accumulator-machine tape
-//                         (ws_compile.cuh), constant slots baked, constants folded.
+//                         (ws_compile.cuh), constant slots baked, constants folded; programs
+//                         are taken in token-count order (count_kernel + a counting sort), so
+//                         a warp's threads parse programs of similar length.
 //   2. sort_*_kernel   -- counting sort of the programs by tape length (longest first).
 //   3. fitness_kernel  -- persistent CTAs pull work items (a block of PB length-sorted programs
 //                         x a range of row chunks).  The block's tapes are staged in shared memory
@@ -91,19 +93,46 @@ __device__ __forceinline__ int find_problem(const ProbDesc<T>* __restrict__ d, i
 
 // ---------------------------------------------------------------------------------------
 // 1. compile (one thread per program of any problem)
+// Pre-pass of the compile: a program's token count before its first PAD as the sort key (in
+// hdr[g].n_instr, status OK) and its problem.  Compiling in that order puts programs of similar
+// length in a warp, so its threads run their parse and emit loops for similar trip counts.
+template <typename T>
+__global__ void __launch_bounds__(256) count_kernel(const ProbDesc<T>* __restrict__ desc,
+                                                   int n_prob, const TokenLut* __restrict__ luts,
+                                                   int64_t total_B, int L,
+                                                   ProgHdr* __restrict__ hdr,
+                                                   int32_t* __restrict__ prob_of) {
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total_B;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int pi = find_problem(desc, n_prob, g, false);
+    const ProbDesc<T>& d = desc[pi];
+    const uint8_t* row = d.pop + (g - d.prog0) * (int64_t)L;
+    const uint8_t* cls = luts[pi].cls;
+    int n = 0;
+    while (n < L && cls[row[n]] != T_PAD) ++n;
+    ProgHdr h;
+    h.n_instr = n;
+    h.status = PROG_OK;
+    h.n_slots = 0;
+    h.n_tok = n;
+    hdr[g] = h;
+    prob_of[g] = pi;
+  }
+}
+
+// One thread per program, programs taken in `perm` order (by token count): tokens ->
+// accumulator-machine tape and header.
 template <typename T, bool STRICT, int LMAX>
-__global__ void __launch_bounds__(128) compile_kernel(const ProbDesc<T>* __restrict__ desc,
-                                                      int n_prob, const TokenLut* __restrict__ luts,
-                                                      int64_t total_B, int L,
-                                                      Instr<T>* __restrict__ tape, int Lcap,
-                                                      ProgHdr* __restrict__ hdr,
-                                                      int32_t* __restrict__ prob_of,
-                                                      unsigned* __restrict__ prog_cnt,
-                                                      unsigned* __restrict__ misc, int S) {
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g == 0) misc[0] = 0u;  // work-queue head of the evaluator launch that follows
-  if (g >= total_B) return;
-  const int pi = find_problem(desc, n_prob, g, false);
+__global__ void __launch_bounds__(128) compile_kernel(
+    const ProbDesc<T>* __restrict__ desc, const TokenLut* __restrict__ luts, int64_t total_B,
+    int L, Instr<T>* __restrict__ tape, int Lcap, ProgHdr* __restrict__ hdr,
+    const int32_t* __restrict__ prob_of, const int64_t* __restrict__ perm,
+    unsigned* __restrict__ prog_cnt, unsigned* __restrict__ misc, int S) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) misc[0] = 0u;  // work-queue head of the evaluator launch that follows
+  if (i >= total_B) return;
+  const int64_t g = perm[i];
+  const int pi = prob_of[g];
   const ProbDesc<T>& d = desc[pi];
   const int64_t p = g - d.prog0;
   ProgHdr h = compile_program_v2<T, STRICT, true, LMAX>(
@@ -115,7 +144,6 @@ __global__ void __launch_bounds__(128) compile_kernel(const ProbDesc<T>* __restr
     atomicAdd(&misc[1], 1u);
   }
   hdr[g] = h;
-  prob_of[g] = pi;
   prog_cnt[g] = 0u;
 }
 
@@ -1422,31 +1450,45 @@ ws_status compile_and_sort(int64_t total_B, int Lcap, int S, const FitnessWorksp
   const TokenLut* luts = reinterpret_cast<const TokenLut*>(wsb + lay.lut_off);
   int32_t* prob_of = reinterpret_cast<int32_t*>(wsb + lay.probof_off);
   if (a.phase != WS_PHASE_EVALUATE) {
-    cudaError_t e0 = cudaMemsetAsync(bins, 0, (size_t)a.n_desc * kSortBins * sizeof(unsigned),
-                                     a.stream);
-    if (e0 != cudaSuccess) return fail_cuda(e0, "sort-bin reset");
-    const int ct = 128;
-    const unsigned grid = (unsigned)((total_B + ct - 1) / ct);
-    if (a.L <= 64)
-      compile_kernel<T, STRICT, 64><<<grid, ct, 0, a.stream>>>(
-          desc, a.n_desc, luts, total_B, (int)a.L, tape, Lcap, hdr, prob_of, cnt, misc, S);
-    else
-      compile_kernel<T, STRICT, 256><<<grid, ct, 0, a.stream>>>(
-          desc, a.n_desc, luts, total_B, (int)a.L, tape, Lcap, hdr, prob_of, cnt, misc, S);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return fail_cuda(e, "compile_kernel launch");
     int64_t hgrid = (total_B + 4095) / 4096;
     if (hgrid < 1) hgrid = 1;
     if (hgrid > (int64_t)device_info().sm_count * 8) hgrid = (int64_t)device_info().sm_count * 8;
     const int64_t per_block = (total_B + hgrid - 1) / hgrid;
-    sort_hist_kernel<<<(unsigned)hgrid, 256, 0, a.stream>>>(hdr, prob_of, total_B, per_block,
-                                                            bins);
-    sort_scan_kernel<<<1, 1024, 0, a.stream>>>(bins, a.n_desc);
     int sgrid = (int)((total_B + 255) / 256);
     if (sgrid > device_info().sm_count * 8) sgrid = device_info().sm_count * 8;
-    sort_scatter_kernel<<<sgrid, 256, 0, a.stream>>>(hdr, prob_of, total_B, bins, perm);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return fail_cuda(e, "sort kernels launch");
+    // order programs by the key in hdr (per problem, descending, invalid last) into perm
+    auto sort = [&]() -> ws_status {
+      cudaError_t e0 = cudaMemsetAsync(bins, 0, (size_t)a.n_desc * kSortBins * sizeof(unsigned),
+                                       a.stream);
+      if (e0 != cudaSuccess) return fail_cuda(e0, "sort-bin reset");
+      sort_hist_kernel<<<(unsigned)hgrid, 256, 0, a.stream>>>(hdr, prob_of, total_B, per_block,
+                                                              bins);
+      sort_scan_kernel<<<1, 1024, 0, a.stream>>>(bins, a.n_desc);
+      sort_scatter_kernel<<<sgrid, 256, 0, a.stream>>>(hdr, prob_of, total_B, bins, perm);
+      const cudaError_t e = cudaGetLastError();
+      return e == cudaSuccess ? WS_OK : fail_cuda(e, "sort kernels launch");
+    };
+    // 1. token counts, ordered: the compile takes programs of similar length per warp
+    const int64_t cg = (total_B + 255) / 256;
+    count_kernel<T><<<(unsigned)(cg < 4096 ? cg : 4096), 256, 0, a.stream>>>(
+        desc, a.n_desc, luts, total_B, (int)a.L, hdr, prob_of);
+    ws_status st = sort();
+    if (st != WS_OK) return st;
+    // 2. compile in that order
+    const int ct = 128;
+    const unsigned grid = (unsigned)((total_B + ct - 1) / ct);
+    if (a.L <= 64)
+      compile_kernel<T, STRICT, 64><<<grid, ct, 0, a.stream>>>(
+          desc, luts, total_B, (int)a.L, tape, Lcap, hdr, prob_of, perm, cnt, misc, S);
+    else
+      compile_kernel<T, STRICT, 256><<<grid, ct, 0, a.stream>>>(
+          desc, luts, total_B, (int)a.L, tape, Lcap, hdr, prob_of, perm, cnt, misc, S);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "compile_kernel launch");
+    // 3. evaluation order: tape length (measured 2% faster on the scale workload than token
+    // count: the tape, not the token count, is what a warp runs)
+    st = sort();
+    if (st != WS_OK) return st;
   }
   if (a.phase == WS_PHASE_EVALUATE) {  // the compile kernel is what resets the queue head
     cudaError_t e = cudaMemsetAsync(misc, 0, 16, a.stream);
