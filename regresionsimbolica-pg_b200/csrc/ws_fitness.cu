@@ -1172,16 +1172,42 @@ __global__ void __launch_bounds__(1024) sort_scan_kernel(unsigned* __restrict__ 
   }
 }
 
+// Each block scatters the contiguous range the histogram block counted, one tile of its threads
+// at a time: the tile's programs of the tile's first problem are ranked within their key by a
+// shared-memory atomic and every key reserves its range of the output with ONE global atomic
+// per tile (programs of a later problem in the tile, at problem boundaries, reserve one by one):
+// a few dozen global atomics per tile instead of one per program on a few dozen addresses.
 __global__ void __launch_bounds__(256) sort_scatter_kernel(const ProgHdr* __restrict__ hdr,
                                                            const int32_t* __restrict__ prob_of,
-                                                           int64_t total_B,
+                                                           int64_t total_B, int64_t per_block,
                                                            unsigned* __restrict__ bins,
                                                            int64_t* __restrict__ perm) {
-  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total_B;
-       g += (int64_t)gridDim.x * blockDim.x) {
-    const int key = sort_key(hdr[g]);
-    const unsigned pos = atomicAdd(&bins[(size_t)prob_of[g] * kSortBins + key], 1u);
-    perm[pos] = g;
+  __shared__ unsigned h[kSortBins], base[kSortBins];
+  const int64_t g0 = (int64_t)blockIdx.x * per_block;
+  const int64_t g1 = min(total_B, g0 + per_block);
+  for (int64_t t0 = g0; t0 < g1; t0 += blockDim.x) {
+    for (int i = threadIdx.x; i < kSortBins; i += blockDim.x) h[i] = 0u;
+    __syncthreads();
+    const int pb = prob_of[t0];
+    const int64_t g = t0 + threadIdx.x;
+    const bool act = g < g1;
+    int key = 0, pi = pb;
+    unsigned rank = 0u;
+    if (act) {
+      key = sort_key(hdr[g]);
+      pi = prob_of[g];
+      if (pi == pb) rank = atomicAdd(&h[key], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kSortBins; i += blockDim.x)
+      if (h[i]) base[i] = atomicAdd(&bins[(size_t)pb * kSortBins + i], h[i]);
+    __syncthreads();
+    if (act) {
+      const unsigned pos = pi == pb ? base[key] + rank
+                                    : atomicAdd(&bins[(size_t)pi * kSortBins + key], 1u);
+      perm[pos] = g;
+    }
+    __syncthreads();
   }
 }
 
@@ -1454,8 +1480,6 @@ ws_status compile_and_sort(int64_t total_B, int Lcap, int S, const FitnessWorksp
     if (hgrid < 1) hgrid = 1;
     if (hgrid > (int64_t)device_info().sm_count * 8) hgrid = (int64_t)device_info().sm_count * 8;
     const int64_t per_block = (total_B + hgrid - 1) / hgrid;
-    int sgrid = (int)((total_B + 255) / 256);
-    if (sgrid > device_info().sm_count * 8) sgrid = device_info().sm_count * 8;
     // order programs by the key in hdr (per problem, descending, invalid last) into perm
     auto sort = [&]() -> ws_status {
       cudaError_t e0 = cudaMemsetAsync(bins, 0, (size_t)a.n_desc * kSortBins * sizeof(unsigned),
@@ -1464,7 +1488,8 @@ ws_status compile_and_sort(int64_t total_B, int Lcap, int S, const FitnessWorksp
       sort_hist_kernel<<<(unsigned)hgrid, 256, 0, a.stream>>>(hdr, prob_of, total_B, per_block,
                                                               bins);
       sort_scan_kernel<<<1, 1024, 0, a.stream>>>(bins, a.n_desc);
-      sort_scatter_kernel<<<sgrid, 256, 0, a.stream>>>(hdr, prob_of, total_B, bins, perm);
+      sort_scatter_kernel<<<(unsigned)hgrid, 256, 0, a.stream>>>(hdr, prob_of, total_B,
+                                                                 per_block, bins, perm);
       const cudaError_t e = cudaGetLastError();
       return e == cudaSuccess ? WS_OK : fail_cuda(e, "sort kernels launch");
     };
