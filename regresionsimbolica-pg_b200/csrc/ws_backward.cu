@@ -959,13 +959,15 @@ __global__ void __launch_bounds__(256) bucket_kernel(const uint8_t* __restrict__
     s_arg[t] = lut.arg[t];
   }
   __syncthreads();
-  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < B;
-       b += (int64_t)gridDim.x * blockDim.x) {
-    if (active && active[b] == 0) continue;
-    const uint8_t* row = pop + b * L;
+  // whole warps step through the programs together (the bucket counters are claimed per warp)
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t b_end = (B + 31) / 32 * 32;
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < b_end; b += stride) {
+    const bool take = b < B && !(active && active[b] == 0);
+    const uint8_t* row = pop + (take ? b : 0) * L;
     int n = 0;
     uint64_t seen = 0;  // variables 0..63; higher ones are counted at every use (a bound)
-    for (int64_t t = 0; t < L; ++t) {
+    for (int64_t t = 0; take && t < L; ++t) {
       const uint8_t k = s_kind[row[t]];
       if (k == BK_PAD) break;
       if (k == BK_BIN || k == BK_UN || (k == BK_CONST && K > 0)) {
@@ -982,8 +984,19 @@ __global__ void __launch_bounds__(256) bucket_kernel(const uint8_t* __restrict__
     }
     int j = 0;
     while (j < n_buckets - 1 && n > c_bucket_slots[j]) ++j;
-    const int pos = atomicAdd(counts + j, 1);
-    lists[(int64_t)j * B + pos] = (int32_t)b;
+    // one atomic per bucket per warp: the lowest lane of each group of lanes with the same
+    // bucket claims the group's slots, the others take theirs by rank
+    const unsigned taking = __ballot_sync(0xFFFFFFFFu, take);
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, take ? j : -1) & taking;
+    if (take) {
+      const int lane = threadIdx.x & 31;
+      const int leader = __ffs(peers) - 1;
+      int pos0 = 0;
+      if (lane == leader) pos0 = atomicAdd(counts + j, __popc(peers));
+      pos0 = __shfl_sync(peers, pos0, leader);
+      const int rank = __popc(peers & ((1u << lane) - 1u));
+      lists[(int64_t)j * B + pos0 + rank] = (int32_t)b;
+    }
   }
 }
 
