@@ -390,6 +390,16 @@ ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* population, int64_t
                                const void* x, int64_t num_vars, int64_t D, const void* constants,
                                int64_t K, const void* grad_output, void* grad_constants,
                                const ws_token_map* ids, void* stream);
+/* The same with caller-provided scratch of ws_eval_rpn_backward_workspace_bytes(B) bytes: the
+ * programs are grouped on the device by the tape they need and each group is launched with a
+ * tape sized for it (more resident warps than one launch sized for the longest program).  Same
+ * results; the Python drop-in's eval_rpn_backward takes this form. */
+ws_status ws_eval_rpn_backward_workspace_bytes(int64_t B, size_t* bytes);
+ws_status ws_eval_rpn_backward_ws(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
+                                  const void* x, int64_t num_vars, int64_t D,
+                                  const void* constants, int64_t K, const void* grad_output,
+                                  void* grad_constants, const ws_token_map* ids, void* workspace,
+                                  size_t workspace_bytes, void* stream);
 
 /*
  * Loss and constant gradient in one launch, without per-row tensors.  Replaces the closure of the

@@ -163,6 +163,9 @@ _SIGS = {
     "ws_sharing_table_slots": (_I64, []),
     "ws_eval_rpn_backward": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
                                     C.POINTER(TokenMap), _P]),
+    "ws_eval_rpn_backward_workspace_bytes": (_I32, [_I64, C.POINTER(C.c_size_t)]),
+    "ws_eval_rpn_backward_ws": (_I32, [_I32, _P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _P,
+                                       C.POINTER(TokenMap), _P, C.c_size_t, _P]),
     "ws_subtree_pick": (_I32, [_P, _P, _I64, _I64, _P, _I32, _P, _P, _P, _P, _I32, _P]),
     "ws_splice_valid": (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _I64, _I64, _P]),
     "ws_splice_rows": (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I64,

@@ -785,9 +785,11 @@ __global__ void __launch_bounds__(128) ref_kernel(BwdParams<T> p, BwdLut lut) {
   const uint32_t my = (uint32_t)tid * (uint32_t)(R * sizeof(T));
 #define WS_AT(addr, mine) reinterpret_cast<T*>(smem + ((uint32_t)(addr) << 4) + ((mine) ? my : 0u))
 
-  for (int64_t item = blockIdx.x; item < p.n_items; item += gridDim.x) {
-    const int64_t b = item / p.n_splits;
-    const int64_t split = item - b * p.n_splits;
+  const int64_t n_items = p.list ? (int64_t)(*p.list_count) * p.n_splits : p.n_items;
+  for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int64_t li = item / p.n_splits;
+    const int64_t split = item - li * p.n_splits;
+    const int64_t b = p.list ? (int64_t)p.list[li] : li;
     __syncthreads();
     if (tid == 0 && s_prog != b) {
       s_root = parse_loss_program<T, R>(p.pop + b * p.L, p.L, p.K, s_tab, s_lit,
@@ -1208,11 +1210,14 @@ BwdParams<T> backward_params(const uint8_t* pop, int64_t B, int64_t L, const voi
   return prm;
 }
 
+// buckets (optional, loss_grad_bucket_bytes(B) of scratch): programs grouped by tape slots and
+// one launch per group with a tape sized for it, as in the loss path; without it one launch
+// sized for L.
 template <typename T>
 ws_status launch_backward_typed(const uint8_t* pop, int64_t B, int64_t L, const void* x,
                                 int64_t V, int64_t D, const void* consts, int64_t K,
-                                const void* gout,
-                                void* grad, const BwdLut& lut, cudaStream_t stream) {
+                                const void* gout, void* grad, const BwdLut& lut,
+                                int32_t* buckets, cudaStream_t stream) {
   BwdPlan plan;
   int per_sm = 0;
   ws_status st = loss_shape<T, true>(L, L, K, &plan, &per_sm);
@@ -1221,8 +1226,37 @@ ws_status launch_backward_typed(const uint8_t* pop, int64_t B, int64_t L, const 
   BwdParams<T> prm = backward_params<T>(pop, B, L, x, V, D, consts, K, plan);
   prm.gout = static_cast<const T*>(gout);
   prm.grad = static_cast<T*>(grad);
-  loss_fn<T, true>(plan.R, K <= kRegSlots)<<<(unsigned)plan.grid, plan.threads, plan.smem,
-                                             stream>>>(prm, lut);
+  const bool kreg = K <= kRegSlots;
+  if (!buckets) {
+    loss_fn<T, true>(plan.R, kreg)<<<(unsigned)plan.grid, plan.threads, plan.smem, stream>>>(
+        prm, lut);
+  } else {
+    int nb = 0;
+    while (nb < kMaxBuckets && (nb == 0 || kBucketSlots[nb - 1] < L)) ++nb;
+    int32_t* counts = buckets;
+    int32_t* lists = buckets + 16;
+    cudaError_t e = cudaMemsetAsync(counts, 0, 16 * sizeof(int32_t), stream);
+    if (e != cudaSuccess) return fail_cuda(e, "eval_rpn_backward");
+    const int64_t cb = (B + 255) / 256;
+    bucket_kernel<<<(unsigned)(cb < 2048 ? cb : 2048), 256, 0, stream>>>(pop, B, L, K, lut,
+                                                                         nullptr, nb, counts,
+                                                                         lists);
+    for (int j = 0; j < nb; ++j) {
+      const int64_t M = kBucketSlots[j] < L ? kBucketSlots[j] : L;
+      BwdPlan pj;
+      int pj_per_sm = 0;
+      st = loss_shape<T, true>(M, L, K, &pj, &pj_per_sm);
+      if (st != WS_OK) return st;
+      BwdParams<T> q = prm;
+      q.tape_stride = pj.threads;
+      q.tape_ops = (int)M;
+      q.list = lists + (int64_t)j * B;
+      q.list_count = counts + j;
+      const int64_t slots = (int64_t)device_info().sm_count * pj_per_sm;
+      const int64_t grid = prm.n_items < slots ? prm.n_items : slots;
+      loss_fn<T, true>(pj.R, kreg)<<<(unsigned)grid, pj.threads, pj.smem, stream>>>(q, lut);
+    }
+  }
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? WS_OK : fail_cuda(e, "eval_rpn_backward");
 }
@@ -1312,14 +1346,15 @@ template ws_status launch_loss_grad<double>(const uint8_t*, int64_t, int64_t, co
                                             cudaStream_t);
 }  // namespace ws
 
-extern "C" ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* population, int64_t B,
-                                          int64_t L, const void* x, int64_t num_vars, int64_t D,
-                                          const void* constants, int64_t K,
-                                          const void* grad_output, void* grad_constants,
-                                          const ws_token_map* ids, void* stream) {
+namespace {
+// The checks and launch shared by ws_eval_rpn_backward and its workspace form (buckets: null, or
+// the program-group scratch in the caller's workspace).
+ws_status eval_rpn_backward_impl(int32_t dtype, const uint8_t* population, int64_t B, int64_t L,
+                                 const void* x, int64_t num_vars, int64_t D,
+                                 const void* constants, int64_t K, const void* grad_output,
+                                 void* grad_constants, const ws_token_map* ids, int32_t* buckets,
+                                 void* stream) {
   using namespace ws;
-  clear_error();
-  NvtxRange nvtx("ws_eval_rpn_backward");
   if (dtype != WS_F32 && dtype != WS_F64) return fail("x must be float32 or float64");
   if (!ids) return fail("token map is required");
   if (B < 0 || L < 0 || D < 0 || K < 0 || num_vars < 0) return fail("negative dimension");
@@ -1333,11 +1368,44 @@ extern "C" ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* populati
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (dtype == WS_F32)
     return launch_backward_typed<float>(population, B, L, x, num_vars, D, constants, K,
-                                        grad_output,
-                                        grad_constants, lut, s);
+                                        grad_output, grad_constants, lut, buckets, s);
   return launch_backward_typed<double>(population, B, L, x, num_vars, D, constants, K,
-                                       grad_output,
-                                       grad_constants, lut, s);
+                                       grad_output, grad_constants, lut, buckets, s);
+}
+}  // namespace
+
+extern "C" ws_status ws_eval_rpn_backward(int32_t dtype, const uint8_t* population, int64_t B,
+                                          int64_t L, const void* x, int64_t num_vars, int64_t D,
+                                          const void* constants, int64_t K,
+                                          const void* grad_output, void* grad_constants,
+                                          const ws_token_map* ids, void* stream) {
+  ws::clear_error();
+  ws::NvtxRange nvtx("ws_eval_rpn_backward");
+  return eval_rpn_backward_impl(dtype, population, B, L, x, num_vars, D, constants, K,
+                                grad_output, grad_constants, ids, nullptr, stream);
+}
+
+extern "C" ws_status ws_eval_rpn_backward_workspace_bytes(int64_t B, size_t* bytes) {
+  ws::clear_error();
+  if (B < 0) return ws::fail("negative dimension");
+  if (!bytes) return ws::fail("null output pointer");
+  *bytes = ws::loss_grad_bucket_bytes(B);
+  return WS_OK;
+}
+
+extern "C" ws_status ws_eval_rpn_backward_ws(int32_t dtype, const uint8_t* population, int64_t B,
+                                             int64_t L, const void* x, int64_t num_vars,
+                                             int64_t D, const void* constants, int64_t K,
+                                             const void* grad_output, void* grad_constants,
+                                             const ws_token_map* ids, void* workspace,
+                                             size_t workspace_bytes, void* stream) {
+  ws::clear_error();
+  ws::NvtxRange nvtx("ws_eval_rpn_backward");
+  if (B > 0 && (!workspace || workspace_bytes < ws::loss_grad_bucket_bytes(B)))
+    return ws::fail("eval_rpn_backward workspace too small");
+  return eval_rpn_backward_impl(dtype, population, B, L, x, num_vars, D, constants, K,
+                                grad_output, grad_constants, ids,
+                                static_cast<int32_t*>(workspace), stream);
 }
 
 namespace {

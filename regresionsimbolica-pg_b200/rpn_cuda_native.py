@@ -248,9 +248,14 @@ def eval_rpn_backward(population, x, constants, grad_output, grad_constants,
                     id_6, id_10, op_add, op_sub, op_mul, op_div, op_pow, op_mod, op_sin, op_cos,
                     op_tan, op_log, op_exp, op_sqrt, op_abs, op_neg, op_fact, op_floor, op_ceil,
                     op_sign, op_gamma, op_lgamma, op_asin, op_acos, op_atan), pi_val, e_val)
-    N.check(N.lib().ws_eval_rpn_backward(dtype_code(x.dtype), ptr(population), B, L, ptr(x), V, D,
-                                         ptr(constants), K, ptr(grad_output),
-                                         ptr(grad_constants), C.byref(m), stream_of(x)))
+    # scratch for grouping the programs by tape size (torch's allocator, stream-ordered)
+    need = C.c_size_t(0)
+    N.check(N.lib().ws_eval_rpn_backward_workspace_bytes(B, C.byref(need)))
+    ws = workspace(need.value, x.device)
+    N.check(N.lib().ws_eval_rpn_backward_ws(dtype_code(x.dtype), ptr(population), B, L, ptr(x), V,
+                                            D, ptr(constants), K, ptr(grad_output),
+                                            ptr(grad_constants), C.byref(m), ptr(ws), ws.numel(),
+                                            stream_of(x)))
 
 
 def decode_rpn(population, constants, vocab, arities, PAD_ID, precision=4):

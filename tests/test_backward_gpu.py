@@ -128,6 +128,40 @@ def test_backward_accumulates_into_grad_and_handles_empty_cases():
                                torch.zeros_like(Ct[:2]), *g.scalar_ids(), math.pi, math.e)
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_backward_without_workspace_matches_grouped_launches(dtype):
+    """ws_eval_rpn_backward (one launch sized for L) against the drop-in's ws_eval_rpn_backward_ws
+    (programs grouped by tape size, a launch per group): the same per-row terms, summed by blocks
+    of other shapes, so equal to rounding; with D = 1 and a slot per constant token every slot
+    receives one term and the two agree bit for bit."""
+    import ctypes as C
+    from warpsymbolic_b200 import _native as N
+    from warpsymbolic_b200._tensors import dtype_code, ptr, stream_of
+    for D, exact in ((1, True), (3000, False)):
+        g, pop, consts, X, gout = mixed_case(21 + D, 700, 40, 12, D, dtype)
+        P, Xt, Ct, Gt = T(pop), T(X), T(consts), T(gout)
+        grouped = ours_backward(g, P, Xt, Ct, Gt)
+        single = torch.zeros_like(Ct)
+        m = tmap(g)
+        N.check(N.lib().ws_eval_rpn_backward(dtype_code(Xt.dtype), ptr(P), 700, 40, ptr(Xt), 3, D,
+                                             ptr(Ct), 12, ptr(Gt), ptr(single), C.byref(m),
+                                             stream_of(Xt)))
+        if exact:
+            assert torch.equal(single.isnan(), grouped.isnan())
+            fin = ~single.isnan()
+            assert torch.equal(single[fin], grouped[fin])
+        else:  # bounded by the sum of the terms' magnitudes (the CPU oracle's)
+            _, absg = O.backward(tmap(g), pop, X.astype(np.float64), consts.astype(np.float64),
+                                 gout.astype(np.float64))
+            a, b = single.cpu().numpy().astype(np.float64), grouped.cpu().numpy().astype(np.float64)
+            assert np.array_equal(np.isnan(a), np.isnan(b))
+            inf = np.isinf(a) | np.isinf(b)
+            assert np.array_equal(a[inf], b[inf])  # overflowed sums overflow alike
+            fin = np.isfinite(a) & np.isfinite(b) & np.isfinite(absg)
+            tol = (1e-5 if dtype == np.float32 else 1e-12) * (absg[fin] + 1e-30)
+            assert (np.abs(a[fin] - b[fin]) <= tol).all()
+
+
 @needs_ref
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_reference_single_row_bit_exact(dtype):
