@@ -661,14 +661,20 @@ extern "C" ws_status ws_fused_pso(int32_t dtype, const uint8_t* population, int6
   a.pad_id = ids->pad_id;
   a.id_C = ids->id_C;
   const PsoLut lut = build_pso_lut(*ids, num_vars);
-  const int per_block = 128 / a.G;
+  // up to four swarms per 128-thread block; fewer when that would leave SMs without a block
+  // (a swarm's results do not depend on its block)
+  const int sms = device_info().sm_count;
+  int per_block = 128 / a.G;
+  while (per_block > 1 && (B + per_block - 1) / per_block < sms) per_block /= 2;
+  const int threads = per_block * a.G;
   const int64_t want = (B + per_block - 1) / per_block;
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_pso_kernel, 128, 0);
+  cudaError_t e =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_pso_kernel, threads, 0);
   if (e != cudaSuccess) return fail_cuda(e, "fused_pso");
-  const int64_t cap = (int64_t)device_info().sm_count * (per_sm > 0 ? per_sm : 1);
+  const int64_t cap = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
   const int grid = (int)(want < cap ? want : cap);
-  fused_pso_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+  fused_pso_kernel<<<grid, threads, 0, static_cast<cudaStream_t>(stream)>>>(
       a, lut, (float)ids->pi_val, (float)ids->e_val);
   e = cudaGetLastError();
   return e == cudaSuccess ? WS_OK : fail_cuda(e, "fused_pso");
