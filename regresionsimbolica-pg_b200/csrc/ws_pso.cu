@@ -9,13 +9,15 @@
 // flags), the swarm-best tie rules are the reference's, and the fused loop draws the same
 // curand XORWOW streams (seed + b * P + p) in the same order.
 //
-// B200 layout of the fused loop: a particle per lane, a program per warp (two warps when the
-// swarm has more than 32 particles), four programs per 128-thread block, instead of one
-// P-thread block per program (20-thread blocks leave 12 lanes of every warp idle and cap
-// residency at 32 blocks per SM).  The program and its constants live in shared memory; the
-// token dispatch is a table lookup instead of a ~40-way comparison chain; each lane carries 16
-// rows through one pass over the program (one decode per token for 16 rows) and then adds the
-// rows' squared errors one at a time in row order, so every RMSE keeps the reference's bits.
+// B200 layout of the fused loop: a particle per lane, instead of one P-thread block per program
+// (20-thread blocks leave 12 lanes of every warp idle and cap residency at 32 blocks per SM).
+// Up to 32 particles, a swarm owns a block of four or eight warps that split its rows (lane p
+// of every warp is particle p); warp 0 adds the row errors in row order and runs the swarm's
+// update.  Above 32 particles, a swarm owns a pair of warps that walk all rows.  The program and
+// its constants live in shared memory; the token dispatch is a table lookup instead of a ~40-way
+// comparison chain; each lane carries 16 rows through one pass over the program (one decode per
+// token for 16 rows), and the rows' squared errors are added one at a time in row order, so
+// every RMSE keeps the reference's bits.
 #include <cuda_runtime.h>
 #include <curand_kernel.h>
 #include <cstdint>
@@ -503,6 +505,184 @@ __global__ void __launch_bounds__(128) fused_pso_kernel(FusedPsoArgs a, PsoLut l
   }
 }
 
+// Row-split form for few swarms (32 particles at most): one swarm per block of W warps.  Lane p
+// of every warp is particle p.  Each step walks the rows in chunks of W * kSplitWarpRows; warp w
+// evaluates rows [w * kSplitWarpRows, (w + 1) * kSplitWarpRows) of the chunk for all particles
+// and leaves each row's difference to the target in shared memory; warp 0 then adds the chunk's
+// squared differences one row at a time in row order (the reference's summation, so every RMSE
+// keeps its bits) and alone holds the curand streams, velocities and personal bests.  A
+// particle whose row fails is flagged and no warp evaluates its later chunks (its RMSE is the
+// error value whatever the other rows give).
+constexpr int kSplitMaxWarps = 8, kSplitWarpRows = 32;
+
+// dynamic shared memory of a W-warp block: the chunk's row differences, [W * 32 rows][32 lanes]
+constexpr size_t split_smem(int W) { return (size_t)W * kSplitWarpRows * 32 * sizeof(float); }
+
+__global__ void __launch_bounds__(kSplitMaxWarps * 32)
+    fused_pso_rows_kernel(FusedPsoArgs a, PsoLut lut, float pi_val, float e_val) {
+  constexpr int R = kPsoRows;
+  __shared__ uint8_t s_cls[256], s_arg[256];
+  __shared__ float s_lit[N_LITERALS];
+  __shared__ SwarmSmem sw;
+  extern __shared__ float s_diff[];  // [chunk rows][32]
+  __shared__ int s_bad[32];
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) {
+    s_cls[t] = lut.cls[t];
+    s_arg[t] = lut.arg[t];
+  }
+  if (threadIdx.x < N_LITERALS) {
+    const float lits[N_LITERALS] = {0.f, 1.f, 2.f, 3.f, 4.f, 5.f, 6.f, 10.f, pi_val, e_val};
+    s_lit[threadIdx.x] = lits[threadIdx.x];
+  }
+  const int warp = threadIdx.x >> 5;
+  const int p = threadIdx.x & 31;
+  const int chunk = (int)(blockDim.x >> 5) * kSplitWarpRows;
+  const int K = a.K;
+  const int D = (int)a.D;
+  const bool active = p < a.P;
+  float* my_pos = sw.pos + p;  // slot k at my_pos[k * 32]
+
+  for (int64_t b = blockIdx.x; b < a.B; b += gridDim.x) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < a.L; i += blockDim.x) sw.prog[i] = a.pop[b * a.L + i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int count = 0;
+      for (int i = 0; i < a.L; ++i) {
+        if (sw.prog[i] == a.pad_id) break;
+        if (sw.prog[i] == a.id_C && count < K) count++;
+      }
+      sw.n_active = count > 0 ? count : 1;
+    }
+    __syncthreads();
+    const int n_active = sw.n_active;
+
+    curandState rng;
+    float vel[kPsoMaxK], pbest_pos[kPsoMaxK];
+    float pbest_err = kPsoInf;
+    if (warp == 0 && active) {
+      curand_init(a.seed + (uint64_t)b * a.P + p, 0, 0, &rng);
+      const float range = (float)(a.cmax - a.cmin);
+      const float jitter_sigma = range * 0.15f;
+      const float vel_sigma = range * 0.02f;
+      const float* init = a.init + b * K;
+#pragma unroll
+      for (int k = 0; k < kPsoMaxK; ++k) {
+        if (k < K) {
+          float pk = init[k];
+          if (p > 0 && k < n_active) {
+            pk += curand_normal(&rng) * jitter_sigma;
+            if (pk < a.cmin) pk = a.cmin;
+            if (pk > a.cmax) pk = a.cmax;
+          }
+          vel[k] = curand_normal(&rng) * vel_sigma;
+          pbest_pos[k] = pk;
+          my_pos[k * 32] = pk;
+        }
+      }
+    }
+    if (threadIdx.x == 0) {
+      sw.gbest_err = kPsoInf;
+      for (int k = 0; k < K; ++k) sw.gbest_pos[k] = a.init[b * K + k];
+    }
+
+    for (int step = 0; step < a.steps; ++step) {
+      if (warp == 0) s_bad[p] = 0;
+      __syncthreads();
+      // 1. evaluate every particle over every row, a chunk at a time
+      float mse_sum = 0.0f;
+      for (int c = 0; c < D; c += chunk) {
+        const int lo = c + warp * kSplitWarpRows;
+        const int hi = lo + kSplitWarpRows < D ? lo + kSplitWarpRows : D;
+        if (active && !s_bad[p]) {
+          for (int d = lo; d < hi; d += R) {
+            const int nr = hi - d < R ? hi - d : R;
+            float pr[R];
+            pso_eval_rows<R>(sw.prog, a.L, s_cls, s_arg, s_lit, a.x, a.D, d, nr, my_pos, 32, K,
+                             pr);
+            bool bad = false;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              if (r < nr) {
+                if (pr[r] >= 1e29f) bad = true;
+                s_diff[(d - c + r) * 32 + p] = pr[r] - a.y[d + r];
+              }
+            }
+            if (bad) {
+              s_bad[p] = 1;
+              break;
+            }
+          }
+        }
+        __syncthreads();
+        if (warp == 0 && active && !s_bad[p]) {
+          const int n = D - c < chunk ? D - c : chunk;
+          for (int r = 0; r < n; ++r) {
+            const float diff = s_diff[r * 32 + p];
+            mse_sum += diff * diff;
+          }
+        }
+        __syncthreads();
+      }
+      // 2. personal best
+      if (warp == 0 && active) {
+        const float rmse = s_bad[p] ? kPsoInf : sqrtf(mse_sum / (float)a.D);
+        if (rmse < pbest_err) {
+          pbest_err = rmse;
+#pragma unroll
+          for (int k = 0; k < kPsoMaxK; ++k)
+            if (k < K) pbest_pos[k] = my_pos[k * 32];
+        }
+        sw.perr[p] = pbest_err;
+      }
+      __syncthreads();
+      // 3. swarm best: serial scan in particle order, strict improvement
+      if (threadIdx.x == 0) {
+        int bp = -1;
+        float be = sw.gbest_err;
+        for (int pp = 0; pp < a.P; ++pp)
+          if (sw.perr[pp] < be) {
+            be = sw.perr[pp];
+            bp = pp;
+          }
+        sw.best_particle = bp;
+        if (bp >= 0) sw.gbest_err = be;
+      }
+      __syncthreads();
+      if (warp == 0 && active && sw.best_particle == p) {
+#pragma unroll
+        for (int k = 0; k < kPsoMaxK; ++k)
+          if (k < K) sw.gbest_pos[k] = pbest_pos[k];
+      }
+      __syncthreads();
+      // 4. inertia decays linearly from w to 0.4; velocity / position update of active slots
+      if (warp == 0 && active) {
+        const float w_curr =
+            a.w - (a.w - 0.4f) * (float)step / (float)(a.steps > 1 ? a.steps - 1 : 1);
+#pragma unroll
+        for (int k = 0; k < kPsoMaxK; ++k) {
+          if (k < n_active) {
+            const float r1 = curand_uniform(&rng);
+            const float r2 = curand_uniform(&rng);
+            float pk = my_pos[k * 32];
+            vel[k] = w_curr * vel[k] + a.c1 * r1 * (pbest_pos[k] - pk) +
+                     a.c2 * r2 * (sw.gbest_pos[k] - pk);
+            pk += vel[k];
+            if (pk < a.cmin) pk = a.cmin;
+            if (pk > a.cmax) pk = a.cmax;
+            my_pos[k * 32] = pk;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      a.out_err[b] = sw.gbest_err;
+      for (int k = 0; k < K; ++k) a.out_pos[b * K + k] = sw.gbest_pos[k];
+    }
+  }
+}
+
 PsoLut build_pso_lut(const ws_token_map& m, int64_t num_vars) {
   PsoLut lut;
   const int lit_ids[N_LITERALS] = {m.id_0, m.id_1, m.id_2, m.id_3, m.id_4,
@@ -661,9 +841,34 @@ extern "C" ws_status ws_fused_pso(int32_t dtype, const uint8_t* population, int6
   a.pad_id = ids->pad_id;
   a.id_C = ids->id_C;
   const PsoLut lut = build_pso_lut(*ids, num_vars);
-  // up to four swarms per 128-thread block; fewer when that would leave SMs without a block
-  // (a swarm's results do not depend on its block)
   const int sms = device_info().sm_count;
+  if (num_particles <= 32) {
+    // Row-split form.  Eight or four warps per swarm, as measured on B200 (20-32 particles,
+    // 1,000-1,024 rows, 200-8,192 swarms): eight while the swarms fill at most 1.5 waves of
+    // 8-warp blocks or between one wave of 4-warp blocks and 14 waves of 8-warp ones; four
+    // otherwise (one wave of 4-warp blocks instead of two partial 8-warp waves; and with many
+    // waves, where warp 0's serial row sum and the barriers weigh more than the spread).
+    int per_sm8 = 0, per_sm4 = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm8, fused_pso_rows_kernel, 8 * 32, split_smem(8));
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm4, fused_pso_rows_kernel, 4 * 32,
+                                                        split_smem(4));
+    if (e != cudaSuccess) return fail_cuda(e, "fused_pso");
+    const int64_t cap8 = (int64_t)sms * (per_sm8 > 0 ? per_sm8 : 1);
+    const int64_t cap4 = (int64_t)sms * (per_sm4 > 0 ? per_sm4 : 1);
+    const bool four = (2 * B > 3 * cap8 && B <= cap4) || B > 14 * cap8;
+    const int W = four ? 4 : 8;
+    const int64_t cap = four ? cap4 : cap8;
+    const int grid = (int)(B < cap ? B : cap);
+    fused_pso_rows_kernel<<<grid, W * 32, split_smem(W), static_cast<cudaStream_t>(stream)>>>(
+        a, lut, (float)ids->pi_val, (float)ids->e_val);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? WS_OK : fail_cuda(e, "fused_pso");
+  }
+  // More than 32 particles: a swarm per pair of warps (a lane per particle), up to two swarms
+  // per 128-thread block; one when that would leave SMs without a block (a swarm's results do
+  // not depend on its block)
   int per_block = 128 / a.G;
   while (per_block > 1 && (B + per_block - 1) / per_block < sms) per_block /= 2;
   const int threads = per_block * a.G;

@@ -140,16 +140,19 @@ def _run_fused(mod, g, pop, consts, X, y, P, steps, seed, w=0.5, c1=1.5, c2=1.5,
 
 @gpu
 @needs_ref
-@pytest.mark.parametrize("P,steps,K,D,ops", [
-    (20, 20, 4, 200, tl.C1_OPERATORS),
-    (40, 10, 10, 96, tl.C1_OPERATORS),
-    (64, 5, 16, 1024, tl.C1_OPERATORS),
-    (7, 12, 3, 333, tl.ALL_OPERATORS),
+@pytest.mark.parametrize("B,P,steps,K,D,ops", [
+    (700, 20, 20, 4, 200, tl.C1_OPERATORS),   # row split, eight warps per swarm
+    (500, 20, 10, 4, 1024, tl.C1_OPERATORS),  # row split, four warps (one wave of 4-warp blocks)
+    (4500, 32, 4, 8, 300, tl.C1_OPERATORS),   # row split, four warps (many waves)
+    (200, 30, 6, 5, 1, tl.C1_OPERATORS),      # a single row
+    (700, 40, 10, 10, 96, tl.C1_OPERATORS),   # above 32 particles: a swarm per pair of warps
+    (700, 64, 5, 16, 1024, tl.C1_OPERATORS),
+    (700, 7, 12, 3, 333, tl.ALL_OPERATORS),
 ])
-def test_fused_pso_bit_exact(P, steps, K, D, ops):
+def test_fused_pso_bit_exact(B, P, steps, K, D, ops):
     ref = refext.load("fastmath")
     from warpsymbolic_b200 import rpn_cuda_native as ours
-    g, pop, consts, X, y = _fused_case(P + K, 700, 30, K, D, ops=ops,
+    g, pop, consts, X, y = _fused_case(P + K, B, 30, K, D, ops=ops,
                                        valid_only=ops is tl.C1_OPERATORS)
     seed = 123456789 + P
     rp, re_ = _run_fused(ref, g, pop, consts, X, y, P, steps, seed)
