@@ -125,6 +125,14 @@ def _cases():
     cases["fused_pso (2048 x 32 particles x 20 steps x 1024 rows)"] = lambda m: (
         lambda: m.fused_pso(Pf[:Bp], cf[:Bp], Xf, yf, gpos, gerr, 32, 20, 0.5, 1.5, 1.5, -25.0,
                             25.0, *ids, math.pi, math.e, 3))
+    # the engine's own call in a normal generation: PSO_K_NORMAL = 500 programs, nano_pso's
+    # default 20 particles, PSO_STEPS_NORMAL = 40 (gpu/config.py:312-315, gpu/engine.py:2137-2174)
+    Bn = 500
+    gpos_n = torch.empty((Bn, 6), dtype=torch.float32, device=DEV)
+    gerr_n = torch.empty(Bn, dtype=torch.float32, device=DEV)
+    cases["fused_pso (500 x 20 particles x 40 steps x 1024 rows)"] = lambda m: (
+        lambda: m.fused_pso(Pf[:Bn], cf[:Bn], Xf, yf, gpos_n, gerr_n, 20, 40, 0.5, 1.5, 1.5,
+                            -25.0, 25.0, *ids, math.pi, math.e, 3))
     gb = tl.GPUGrammar(num_variables=3, operators=('+', '-', '*', '/'))
     popb = tl.synthetic.random_programs(gb, 64, 5, 39, 40, rng, max_consts=6)
     Pb = T(popb)
