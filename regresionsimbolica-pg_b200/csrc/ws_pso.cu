@@ -843,24 +843,19 @@ extern "C" ws_status ws_fused_pso(int32_t dtype, const uint8_t* population, int6
   const PsoLut lut = build_pso_lut(*ids, num_vars);
   const int sms = device_info().sm_count;
   if (num_particles <= 32) {
-    // Row-split form.  Eight or four warps per swarm, as measured on B200 (20-32 particles,
-    // 1,000-1,024 rows, 200-8,192 swarms): eight while the swarms fill at most 1.5 waves of
-    // 8-warp blocks or between one wave of 4-warp blocks and 14 waves of 8-warp ones; four
-    // otherwise (one wave of 4-warp blocks instead of two partial 8-warp waves; and with many
-    // waves, where warp 0's serial row sum and the barriers weigh more than the spread).
-    int per_sm8 = 0, per_sm4 = 0;
+    // Row-split form, a block per swarm: the block scheduler hands the next swarm to whichever
+    // SM frees a slot first, which balances programs of different lengths (a persistent grid
+    // striding over the swarms left the SMs idle half of the time on 1,024 swarms).  Eight warps
+    // per swarm, four beyond seven waves of 8-warp blocks, where warp 0's serial row sum and the
+    // barriers weigh more than the spread (measured on B200 with 20-32 particles and 100-1,024
+    // rows: 100-2,048 swarms favour eight, 4,000 and 8,192 four).
+    int per_sm8 = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         &per_sm8, fused_pso_rows_kernel, 8 * 32, split_smem(8));
-    if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm4, fused_pso_rows_kernel, 4 * 32,
-                                                        split_smem(4));
     if (e != cudaSuccess) return fail_cuda(e, "fused_pso");
     const int64_t cap8 = (int64_t)sms * (per_sm8 > 0 ? per_sm8 : 1);
-    const int64_t cap4 = (int64_t)sms * (per_sm4 > 0 ? per_sm4 : 1);
-    const bool four = (2 * B > 3 * cap8 && B <= cap4) || B > 14 * cap8;
-    const int W = four ? 4 : 8;
-    const int64_t cap = four ? cap4 : cap8;
-    const int grid = (int)(B < cap ? B : cap);
+    const int W = B > 7 * cap8 ? 4 : 8;
+    const int grid = (int)(B < 0x7fffffff ? B : 0x7fffffff);
     fused_pso_rows_kernel<<<grid, W * 32, split_smem(W), static_cast<cudaStream_t>(stream)>>>(
         a, lut, (float)ids->pi_val, (float)ids->e_val);
     e = cudaGetLastError();

@@ -142,8 +142,8 @@ def _run_fused(mod, g, pop, consts, X, y, P, steps, seed, w=0.5, c1=1.5, c2=1.5,
 @needs_ref
 @pytest.mark.parametrize("B,P,steps,K,D,ops", [
     (700, 20, 20, 4, 200, tl.C1_OPERATORS),   # row split, eight warps per swarm
-    (500, 20, 10, 4, 1024, tl.C1_OPERATORS),  # row split, four warps (one wave of 4-warp blocks)
-    (4500, 32, 4, 8, 300, tl.C1_OPERATORS),   # row split, four warps (many waves)
+    (500, 20, 10, 4, 1024, tl.C1_OPERATORS),  # row split, eight warps, four 256-row chunks
+    (4500, 32, 4, 8, 300, tl.C1_OPERATORS),   # row split, four warps (beyond seven waves)
     (200, 30, 6, 5, 1, tl.C1_OPERATORS),      # a single row
     (700, 40, 10, 10, 96, tl.C1_OPERATORS),   # above 32 particles: a swarm per pair of warps
     (700, 64, 5, 16, 1024, tl.C1_OPERATORS),
