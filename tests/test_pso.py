@@ -172,6 +172,21 @@ def test_fused_pso_bit_exact(B, P, steps, K, D, ops):
 
 
 @gpu
+@needs_ref
+@pytest.mark.parametrize("P", [20, 48])
+def test_fused_pso_zero_steps(P):
+    """No step: the swarm best stays the initial constants with the error sentinel."""
+    ref = refext.load("fastmath")
+    from warpsymbolic_b200 import rpn_cuda_native as ours
+    g, pop, consts, X, y = _fused_case(5, 300, 30, 4, 128)
+    rp, re_ = _run_fused(ref, g, pop, consts, X, y, P, 0, 77)
+    op, oe = _run_fused(ours, g, pop, consts, X, y, P, 0, 77)
+    assert np.array_equal(re_, oe, equal_nan=True)
+    assert np.array_equal(rp, op, equal_nan=True)
+    assert np.array_equal(op, consts) and (oe == np.float32(1e30)).all()
+
+
+@gpu
 def test_fused_pso_argument_checks():
     from warpsymbolic_b200 import rpn_cuda_native as ours
     g, pop, consts, X, y = _fused_case(1, 4, 10, 3, 50)
