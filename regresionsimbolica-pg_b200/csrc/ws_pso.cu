@@ -11,13 +11,12 @@
 //
 // B200 layout of the fused loop: a particle per lane, instead of one P-thread block per program
 // (20-thread blocks leave 12 lanes of every warp idle and cap residency at 32 blocks per SM).
-// Up to 32 particles, a swarm owns a block of four or eight warps that split its rows (lane p
-// of every warp is particle p); warp 0 adds the row errors in row order and runs the swarm's
-// update.  Above 32 particles, a swarm owns a pair of warps that walk all rows.  The program and
-// its constants live in shared memory; the token dispatch is a table lookup instead of a ~40-way
-// comparison chain; each lane carries 16 rows through one pass over the program (one decode per
-// token for 16 rows), and the rows' squared errors are added one at a time in row order, so
-// every RMSE keeps the reference's bits.
+// A swarm owns a block of four or eight warps that split its rows (one warp per row group up to
+// 32 particles, two above); row group 0 adds the row errors in row order and runs the swarm's
+// update.  The program and its constants live in shared memory; the token dispatch is a table
+// lookup instead of a ~40-way comparison chain; each lane carries 16 rows through one pass over
+// the program (one decode per token for 16 rows), and the rows' squared errors are added one at
+// a time in row order, so every RMSE keeps the reference's bits.
 #include <cuda_runtime.h>
 #include <curand_kernel.h>
 #include <cstdint>
@@ -335,14 +334,14 @@ struct FusedPsoArgs {
   float* out_pos;
   float* out_err;
   int64_t B;
-  int L, K, P, steps, G;  // G = lanes per swarm (32 or 64)
+  int L, K, P, steps, G;  // G = particles of a row group: 32, or 64 above 32 particles
   int64_t D;
   float w, c1, c2, cmin, cmax;
   uint64_t seed;
   int pad_id, id_C;
 };
 
-// Per-swarm shared state: program bytes, the lanes' positions [K][G] (constants are read by
+// Per-swarm shared state: program bytes, the particles' positions [K][G] (constants are read by
 // slot), the swarm best, and the per-particle personal-best errors for the swarm reduction.
 struct SwarmSmem {
   uint8_t prog[kPsoMaxL];
@@ -354,178 +353,30 @@ struct SwarmSmem {
   int n_active;
 };
 
-__global__ void __launch_bounds__(128) fused_pso_kernel(FusedPsoArgs a, PsoLut lut,
-                                                        float pi_val, float e_val) {
-  __shared__ uint8_t s_cls[256], s_arg[256];
-  __shared__ float s_lit[N_LITERALS];
-  __shared__ SwarmSmem s_sw[4];
-  for (int t = threadIdx.x; t < 256; t += blockDim.x) {
-    s_cls[t] = lut.cls[t];
-    s_arg[t] = lut.arg[t];
-  }
-  if (threadIdx.x < N_LITERALS) {
-    const float lits[N_LITERALS] = {0.f, 1.f, 2.f, 3.f, 4.f, 5.f, 6.f, 10.f, pi_val, e_val};
-    s_lit[threadIdx.x] = lits[threadIdx.x];
-  }
-  const int swarms_per_block = blockDim.x / a.G;
-  const int slot = threadIdx.x / a.G;
-  const int p = threadIdx.x % a.G;
-  SwarmSmem& sw = s_sw[slot];
-  const int K = a.K;
-  const bool active = p < a.P;
-
-  for (int64_t base = (int64_t)blockIdx.x * swarms_per_block; base < a.B;
-       base += (int64_t)gridDim.x * swarms_per_block) {
-    const int64_t b = base + slot;
-    const bool live = b < a.B;
-    __syncthreads();
-    if (live)
-      for (int i = p; i < a.L; i += a.G) sw.prog[i] = a.pop[b * a.L + i];
-    __syncthreads();
-    if (live && p == 0) {
-      int count = 0;
-      for (int i = 0; i < a.L; ++i) {
-        if (sw.prog[i] == a.pad_id) break;
-        if (sw.prog[i] == a.id_C && count < K) count++;
-      }
-      sw.n_active = count > 0 ? count : 1;
-    }
-    __syncthreads();
-    const int n_active = live ? sw.n_active : 1;
-
-    curandState rng;
-    float vel[kPsoMaxK], pbest_pos[kPsoMaxK];
-    float pbest_err = kPsoInf;
-    float* my_pos = sw.pos + p;  // slot k at my_pos[k * G]
-    if (live && active) {
-      curand_init(a.seed + (uint64_t)b * a.P + p, 0, 0, &rng);
-      const float range = (float)(a.cmax - a.cmin);
-      const float jitter_sigma = range * 0.15f;
-      const float vel_sigma = range * 0.02f;
-      const float* init = a.init + b * K;
-#pragma unroll
-      for (int k = 0; k < kPsoMaxK; ++k) {
-        if (k < K) {
-          float pk = init[k];
-          if (p > 0 && k < n_active) {
-            pk += curand_normal(&rng) * jitter_sigma;
-            if (pk < a.cmin) pk = a.cmin;
-            if (pk > a.cmax) pk = a.cmax;
-          }
-          vel[k] = curand_normal(&rng) * vel_sigma;
-          pbest_pos[k] = pk;
-          my_pos[k * a.G] = pk;
-        }
-      }
-    }
-    if (live && p == 0) {
-      sw.gbest_err = kPsoInf;
-      for (int k = 0; k < K; ++k) sw.gbest_pos[k] = a.init[b * K + k];
-    }
-    __syncthreads();
-
-    for (int step = 0; step < a.steps; ++step) {
-      if (live && active) {
-        // 1. evaluate this particle over every row
-        // (kPsoRows rows per decode; the squared errors are summed one row at a time, in row
-        // order, as the reference does)
-        float mse_sum = 0.0f;
-        bool any_error = false;
-        for (int d = 0; d < (int)a.D && !any_error; d += kPsoRows) {
-          const int nr = (int)a.D - d < kPsoRows ? (int)a.D - d : kPsoRows;
-          float pr[kPsoRows];
-          pso_eval_rows<kPsoRows>(sw.prog, a.L, s_cls, s_arg, s_lit, a.x, a.D, d, nr, my_pos,
-                                  a.G, K, pr);
-#pragma unroll
-          for (int r = 0; r < kPsoRows; ++r) {
-            if (r >= nr || any_error) break;
-            if (pr[r] >= 1e29f) {
-              any_error = true;
-              break;
-            }
-            const float diff = pr[r] - a.y[d + r];
-            mse_sum += diff * diff;
-          }
-        }
-        const float rmse = any_error ? kPsoInf : sqrtf(mse_sum / (float)a.D);
-        // 2. personal best
-        if (rmse < pbest_err) {
-          pbest_err = rmse;
-#pragma unroll
-          for (int k = 0; k < kPsoMaxK; ++k)
-            if (k < K) pbest_pos[k] = my_pos[k * a.G];
-        }
-        sw.perr[p] = pbest_err;
-      }
-      __syncthreads();
-      // 3. swarm best: serial scan in particle order, strict improvement
-      if (live && p == 0) {
-        int bp = -1;
-        float be = sw.gbest_err;
-        for (int pp = 0; pp < a.P; ++pp)
-          if (sw.perr[pp] < be) {
-            be = sw.perr[pp];
-            bp = pp;
-          }
-        sw.best_particle = bp;
-        if (bp >= 0) sw.gbest_err = be;
-      }
-      __syncthreads();
-      if (live && active && sw.best_particle == p) {
-#pragma unroll
-        for (int k = 0; k < kPsoMaxK; ++k)
-          if (k < K) sw.gbest_pos[k] = pbest_pos[k];
-      }
-      __syncthreads();
-      // 4. inertia decays linearly from w to 0.4; velocity / position update of active slots
-      if (live && active) {
-        const float w_curr =
-            a.w - (a.w - 0.4f) * (float)step / (float)(a.steps > 1 ? a.steps - 1 : 1);
-#pragma unroll
-        for (int k = 0; k < kPsoMaxK; ++k) {
-          if (k < n_active) {
-            const float r1 = curand_uniform(&rng);
-            const float r2 = curand_uniform(&rng);
-            float pk = my_pos[k * a.G];
-            vel[k] = w_curr * vel[k] + a.c1 * r1 * (pbest_pos[k] - pk) +
-                     a.c2 * r2 * (sw.gbest_pos[k] - pk);
-            pk += vel[k];
-            if (pk < a.cmin) pk = a.cmin;
-            if (pk > a.cmax) pk = a.cmax;
-            my_pos[k * a.G] = pk;
-          }
-        }
-      }
-      __syncthreads();
-    }
-    if (live && p == 0) {
-      a.out_err[b] = sw.gbest_err;
-      for (int k = 0; k < K; ++k) a.out_pos[b * K + k] = sw.gbest_pos[k];
-    }
-  }
-}
-
-// Row-split form for few swarms (32 particles at most): one swarm per block of W warps.  Lane p
-// of every warp is particle p.  Each step walks the rows in chunks of W * kSplitWarpRows; warp w
-// evaluates rows [w * kSplitWarpRows, (w + 1) * kSplitWarpRows) of the chunk for all particles
-// and leaves each row's difference to the target in shared memory; warp 0 then adds the chunk's
-// squared differences one row at a time in row order (the reference's summation, so every RMSE
-// keeps its bits) and alone holds the curand streams, velocities and personal bests.  A
-// particle whose row fails is flagged and no warp evaluates its later chunks (its RMSE is the
-// error value whatever the other rows give).
+// Row-split form: one swarm per block of W warps.  The swarm's G = 32 * H particles (H = 1 up
+// to 32 particles, 2 up to 64) take H warps, lane l of the h-th being particle 32 h + l; the
+// block's W / H such row groups split the rows.  Each step walks the rows in chunks of
+// (W / H) * kSplitWarpRows; row group g evaluates rows [g * kSplitWarpRows, (g + 1) *
+// kSplitWarpRows) of the chunk for all particles and leaves each row's difference to the target
+// in shared memory; row group 0 then adds the chunk's squared differences one row at a time in
+// row order (the reference's summation, so every RMSE keeps its bits) and alone holds the curand
+// streams, velocities and personal bests.  A particle whose row fails is flagged and no warp
+// evaluates its later chunks (its RMSE is the error value whatever the other rows give).
 constexpr int kSplitMaxWarps = 8, kSplitWarpRows = 32;
 
-// dynamic shared memory of a W-warp block: the chunk's row differences, [W * 32 rows][32 lanes]
+// dynamic shared memory of a W-warp block: the chunk's row differences, [W / H * 32 rows][G]
 constexpr size_t split_smem(int W) { return (size_t)W * kSplitWarpRows * 32 * sizeof(float); }
 
+template <int H>
 __global__ void __launch_bounds__(kSplitMaxWarps * 32)
     fused_pso_rows_kernel(FusedPsoArgs a, PsoLut lut, float pi_val, float e_val) {
   constexpr int R = kPsoRows;
+  constexpr int G = 32 * H;
   __shared__ uint8_t s_cls[256], s_arg[256];
   __shared__ float s_lit[N_LITERALS];
   __shared__ SwarmSmem sw;
-  extern __shared__ float s_diff[];  // [chunk rows][32]
-  __shared__ int s_bad[32];
+  extern __shared__ float s_diff[];  // [chunk rows][G]
+  __shared__ int s_bad[G];
   for (int t = threadIdx.x; t < 256; t += blockDim.x) {
     s_cls[t] = lut.cls[t];
     s_arg[t] = lut.arg[t];
@@ -535,12 +386,14 @@ __global__ void __launch_bounds__(kSplitMaxWarps * 32)
     s_lit[threadIdx.x] = lits[threadIdx.x];
   }
   const int warp = threadIdx.x >> 5;
-  const int p = threadIdx.x & 31;
-  const int chunk = (int)(blockDim.x >> 5) * kSplitWarpRows;
+  const int grp = warp / H;                           // row group
+  const int p = (warp % H) * 32 + (threadIdx.x & 31);  // particle
+  const bool lead = grp == 0;                          // row group 0 owns the swarm's state
+  const int chunk = (int)(blockDim.x >> 5) / H * kSplitWarpRows;
   const int K = a.K;
   const int D = (int)a.D;
   const bool active = p < a.P;
-  float* my_pos = sw.pos + p;  // slot k at my_pos[k * 32]
+  float* my_pos = sw.pos + p;  // slot k at my_pos[k * G]
 
   for (int64_t b = blockIdx.x; b < a.B; b += gridDim.x) {
     __syncthreads();
@@ -560,7 +413,7 @@ __global__ void __launch_bounds__(kSplitMaxWarps * 32)
     curandState rng;
     float vel[kPsoMaxK], pbest_pos[kPsoMaxK];
     float pbest_err = kPsoInf;
-    if (warp == 0 && active) {
+    if (lead && active) {
       curand_init(a.seed + (uint64_t)b * a.P + p, 0, 0, &rng);
       const float range = (float)(a.cmax - a.cmin);
       const float jitter_sigma = range * 0.15f;
@@ -577,7 +430,7 @@ __global__ void __launch_bounds__(kSplitMaxWarps * 32)
           }
           vel[k] = curand_normal(&rng) * vel_sigma;
           pbest_pos[k] = pk;
-          my_pos[k * 32] = pk;
+          my_pos[k * G] = pk;
         }
       }
     }
@@ -587,25 +440,25 @@ __global__ void __launch_bounds__(kSplitMaxWarps * 32)
     }
 
     for (int step = 0; step < a.steps; ++step) {
-      if (warp == 0) s_bad[p] = 0;
+      if (lead) s_bad[p] = 0;
       __syncthreads();
       // 1. evaluate every particle over every row, a chunk at a time
       float mse_sum = 0.0f;
       for (int c = 0; c < D; c += chunk) {
-        const int lo = c + warp * kSplitWarpRows;
+        const int lo = c + grp * kSplitWarpRows;
         const int hi = lo + kSplitWarpRows < D ? lo + kSplitWarpRows : D;
         if (active && !s_bad[p]) {
           for (int d = lo; d < hi; d += R) {
             const int nr = hi - d < R ? hi - d : R;
             float pr[R];
-            pso_eval_rows<R>(sw.prog, a.L, s_cls, s_arg, s_lit, a.x, a.D, d, nr, my_pos, 32, K,
+            pso_eval_rows<R>(sw.prog, a.L, s_cls, s_arg, s_lit, a.x, a.D, d, nr, my_pos, G, K,
                              pr);
             bool bad = false;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
               if (r < nr) {
                 if (pr[r] >= 1e29f) bad = true;
-                s_diff[(d - c + r) * 32 + p] = pr[r] - a.y[d + r];
+                s_diff[(d - c + r) * G + p] = pr[r] - a.y[d + r];
               }
             }
             if (bad) {
@@ -615,23 +468,23 @@ __global__ void __launch_bounds__(kSplitMaxWarps * 32)
           }
         }
         __syncthreads();
-        if (warp == 0 && active && !s_bad[p]) {
+        if (lead && active && !s_bad[p]) {
           const int n = D - c < chunk ? D - c : chunk;
           for (int r = 0; r < n; ++r) {
-            const float diff = s_diff[r * 32 + p];
+            const float diff = s_diff[r * G + p];
             mse_sum += diff * diff;
           }
         }
         __syncthreads();
       }
       // 2. personal best
-      if (warp == 0 && active) {
+      if (lead && active) {
         const float rmse = s_bad[p] ? kPsoInf : sqrtf(mse_sum / (float)a.D);
         if (rmse < pbest_err) {
           pbest_err = rmse;
 #pragma unroll
           for (int k = 0; k < kPsoMaxK; ++k)
-            if (k < K) pbest_pos[k] = my_pos[k * 32];
+            if (k < K) pbest_pos[k] = my_pos[k * G];
         }
         sw.perr[p] = pbest_err;
       }
@@ -649,14 +502,14 @@ __global__ void __launch_bounds__(kSplitMaxWarps * 32)
         if (bp >= 0) sw.gbest_err = be;
       }
       __syncthreads();
-      if (warp == 0 && active && sw.best_particle == p) {
+      if (lead && active && sw.best_particle == p) {
 #pragma unroll
         for (int k = 0; k < kPsoMaxK; ++k)
           if (k < K) sw.gbest_pos[k] = pbest_pos[k];
       }
       __syncthreads();
       // 4. inertia decays linearly from w to 0.4; velocity / position update of active slots
-      if (warp == 0 && active) {
+      if (lead && active) {
         const float w_curr =
             a.w - (a.w - 0.4f) * (float)step / (float)(a.steps > 1 ? a.steps - 1 : 1);
 #pragma unroll
@@ -664,13 +517,13 @@ __global__ void __launch_bounds__(kSplitMaxWarps * 32)
           if (k < n_active) {
             const float r1 = curand_uniform(&rng);
             const float r2 = curand_uniform(&rng);
-            float pk = my_pos[k * 32];
+            float pk = my_pos[k * G];
             vel[k] = w_curr * vel[k] + a.c1 * r1 * (pbest_pos[k] - pk) +
                      a.c2 * r2 * (sw.gbest_pos[k] - pk);
             pk += vel[k];
             if (pk < a.cmin) pk = a.cmin;
             if (pk > a.cmax) pk = a.cmax;
-            my_pos[k * 32] = pk;
+            my_pos[k * G] = pk;
           }
         }
       }
@@ -842,40 +695,29 @@ extern "C" ws_status ws_fused_pso(int32_t dtype, const uint8_t* population, int6
   a.id_C = ids->id_C;
   const PsoLut lut = build_pso_lut(*ids, num_vars);
   const int sms = device_info().sm_count;
-  if (num_particles <= 32) {
-    // Row-split form, a block per swarm: the block scheduler hands the next swarm to whichever
-    // SM frees a slot first, which balances programs of different lengths (a persistent grid
-    // striding over the swarms left the SMs idle half of the time on 1,024 swarms).  Eight warps
-    // per swarm, four beyond seven waves of 8-warp blocks, where warp 0's serial row sum and the
-    // barriers weigh more than the spread (measured on B200 with 20-32 particles and 100-1,024
-    // rows: 100-2,048 swarms favour eight, 4,000 and 8,192 four).
-    int per_sm8 = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm8, fused_pso_rows_kernel, 8 * 32, split_smem(8));
-    if (e != cudaSuccess) return fail_cuda(e, "fused_pso");
-    const int64_t cap8 = (int64_t)sms * (per_sm8 > 0 ? per_sm8 : 1);
-    const int W = B > 7 * cap8 ? 4 : 8;
-    const int grid = (int)(B < 0x7fffffff ? B : 0x7fffffff);
-    fused_pso_rows_kernel<<<grid, W * 32, split_smem(W), static_cast<cudaStream_t>(stream)>>>(
-        a, lut, (float)ids->pi_val, (float)ids->e_val);
-    e = cudaGetLastError();
-    return e == cudaSuccess ? WS_OK : fail_cuda(e, "fused_pso");
-  }
-  // More than 32 particles: a swarm per pair of warps (a lane per particle), up to two swarms
-  // per 128-thread block; one when that would leave SMs without a block (a swarm's results do
-  // not depend on its block)
-  int per_block = 128 / a.G;
-  while (per_block > 1 && (B + per_block - 1) / per_block < sms) per_block /= 2;
-  const int threads = per_block * a.G;
-  const int64_t want = (B + per_block - 1) / per_block;
-  int per_sm = 0;
-  cudaError_t e =
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_pso_kernel, threads, 0);
+  // Row-split form, a block per swarm: the block scheduler hands the next swarm to whichever
+  // SM frees a slot first, which balances programs of different lengths (a persistent grid
+  // striding over the swarms left the SMs idle half of the time on 1,024 swarms).  Eight warps
+  // per swarm, four beyond seven waves of 8-warp blocks, where row group 0's serial row sum and
+  // the barriers weigh more than the spread (measured on B200 with 20-32 particles and
+  // 100-1,024 rows: 100-2,048 swarms favour eight, 4,000 and 8,192 four).  Above 32 particles a
+  // row group is two warps.
+  const bool two = a.G == 64;
+  int per_sm8 = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm8, two ? fused_pso_rows_kernel<2> : fused_pso_rows_kernel<1>, 8 * 32,
+      split_smem(8));
   if (e != cudaSuccess) return fail_cuda(e, "fused_pso");
-  const int64_t cap = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
-  const int grid = (int)(want < cap ? want : cap);
-  fused_pso_kernel<<<grid, threads, 0, static_cast<cudaStream_t>(stream)>>>(
-      a, lut, (float)ids->pi_val, (float)ids->e_val);
+  const int64_t cap8 = (int64_t)sms * (per_sm8 > 0 ? per_sm8 : 1);
+  const int W = B > 7 * cap8 ? 4 : 8;
+  const int grid = (int)(B < 0x7fffffff ? B : 0x7fffffff);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (two)
+    fused_pso_rows_kernel<2><<<grid, W * 32, split_smem(W), st>>>(a, lut, (float)ids->pi_val,
+                                                                 (float)ids->e_val);
+  else
+    fused_pso_rows_kernel<1><<<grid, W * 32, split_smem(W), st>>>(a, lut, (float)ids->pi_val,
+                                                                 (float)ids->e_val);
   e = cudaGetLastError();
   return e == cudaSuccess ? WS_OK : fail_cuda(e, "fused_pso");
 }

@@ -145,8 +145,9 @@ def _run_fused(mod, g, pop, consts, X, y, P, steps, seed, w=0.5, c1=1.5, c2=1.5,
     (500, 20, 10, 4, 1024, tl.C1_OPERATORS),  # row split, eight warps, four 256-row chunks
     (4500, 32, 4, 8, 300, tl.C1_OPERATORS),   # row split, four warps (beyond seven waves)
     (200, 30, 6, 5, 1, tl.C1_OPERATORS),      # a single row
-    (700, 40, 10, 10, 96, tl.C1_OPERATORS),   # above 32 particles: a swarm per pair of warps
+    (700, 40, 10, 10, 96, tl.C1_OPERATORS),   # above 32 particles: row groups of two warps
     (700, 64, 5, 16, 1024, tl.C1_OPERATORS),
+    (4500, 48, 3, 4, 200, tl.C1_OPERATORS),   # two-warp row groups, four warps per swarm
     (700, 7, 12, 3, 333, tl.ALL_OPERATORS),
 ])
 def test_fused_pso_bit_exact(B, P, steps, K, D, ops):
