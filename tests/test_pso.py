@@ -64,6 +64,55 @@ def test_oracle_bests_tie_rule():
     assert (pe[0] == np.minimum(9.0, cur[0])).all()
 
 
+def test_oracle_pso_fitness_rules():
+    """The fused PSO's fitness on hand cases with exactly representable values: eval_rpn_single's
+    domain errors, underflow / leftover values, the constant-slot clamp, the push-drop at depth
+    32, unknown tokens (pop one, push 0) and the sequential RMSE (fused_pso_kernels.cu:57-197,
+    330-351)."""
+    g = tl.GPUGrammar(num_variables=2, operators=tl.ALL_OPERATORS)
+    tm = tl.token_map(g)
+    L = 64
+    X = np.array([[1, 2, 3, 4], [0.5, -1, 0, 2]], dtype=np.float32)
+    y = np.array([1, 3, 5, 7], dtype=np.float32)
+    inf = np.float32(1e30)
+    rms = lambda pred: np.float32(np.sqrt(np.mean((np.asarray(pred, np.float64) - y) ** 2)))  # noqa: E731
+    cases = [  # (tokens, constants, expected RMSE)
+        (["x0", "C", "*"], [2.0], 1.0),                       # 2 x0 - y = 1 on every row
+        (["x0", "x1", "/"], [0.0], inf),                      # x1 = 0 on row 2: |b| < 1e-12
+        (["x1", "log"], [0.0], inf),                          # log of <= 1e-12
+        (["x1", "sqrt"], [0.0], inf),                         # sqrt of a negative
+        (["x0", "sqrt"], [0.0], rms(np.sqrt(X[0]))),
+        (["C", "exp"], [81.0], inf),                          # exp above 80: error
+        (["C", "exp"], [-81.0], rms([0, 0, 0, 0])),           # exp below -80: 0, no error
+        (["+"], [0.0], inf),                                  # underflow
+        (["x0", "x1"], [0.0], inf),                           # two values left
+        (["C", "C", "+", "x0", "+"], [3.0], rms(6 + X[0])),   # the second C clamps to slot K-1
+        (["x0", "2", "pow"], [0.0], rms(X[0] ** 2)),
+        (["C", "fact"], [-1.0], inf),                         # fact at a negative integer
+        (["C", "fact", "x0", "*"], [3.0], rms(6 * X[0])),
+        (["C", "C", "*"], [1e15], inf),                       # finite 1e30 >= 1e29: an error
+        (["x0", "1", "asin"], [0.0], inf),                    # asin(1) fine, two values left
+        (["C", "x0", "%"], [0.0], rms(np.zeros(4))),          # 0 mod x0 = 0
+    ]
+    pop = np.array([g.encode(t, L) for t, _, _ in cases], dtype=np.uint8)
+    consts = np.array([c for _, c, _ in cases], dtype=np.float32)
+    extra = []
+    # push-drop: 33 pushes keep 32 values, 31 additions then leave one: 32 x0
+    extra.append((g.encode(["x0"] * 33 + ["+"] * 31, L), rms(32 * X[0])))
+    # an unknown token pops one value and pushes 0
+    row = g.encode(["x0", "x1"], L)
+    row[2] = 250
+    extra.append((row, inf))                                  # x0 0: two values left
+    row = g.encode(["x0"], L)
+    row[1] = 250
+    extra.append((row, rms(np.zeros(4))))
+    pop = np.concatenate([pop, np.array([r for r, _ in extra], dtype=np.uint8)])
+    consts = np.concatenate([consts, np.zeros((len(extra), 1), np.float32)])
+    want = np.array([e for _, _, e in cases] + [e for _, e in extra], dtype=np.float32)
+    got = O.pso_rmse(tm, pop, X, consts, y)
+    np.testing.assert_allclose(got, want, rtol=1e-6)
+
+
 # ---------------------------------------------------------------------------------------------
 DEV = torch.device("cuda:0") if torch.cuda.is_available() else None
 
